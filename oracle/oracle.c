@@ -1,0 +1,522 @@
+/*
+ * CPU oracle for the GSWITCH level-loop hot path.  TEST INFRASTRUCTURE ONLY:
+ * loaded by tests/, the smoke check and bench.py's cpu_baseline leg as the
+ * checker; never linked into the product.
+ *
+ * Reference citations are paths inside the PAA-NCIC/GSWITCH tree.
+ */
+#include "oracle.h"
+
+#include <limits.h>
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+/* ------------------------------------------------------------------------ */
+/* counter-based hashing (SplitMix64 finaliser, Steele/Lea/Flood 2014)        */
+/* ------------------------------------------------------------------------ */
+uint64_t or_sm64(uint64_t x) {
+  x += 0x9E3779B97F4A7C15ull;
+  x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+  x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+  return x ^ (x >> 31);
+}
+
+uint64_t or_stream_key(uint64_t seed, uint64_t stream) {
+  return or_sm64(seed ^ or_sm64(stream));
+}
+
+enum { ST_RMAT = 1, ST_W = 2, ST_GRID = 3, ST_ER = 4, ST_ERB = 5, ST_ROOT = 7 };
+
+void or_free(void *p) { free(p); }
+
+/* Graph500-style recursive quadrant choice, no noise, no permutation.
+ * Level l fixes bit (scale-1-l) of (src, dst); 32 random bits per level,
+ * compared against integer thresholds so every platform picks the same
+ * quadrant. */
+void or_rmat_edges(int scale, int ef, double a, double b, double c,
+                   uint64_t seed, uint32_t *src, uint32_t *dst) {
+  const uint64_t key = or_stream_key(seed, ST_RMAT);
+  const uint32_t ta = (uint32_t)(a * 4294967296.0);
+  const uint32_t tab = (uint32_t)((a + b) * 4294967296.0);
+  const uint32_t tabc = (uint32_t)((a + b + c) * 4294967296.0);
+  const int64_t ne = (int64_t)ef << scale;
+  for (int64_t i = 0; i < ne; ++i) {
+    uint64_t base = or_sm64(key + (uint64_t)i);
+    uint32_t s = 0, d = 0;
+    uint64_t h = 0;
+    for (int l = 0; l < scale; ++l) {
+      uint32_t r;
+      if ((l & 1) == 0) {
+        h = or_sm64(base + (uint64_t)(l >> 1));
+        r = (uint32_t)h;
+      } else {
+        r = (uint32_t)(h >> 32);
+      }
+      const uint32_t bit = 1u << (scale - 1 - l);
+      if (r < ta) {
+      } else if (r < tab) {
+        d |= bit;
+      } else if (r < tabc) {
+        s |= bit;
+      } else {
+        s |= bit;
+        d |= bit;
+      }
+    }
+    src[i] = s;
+    dst[i] = d;
+  }
+}
+
+int64_t or_grid_nedges(int rows, int cols, int lr_div) {
+  int64_t eg = (int64_t)rows * (cols - 1) + (int64_t)(rows - 1) * cols;
+  return eg + (lr_div > 0 ? eg / lr_div : 0);
+}
+
+int64_t or_grid_edges(int rows, int cols, int lr_div, uint64_t seed,
+                      uint32_t *src, uint32_t *dst) {
+  int64_t k = 0;
+  for (int r = 0; r < rows; ++r)
+    for (int c = 0; c < cols; ++c) {
+      uint32_t v = (uint32_t)r * (uint32_t)cols + (uint32_t)c;
+      if (c + 1 < cols) {
+        src[k] = v;
+        dst[k] = v + 1;
+        ++k;
+      }
+      if (r + 1 < rows) {
+        src[k] = v;
+        dst[k] = v + (uint32_t)cols;
+        ++k;
+      }
+    }
+  const int64_t eg = k;
+  const int64_t nlr = lr_div > 0 ? eg / lr_div : 0;
+  const uint64_t key = or_stream_key(seed, ST_GRID);
+  const uint64_t n = (uint64_t)rows * (uint64_t)cols;
+  for (int64_t j = 0; j < nlr; ++j) {
+    src[k] = (uint32_t)(or_sm64(key + 2 * (uint64_t)j) % n);
+    dst[k] = (uint32_t)(or_sm64(key + 2 * (uint64_t)j + 1) % n);
+    ++k;
+  }
+  return k;
+}
+
+void or_er_edges(int64_t n, int64_t m, uint64_t seed, uint32_t *src,
+                 uint32_t *dst) {
+  const uint64_t key = or_stream_key(seed, ST_ER);
+  for (int64_t j = 0; j < m; ++j) {
+    src[j] = (uint32_t)(or_sm64(key + 2 * (uint64_t)j) % (uint64_t)n);
+    dst[j] = (uint32_t)(or_sm64(key + 2 * (uint64_t)j + 1) % (uint64_t)n);
+  }
+}
+
+static double unit53(uint64_t h) { return (double)(h >> 11) * (1.0 / 9007199254740992.0); }
+
+void or_er_batch_params(uint64_t seed, int64_t i, int64_t nlo, int64_t nhi,
+                        double dlo, double dhi, int64_t *n, int64_t *m,
+                        uint64_t *iseed) {
+  const uint64_t key = or_stream_key(seed, ST_ERB);
+  double u1 = unit53(or_sm64(key + 3 * (uint64_t)i));
+  double u2 = unit53(or_sm64(key + 3 * (uint64_t)i + 1));
+  double ln = log((double)nlo) + u1 * (log((double)nhi) - log((double)nlo));
+  int64_t nn = (int64_t)llround(exp(ln));
+  if (nn < nlo) nn = nlo;
+  if (nn > nhi) nn = nhi;
+  double deg = dlo + u2 * (dhi - dlo);
+  *n = nn;
+  *m = (int64_t)floor((double)nn * deg / 2.0);
+  *iseed = or_sm64(key + 3 * (uint64_t)i + 2);
+}
+
+/* LSD radix sort of 64-bit keys, 16-bit digits, constant digits skipped. */
+static void radix_sort_u64(uint64_t *a, uint64_t *tmp, int64_t len) {
+  int64_t *cnt = (int64_t *)malloc(sizeof(int64_t) * 65536);
+  for (int pass = 0; pass < 4; ++pass) {
+    const int sh = pass * 16;
+    memset(cnt, 0, sizeof(int64_t) * 65536);
+    for (int64_t i = 0; i < len; ++i) cnt[(a[i] >> sh) & 0xFFFF]++;
+    int nonzero = 0;
+    for (int d = 0; d < 65536; ++d) nonzero += cnt[d] != 0;
+    if (nonzero <= 1) continue;
+    int64_t s = 0;
+    for (int d = 0; d < 65536; ++d) {
+      int64_t t = cnt[d];
+      cnt[d] = s;
+      s += t;
+    }
+    for (int64_t i = 0; i < len; ++i) tmp[cnt[(a[i] >> sh) & 0xFFFF]++] = a[i];
+    memcpy(a, tmp, sizeof(uint64_t) * (size_t)len);
+  }
+  free(cnt);
+}
+
+int64_t or_csr_build(int64_t n, int64_t npairs, const uint32_t *src,
+                     const uint32_t *dst, int64_t **off_out,
+                     int32_t **col_out) {
+  uint64_t *keys = (uint64_t *)malloc(sizeof(uint64_t) * (size_t)(2 * npairs + 1));
+  int64_t k = 0;
+  for (int64_t i = 0; i < npairs; ++i) {
+    uint64_t s = src[i], d = dst[i];
+    if (s == d) continue;
+    keys[k++] = (s << 32) | d;
+    keys[k++] = (d << 32) | s;
+  }
+  uint64_t *tmp = (uint64_t *)malloc(sizeof(uint64_t) * (size_t)(k + 1));
+  radix_sort_u64(keys, tmp, k);
+  free(tmp);
+  int64_t m = 0;
+  for (int64_t i = 0; i < k; ++i)
+    if (i == 0 || keys[i] != keys[i - 1]) keys[m++] = keys[i];
+  int64_t *off = (int64_t *)calloc((size_t)n + 1, sizeof(int64_t));
+  int32_t *col = (int32_t *)malloc(sizeof(int32_t) * (size_t)(m + 1));
+  for (int64_t i = 0; i < m; ++i) {
+    off[(keys[i] >> 32) + 1]++;
+    col[i] = (int32_t)(keys[i] & 0xFFFFFFFFu);
+  }
+  for (int64_t v = 0; v < n; ++v) off[v + 1] += off[v];
+  free(keys);
+  *off_out = off;
+  *col_out = col;
+  return m;
+}
+
+void or_weights(uint64_t seed, int wmax, int64_t n, const int64_t *off,
+                const int32_t *col, int32_t *w) {
+  const uint64_t key = or_stream_key(seed, ST_W);
+  for (int64_t v = 0; v < n; ++v)
+    for (int64_t e = off[v]; e < off[v + 1]; ++e) {
+      uint64_t u = (uint64_t)col[e];
+      uint64_t lo = (uint64_t)v < u ? (uint64_t)v : u;
+      uint64_t hi = (uint64_t)v < u ? u : (uint64_t)v;
+      w[e] = 1 + (int32_t)(or_sm64(key + ((lo << 32) | hi)) % (uint64_t)wmax);
+    }
+}
+
+void or_roots(uint64_t seed, int64_t n, const int64_t *off, int count,
+              int32_t *roots) {
+  const uint64_t key = or_stream_key(seed, ST_ROOT);
+  int got = 0;
+  uint64_t j = 0;
+  const uint64_t budget = 64ull * (uint64_t)n + 4096;
+  while (got < count && j < budget) {
+    int32_t v = (int32_t)(or_sm64(key + j) % (uint64_t)n);
+    ++j;
+    if (off[v + 1] == off[v]) continue;
+    int dup = 0;
+    for (int q = 0; q < got; ++q) dup |= roots[q] == v;
+    if (!dup) roots[got++] = v;
+  }
+  for (int64_t v = 0; got < count && v < n; ++v) { /* tiny graphs */
+    if (off[v + 1] == off[v]) continue;
+    int dup = 0;
+    for (int q = 0; q < got; ++q) dup |= roots[q] == (int32_t)v;
+    if (!dup) roots[got++] = (int32_t)v;
+  }
+  while (got < count) roots[got++] = -1;
+}
+
+/* ------------------------------------------------------------------------ */
+/* validators                                                                 */
+/* ------------------------------------------------------------------------ */
+
+/* bfs_cpu: application/bfs.cu:38-62 (FIFO queue, first discovery wins). */
+void or_bfs(int64_t n, const int64_t *off, const int32_t *col, int32_t root,
+            int32_t *lvl) {
+  int32_t *q = (int32_t *)malloc(sizeof(int32_t) * (size_t)(n + 1));
+  for (int64_t i = 0; i < n; ++i) lvl[i] = -1;
+  int64_t head = 0, tail = 0;
+  lvl[root] = 0;
+  q[tail++] = root;
+  while (head < tail) {
+    int32_t v = q[head++];
+    for (int64_t j = off[v]; j < off[v + 1]; ++j) {
+      int32_t u = col[j];
+      if (lvl[u] == -1) {
+        lvl[u] = lvl[v] + 1;
+        q[tail++] = u;
+      }
+    }
+  }
+  free(q);
+}
+
+/* spfa: application/sssp.cu:55-89 (FIFO label-correcting, in-queue flags,
+ * INT_MAX for unreached). */
+void or_sssp_spfa(int64_t n, const int64_t *off, const int32_t *col,
+                  const int32_t *w, int32_t root, int32_t *dis) {
+  /* circular FIFO: at most n vertices are queued at once (in-queue flag) */
+  int32_t *q = (int32_t *)malloc(sizeof(int32_t) * (size_t)(n + 1));
+  char *inq = (char *)calloc((size_t)n, 1);
+  for (int64_t i = 0; i < n; ++i) dis[i] = INT_MAX;
+  int64_t head = 0, cnt = 0, cap = n + 1;
+  dis[root] = 0;
+  inq[root] = 1;
+  q[0] = root;
+  cnt = 1;
+  while (cnt > 0) {
+    int32_t v = q[head];
+    head = (head + 1) % cap;
+    --cnt;
+    inq[v] = 0;
+    for (int64_t j = off[v]; j < off[v + 1]; ++j) {
+      int32_t u = col[j];
+      int32_t nd = dis[v] + w[j];
+      if (dis[u] > nd) {
+        dis[u] = nd;
+        if (!inq[u]) {
+          q[(head + cnt) % cap] = u;
+          ++cnt;
+          inq[u] = 1;
+        }
+      }
+    }
+  }
+  free(q);
+  free(inq);
+}
+
+/* Dijkstra with a binary heap (lazy deletion); cross-check for SPFA. */
+typedef struct {
+  int32_t d;
+  int32_t v;
+} hnode;
+static void hpush(hnode *h, int64_t *sz, hnode x) {
+  int64_t i = (*sz)++;
+  while (i > 0) {
+    int64_t p = (i - 1) >> 1;
+    if (h[p].d <= x.d) break;
+    h[i] = h[p];
+    i = p;
+  }
+  h[i] = x;
+}
+static hnode hpop(hnode *h, int64_t *sz) {
+  hnode top = h[0], x = h[--(*sz)];
+  int64_t i = 0;
+  for (;;) {
+    int64_t l = 2 * i + 1, r = l + 1, s = i;
+    int32_t sd = x.d;
+    if (l < *sz && h[l].d < sd) { s = l; sd = h[l].d; }
+    if (r < *sz && h[r].d < sd) { s = r; }
+    if (s == i) break;
+    h[i] = h[s];
+    i = s;
+  }
+  h[i] = x;
+  return top;
+}
+void or_sssp_dijkstra(int64_t n, const int64_t *off, const int32_t *col,
+                      const int32_t *w, int32_t root, int32_t *dis) {
+  hnode *h = (hnode *)malloc(sizeof(hnode) * (size_t)(off[n] + 2));
+  int64_t sz = 0;
+  for (int64_t i = 0; i < n; ++i) dis[i] = INT_MAX;
+  dis[root] = 0;
+  hnode s0 = {0, root};
+  hpush(h, &sz, s0);
+  while (sz > 0) {
+    hnode t = hpop(h, &sz);
+    if (t.d != dis[t.v]) continue;
+    for (int64_t j = off[t.v]; j < off[t.v + 1]; ++j) {
+      int32_t u = col[j];
+      int32_t nd = t.d + w[j];
+      if (nd < dis[u]) {
+        dis[u] = nd;
+        hnode x = {nd, u};
+        hpush(h, &sz, x);
+      }
+    }
+  }
+  free(h);
+}
+
+/* CC_CPU: application/cc.cu:34-66 - components seeded in increasing id
+ * order, so every label is the minimum vertex id of its component. */
+void or_cc(int64_t n, const int64_t *off, const int32_t *col, int32_t *id) {
+  int32_t *q = (int32_t *)malloc(sizeof(int32_t) * (size_t)(off[n] + n + 1));
+  for (int64_t i = 0; i < n; ++i) id[i] = (int32_t)i;
+  for (int64_t i = 0; i < n; ++i) {
+    if (id[i] != i) continue;
+    int32_t c = id[i];
+    int64_t head = 0, tail = 0;
+    q[tail++] = (int32_t)i;
+    while (head < tail) {
+      int32_t v = q[head++];
+      for (int64_t j = off[v]; j < off[v + 1]; ++j) {
+        int32_t u = col[j];
+        if (id[u] == u) {
+          id[u] = c;
+          q[tail++] = u;
+        }
+      }
+    }
+  }
+  free(q);
+}
+
+/* bc_cpu: application/bc.cu:162-214, single source, int32 path counts and
+ * FP32 dependencies exactly as the reference types them. */
+void or_bc_f32(int64_t n, const int64_t *off, const int32_t *col, int32_t root,
+               int32_t *nsp, float *dep) {
+  int32_t *vis = (int32_t *)malloc(sizeof(int32_t) * (size_t)n);
+  int32_t *order = (int32_t *)malloc(sizeof(int32_t) * (size_t)(n + 1));
+  for (int64_t i = 0; i < n; ++i) { nsp[i] = 0; vis[i] = -1; dep[i] = 0; }
+  nsp[root] = 1;
+  vis[root] = 1;
+  int64_t head = 0, tail = 0;
+  order[tail++] = root;
+  while (head < tail) { /* forward: order[] doubles as queue and stack */
+    int32_t v = order[head++];
+    for (int64_t j = off[v]; j < off[v + 1]; ++j) {
+      int32_t u = col[j];
+      if (vis[u] == -1) { order[tail++] = u; vis[u] = vis[v] + 1; }
+      /* int32 wrap-around as the reference's int counter, without UB */
+      if (vis[u] == vis[v] + 1) nsp[u] = (int32_t)((uint32_t)nsp[u] + (uint32_t)nsp[v]);
+    }
+  }
+  for (int64_t k = tail - 1; k >= 0; --k) { /* backward: pop in reverse */
+    int32_t v = order[k];
+    dep[v] *= nsp[v];
+    for (int64_t j = off[v]; j < off[v + 1]; ++j) {
+      int32_t u = col[j];
+      if (vis[u] + 1 == vis[v]) {
+        float tmp = (1 + dep[v]) / nsp[v];
+        dep[u] += tmp;
+      }
+    }
+  }
+  free(vis);
+  free(order);
+}
+
+/* The same Brandes recurrence in FP64 with FP64 path counts (no overflow). */
+void or_bc_f64(int64_t n, const int64_t *off, const int32_t *col, int32_t root,
+               double *nsp, double *dep, int32_t *lvl) {
+  int32_t *order = (int32_t *)malloc(sizeof(int32_t) * (size_t)(n + 1));
+  for (int64_t i = 0; i < n; ++i) { nsp[i] = 0; lvl[i] = -1; dep[i] = 0; }
+  nsp[root] = 1;
+  lvl[root] = 0;
+  int64_t head = 0, tail = 0;
+  order[tail++] = root;
+  while (head < tail) {
+    int32_t v = order[head++];
+    for (int64_t j = off[v]; j < off[v + 1]; ++j) {
+      int32_t u = col[j];
+      if (lvl[u] == -1) { order[tail++] = u; lvl[u] = lvl[v] + 1; }
+      if (lvl[u] == lvl[v] + 1) nsp[u] += nsp[v];
+    }
+  }
+  for (int64_t k = tail - 1; k >= 0; --k) {
+    int32_t v = order[k];
+    dep[v] *= nsp[v];
+    for (int64_t j = off[v]; j < off[v + 1]; ++j) {
+      int32_t u = col[j];
+      if (lvl[u] + 1 == lvl[v]) dep[u] += (1.0 + dep[v]) / nsp[v];
+    }
+  }
+  free(order);
+}
+
+/* PageRank in the reference's unnormalised form (application/pagerank.cu:
+ * 19-32,120-125): pr_0 = 1-d; pr_{k+1}(v) = (1-d) + d * sum_{u in N(v)}
+ * pr_k(u)/od(u).  FP64 Jacobi for exactly iters steps; returns pr_iters. */
+void or_pagerank(int64_t n, const int64_t *off, const int32_t *col, int iters,
+                 double damp, double *pr) {
+  double *contrib = (double *)malloc(sizeof(double) * (size_t)n);
+  for (int64_t v = 0; v < n; ++v) pr[v] = 1.0 - damp;
+  for (int it = 0; it < iters; ++it) {
+    for (int64_t v = 0; v < n; ++v) {
+      int64_t od = off[v + 1] - off[v];
+      contrib[v] = od ? pr[v] / (double)od : pr[v];
+    }
+    for (int64_t v = 0; v < n; ++v) {
+      double s = 0;
+      for (int64_t j = off[v]; j < off[v + 1]; ++j) s += contrib[col[j]];
+      pr[v] = (1.0 - damp) + damp * s;
+    }
+  }
+  free(contrib);
+}
+
+/* validation(): application/pagerank.cu:44-79, the fix-point residual test
+ * in FP32 on the device's pr/od output.  Returns the first failing vertex or
+ * -1 when every vertex passes. */
+int64_t or_pagerank_check(int64_t n, const int64_t *off, const int32_t *col,
+                          const float *pr_over_od, float damp, float eps) {
+  float *pr = (float *)malloc(sizeof(float) * (size_t)n);
+  for (int64_t i = 0; i < n; ++i) {
+    int64_t od = off[i + 1] - off[i];
+    pr[i] = od ? pr_over_od[i] * (float)od : pr_over_od[i];
+  }
+  int64_t bad = -1;
+  for (int64_t i = 0; i < n && bad < 0; ++i) {
+    float sum = 0;
+    for (int64_t j = off[i]; j < off[i + 1]; ++j) {
+      int32_t u = col[j];
+      sum += pr[u] / (float)(off[u + 1] - off[u]);
+    }
+    sum = sum * damp + 1 - damp;
+    float diff = (sum - pr[i]) / sum;
+    if (!(fabsf(diff) < eps)) bad = i;
+  }
+  free(pr);
+  return bad;
+}
+
+/* validation(): application/gc.cu:45-74 - no edge joins two equal colours
+ * and no vertex with an edge stays uncoloured (-1).  Returns the first
+ * failing vertex or -1. */
+int64_t or_gc_check(int64_t n, const int64_t *off, const int32_t *col,
+                    const int32_t *color) {
+  for (int64_t i = 0; i < n; ++i) {
+    int32_t vc = color[i];
+    for (int64_t j = off[i]; j < off[i + 1]; ++j) {
+      int32_t uc = color[col[j]];
+      if (uc == vc && uc != -1) return i;
+      if (uc == -1 || vc == -1) return i;
+    }
+  }
+  return -1;
+}
+
+void or_mbfs(int64_t n, const int64_t *off, const int32_t *col, int nsrc,
+             const int32_t *roots, int32_t *lvl) {
+  for (int s = 0; s < nsrc; ++s) or_bfs(n, off, col, roots[s], lvl + (int64_t)s * n);
+}
+
+static int cmp_double(const void *a, const void *b) {
+  double x = *(const double *)a, y = *(const double *)b;
+  return (x > y) - (x < y);
+}
+
+/* graph_attr_t::fill: src/utils/fileIO.cuh:35-67, same summation order
+ * (ascending degrees) so the doubles agree bit for bit. */
+void or_degree_attr(int64_t n, const int64_t *off, double *out) {
+  double *t = (double *)malloc(sizeof(double) * (size_t)n);
+  for (int64_t i = 0; i < n; ++i) t[i] = (double)(off[i + 1] - off[i]);
+  qsort(t, (size_t)n, sizeof(double), cmp_double);
+  double avg = 0, sd = 0, gi = 0, her = 0, sum = 0;
+  for (int64_t i = 0; i < n; ++i) { avg += t[i]; sd += t[i] * t[i]; }
+  sd = sqrt((sd - avg * avg / n) / (n - 1));
+  avg /= n;
+  double range = t[n - 1] - t[0];
+  double mx = t[n - 1];
+  for (int64_t i = 1; i <= n; ++i) sum += t[i - 1];
+  for (int64_t i = 1; i <= n; ++i) {
+    double du = t[i - 1];
+    gi += (n - i + 0.5) * du / n / sum;
+    if (du != 0) her += du * (log(sum) - log(du)) / sum;
+  }
+  gi = 1 - 2 * gi;
+  her = her / log((double)n);
+  out[0] = avg; out[1] = sd; out[2] = range; out[3] = mx; out[4] = gi; out[5] = her;
+  free(t);
+}
+
+int64_t or_traversed_edges(int64_t n, const int64_t *off, const int32_t *lvl) {
+  int64_t s = 0;
+  for (int64_t v = 0; v < n; ++v)
+    if (lvl[v] >= 0) s += off[v + 1] - off[v];
+  return s / 2;
+}
