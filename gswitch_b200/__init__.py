@@ -1,0 +1,315 @@
+"""gswitch-b200: GSWITCH's level-loop graph engine for one NVIDIA B200.
+
+Host-side mirror of the C ABI (include/gsw.h, libgsw.so).  It follows the
+reference's operator/plugin vocabulary: an application runs the
+inspect -> select -> filter -> expand level loop, and any subset of the
+selector's choices can be forced with the reference's ``-c`` string
+(``"Push-Queue-WM-Fused"``, ``x`` leaves a choice to the selector;
+src/utils/cmdline.cuh:51-94).  Errors raise :class:`GswError` carrying the
+C status code.  There is no CPU fallback: importing works anywhere, but every
+call needs libgsw.so and a CUDA device.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libgsw.so")
+
+GSW_OK = 0
+STATUS = {0: "OK", 1: "INVALID_ARG", 2: "OOM", 3: "CUDA", 4: "TIMEOUT", 5: "OVERFLOW",
+          6: "UNSUPPORTED", 7: "NO_DEVICE"}
+AUTO = -1
+PUSH, PULL = 0, 1
+QUEUE, BITMAP = 0, 1
+LB = {"TM": 0, "WM": 1, "CM": 2, "STRICT": 3, "TWOD": 4, "TWC": 6}
+LB_NAMES = {v: k for k, v in LB.items()}
+FUSED, STANDALONE = 0, 1
+MAX_TRACE = 4096
+
+# exported symbols of libgsw.so, one per declaration in include/gsw.h
+ABI_SYMBOLS = (
+    "gsw_init", "gsw_destroy", "gsw_last_error_string", "gsw_version",
+    "gsw_graph_upload", "gsw_graph_generate_rmat", "gsw_graph_generate_grid",
+    "gsw_graph_generate_er", "gsw_graph_info", "gsw_graph_attr", "gsw_graph_download",
+    "gsw_graph_destroy", "gsw_graph_roots", "gsw_ctx_stream", "gsw_run_opts_default", "gsw_bfs", "gsw_sssp", "gsw_cc",
+    "gsw_pagerank", "gsw_bc", "gsw_gc", "gsw_mbfs",
+)
+
+
+class GswError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"gsw error {code} ({STATUS.get(code, '?')}): {msg}")
+        self.code = code
+
+
+class _Opts(C.Structure):
+    _fields_ = [("direction", C.c_int), ("asfmt", C.c_int), ("lb", C.c_int), ("fusion", C.c_int),
+                ("sorted_queue", C.c_int), ("max_iters", C.c_int), ("damping", C.c_float),
+                ("eps", C.c_float), ("selector", C.c_int), ("verbose", C.c_int), ("timing", C.c_int),
+                ("expand_grid", C.c_int), ("account", C.c_int), ("reserved", C.c_int * 7)]
+
+
+class _Stats(C.Structure):
+    _fields_ = [("ms", C.c_double), ("levels", C.c_int), ("edges", C.c_int64),
+                ("device_error", C.c_uint), ("launches", C.c_int64), ("ntrace", C.c_int),
+                ("level_cfg", C.c_int32 * MAX_TRACE), ("level_frontier", C.c_int64 * MAX_TRACE),
+                ("level_ms", C.c_float * MAX_TRACE), ("level_inspect_ms", C.c_float * MAX_TRACE),
+                ("level_edges", C.c_int64 * MAX_TRACE)]
+
+
+_LIB = None
+
+
+def lib():
+    """Load libgsw.so; raise if it is missing (no fallback exists)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(LIB_PATH):
+        raise GswError(7, f"{LIB_PATH} is not built; run gswitch_b200/build.py")
+    L = C.CDLL(LIB_PATH)
+    vp, i64, i32, u64 = C.c_void_p, C.c_int64, C.c_int32, C.c_uint64
+    pvp = C.POINTER(C.c_void_p)
+    L.gsw_init.argtypes = [C.c_int, pvp]
+    L.gsw_destroy.argtypes = [vp]
+    L.gsw_last_error_string.restype = C.c_char_p
+    L.gsw_graph_upload.argtypes = [vp, i64, i64, vp, vp, vp, C.c_int, pvp]
+    L.gsw_graph_generate_rmat.argtypes = [vp, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, u64,
+                                          C.c_int, u64, pvp]
+    L.gsw_graph_generate_grid.argtypes = [vp, C.c_int, C.c_int, C.c_int, u64, C.c_int, u64, pvp]
+    L.gsw_graph_generate_er.argtypes = [vp, i64, i64, u64, C.c_int, u64, pvp]
+    L.gsw_graph_info.argtypes = [vp, C.POINTER(i64), C.POINTER(i64), C.POINTER(C.c_int)]
+    L.gsw_graph_attr.argtypes = [vp, vp]
+    L.gsw_graph_download.argtypes = [vp, vp, vp, vp]
+    L.gsw_graph_destroy.argtypes = [vp]
+    L.gsw_graph_roots.argtypes = [vp, u64, C.c_int, vp]
+    L.gsw_ctx_stream.argtypes = [vp, pvp]
+    L.gsw_run_opts_default.argtypes = [C.POINTER(_Opts)]
+    L.gsw_run_opts_default.restype = None
+    po, ps = C.POINTER(_Opts), C.POINTER(_Stats)
+    L.gsw_bfs.argtypes = [vp, vp, i32, po, vp, ps]
+    L.gsw_sssp.argtypes = [vp, vp, i32, po, vp, ps]
+    L.gsw_cc.argtypes = [vp, vp, po, vp, ps]
+    L.gsw_pagerank.argtypes = [vp, vp, po, vp, ps]
+    L.gsw_bc.argtypes = [vp, vp, i32, po, vp, vp, ps]
+    L.gsw_gc.argtypes = [vp, vp, po, vp, ps]
+    L.gsw_mbfs.argtypes = [vp, vp, C.c_int, vp, C.c_int, po, vp, ps]
+    _LIB = L
+    return L
+
+
+def _check(code):
+    if code != GSW_OK:
+        raise GswError(code, lib().gsw_last_error_string().decode(errors="replace"))
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+class RunOpts:
+    """Forced choices and knobs of one run (None = selector decides)."""
+
+    def __init__(self, direction=None, asfmt=None, lb=None, fusion=None, sorted_queue=True,
+                 max_iters=0, damping=0.85, eps=0.01, verbose=False, timing=False, expand_grid=0,
+                 account=False):
+        self.direction, self.asfmt, self.lb, self.fusion = direction, asfmt, lb, fusion
+        self.sorted_queue, self.max_iters, self.damping, self.eps = sorted_queue, max_iters, damping, eps
+        self.verbose, self.timing, self.expand_grid = verbose, timing, expand_grid
+        self.account = account
+
+    @classmethod
+    def from_config(cls, cfg: str, **kw):
+        """Parse the reference's ``-c Dir-Fmt-LB-Fusion`` string."""
+        parts = (cfg.split("-") + ["x"] * 4)[:4] if cfg else ["x"] * 4
+        o = cls(**kw)
+        o.direction = {"Push": PUSH, "Pull": PULL}.get(parts[0])
+        o.asfmt = {"Queue": QUEUE, "Bitmap": BITMAP}.get(parts[1])
+        o.lb = LB.get(parts[2])
+        o.fusion = {"Fused": FUSED, "Standalone": STANDALONE}.get(parts[3])
+        return o
+
+    def to_c(self) -> _Opts:
+        o = _Opts()
+        lib().gsw_run_opts_default(C.byref(o))
+        f = lambda x: AUTO if x is None else int(x)
+        o.direction, o.asfmt, o.lb, o.fusion = f(self.direction), f(self.asfmt), f(self.lb), f(self.fusion)
+        o.sorted_queue = int(bool(self.sorted_queue))
+        o.max_iters = int(self.max_iters)
+        o.damping, o.eps = float(self.damping), float(self.eps)
+        o.verbose, o.timing, o.expand_grid = int(self.verbose), int(self.timing), int(self.expand_grid)
+        o.account = int(self.account)
+        return o
+
+
+class RunStats:
+    def __init__(self, s: _Stats):
+        self.ms = s.ms
+        self.levels = s.levels
+        self.edges = s.edges
+        self.device_error = s.device_error
+        self.launches = s.launches
+        n = min(s.ntrace, MAX_TRACE)
+        self.trace = [decode_cfg(s.level_cfg[i]) + (int(s.level_frontier[i]),) for i in range(n)]
+        self.level_ms = [float(s.level_ms[i]) for i in range(n)]
+        self.level_inspect_ms = [float(s.level_inspect_ms[i]) for i in range(n)]
+        self.level_edges = [int(s.level_edges[i]) for i in range(n)]
+
+    @property
+    def gteps(self) -> float:
+        return self.edges / (self.ms * 1e6) if self.ms > 0 else 0.0
+
+    def variants(self):
+        return {f"{d}-{f}-{lb}-{fu}" for d, f, lb, fu, _ in self.trace}
+
+
+def decode_cfg(c: int):
+    return ("Pull" if c & 1 else "Push", "Bitmap" if c & 2 else "Queue", LB_NAMES.get((c >> 2) & 7, "?"),
+            "Fused" if c & 32 else "Standalone")
+
+
+class Context:
+    """One device and one stream (gsw_init / gsw_destroy)."""
+
+    def __init__(self, device: int = 0):
+        self._h = C.c_void_p()
+        _check(lib().gsw_init(device, C.byref(self._h)))
+
+    def close(self):
+        if self._h:
+            lib().gsw_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def stream_ptr(self) -> int:
+        s = C.c_void_p()
+        _check(lib().gsw_ctx_stream(self._h, C.byref(s)))
+        return s.value or 0
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def upload(self, off, col, w=None, directed=False) -> "Graph":
+        off = np.ascontiguousarray(off, dtype=np.int64)
+        col = np.ascontiguousarray(col, dtype=np.int32)
+        w = None if w is None else np.ascontiguousarray(w, dtype=np.int32)
+        h = C.c_void_p()
+        _check(lib().gsw_graph_upload(self._h, len(off) - 1, len(col), _ptr(off), _ptr(col), _ptr(w),
+                                      int(directed), C.byref(h)))
+        return Graph(self, h)
+
+    def rmat(self, scale, ef=16, a=0.57, b=0.19, c=0.19, seed=1, wmax=0, wseed=0) -> "Graph":
+        h = C.c_void_p()
+        _check(lib().gsw_graph_generate_rmat(self._h, scale, ef, a, b, c, seed, wmax, wseed, C.byref(h)))
+        return Graph(self, h)
+
+    def grid(self, rows, cols, lr_div=100, seed=1, wmax=0, wseed=0) -> "Graph":
+        h = C.c_void_p()
+        _check(lib().gsw_graph_generate_grid(self._h, rows, cols, lr_div, seed, wmax, wseed, C.byref(h)))
+        return Graph(self, h)
+
+    def er(self, n, m_pairs, seed=1, wmax=0, wseed=0) -> "Graph":
+        h = C.c_void_p()
+        _check(lib().gsw_graph_generate_er(self._h, n, m_pairs, seed, wmax, wseed, C.byref(h)))
+        return Graph(self, h)
+
+
+class Graph:
+    """A device-resident graph (gsw_graph)."""
+
+    def __init__(self, ctx: Context, h):
+        self.ctx, self._h = ctx, h
+        n, m, wt = C.c_int64(), C.c_int64(), C.c_int()
+        _check(lib().gsw_graph_info(h, C.byref(n), C.byref(m), C.byref(wt)))
+        self.n, self.m, self.weighted = n.value, m.value, bool(wt.value)
+
+    def close(self):
+        if self._h:
+            lib().gsw_graph_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def roots(self, seed, count):
+        r = np.empty(count, dtype=np.int32)
+        _check(lib().gsw_graph_roots(self._h, seed, count, _ptr(r)))
+        return r
+
+    def attr(self):
+        out = np.empty(6, dtype=np.float64)
+        _check(lib().gsw_graph_attr(self._h, _ptr(out)))
+        return out
+
+    def download(self):
+        off = np.empty(self.n + 1, dtype=np.int64)
+        col = np.empty(self.m, dtype=np.int32)
+        w = np.empty(self.m, dtype=np.int32) if self.weighted else None
+        _check(lib().gsw_graph_download(self._h, _ptr(off), _ptr(col), _ptr(w)))
+        return off, col, w
+
+    @staticmethod
+    def _opts(opts):
+        if opts is None:
+            opts = RunOpts()
+        elif isinstance(opts, str):
+            opts = RunOpts.from_config(opts)
+        return opts.to_c()
+
+    def _run(self, fn, *args, outs, opts):
+        st = _Stats()
+        o = self._opts(opts)
+        _check(fn(self.ctx._h, self._h, *args, C.byref(o), *[_ptr(x) for x in outs], C.byref(st)))
+        return RunStats(st)
+
+    def bfs(self, root, opts=None, out=True):
+        lv = np.empty(self.n, dtype=np.int32) if out else None
+        st = self._run(lib().gsw_bfs, C.c_int32(root), outs=[lv], opts=opts)
+        return lv, st
+
+    def sssp(self, root, opts=None, out=True):
+        d = np.empty(self.n, dtype=np.int32) if out else None
+        st = self._run(lib().gsw_sssp, C.c_int32(root), outs=[d], opts=opts)
+        return d, st
+
+    def cc(self, opts=None, out=True):
+        lab = np.empty(self.n, dtype=np.int32) if out else None
+        st = self._run(lib().gsw_cc, outs=[lab], opts=opts)
+        return lab, st
+
+    def pagerank(self, iters=20, damping=0.85, eps=0.01, opts=None, out=True):
+        if opts is None or isinstance(opts, str):
+            opts = RunOpts.from_config(opts) if isinstance(opts, str) else RunOpts()
+        opts.max_iters, opts.damping, opts.eps = iters, damping, eps
+        pr = np.empty(self.n, dtype=np.float32) if out else None
+        st = self._run(lib().gsw_pagerank, outs=[pr], opts=opts)
+        return pr, st
+
+    def bc(self, root, opts=None, out=True):
+        nsp = np.empty(self.n, dtype=np.int32) if out else None
+        dep = np.empty(self.n, dtype=np.float32) if out else None
+        st = self._run(lib().gsw_bc, C.c_int32(root), outs=[nsp, dep], opts=opts)
+        return nsp, dep, st
+
+    def gc(self, opts=None, out=True):
+        col = np.empty(self.n, dtype=np.int32) if out else None
+        st = self._run(lib().gsw_gc, outs=[col], opts=opts)
+        return col, st
+
+    def mbfs(self, roots, batched=True, opts=None, out=True):
+        roots = np.ascontiguousarray(roots, dtype=np.int32)
+        lv = np.empty((len(roots), self.n), dtype=np.int32) if out else None
+        st = _Stats()
+        o = self._opts(opts)
+        _check(lib().gsw_mbfs(self.ctx._h, self._h, len(roots), _ptr(roots), int(batched), C.byref(o), _ptr(lv),
+                              C.byref(st)))
+        return lv, RunStats(st)

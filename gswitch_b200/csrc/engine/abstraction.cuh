@@ -1,0 +1,451 @@
+// Operator-facing state: vdata_t / Functor, the SSSP window, and the
+// feature / statistics / configuration records of the level loop.
+//
+// Names, fields and meanings follow the reference (src/data_structures/
+// functor.cuh:12-98, window.cuh:44-123, src/abstraction/features.cuh:13-84,
+// statistics.cuh:11-30, config.cuh:9-122) so functors and level loops
+// written against it compile unchanged.  Differences: the Functor base has no
+// virtual methods (user functors are concrete template arguments, so calls
+// bind statically and the object stays a plain kernel argument); statistics
+// counters are 64-bit (frontier workloads exceed 2^31 on scale-26 graphs);
+// a forced-variant override (the reference's `-c Dir-Fmt-LB-Fusion`) lives
+// in config_t so one process can run several forced configurations.
+#pragma once
+#include <cmath>
+#include <cstdlib>
+#include <vector>
+
+#include "frontier.cuh"
+#include "graph.cuh"
+#include "selector_trees.h"
+
+namespace gsw {
+
+inline int eval_tree(const tree_node *t, const double *fv) {
+  int i = 0;
+  for (int guard = 0; guard < 4096 && t[i].feat >= 0; ++guard)
+    i = fv[t[i].feat] <= t[i].thr ? t[i].left : t[i].right;
+  return t[i].left;
+}
+inline int eval_tree(const tree_node *t, const std::vector<double> &fv) { return eval_tree(t, fv.data()); }
+
+}  // namespace gsw
+
+// ---------------------------------------------------------------------------
+// SSSP stepping window (src/data_structures/window.cuh:44-123): vertices are
+// admitted while their value lies in [th, th + wsz); the size shrinks,
+// inflates or resets per level from a two-feature tree.
+// ---------------------------------------------------------------------------
+struct window_t {
+  double th = 0, wsz_lim = 0, wsz = 0;
+  double shrink_rate = 0.3;
+  double inflat_rate = 0.1;
+  double reset_rate = 1;
+  int win_bot = 3328;
+  int win_top = 33679;
+  bool enable = false;
+
+  bool too_large(double size) const { return size > 5 * 33679; }
+  bool ok(int size) const { return size <= win_top && size > win_bot; }
+  void set_lim(int bot, int top) {
+    win_bot = bot;
+    win_top = top;
+  }
+  template <typename FT, typename CT>
+  void adjust(const FT &fets, const CT &conf) {
+    if (conf.conf_fusion) {
+      wsz = wsz_lim;
+      return;
+    }
+    double v1[2];
+    v1[0] = fets.active_vertex;
+    v1[1] = v1[0] * fets.cur_avg_deg_active;
+    int l = gsw::eval_tree(gsw::select_stepping_tree, v1);
+    if (enable) {
+      if (l == 1) {
+        shrink();
+        if (too_large(v1[1])) shrink();
+      } else if (l == 0) {
+        inflat();
+      }
+    }
+  }
+  void set_init_winsize(double lim) {
+    th = 0;
+    wsz_lim = lim;
+    wsz = lim;
+  }
+  void shrink() { wsz = wsz * shrink_rate; }
+  void inflat() {
+    wsz = wsz / inflat_rate;
+    if (wsz > wsz_lim) wsz = wsz_lim;
+  }
+  __host__ __device__ __forceinline__ bool in(float x) const {
+    if (!enable) return true;
+    return x < th + wsz && x >= th;
+  }
+  __host__ __device__ __forceinline__ bool less(float x) const { return x < th; }
+  __host__ __device__ __forceinline__ bool greater(float x) const { return x >= th + wsz; }
+  void reset() {
+    th = th + wsz;
+    wsz = wsz_lim * reset_rate;
+  }
+};
+
+// ---------------------------------------------------------------------------
+// Per-vertex data: WA (read/write) and RA (read-only) arrays plus host
+// mirrors (functor.cuh:12-66).
+// ---------------------------------------------------------------------------
+template <typename WA, typename RA>
+struct vdata_t {
+  WA zero;
+  RA *dg_ra = nullptr;
+  WA *dg_wa = nullptr;
+  RA *h_ra = nullptr;
+  WA *h_wa = nullptr;
+  int64_t size = 0;
+  WA *sb = nullptr;  // 2D-partition partial-contribution buffer
+  int64_t sb_size = 0;
+  window_t window;
+
+  void build(int64_t n) {
+    size = n;
+    if (!std::is_same<Empty, WA>::value) {
+      GSW_CUDA(cudaMalloc((void **)&dg_wa, sizeof(WA) * (n + 1)));
+      h_wa = (WA *)malloc(sizeof(WA) * (n + 1));
+    }
+    if (!std::is_same<Empty, RA>::value) {
+      GSW_CUDA(cudaMalloc((void **)&dg_ra, sizeof(RA) * (n + 1)));
+      h_ra = (RA *)malloc(sizeof(RA) * (n + 1));
+    }
+  }
+  void destroy() {
+    cudaFree(dg_wa);
+    cudaFree(dg_ra);
+    cudaFree(sb);
+    free(h_wa);
+    free(h_ra);
+    dg_wa = nullptr;
+    dg_ra = nullptr;
+    sb = nullptr;
+    h_wa = nullptr;
+    h_ra = nullptr;
+  }
+  template <typename X>
+  void init_wa(X init) {
+    for (int64_t i = 0; i < size; ++i) h_wa[i] = init((int)i);
+    GSW_CUDA(cudaMemcpyAsync(dg_wa, h_wa, sizeof(WA) * size, cudaMemcpyHostToDevice, gsw::stream()));
+    GSW_CUDA(cudaStreamSynchronize(gsw::stream()));
+  }
+  template <typename X>
+  void init_ra(X init) {
+    for (int64_t i = 0; i < size; ++i) h_ra[i] = init((int)i);
+    GSW_CUDA(cudaMemcpyAsync(dg_ra, h_ra, sizeof(RA) * size, cudaMemcpyHostToDevice, gsw::stream()));
+    GSW_CUDA(cudaStreamSynchronize(gsw::stream()));
+  }
+  void set_zero(WA z) { zero = z; }
+  void sync_wa() {
+    GSW_CUDA(cudaMemcpyAsync(h_wa, dg_wa, sizeof(WA) * size, cudaMemcpyDeviceToHost, gsw::stream()));
+    GSW_CUDA(cudaStreamSynchronize(gsw::stream()));
+  }
+  void sync_ra() {
+    GSW_CUDA(cudaMemcpyAsync(h_ra, dg_ra, sizeof(RA) * size, cudaMemcpyDeviceToHost, gsw::stream()));
+    GSW_CUDA(cudaStreamSynchronize(gsw::stream()));
+  }
+  __device__ __forceinline__ WA *fetch_wa(int v) const { return dg_wa + v; }
+  __device__ __forceinline__ RA *fetch_ra(int v) const { return dg_ra + v; }
+};
+
+template <Centric C, typename WA, typename RA, typename E>
+struct Functor {};
+
+template <typename WA, typename RA, typename E>
+struct Functor<EC, WA, RA, E> {
+  typedef WA wa_t;
+  typedef RA ra_t;
+  typedef E e_t;
+  using G = device_graph_t<COO, E>;
+  vdata_t<WA, RA> data;
+  __device__ __forceinline__ WA *wa_of(int v) const { return data.fetch_wa(v); }
+  __device__ __forceinline__ RA *ra_of(int v) const { return data.fetch_ra(v); }
+  __device__ Status filter(int, int, E *) { return Inactive; }
+  __device__ void update(int, int, E *) {}
+};
+
+template <typename WA, typename RA, typename E>
+struct Functor<VC, WA, RA, E> {
+  typedef WA wa_t;
+  typedef RA ra_t;
+  typedef E e_t;
+  using G = device_graph_t<CSR, E>;
+  vdata_t<WA, RA> data;
+  __device__ __forceinline__ WA *wa_of(int v) const { return data.fetch_wa(v); }
+  __device__ __forceinline__ RA *ra_of(int v) const { return data.fetch_ra(v); }
+  __device__ Status filter(int, G) { return Inactive; }
+  __device__ WA emit(int v, E *, G) { return *data.fetch_wa(v); }
+  __device__ bool cond(int, WA, G) { return false; }
+  __device__ bool comp(WA *, WA, G) { return true; }
+  __device__ bool compAtomic(WA *, WA, G) { return true; }
+  __device__ bool exit(int, G) { return false; }
+};
+
+template <Centric C = VC, LB S = WM, Direction D = Push>
+struct ExpandProxy {};
+
+// ---------------------------------------------------------------------------
+// Forced-variant override (the `-c Push-Queue-CM-Fused` flag of
+// src/utils/cmdline.cuh:51-94): any subset of the four choices.
+// ---------------------------------------------------------------------------
+struct ins_t {
+  Direction d = Push;
+  ASFmt asf = Queue;
+  LB lb = WM;
+  Fusion fusion = Standalone;
+  bool has_direction = false;
+  bool has_asfmt = false;
+  bool has_lb = false;
+  bool has_fusion = false;
+};
+
+// ---------------------------------------------------------------------------
+// config_t (src/abstraction/config.cuh:9-122)
+// ---------------------------------------------------------------------------
+struct config_t {
+  Direction conf_dir = Push;
+  Status conf_target = Active;
+  CullMode conf_cm = Interleave;
+  ASFmt conf_asfmt = Queue;
+  LB conf_lb = WM;
+  Centric conf_centric = VC;
+  QueueMode conf_qmode = Normal;
+
+  bool conf_fromall = false;
+  bool conf_toall = false;
+  bool conf_fixed = false;
+  bool conf_inherit = false;
+  bool conf_2d_partition = false;
+
+  bool conf_first_round = true;
+  bool conf_switch_to_fusion = false;
+  bool conf_switch_to_standalone = false;
+  bool conf_pruning = false;
+  bool conf_once = false;
+  bool conf_ignore_u_state = false;
+  bool conf_fuse_inspect = false;
+  bool conf_lite = false;
+  bool conf_window = false;
+  bool conf_compensation = false;
+  bool conf_super_fusion = false;
+  bool conf_fusion = false;
+  int conf_idle = 0;
+  int ctanum = CTANUM_EXPAND;
+  int thdnum = THDNUM_EXPAND;
+
+  // engine extensions
+  bool conf_sorted_queue = true;   // bitmap->queue in vertex order
+  bool conf_persistent = false;    // run fused levels in one grid-wide launch
+  bool conf_count_edges = false;   // accounting pass: expands count edges
+  ins_t force;                     // forced choices (empty = selector decides)
+
+  void reset() {
+    conf_first_round = true;
+    conf_switch_to_fusion = false;
+    conf_switch_to_standalone = false;
+    conf_fuse_inspect = false;
+    conf_idle = 0;
+  }
+  __host__ __device__ __forceinline__ bool ignore_u_state() const { return conf_ignore_u_state; }
+  __host__ __device__ __forceinline__ Status want() const { return conf_target; }
+  __host__ __device__ __forceinline__ bool pruning() const { return conf_pruning; }
+  __host__ __device__ __forceinline__ bool fuse_inspect() const { return conf_fuse_inspect; }
+
+  const char *lb_name() const {
+    switch (conf_lb) {
+      case TM: return "TM";
+      case WM: return "WM";
+      case CM: return "CM";
+      case STRICT: return "STRICT";
+      case TWOD: return "2D-partition";
+      case ELB: return "ELB";
+      case TWC: return "TWC";
+    }
+    return "Unknown";
+  }
+  void show_hints() const {
+    printf("[%s|%s|%s|%s] ", conf_dir == Push ? "Push" : "Pull", conf_asfmt == Queue ? "Queue" : "Bitmap",
+           lb_name(), conf_fuse_inspect ? "Fused" : "Standalone");
+  }
+};
+
+// ---------------------------------------------------------------------------
+// stat_t (src/abstraction/statistics.cuh:11-30): device counters reduced by
+// the inspector plus per-level timing history.
+//   [0] active vertices  [1] inactive vertices  [2] push workload
+//   [3] pull workload    [4] max push degree    [5] max pull degree
+// The last two keep the reference's definition (inspector.cuh:101-109): each
+// block of the 256x512 inspection grid sums its threads' maxima, then the
+// push figure takes the maximum over blocks and the pull figure the sum.
+// ---------------------------------------------------------------------------
+struct stat_t {
+  unsigned long long *dg_runtime_info = nullptr;
+  unsigned long long *h_runtime_info = nullptr;
+  int size = 0;
+  double last_time = 0, avg_time = 0;
+  double last_filter_time = 0, last_expand_time = 0;
+  double avg_filter_time = 0, avg_expand_time = 0;
+  int level = 0;
+  int64_t last_scanned = 0;  // edges the last expand touched (accounting)
+
+  void build(int _size = 8) {
+    if (dg_runtime_info) return;
+    size = _size;
+    GSW_CUDA(cudaMalloc((void **)&dg_runtime_info, size * sizeof(unsigned long long)));
+    GSW_CUDA(cudaMallocHost((void **)&h_runtime_info, size * sizeof(unsigned long long)));
+    memset(h_runtime_info, 0, size * sizeof(unsigned long long));
+    clean();
+  }
+  void destroy() {
+    cudaFree(dg_runtime_info);
+    cudaFreeHost(h_runtime_info);
+    dg_runtime_info = nullptr;
+    h_runtime_info = nullptr;
+  }
+  void reset() {}
+  void collect(int num) {
+    GSW_CUDA(cudaMemcpyAsync(h_runtime_info, dg_runtime_info, num * sizeof(unsigned long long),
+                             cudaMemcpyDeviceToHost, gsw::stream()));
+    GSW_CUDA(cudaStreamSynchronize(gsw::stream()));
+  }
+  void clean() {
+    GSW_CUDA(cudaMemsetAsync(dg_runtime_info, 0, sizeof(unsigned long long) * size, gsw::stream()));
+  }
+  int64_t active_num() const { return (int64_t)h_runtime_info[0]; }
+  int64_t unactive_num() const { return (int64_t)h_runtime_info[1]; }
+  int64_t push_workload() const { return (int64_t)h_runtime_info[2]; }
+  int64_t pull_workload() const { return (int64_t)h_runtime_info[3]; }
+  int64_t max_deg_active() const { return (int64_t)h_runtime_info[4]; }
+  int64_t max_deg_unactive() const { return (int64_t)h_runtime_info[5]; }
+  void show_hints() const { printf("Iteration %d: (Filter %.3f ms) (Expand %.3f ms) ", level, last_filter_time, last_expand_time); }
+};
+
+// ---------------------------------------------------------------------------
+// feature_t (src/abstraction/features.cuh:13-84): the 21-entry feature
+// vector the selector reads, with the from-all / to-all folding of cross().
+// ---------------------------------------------------------------------------
+struct feature_t {
+  Centric centric = VC;
+  Computation pattern = Idem;
+  int use_root = -1;
+  bool fromall = false;
+  bool toall = false;
+
+  int64_t nvertexs = 0;
+  int64_t nedges = 0;
+  double avg_deg = 0, std_deg = 0, max_deg = 0, range = 0, GI = 0, Her = 0;
+  double avg_edata = 0;
+
+  double active_vertex = 0, unactive_vertex = 0;
+  double active_vertex_ratio = 0, unactive_vertex_ratio = 0;
+  double push_workload = 0, pull_workload = 0;
+  double push_workload_ratio = 0, pull_workload_ratio = 0;
+  double cur_max_deg_active = 0, cur_avg_deg_active = 0;
+  double cur_max_deg_unactive = 0, cur_avg_deg_unactive = 0;
+
+  int level = 0;
+  double last_time = 0, avg_time = 0;
+  double last_filter_time = 0, last_expand_time = 0;
+  double avg_filter_time = 0, avg_expand_time = 0;
+  double growing_rate = 0;
+  double first_workload = 0;
+
+  double cap = 0;
+  int thread_lim = 0, register_lim = 0, sm_num = 0;
+
+  double fv[21] = {0};
+  const char *record_path = nullptr;  // JSON-lines sink for record()
+
+  void reset() {}
+
+  void flatten() {
+    fv[0] = (double)nvertexs;
+    fv[1] = (double)nedges;
+    fv[2] = avg_deg;
+    fv[3] = std_deg;
+    fv[4] = range;
+    fv[5] = GI;
+    fv[6] = Her;
+    fv[7] = active_vertex;
+    fv[8] = unactive_vertex;
+    fv[9] = push_workload;
+    fv[10] = pull_workload;
+    fv[11] = active_vertex_ratio;
+    fv[12] = unactive_vertex_ratio;
+    fv[13] = push_workload_ratio;
+    fv[14] = pull_workload_ratio;
+    fv[15] = cur_avg_deg_active;
+    fv[16] = cur_avg_deg_unactive;
+    fv[17] = cur_max_deg_active;
+    fv[18] = cur_max_deg_unactive;
+    fv[19] = DIV(last_filter_time, avg_filter_time);
+    fv[20] = DIV(last_expand_time, avg_expand_time);
+    cross();
+  }
+
+  // from-all patterns see every vertex as a source, to-all patterns every
+  // vertex as a target: fold the other side's workload in (features.cuh:46-84)
+  void cross() {
+    const double av = active_vertex, uv = unactive_vertex;
+    const double mixed = (av + uv == 0) ? 0 : ((cur_avg_deg_active * av + cur_avg_deg_unactive * uv) / (av + uv));
+    if (fromall) {
+      fv[7] += unactive_vertex;
+      fv[9] += pull_workload;
+      fv[11] += unactive_vertex_ratio;
+      fv[13] += pull_workload_ratio;
+      fv[15] += mixed;
+      fv[17] = MAX(cur_max_deg_unactive, cur_max_deg_active);
+    }
+    if (toall) {
+      fv[8] += active_vertex;
+      fv[10] += push_workload;
+      fv[12] += active_vertex_ratio;
+      fv[14] += push_workload_ratio;
+      fv[16] += mixed;
+      fv[18] = MAX(cur_max_deg_active, cur_max_deg_unactive);
+    }
+    active_vertex = fv[7];
+    unactive_vertex = fv[8];
+    push_workload = fv[9];
+    pull_workload = fv[10];
+    active_vertex_ratio = fv[11];
+    unactive_vertex_ratio = fv[12];
+    push_workload_ratio = fv[13];
+    pull_workload_ratio = fv[14];
+    cur_avg_deg_active = fv[15];
+    cur_avg_deg_unactive = fv[16];
+    cur_max_deg_active = fv[17];
+    cur_max_deg_unactive = fv[18];
+  }
+
+  void record() {
+    flatten();
+    if (!record_path) return;
+    FILE *f = fopen(record_path, "a");
+    if (!f) return;
+    fprintf(f, "{");
+    for (int i = 0; i < 21; ++i) fprintf(f, "\"%d\": %.17g, ", i, fv[i]);
+    fprintf(f, "\"21\": %.17g, \"22\": %.17g}\n", last_filter_time, last_expand_time);
+    fclose(f);
+  }
+
+  void architecture_features(int device = -1) {
+    if (device < 0) cudaGetDevice(&device);
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return;
+    cap = prop.minor;
+    while (cap > 1) cap /= 10;
+    cap += prop.major;
+    register_lim = prop.regsPerBlock / 512;
+    thread_lim = prop.maxThreadsPerBlock;
+    sm_num = prop.multiProcessorCount;
+  }
+};

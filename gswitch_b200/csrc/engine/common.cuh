@@ -1,0 +1,251 @@
+// GSWITCH-on-B200 engine: shared vocabulary, error state and warp/block
+// primitives.
+//
+// The enums, the ALL_ACTIVE/ALL_INACTIVE roots and the Empty edge type are
+// the reference's operator-API vocabulary (src/utils/common.cuh:6-37,
+// src/utils/utils.cuh:247-249) and keep their names and values so user
+// functors written against the reference compile unchanged.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cstdio>
+#include <cstring>
+#include <type_traits>
+
+#include "../../../include/gsw.h"
+
+#define ALL_ACTIVE -1
+#define ALL_INACTIVE -2
+
+enum Status { Inactive = 0, Active = 1, All = 2, Fixed = 3 };
+enum GraphFmt { CSR, COO };
+enum Centric { EC, VC };
+enum Computation { Idem, Mono, ASSO };
+enum QueueMode { Normal, Cached };
+enum Direction { Push, Pull };
+enum ASFmt { Queue, Bitmap };
+enum LB { TM, WM, CM, STRICT, TWOD, ELB, TWC };
+enum Fusion { Fused, Standalone };
+enum CullMode { Interleave, Stride };
+
+// Launch-shape constants of the reference API (src/utils/common.cuh:12-24).
+// The engine's own kernels size their grids from the SM count instead; these
+// remain for code that names them.
+const int CTANUM = 256;
+const int THDNUM = 512;
+const int CTANUM_EXPAND = 256;
+const int THDNUM_EXPAND = 512;
+const int BSZ = THDNUM_EXPAND * 6;      // 2D-partition tile (vertices)
+const int THRESHOLD = 6144 * 4;         // 2D-partition heavy-tile edge count
+
+struct Empty {
+  char placeholder;
+};
+
+typedef int64_t packed_t;
+
+#ifndef MIN
+#define MIN(a, b) ((a) < (b) ? (a) : (b))
+#endif
+#ifndef MAX
+#define MAX(a, b) ((a) > (b) ? (a) : (b))
+#endif
+#define DIV(a, b) ((b) == 0 ? 0 : ((a + .0) / (b)))
+
+namespace gsw {
+
+// status codes are the C ABI's (GSW_OK, GSW_ERR_*), include/gsw.h
+
+// Device error word bits, written by kernels and read by the host.
+enum device_error_bits : unsigned {
+  DEV_ERR_QUEUE_OVERFLOW = 1u,
+  DEV_ERR_BARRIER_TIMEOUT = 2u,
+  DEV_ERR_BAD_VERTEX = 4u,
+  DEV_ERR_SCRATCH_OVERFLOW = 8u,
+};
+
+// Sticky host-side error (first error wins until cleared), one per thread.
+struct error_state {
+  int code = GSW_OK;
+  char msg[512] = {0};
+};
+inline error_state &err() {
+  static thread_local error_state e;
+  return e;
+}
+inline int set_error(int code, const char *fmt, const char *a = "", int line = 0) {
+  error_state &e = err();
+  if (e.code == GSW_OK) {
+    e.code = code;
+    snprintf(e.msg, sizeof(e.msg), fmt, a, line);
+  }
+  return code;
+}
+inline void clear_error() {
+  err().code = GSW_OK;
+  err().msg[0] = 0;
+}
+inline bool ok() { return err().code == GSW_OK; }
+
+inline int cuda_check(cudaError_t e, const char *file, int line) {
+  if (e == cudaSuccess) return GSW_OK;
+  char buf[256];
+  snprintf(buf, sizeof(buf), "%s: %%s:%%d", cudaGetErrorString(e));
+  return set_error(e == cudaErrorMemoryAllocation ? GSW_ERR_OOM : GSW_ERR_CUDA, buf, file, line);
+}
+#define GSW_CUDA(x) ::gsw::cuda_check((x), __FILE__, __LINE__)
+// kernels launched by the engine on this thread (reported per run)
+inline long long &launch_count() {
+  static thread_local long long c = 0;
+  return c;
+}
+#define GSW_LAUNCHED() (++::gsw::launch_count(), ::gsw::cuda_check(cudaGetLastError(), __FILE__, __LINE__))
+
+// ---- device primitives --------------------------------------------------
+static constexpr unsigned FULL = 0xffffffffu;
+
+__device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
+__device__ __forceinline__ int warp_id() { return threadIdx.x >> 5; }
+
+template <typename T>
+__device__ __forceinline__ T warp_inclusive_sum(T x) {
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    T y = __shfl_up_sync(FULL, x, d);
+    if (lane_id() >= d) x += y;
+  }
+  return x;
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T x) {
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) x += __shfl_xor_sync(FULL, x, d);
+  return x;
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_max(T x) {
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) {
+    T y = __shfl_xor_sync(FULL, x, d);
+    x = x > y ? x : y;
+  }
+  return x;
+}
+
+// Block-wide reduction; every thread of the block must call it.
+// smem needs 32 slots of T.
+template <typename T, bool IS_MAX = false>
+__device__ __forceinline__ T block_reduce(T x, T *smem) {
+  x = IS_MAX ? warp_max(x) : warp_sum(x);
+  __syncthreads();
+  if (lane_id() == 0) smem[warp_id()] = x;
+  __syncthreads();
+  const int nw = (blockDim.x + 31) >> 5;
+  T r = threadIdx.x < nw ? smem[threadIdx.x] : T(0);
+  if (warp_id() == 0) r = IS_MAX ? warp_max(r) : warp_sum(r);
+  if (threadIdx.x == 0) smem[0] = r;
+  __syncthreads();
+  r = smem[0];
+  __syncthreads();
+  return r;
+}
+
+// Block-wide exclusive scan of ints; returns the block total in *total.
+// smem needs 33 ints.  Every thread of the block must call it.
+__device__ __forceinline__ int block_exclusive_scan(int x, int *smem, int *total) {
+  int incl = warp_inclusive_sum(x);
+  __syncthreads();
+  if (lane_id() == 31) smem[warp_id()] = incl;
+  __syncthreads();
+  const int nw = (blockDim.x + 31) >> 5;
+  if (warp_id() == 0) {
+    int s = lane_id() < nw ? smem[lane_id()] : 0;
+    int si = warp_inclusive_sum(s);
+    if (lane_id() < nw) smem[lane_id()] = si - s;
+    if (lane_id() == 31) smem[32] = si;
+  }
+  __syncthreads();
+  int r = smem[warp_id()] + incl - x;
+  *total = smem[32];
+  __syncthreads();
+  return r;
+}
+
+// Number of entries of the ascending array a[0..n) that are <= key, i.e. the
+// index of the segment that owns `key` plus one (src/utils/intrinsics.cuh:
+// 78-91 computes the same bound).
+template <typename T>
+__device__ __forceinline__ int upper_bound(const T *a, int n, T key) {
+  int lo = 0, hi = n;
+  while (lo < hi) {
+    int mid = (lo + hi) >> 1;
+    if (a[mid] <= key)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+template <typename T>
+__device__ __forceinline__ int64_t upper_bound64(const T *a, int64_t n, T key) {
+  int64_t lo = 0, hi = n;
+  while (lo < hi) {
+    int64_t mid = (lo + hi) >> 1;
+    if (a[mid] <= key)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+
+// 4-byte-packed shuffle of an arbitrary value type (the reference's
+// __exshfl_down, src/utils/intrinsics.cuh:293-302).
+template <typename T>
+__device__ __forceinline__ T shfl_down_any(T v, int delta) {
+  static_assert(sizeof(T) % 4 == 0 || sizeof(T) < 4, "4-byte packed type");
+  if (sizeof(T) < 4) {
+    int x = 0;
+    memcpy(&x, &v, sizeof(T));
+    x = __shfl_down_sync(FULL, x, delta);
+    memcpy(&v, &x, sizeof(T));
+    return v;
+  }
+  int x[sizeof(T) / 4 > 0 ? sizeof(T) / 4 : 1];
+  memcpy(x, &v, sizeof(T));
+#pragma unroll
+  for (int i = 0; i < (int)(sizeof(T) / 4); ++i) x[i] = __shfl_down_sync(FULL, x[i], delta);
+  memcpy(&v, x, sizeof(T));
+  return v;
+}
+
+template <typename T>
+__device__ __forceinline__ bool equals_any(const T &a, const T &b) {
+  return memcmp(&a, &b, sizeof(T)) == 0;
+}
+
+__device__ __forceinline__ uint64_t globaltimer_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+}  // namespace gsw
+
+// float atomicMin used by user functors (src/utils/intrinsics.cuh:304-313
+// offers the same overload): CAS loop on the bit pattern.
+__device__ __forceinline__ float atomicMin(float *address, float val) {
+  int *ai = (int *)address;
+  int old = *ai, assumed;
+  do {
+    assumed = old;
+    float cur = __int_as_float(assumed);
+    if (!(val < cur)) break;
+    old = atomicCAS(ai, assumed, __float_as_int(val));
+  } while (assumed != old);
+  return __int_as_float(old);
+}

@@ -1,0 +1,758 @@
+// Host side of the level loop: inspector_t, selector_t, executor_t,
+// init_conf / reset_conf, active-set convergence and CC pointer jumping.
+//
+// The decision logic restates the reference (src/abstraction/inspector.cuh:
+// 112-244, selector.cuh:20-304, executor.cuh:17-151, src/gswitch.h:19-108,
+// data_structures/active_set.cuh:37-43, notification.cuh:233-254).  What
+// changes is the host/device traffic: a standalone level costs one host
+// synchronisation (the inspector's counters), not four.  The frontier size
+// the kernels need is read on the device; grid sizes come from the counters
+// the host already holds.  Fused levels synchronise once (convergence flag
+// and next frontier size).  Explicit deviations:
+//   * a forced fusion mode (`-c ...-Fused|Standalone`) holds for every level
+//     (the reference lets trigger_fusion re-enable fusion for Idem patterns);
+//   * a forced load balance also applies to fused levels (the reference's
+//     fusion() always picks WM);
+//   * the selector's label mapping quirk is kept: tree class 0 -> WM,
+//     1 -> CM, anything else -> STRICT (selector.cuh:126-131, 209-214).
+#pragma once
+#include <chrono>
+#include <unordered_map>
+
+#include "k_expand.cuh"
+
+namespace gsw {
+
+inline int sm_count() {
+  static thread_local int c = 0;
+  if (!c) {
+    int d = 0;
+    cudaGetDevice(&d);
+    cudaDeviceGetAttribute(&c, cudaDevAttrMultiProcessorCount, d);
+    if (c <= 0) c = 148;
+  }
+  return c;
+}
+
+// resident-grid size of a kernel (SMs x resident blocks per SM), cached
+template <typename K>
+inline int resident_grid(K kernel, int block, size_t smem = 0) {
+  static thread_local std::unordered_map<const void *, int> cache;
+  auto it = cache.find((const void *)kernel);
+  if (it != cache.end()) return it->second;
+  int per = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, block, smem) != cudaSuccess || per <= 0) per = 1;
+  int gsz = per * sm_count();
+  cache[(const void *)kernel] = gsz;
+  return gsz;
+}
+
+inline int clamp_grid(int64_t want, int cap) {
+  if (want < 1) want = 1;
+  return (int)MIN(want, (int64_t)cap);
+}
+
+inline double now_ms() {
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+// per-run knobs of the engine (defaults reproduce the reference's behaviour)
+struct engine_opts_t {
+  bool verbose = false;
+  bool timing = false;        // per-level CUDA-event timing into the stats
+  int force_grid = 0;         // autotuner: fixed expand grid (0 = derive)
+};
+inline engine_opts_t &opts() {
+  static thread_local engine_opts_t o;
+  return o;
+}
+
+// sizes the host knows without a device round trip
+struct hints_t {
+  int64_t frontier = -1;  // entries in the expand's work list
+  int64_t edges = -1;     // edges they touch
+};
+inline hints_t &hints() {
+  static thread_local hints_t h;
+  return h;
+}
+
+// Event pairs recorded around kernels when per-level timing is on; they are
+// resolved after the run, so timing adds no synchronisation.
+struct event_pool {
+  std::vector<cudaEvent_t> ev;
+  size_t used = 0;
+  int record() {
+    if (used == ev.size()) {
+      cudaEvent_t e;
+      if (cudaEventCreate(&e) != cudaSuccess) return -1;
+      ev.push_back(e);
+    }
+    cudaEventRecord(ev[used], stream());
+    return (int)used++;
+  }
+  float elapsed(int a, int b) const {
+    float ms = 0;
+    if (a < 0 || b < 0 || cudaEventElapsedTime(&ms, ev[a], ev[b]) != cudaSuccess) return 0;
+    return ms;
+  }
+};
+inline event_pool &timing_pool() {
+  static thread_local event_pool p;
+  return p;
+}
+// event indices of the last inspect and expand launches (-1 = none)
+struct kernel_marks {
+  int insp0 = -1, insp1 = -1, exp0 = -1, exp1 = -1;
+};
+inline kernel_marks &marks() {
+  static thread_local kernel_marks m;
+  return m;
+}
+
+// ===========================================================================
+// inspector_t
+// ===========================================================================
+struct inspector_t {
+  template <typename E, typename F>
+  void inspect(active_set_t &as, device_graph_t<CSR, E> g, F &f, stat_t &stat, feature_t &fets, config_t &conf) {
+    stat.last_filter_time = now_ms();
+    f.data.window.adjust(fets, conf);
+    bool need_inspect = !conf.conf_fuse_inspect;
+    init_fets(stat, fets, g.nvertexs, g.nedges);
+    if (need_inspect && conf.conf_first_round) {
+      set_first_fets(fets, g.nvertexs, g.nedges);
+      need_inspect = false;
+    }
+    marks().insp0 = marks().insp1 = -1;
+    if (need_inspect) {
+      if (opts().timing) marks().insp0 = timing_pool().record();
+      k_inspect_vc<<<INSPECT_CTAS, INSPECT_THREADS, 0, stream()>>>(as, g, f, stat.dg_runtime_info);
+      GSW_LAUNCHED();
+      if (opts().timing) marks().insp1 = timing_pool().record();
+      set_fets(as, stat, fets, conf, g.nvertexs, g.nedges);
+    }
+    fets.flatten();
+  }
+
+  template <typename E, typename F>
+  void inspect(active_set_t &as, device_graph_t<COO, E> g, F &f, stat_t &stat, feature_t &fets, config_t &conf) {
+    stat.last_filter_time = now_ms();
+    init_fets(stat, fets, g.nvertexs, g.nedges);
+    if (conf.conf_first_round) {
+      conf.conf_first_round = false;
+      fets.active_vertex = (double)g.nedges;
+      fets.active_vertex_ratio = 1;
+      raw_frontier = g.nedges;
+      return;
+    }
+    marks().insp0 = marks().insp1 = -1;
+    if (opts().timing) marks().insp0 = timing_pool().record();
+    k_inspect_ec<<<INSPECT_CTAS, INSPECT_THREADS, 0, stream()>>>(as, g, f, stat.dg_runtime_info);
+    GSW_LAUNCHED();
+    if (opts().timing) marks().insp1 = timing_pool().record();
+    set_fets(as, stat, fets, conf, g.nvertexs, g.nedges);
+    fets.flatten();
+  }
+
+  void init_fets(stat_t &stat, feature_t &fets, int64_t nvertexs, int64_t edges) {
+    fets.level = stat.level;
+    fets.active_vertex = 0;
+    fets.active_vertex_ratio = 0;
+    fets.unactive_vertex = (double)nvertexs;
+    fets.unactive_vertex_ratio = 1;
+    fets.growing_rate = fets.push_workload;
+    fets.push_workload = 0;
+    fets.pull_workload = (double)edges;
+    fets.push_workload_ratio = 0;
+    fets.pull_workload_ratio = 1;
+    fets.cur_avg_deg_active = 0;
+    fets.cur_avg_deg_unactive = fets.avg_deg;
+  }
+
+  void set_first_fets(feature_t &fets, int64_t nvertexs, int64_t nedges) {
+    if (fets.use_root < 0) {
+      fets.active_vertex = (double)nvertexs;
+      fets.unactive_vertex = 0;
+      fets.push_workload = (double)nedges;
+      fets.pull_workload = 0;
+    } else {
+      fets.active_vertex = 1;
+      fets.unactive_vertex = (double)(nvertexs - 1);
+      fets.push_workload = fets.first_workload;
+      fets.pull_workload = nedges - fets.first_workload;
+    }
+    fets.active_vertex_ratio = fets.active_vertex / nvertexs;
+    fets.unactive_vertex_ratio = fets.unactive_vertex / nvertexs;
+    fets.push_workload_ratio = fets.push_workload / nedges;
+    fets.pull_workload_ratio = fets.pull_workload / nedges;
+    fets.cur_avg_deg_active = DIV(fets.push_workload, fets.active_vertex);
+    fets.cur_avg_deg_unactive = DIV(fets.pull_workload, fets.unactive_vertex);
+    fets.cur_max_deg_active = fets.push_workload;
+    fets.cur_max_deg_unactive = fets.avg_deg;
+    raw_frontier = (int64_t)fets.active_vertex;
+    raw_inactive = (int64_t)fets.unactive_vertex;
+    raw_push = (int64_t)fets.push_workload;
+    raw_pull = (int64_t)fets.pull_workload;
+  }
+
+  void set_fets(active_set_t &as, stat_t &stat, feature_t &fets, const config_t &conf, int64_t nvertexs,
+                int64_t nedges) {
+    stat.collect(6);  // the one synchronisation of a standalone level
+    stat.clean();
+    raw_frontier = stat.active_num();
+    raw_inactive = stat.unactive_num();
+    raw_push = stat.push_workload();
+    raw_pull = stat.pull_workload();
+    fets.active_vertex = (double)stat.active_num();
+    fets.unactive_vertex = (double)stat.unactive_num();
+    fets.active_vertex_ratio = (double)stat.active_num() / nvertexs;
+    fets.unactive_vertex_ratio = (double)stat.unactive_num() / nvertexs;
+    bool done = fets.active_vertex <= 0;
+    if (fets.pattern == Idem && fets.unactive_vertex <= 0) done = true;
+    if (done) {
+      if (conf.conf_qmode == Cached) as.queue.swap();
+      as.halt_host();
+    }
+    fets.growing_rate = (0.0 + stat.push_workload()) / fets.growing_rate;
+    fets.push_workload = (double)stat.push_workload();
+    fets.pull_workload = (double)stat.pull_workload();
+    fets.push_workload_ratio = (double)stat.push_workload() / nedges;
+    fets.pull_workload_ratio = (double)stat.pull_workload() / nedges;
+    fets.cur_avg_deg_active = DIV(fets.push_workload, fets.active_vertex);
+    fets.cur_avg_deg_unactive = DIV(fets.pull_workload, fets.unactive_vertex);
+    fets.cur_max_deg_active = (double)stat.max_deg_active();
+    fets.cur_max_deg_unactive = (double)stat.max_deg_unactive();
+  }
+
+  // raw counters of the last inspection (before cross() folding)
+  int64_t raw_frontier = 0, raw_inactive = 0, raw_push = 0, raw_pull = 0;
+};
+
+// ===========================================================================
+// selector_t
+// ===========================================================================
+inline LB lb_from_class(int l) { return l == 0 ? WM : (l == 1 ? CM : STRICT); }
+
+struct selector_t {
+  void select(stat_t &stats, feature_t &fets, config_t &conf) { select_based_on_model(stats, fets, conf); }
+
+  void trigger_fusion(const feature_t &fets, config_t &conf) {
+    if (conf.force.has_fusion) return;
+    if (!conf.conf_fuse_inspect) {
+      const double potential = fets.push_workload_ratio + fets.pull_workload_ratio;
+      if (potential < 0.001) {
+        conf.conf_fuse_inspect = true;
+        conf.conf_switch_to_fusion = true;
+      }
+      if (fets.growing_rate > 2) conf.conf_idle = 0;
+      if (conf.conf_idle >= 3) {
+        conf.conf_fuse_inspect = true;
+        conf.conf_switch_to_fusion = true;
+        conf.conf_idle = 0;
+      }
+    }
+  }
+
+  void fusion(const feature_t &fets, config_t &conf) {
+    conf.conf_dir = Push;
+    conf.conf_asfmt = Queue;
+    conf.conf_cm = Interleave;
+    conf.conf_lb = conf.force.has_lb && conf.force.lb != TWOD ? conf.force.lb : WM;
+    conf.conf_fuse_inspect = true;
+    conf.conf_centric = fets.centric;
+    conf.conf_fromall = fets.fromall;
+    conf.conf_toall = fets.toall;
+    set_target(conf);
+  }
+
+  static void set_target(config_t &conf) {
+    if (conf.conf_dir == Push)
+      conf.conf_target = conf.conf_fromall ? All : Active;
+    else
+      conf.conf_target = (conf.conf_toall && conf.conf_dir == Pull) ? All : Inactive;
+  }
+
+  static void dir_ratios(const feature_t &fets, double *v) {
+    const double *fv = fets.fv;
+    v[0] = fv[8] / (fv[7] + 0.1);
+    v[1] = fv[10] / (fv[9] + 0.1);
+    v[2] = fv[16] / (fv[15] + 0.1);
+    v[3] = fv[18] / (fv[17] + 0.1);
+    v[4] = fv[9] / (fv[15] + 0.1);
+    v[5] = fv[10] / (fv[16] + 0.1);
+    v[6] = fv[9] / (fv[17] + 0.1);
+    v[7] = fv[10] / (fv[18] + 0.1);
+  }
+
+  void select_idem(feature_t &fets, config_t &conf) {
+    double v[16];
+    dir_ratios(fets, v);
+    conf.conf_dir = eval_tree(select_dir_idem_tree, v) == 1 ? Pull : Push;
+    if (fets.push_workload_ratio * 5 < fets.pull_workload_ratio) conf.conf_dir = Push;
+    if (conf.force.has_direction) conf.conf_dir = conf.force.d;
+    if (conf.conf_dir == Pull) {
+      conf.conf_asfmt = fets.fv[12] < 0.01 ? Queue : Bitmap;
+    } else {
+      v[0] = fets.fv[11];
+      conf.conf_asfmt = eval_tree(select_fmt_tree, v) ? Bitmap : Queue;
+    }
+    if (conf.force.has_asfmt) conf.conf_asfmt = conf.force.asf;
+    if (conf.conf_dir == Pull) {
+      conf.conf_lb = TM;
+    } else {
+      int k = 0;
+      for (int i = 0; i < 7; ++i) v[k++] = fets.fv[i];
+      for (int i = 7; i < 18; i += 2) v[k++] = fets.fv[i];
+      conf.conf_lb = lb_from_class(eval_tree(select_lb_idem_tree, v));
+    }
+    if (conf.force.has_lb) conf.conf_lb = conf.force.lb;
+  }
+
+  void select_ASSO(feature_t &fets, config_t &conf) {
+    double v[24];
+    dir_ratios(fets, v);
+    conf.conf_dir = eval_tree(select_dir_asso_tree, v) == 1 ? Pull : Push;
+    if (conf.force.has_direction) conf.conf_dir = conf.force.d;
+    if (conf.conf_fromall && conf.conf_toall) {
+      for (int i = 0; i < 7; ++i) v[i] = fets.fv[i];
+      conf.conf_dir = eval_tree(select_dir_asso_backup_tree, v) ? Pull : Push;
+      if (conf.force.has_direction) conf.conf_dir = conf.force.d;
+    }
+    v[0] = conf.conf_dir == Push ? fets.fv[11] : fets.fv[12];
+    conf.conf_asfmt = eval_tree(select_fmt_tree, v) ? Bitmap : Queue;
+    if (fets.fromall && fets.toall && !conf.conf_fixed) conf.conf_asfmt = Bitmap;
+    if (conf.force.has_asfmt) conf.conf_asfmt = conf.force.asf;
+    int k = 0;
+    for (int i = 0; i < 7; ++i) v[k++] = fets.fv[i];
+    int l;
+    const bool all2all = conf.conf_fromall && conf.conf_toall && !conf.conf_fixed;
+    if (conf.conf_dir == Pull) {
+      if (all2all) {
+        l = eval_tree(select_lb_asso_backward_backup_tree, v);
+      } else {
+        for (int i = 8; i <= 18; i += 2) v[k++] = fets.fv[i];
+        l = eval_tree(select_lb_asso_backward_tree, v);
+      }
+    } else {
+      if (all2all) {
+        l = eval_tree(select_lb_asso_backward_backup_tree, v);
+      } else {
+        for (int i = 7; i < 18; i += 2) v[k++] = fets.fv[i];
+        l = eval_tree(select_lb_asso_forward_tree, v);
+      }
+    }
+    conf.conf_lb = lb_from_class(l);
+    if (conf.force.has_lb) conf.conf_lb = conf.force.lb;
+  }
+
+  void select_Mono(feature_t &fets, config_t &conf) {
+    conf.conf_dir = conf.force.has_direction ? conf.force.d : Push;
+    conf.conf_asfmt = conf.force.has_asfmt ? conf.force.asf : Queue;
+    double v[16];
+    int k = 0;
+    for (int i = 0; i < 7; ++i) v[k++] = fets.fv[i];
+    for (int i = 7; i < 18; i += 2) v[k++] = fets.fv[i];
+    conf.conf_lb = lb_from_class(eval_tree(select_lb_asso_forward_tree, v));
+    if (conf.force.has_lb) conf.conf_lb = conf.force.lb;
+  }
+
+  void select_based_on_model(stat_t &, feature_t &fets, config_t &conf) {
+    if (fets.centric == EC) {
+      conf.conf_target = Active;
+      conf.conf_asfmt = fets.active_vertex_ratio > 0.8 ? Bitmap : Queue;
+      if (conf.force.has_asfmt) conf.conf_asfmt = conf.force.asf;
+      conf.conf_fuse_inspect = false;
+      return;
+    }
+    if (conf.conf_toall && conf.conf_fromall && !conf.conf_fixed) {
+      conf.conf_inherit = true;
+      return;
+    }
+    conf.conf_centric = fets.centric;
+    conf.conf_fromall = fets.fromall;
+    conf.conf_toall = fets.toall;
+    if (fets.pattern == Idem)
+      trigger_fusion(fets, conf);
+    else
+      conf.conf_fuse_inspect = conf.conf_fusion;
+    if (conf.conf_fuse_inspect) {
+      fusion(fets, conf);
+      return;
+    }
+    if (fets.pattern == Idem)
+      select_idem(fets, conf);
+    else if (fets.pattern == ASSO)
+      select_ASSO(fets, conf);
+    else
+      select_Mono(fets, conf);
+    set_target(conf);
+  }
+};
+
+// ===========================================================================
+// executor_t
+// ===========================================================================
+struct executor_t {
+  int *dg_tile = nullptr;  // STRICT tile owners
+  int64_t tile_cap = 0;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  inspector_t *insp = nullptr;  // source of the host-known frontier sizes
+
+  void destroy() {
+    cudaFree(dg_tile);
+    dg_tile = nullptr;
+    tile_cap = 0;
+    for (auto &e : ev)
+      if (e) {
+        cudaEventDestroy(e);
+        e = nullptr;
+      }
+  }
+
+  // bitmap -> queue (src/kernel_libs/filter.cuh:197-252)
+  void build_queue(active_set_t &as, Status target, bool sorted) {
+    const int64_t nwords = (as.size + 31) >> 5;
+    if (sorted) {
+      const int64_t nb = (nwords + FILTER_WORDS - 1) / FILTER_WORDS;
+      if (nb + 1 > as.workset.bsum_cap) return (void)set_error(GSW_ERR_OVERFLOW, "filter: %s", "block sums");
+      k_filter_count<<<(unsigned)nb, FILTER_WORDS, 0, stream()>>>(as, target, as.workset.dg_bsum);
+      k_scan_single_block<<<1, 1024, 0, stream()>>>(as.workset.dg_bsum, nb);
+      k_filter_write<<<(unsigned)nb, FILTER_WORDS, 0, stream()>>>(as, target, as.workset.dg_bsum, nb);
+    } else {
+      const int grid = clamp_grid((nwords + 255) / 256, resident_grid(k_filter_unsorted, 256));
+      k_filter_unsorted<<<grid, 256, 0, stream()>>>(as, target);
+    }
+    GSW_LAUNCHED();
+  }
+
+  template <typename G, typename F>
+  void filter(active_set_t &as, G &g, F &f, stat_t &stat, feature_t &fets, config_t &conf) {
+    const double s = stat.last_filter_time;
+    as.set_fmt(conf.conf_asfmt);
+    if (conf.conf_asfmt == Queue) {
+      bool tofilter = !conf.conf_fuse_inspect;
+      if (conf.conf_switch_to_fusion) {
+        tofilter = true;
+        conf.conf_switch_to_fusion = false;
+      }
+      if (conf.conf_first_round) tofilter = true;
+      if (tofilter) {
+        if (!(as.queue.mode == Cached && as.queue.traceback)) build_queue(as, conf.conf_target, conf.conf_sorted_queue);
+      } else if (!conf.conf_pruning) {
+        fill_u32(as.bitmap.visited.dg_bits, 0, as.bitmap.visited.n_words);
+      }
+      as.queue.swap();
+    }
+    // grid bookkeeping of the reference (executor.cuh:30-52): idle levels
+    // feed trigger_fusion, tiny STRICT levels fall back to CM
+    conf.thdnum = THDNUM_EXPAND;
+    if (conf.conf_fuse_inspect) {
+      conf.ctanum = 32;
+    } else {
+      const double workloads = conf.conf_dir == Push ? fets.push_workload : fets.pull_workload;
+      conf.ctanum = (int)MIN((double)CTANUM_EXPAND, workloads / conf.thdnum / 2 + 1);
+      conf.conf_idle = conf.ctanum < 4 ? conf.conf_idle + 1 : 0;
+      if (conf.ctanum < 5 && conf.conf_lb == STRICT && !conf.force.has_lb) conf.conf_lb = CM;
+    }
+    set_hints(as, fets, conf);
+    if (conf.conf_centric == VC && conf.conf_fuse_inspect && !conf.conf_first_round && conf.conf_compensation &&
+        as.fmt == Queue)
+      compensation(as, g, f);
+    const double e = now_ms();
+    stat.level = g.level;
+    stat.last_filter_time = e - s;
+    stat.avg_filter_time = (stat.avg_filter_time * g.level + stat.last_filter_time) / (g.level + 1);
+    fets.last_filter_time = stat.last_filter_time;
+    fets.avg_filter_time = stat.avg_filter_time;
+  }
+
+  void set_hints(active_set_t &as, const feature_t &fets, const config_t &conf) {
+    hints_t &h = hints();
+    if (as.fmt == Bitmap) {
+      h.frontier = as.size;
+    } else if (!conf.conf_fuse_inspect && insp) {
+      const Status t = conf.conf_target;
+      h.frontier = t == Active ? insp->raw_frontier : (t == Inactive ? insp->raw_inactive : insp->raw_frontier + insp->raw_inactive);
+      if (conf.conf_qmode == Cached && as.queue.traceback) h.frontier = as.size;
+    } else {
+      h.frontier = -1;  // fused: the device knows; use resident grids
+    }
+    if (!conf.conf_fuse_inspect && insp)
+      h.edges = conf.conf_dir == Push ? insp->raw_push + (conf.conf_target == All ? insp->raw_pull : 0)
+                                      : insp->raw_pull + (conf.conf_target == All ? insp->raw_push : 0);
+    else
+      h.edges = -1;
+    if (h.frontier < 0 || h.frontier > as.size) h.frontier = -1;
+  }
+
+  // deferred filter updates of fused levels (kernel_fusion.cuh:54-109)
+  template <typename E, typename F>
+  void compensation(active_set_t &as, device_graph_t<CSR, E> &g, F &f) {
+    using G = device_graph_t<CSR, E>;
+    const int grid = resident_grid(k_compensation<G, F>, 512);
+    k_compensation<G, F><<<grid, 512, 0, stream()>>>(as, g, f);
+    GSW_LAUNCHED();
+  }
+  template <typename E, typename F>
+  void compensation(active_set_t &, device_graph_t<COO, E> &, F &) {}
+
+  void ensure_tiles(int64_t slots_cap) {
+    const int64_t need = slots_cap / STRICT_TILE + 2;
+    if (need <= tile_cap) return;
+    cudaFree(dg_tile);
+    dg_tile = nullptr;
+    if (GSW_CUDA(cudaMalloc((void **)&dg_tile, sizeof(int) * need))) return;
+    tile_cap = need;
+  }
+
+  template <bool PULL, typename G>
+  void strict_prepare(active_set_t &as, G &g, Status want) {
+    const int64_t items = hints().frontier >= 0 ? hints().frontier : (as.fmt == Queue ? as.size + 1 : as.size);
+    const int64_t nb = items / STRICT_ITEMS + 1;
+    ensure_tiles(g.nedges + as.size + 1);
+    if (!ok()) return;
+    if (nb + 1 > as.workset.bsum_cap) return (void)set_error(GSW_ERR_OVERFLOW, "strict: %s", "block sums");
+    k_strict_count<PULL><<<(unsigned)nb, 256, 0, stream()>>>(as, g, want, as.workset.dg_bsum);
+    k_scan_single_block<<<1, 1024, 0, stream()>>>(as.workset.dg_bsum, nb);
+    k_strict_scan<PULL><<<(unsigned)nb, 256, 0, stream()>>>(as, g, want, as.workset.dg_bsum, nb, dg_tile, tile_cap);
+    GSW_LAUNCHED();
+  }
+
+  template <typename E, typename F>
+  void launch_vc(active_set_t &as, device_graph_t<CSR, E> &g, F &f, config_t &conf) {
+    using G = device_graph_t<CSR, E>;
+    const bool fused = conf.conf_fuse_inspect;
+    const int64_t fr = hints().frontier;
+    const int64_t ed = hints().edges;
+    const int B = EXPAND_THREADS;
+    const int fg = opts().force_grid;
+    auto grid_for = [&](auto kern, int64_t want) {
+      const int cap = resident_grid(kern, B);
+      if (fg > 0) return fg;
+      return want < 0 ? cap : clamp_grid(want, cap);
+    };
+#define GSW_GO(kern, want, ...)                                   \
+  do {                                                            \
+    auto _k = kern;                                               \
+    _k<<<grid_for(_k, want), B, 0, stream()>>>(__VA_ARGS__);      \
+  } while (0)
+    if (conf.conf_dir == Push) {
+      switch (conf.conf_lb) {
+        case TM:
+          if (fused) GSW_GO((k_push_tm<true, G, F>), fr < 0 ? -1 : fr / B + 1, as, g, f, conf);
+          else GSW_GO((k_push_tm<false, G, F>), fr < 0 ? -1 : fr / B + 1, as, g, f, conf);
+          break;
+        case CM:
+          if (fused) GSW_GO((k_push_cm<true, G, F>), fr < 0 ? -1 : fr / B + 1, as, g, f, conf);
+          else GSW_GO((k_push_cm<false, G, F>), fr < 0 ? -1 : fr / B + 1, as, g, f, conf);
+          break;
+        case TWC:
+          if (fused) GSW_GO((k_push_twc<true, G, F>), fr < 0 ? -1 : fr / B + 1, as, g, f, conf);
+          else GSW_GO((k_push_twc<false, G, F>), fr < 0 ? -1 : fr / B + 1, as, g, f, conf);
+          break;
+        case STRICT: {
+          strict_prepare<false>(as, g, conf.want());
+          if (!ok()) return;
+          const int64_t want = (ed < 0 || fr < 0) ? -1 : (ed + fr) / STRICT_TILE + 1;
+          if (fused) GSW_GO((k_push_strict<true, G, F>), want, as, g, f, conf, dg_tile);
+          else GSW_GO((k_push_strict<false, G, F>), want, as, g, f, conf, dg_tile);
+          break;
+        }
+        case WM:
+        default:
+          if (fused) GSW_GO((k_push_wm<true, G, F>), fr < 0 ? -1 : fr / B + 1, as, g, f, conf);
+          else GSW_GO((k_push_wm<false, G, F>), fr < 0 ? -1 : fr / B + 1, as, g, f, conf);
+          break;
+      }
+    } else {
+      switch (conf.conf_lb) {
+        case WM: GSW_GO((k_pull_wm<G, F>), fr < 0 ? -1 : fr / B + 1, as, g, f, conf); break;
+        case CM: GSW_GO((k_pull_cm<G, F>), fr < 0 ? -1 : fr / B + 1, as, g, f, conf); break;
+        case TWC: GSW_GO((k_pull_twc<G, F>), fr < 0 ? -1 : fr / B + 1, as, g, f, conf); break;
+        case STRICT: {
+          strict_prepare<true>(as, g, conf.want());
+          if (!ok()) return;
+          const int64_t want = (ed < 0 || fr < 0) ? -1 : (ed + fr) / STRICT_TILE + 1;
+          GSW_GO((k_pull_strict<G, F>), want, as, g, f, conf, dg_tile);
+          break;
+        }
+        case TM:
+        default: GSW_GO((k_pull_tm<G, F>), fr < 0 ? -1 : fr / B + 1, as, g, f, conf); break;
+      }
+    }
+#undef GSW_GO
+    GSW_LAUNCHED();
+  }
+
+  template <typename E, typename F>
+  void launch_ec(active_set_t &as, device_graph_t<COO, E> &g, F &f) {
+    const int grid = resident_grid(k_expand_ec<device_graph_t<COO, E>, F>, 512);
+    k_expand_ec<<<grid, 512, 0, stream()>>>(as, g, f);
+    GSW_LAUNCHED();
+  }
+
+  template <typename E, typename F>
+  void dispatch(active_set_t &as, device_graph_t<CSR, E> &g, F &f, config_t &conf) {
+    if (conf.conf_lb == TWOD && twod_hook) {
+      twod_hook(this, &as, (void *)&g, (void *)&f, &conf);
+      return;
+    }
+    launch_vc(as, g, f, conf);
+  }
+  template <typename E, typename F>
+  void dispatch(active_set_t &as, device_graph_t<COO, E> &g, F &f, config_t &) {
+    launch_ec(as, g, f);
+  }
+
+  template <typename G, typename F>
+  void expand(active_set_t &as, G &g, F &f, stat_t &stat, feature_t &fets, config_t &conf) {
+    const double s = now_ms();
+    // fused levels read the convergence flag right after the expand
+    const bool sync_needed = conf.conf_fuse_inspect || opts().verbose;
+    if (sync_needed && !ev[0])
+      for (auto &e : ev) cudaEventCreate(&e);
+    if (conf.conf_count_edges) GSW_CUDA(cudaMemsetAsync(&as.dg_cnt->scanned, 0, sizeof(unsigned long long), stream()));
+    if (sync_needed) cudaEventRecord(ev[0], stream());
+    marks().exp0 = opts().timing ? timing_pool().record() : -1;
+    dispatch(as, g, f, conf);
+    marks().exp1 = opts().timing ? timing_pool().record() : -1;
+    double e = s;
+    if (sync_needed) {
+      cudaEventRecord(ev[1], stream());
+      GSW_CUDA(cudaStreamSynchronize(stream()));
+      float ms = 0;
+      cudaEventElapsedTime(&ms, ev[0], ev[1]);
+      e = s + ms;
+    }
+    stat.last_scanned = 0;
+    if (conf.conf_count_edges) {
+      unsigned long long c = 0;
+      GSW_CUDA(cudaMemcpyAsync(&c, &as.dg_cnt->scanned, sizeof(c), cudaMemcpyDeviceToHost, stream()));
+      GSW_CUDA(cudaStreamSynchronize(stream()));
+      stat.last_scanned = (int64_t)c;
+    }
+    stat.last_time = stat.last_filter_time + e - s;
+    const int lv = g.level > 0 ? g.level : 1;
+    stat.avg_time = (stat.avg_time * (lv - 1) + stat.last_time) / lv;
+    stat.last_expand_time = e - s;
+    stat.avg_expand_time = (stat.avg_expand_time * (lv - 1) + stat.last_expand_time) / lv;
+    fets.last_expand_time = stat.last_expand_time;
+    // a fused level that is far slower than average goes back to the
+    // standalone form (executor.cuh:128-131)
+    if (fets.pattern == Idem && fets.avg_expand_time > 0 && fets.last_expand_time > 5 * fets.avg_expand_time &&
+        !conf.force.has_fusion) {
+      conf.conf_fuse_inspect = false;
+      as.queue.swap();
+    }
+    fets.avg_expand_time = stat.avg_expand_time;
+    fets.last_time = stat.last_time;
+    fets.avg_time = stat.avg_time;
+    if (opts().verbose) {
+      stat.show_hints();
+      conf.show_hints();
+      printf("\n");
+    }
+    conf.conf_first_round = false;
+  }
+
+  // optional 2D-partition expand, installed by code that owns the tiling
+  void (*twod_hook)(executor_t *, active_set_t *, void *, void *, config_t *) = nullptr;
+};
+
+// ===========================================================================
+// convergence (active_set.cuh:37-43, notification.cuh:233-254)
+// ===========================================================================
+template <typename E, typename F>
+bool window_exit(active_set_t &as, device_graph_t<CSR, E> &g, F &f, config_t &conf) {
+  if (!conf.conf_window) return true;
+  GSW_CUDA(cudaMemsetAsync(&as.dg_cnt->cnt, 0, sizeof(int), stream()));
+  k_exit<<<resident_grid(k_exit<device_graph_t<CSR, E>, F>, 512), 512, 0, stream()>>>(g, f, &as.dg_cnt->cnt);
+  int c = 0;
+  GSW_CUDA(cudaMemcpyAsync(&c, &as.dg_cnt->cnt, sizeof(int), cudaMemcpyDeviceToHost, stream()));
+  GSW_CUDA(cudaStreamSynchronize(stream()));
+  if (c) {
+    as.nt.reset();
+    f.data.window.reset();
+    if (conf.conf_fusion) {
+      conf.conf_fuse_inspect = false;
+      conf.conf_switch_to_fusion = true;
+    }
+    return false;
+  }
+  return true;
+}
+template <typename E, typename F>
+bool window_exit(active_set_t &, device_graph_t<COO, E> &, F &, config_t &) {
+  return true;
+}
+
+template <typename E, typename F>
+void window_delay_update(active_set_t &as, device_graph_t<CSR, E> &g, F &f) {
+  k_filter_all<<<resident_grid(k_filter_all<device_graph_t<CSR, E>, F>, 512), 512, 0, stream()>>>(g, f, as.size);
+  GSW_LAUNCHED();
+}
+template <typename E, typename F>
+void window_delay_update(active_set_t &, device_graph_t<COO, E> &, F &) {}
+
+template <typename G, typename F>
+bool finish(active_set_t &as, G &g, F &f, config_t &conf) {
+  if (!ok()) return true;  // an error ends the loop; the caller reports it
+  const bool converged = as.is_converged();
+  if (conf.conf_window && conf.conf_fusion && converged) window_delay_update(as, g, f);
+  return converged && window_exit(as, g, f, conf);
+}
+
+// ===========================================================================
+// init_conf / reset_conf (src/gswitch.h:19-108)
+// ===========================================================================
+template <typename E>
+int64_t root_degree(const device_graph_t<CSR, E> &g, int root) {
+  int d = 0;
+  GSW_CUDA(cudaMemcpyAsync(&d, g.dg_odegree + root, sizeof(int), cudaMemcpyDeviceToHost, stream()));
+  GSW_CUDA(cudaStreamSynchronize(stream()));
+  return d;
+}
+template <typename E>
+int64_t root_degree(const device_graph_t<COO, E> &, int) {
+  return 0;
+}
+
+template <typename G, typename F>
+void init_conf_impl(stat_t &stats, feature_t &fets, config_t &conf, G &dg, F &f, double mean_weight,
+                    double avg_deg_attr, bool reset_only) {
+  if (reset_only)
+    conf.reset();
+  else
+    stats.build();
+  fets.architecture_features();
+  conf.conf_inherit = false;
+  if (fets.use_root >= 0) fets.first_workload = (double)root_degree(dg, fets.use_root);
+  if (fets.centric == VC) {
+    fets.flatten();
+    double v[5];
+    for (int i = 2; i < 7; ++i) v[i - 2] = fets.fv[i];
+    conf.conf_fuse_inspect = eval_tree(select_fusion_tree, v) != 0;
+    if (conf.force.has_fusion) conf.conf_fuse_inspect = conf.force.fusion == Fused;
+    // from-all/to-all patterns update vertex state only in the inspector's
+    // filter pass, so a fused level (which skips it) cannot advance them:
+    // they stay standalone even when fusion is forced
+    if (fets.toall && fets.fromall) conf.conf_fuse_inspect = false;
+    if (conf.conf_fuse_inspect) conf.conf_fusion = true;
+    if (!conf.conf_fuse_inspect) conf.conf_qmode = Normal;
+  }
+  if (conf.conf_window) {
+    f.data.window.enable = true;
+    f.data.window.set_init_winsize(DIV(8 * mean_weight * 32, avg_deg_attr));
+  }
+}
+
+// CC root compression after each hooking level (intrinsics.cuh:351-362)
+template <typename F>
+void p_jump(F &f, int64_t nvertexs, active_set_t &as) {
+  const int grid = resident_grid(k_pointer_jump, 512);
+  k_pointer_jump<<<grid, 512, 0, stream()>>>((int *)f.data.dg_wa, nvertexs, &as.dg_cnt->err);
+  GSW_LAUNCHED();
+}
+
+}  // namespace gsw

@@ -1,0 +1,887 @@
+// Expand kernels: every load-balance variant, push and pull, standalone and
+// fused (the expand enqueues the next frontier itself).
+//
+// Per-edge semantics are the reference's (src/kernel_libs/expand_VC_TM.cuh,
+// expand_VC_WM.cuh, expand_VC_CM.cuh, expand_VC_STRICT.cuh):
+//   push/standalone  prune (mark visited) -> target must be Inactive unless
+//                    to-all -> compAtomic(wa[u], emit(v))
+//   push/fused       emit(v) -> cond(u) unless to-all -> compAtomic ->
+//                    exactly-once enqueue through the visited bitmap
+//   pull             for a candidate v, combine emit(u) of active (or all,
+//                    when from-all) in-neighbours u with comp, stop at the
+//                    first hit when the pattern allows pruning.
+// The work decompositions are this engine's:
+//   TM      one thread per frontier vertex;
+//   WM      one warp per 32 frontier vertices, degrees scanned with warp
+//           shuffles, 32 edges per round, owner found by a 5-step search;
+//   CM      one CTA per 256 frontier vertices, block scan, 256 edges/round;
+//   STRICT  exact edge balance: a (degree+1) scan over the frontier whose
+//           epilogue also records, for every tile of STRICT_TILE slots, the
+//           frontier index owning the tile's first slot (this replaces the
+//           reference's moderngpu scan + sorted search); every CTA stages a
+//           tile's owners in shared memory;
+//   TWC     thread/warp/CTA tiers by degree inside one kernel: CTA-wide
+//           sweeps for degree >= 256, warp sweeps for degree >= 32, and a
+//           CTA-scan mapping for the rest (the intent recorded in
+//           src/kernel_libs/expand_VC_TWC.cuh:11-63).
+// Loops that enqueue run with warp-uniform trip counts so the enqueue can be
+// aggregated with a full-warp ballot (one atomic per warp).
+#pragma once
+#include "k_inspect_filter.cuh"
+
+namespace gsw {
+
+constexpr int EXPAND_THREADS = 256;
+constexpr int STRICT_TILE = 1024;   // slots per STRICT tile (4 per thread)
+constexpr int STRICT_ITEMS = 1024;  // frontier entries per STRICT scan block
+
+// ---- per-edge operations ---------------------------------------------------
+template <typename G, typename F>
+__device__ __forceinline__ void push_edge_std(active_set_t &as, const G &g, F &f, const config_t &conf, int v,
+                                              int u, int64_t ei) {
+  bool tp = true;
+  if (conf.conf_pruning) tp = as.bitmap.mark_duplicate_lite(u);
+  if (tp && !conf.conf_toall) tp = as.bitmap.is_inactive(u);
+  if (tp) {
+    auto vd = f.emit(v, g.fetch_edata(ei), g);
+    f.compAtomic(f.wa_of(u), vd, g);
+  }
+}
+
+template <typename G, typename F>
+__device__ __forceinline__ bool push_edge_fused(active_set_t &as, const G &g, F &f, const config_t &conf, int v,
+                                                int u, int64_t ei) {
+  auto vd = f.emit(v, g.fetch_edata(ei), g);
+  bool tp = true;
+  if (!conf.conf_toall) tp = f.cond(u, vd, g);
+  if (tp) tp = f.compAtomic(f.wa_of(u), vd, g);
+  if (tp) tp = as.bitmap.mark_duplicate_atomic(u);
+  return tp;
+}
+
+// full-warp aggregated enqueue; every lane of the warp must call it
+__device__ __forceinline__ void warp_enqueue(active_set_t &as, bool tp, int u) {
+  const unsigned m = __ballot_sync(FULL, tp);
+  if (!m) return;
+  const int leader = __ffs(m) - 1;
+  int64_t base = 0;
+  if (lane_id() == leader) base = as.queue.reserve(__popc(m));
+  base = __shfl_sync(FULL, base, leader);
+  if (tp && base >= 0) as.queue.output_base()[base + __popc(m & ((1u << lane_id()) - 1u))] = u;
+}
+
+template <typename G>
+__device__ __forceinline__ void vertex_range(const G &g, bool pull, int v, int64_t &st, int &deg) {
+  if (v < 0) {
+    st = 0;
+    deg = 0;
+    return;
+  }
+  const int64_t *off = pull ? g.dgr_row_off : g.dg_row_off;
+  st = __ldg(off + v);
+  deg = (int)(__ldg(off + v + 1) - st);
+}
+
+// accounting pass only: one atomic per thread at kernel exit
+__device__ __forceinline__ void account(const active_set_t &as, const config_t &conf, unsigned long long c) {
+  if (conf.conf_count_edges && c) atomicAdd(&as.dg_cnt->scanned, c);
+}
+
+#define GSW_HALT_IF_EMPTY(n)                                     \
+  if ((n) == 0) {                                                \
+    if (blockIdx.x == 0 && threadIdx.x == 0) as.halt_device();   \
+    return;                                                      \
+  }
+
+// ===========================================================================
+// TM
+// ===========================================================================
+template <bool FUSED, typename G, typename F>
+__global__ void __launch_bounds__(EXPAND_THREADS) k_push_tm(active_set_t as, G g, F f, config_t conf) {
+  const int64_t n = as.get_size();
+  GSW_HALT_IF_EMPTY(n);
+  const Status want = conf.want();
+  const int64_t STRIDE = (int64_t)blockDim.x * gridDim.x;
+  unsigned long long cnt = 0;
+  for (int64_t idx = threadIdx.x + (int64_t)blockIdx.x * blockDim.x; idx < n; idx += STRIDE) {
+    const int v = as.fetch(idx, want);
+    if (v < 0) continue;
+    int64_t st;
+    int deg;
+    vertex_range(g, false, v, st, deg);
+    cnt += deg;
+    for (int k = 0; k < deg; ++k) {
+      const int u = __ldg(g.dg_adj_list + st + k);
+      if (FUSED) {
+        if (push_edge_fused(as, g, f, conf, v, u, st + k)) as.queue.push(u);
+      } else {
+        push_edge_std(as, g, f, conf, v, u, st + k);
+      }
+    }
+  }
+  account(as, conf, cnt);
+}
+
+template <typename G, typename F>
+__global__ void __launch_bounds__(EXPAND_THREADS) k_pull_tm(active_set_t as, G g, F f, config_t conf) {
+  using WA = typename F::wa_t;
+  const int64_t n = as.get_size();
+  GSW_HALT_IF_EMPTY(n);
+  const Status want = conf.want();
+  const int64_t STRIDE = (int64_t)blockDim.x * gridDim.x;
+  unsigned long long cnt = 0;
+  for (int64_t idx = threadIdx.x + (int64_t)blockIdx.x * blockDim.x; idx < n; idx += STRIDE) {
+    const int v = as.fetch(idx, want);
+    if (v < 0) continue;
+    int64_t st;
+    int deg;
+    vertex_range(g, true, v, st, deg);
+    WA acc;
+    bool have = false;
+    int k = 0;
+    for (; k < deg; ++k) {
+      const int u = __ldg(g.dgr_adj_list + st + k);
+      if (conf.conf_fromall || as.bitmap.is_active(u)) {
+        WA x = f.emit(u, g.fetch_edata_r(st + k), g);
+        if (have)
+          f.comp(&acc, x, g);
+        else {
+          acc = x;
+          have = true;
+        }
+        if (conf.conf_pruning) {
+          ++k;
+          break;
+        }
+      }
+    }
+    cnt += k;
+    if (have) f.comp(f.wa_of(v), acc, g);
+  }
+  account(as, conf, cnt);
+}
+
+// ===========================================================================
+// WM: warp per 32 frontier vertices
+// ===========================================================================
+template <bool FUSED, typename G, typename F>
+__global__ void __launch_bounds__(EXPAND_THREADS) k_push_wm(active_set_t as, G g, F f, config_t conf) {
+  constexpr int W = EXPAND_THREADS / 32;
+  __shared__ int s_scan[W][32];
+  __shared__ int s_v[W][32];
+  __shared__ int64_t s_st[W][32];
+  const int64_t n = as.get_size();
+  GSW_HALT_IF_EMPTY(n);
+  const Status want = conf.want();
+  const int lane = lane_id(), w = warp_id();
+  const int64_t nwarps = (int64_t)gridDim.x * W;
+  for (int64_t tile = (int64_t)blockIdx.x * W + w; tile * 32 < n; tile += nwarps) {
+    const int64_t idx = tile * 32 + lane;
+    const int v = idx < n ? as.fetch(idx, want) : -1;
+    int64_t st;
+    int deg;
+    vertex_range(g, false, v, st, deg);
+    const int incl = warp_inclusive_sum(deg);
+    const int total = __shfl_sync(FULL, incl, 31);
+    if (lane == 0) account(as, conf, (unsigned long long)total);
+    s_scan[w][lane] = incl - deg;
+    s_v[w][lane] = v;
+    s_st[w][lane] = st;
+    __syncwarp();
+    for (int base = 0; base < total; base += 32) {
+      const int i = base + lane;
+      bool tp = false;
+      int u = -1;
+      if (i < total) {
+        const int id = upper_bound(s_scan[w], 32, i) - 1;
+        const int64_t ei = s_st[w][id] + (i - s_scan[w][id]);
+        u = __ldg(g.dg_adj_list + ei);
+        if (FUSED)
+          tp = push_edge_fused(as, g, f, conf, s_v[w][id], u, ei);
+        else
+          push_edge_std(as, g, f, conf, s_v[w][id], u, ei);
+      }
+      if (FUSED) warp_enqueue(as, tp, u);
+    }
+    __syncwarp();
+  }
+}
+
+template <typename G, typename F>
+__global__ void __launch_bounds__(EXPAND_THREADS) k_pull_wm(active_set_t as, G g, F f, config_t conf) {
+  using WA = typename F::wa_t;
+  constexpr int W = EXPAND_THREADS / 32;
+  __shared__ int s_scan[W][33];
+  __shared__ int s_v[W][32];
+  __shared__ int64_t s_st[W][32];
+  const int64_t n = as.get_size();
+  GSW_HALT_IF_EMPTY(n);
+  const Status want = conf.want();
+  const int lane = lane_id(), w = warp_id();
+  const int64_t nwarps = (int64_t)gridDim.x * W;
+  for (int64_t tile = (int64_t)blockIdx.x * W + w; tile * 32 < n; tile += nwarps) {
+    const int64_t idx = tile * 32 + lane;
+    const int v = idx < n ? as.fetch(idx, want) : -1;
+    int64_t st;
+    int deg;
+    vertex_range(g, true, v, st, deg);
+    const int incl = warp_inclusive_sum(deg);
+    const int total = __shfl_sync(FULL, incl, 31);
+    if (lane == 0) account(as, conf, (unsigned long long)total);
+    s_scan[w][lane] = incl - deg;
+    if (lane == 31) s_scan[w][32] = total;
+    s_v[w][lane] = v;
+    s_st[w][lane] = st;
+    __syncwarp();
+    for (int base = 0; base < total; base += 32) {
+      const int i = base + lane;
+      int id = 31;
+      bool vote = false;
+      WA val;
+      memset(&val, 0, sizeof(WA));
+      if (i < total) {
+        id = upper_bound(s_scan[w], 32, i) - 1;
+        const int64_t ei = s_st[w][id] + (i - s_scan[w][id]);
+        const int u = __ldg(g.dgr_adj_list + ei);
+        if (conf.conf_fromall || as.bitmap.is_active(u)) {
+          vote = true;
+          val = f.emit(u, g.fetch_edata_r(ei), g);
+        }
+      } else {
+        id = 32 + lane;  // past-the-end lanes form their own segments
+      }
+      // segmented reduction toward the first lane of each owner's run
+#pragma unroll
+      for (int d = 1; d < 32; d <<= 1) {
+        const int oid = __shfl_down_sync(FULL, id, d);
+        const bool ovote = __shfl_down_sync(FULL, vote, d);
+        const WA oval = shfl_down_any(val, d);
+        if (lane + d < 32 && oid == id && ovote) {
+          if (vote)
+            f.comp(&val, oval, g);
+          else
+            val = oval;
+          vote = true;
+        }
+      }
+      const int pid = __shfl_up_sync(FULL, id, 1);
+      const bool head = (lane == 0) || (pid != id);
+      if (i < total && head && vote) f.comp(f.wa_of(s_v[w][id]), val, g);
+    }
+    __syncwarp();
+  }
+}
+
+// ===========================================================================
+// CM: CTA per 256 frontier vertices
+// ===========================================================================
+template <bool FUSED, typename G, typename F>
+__global__ void __launch_bounds__(EXPAND_THREADS) k_push_cm(active_set_t as, G g, F f, config_t conf) {
+  constexpr int B = EXPAND_THREADS;
+  __shared__ int s_scan[B];
+  __shared__ int s_v[B];
+  __shared__ int64_t s_st[B];
+  __shared__ int s_tmp[33];
+  const int64_t n = as.get_size();
+  GSW_HALT_IF_EMPTY(n);
+  const Status want = conf.want();
+  for (int64_t tile = blockIdx.x; tile * B < n; tile += gridDim.x) {
+    const int64_t idx = tile * B + threadIdx.x;
+    const int v = idx < n ? as.fetch(idx, want) : -1;
+    int64_t st;
+    int deg;
+    vertex_range(g, false, v, st, deg);
+    int total;
+    const int ex = block_exclusive_scan(deg, s_tmp, &total);
+    if (threadIdx.x == 0) account(as, conf, (unsigned long long)total);
+    s_scan[threadIdx.x] = ex;
+    s_v[threadIdx.x] = v;
+    s_st[threadIdx.x] = st;
+    __syncthreads();
+    for (int base = 0; base < total; base += B) {
+      const int i = base + threadIdx.x;
+      bool tp = false;
+      int u = -1;
+      if (i < total) {
+        const int id = upper_bound(s_scan, B, i) - 1;
+        const int64_t ei = s_st[id] + (i - s_scan[id]);
+        u = __ldg(g.dg_adj_list + ei);
+        if (FUSED)
+          tp = push_edge_fused(as, g, f, conf, s_v[id], u, ei);
+        else
+          push_edge_std(as, g, f, conf, s_v[id], u, ei);
+      }
+      if (FUSED) warp_enqueue(as, tp, u);
+    }
+    __syncthreads();
+  }
+}
+
+template <typename G, typename F>
+__global__ void __launch_bounds__(EXPAND_THREADS) k_pull_cm(active_set_t as, G g, F f, config_t conf) {
+  constexpr int B = EXPAND_THREADS;
+  __shared__ int s_scan[B];
+  __shared__ int s_v[B];
+  __shared__ int64_t s_st[B];
+  __shared__ int s_tmp[33];
+  const int64_t n = as.get_size();
+  GSW_HALT_IF_EMPTY(n);
+  const Status want = conf.want();
+  for (int64_t tile = blockIdx.x; tile * B < n; tile += gridDim.x) {
+    const int64_t idx = tile * B + threadIdx.x;
+    const int v = idx < n ? as.fetch(idx, want) : -1;
+    int64_t st;
+    int deg;
+    vertex_range(g, true, v, st, deg);
+    int total;
+    const int ex = block_exclusive_scan(deg, s_tmp, &total);
+    if (threadIdx.x == 0) account(as, conf, (unsigned long long)total);
+    s_scan[threadIdx.x] = ex;
+    s_v[threadIdx.x] = v;
+    s_st[threadIdx.x] = st;
+    __syncthreads();
+    for (int base = 0; base < total; base += B) {
+      const int i = base + threadIdx.x;
+      if (i < total) {
+        const int id = upper_bound(s_scan, B, i) - 1;
+        const int64_t ei = s_st[id] + (i - s_scan[id]);
+        const int u = __ldg(g.dgr_adj_list + ei);
+        if (conf.conf_fromall || as.bitmap.is_active(u)) {
+          auto vd = f.emit(u, g.fetch_edata_r(ei), g);
+          f.compAtomic(f.wa_of(s_v[id]), vd, g);
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// ===========================================================================
+// STRICT: exact edge balance
+// ===========================================================================
+template <bool PULL, typename G>
+__device__ __forceinline__ int64_t strict_slots(const active_set_t &as, const G &g, int64_t idx, Status want) {
+  const int v = as.fetch(idx, want);
+  if (v < 0) return 1;
+  const int64_t *off = PULL ? g.dgr_row_off : g.dg_row_off;
+  return __ldg(off + v + 1) - __ldg(off + v) + 1;
+}
+
+template <bool PULL, typename G>
+__global__ void __launch_bounds__(256) k_strict_count(active_set_t as, G g, Status want, int64_t *bsum) {
+  __shared__ int64_t s_red[32];
+  const int64_t n = as.get_size();
+  const int64_t b0 = (int64_t)blockIdx.x * STRICT_ITEMS;
+  int64_t s = 0;
+  for (int k = threadIdx.x; k < STRICT_ITEMS; k += blockDim.x) {
+    const int64_t idx = b0 + k;
+    if (idx < n) s += strict_slots<PULL>(as, g, idx, want);
+  }
+  s = block_reduce(s, s_red);
+  if (threadIdx.x == 0) bsum[blockIdx.x] = s;
+}
+
+// eoff[idx] = exclusive scan of (degree+1); tile_lo[t] = frontier index that
+// owns slot t*STRICT_TILE.  Each thread scans 4 consecutive entries.
+template <bool PULL, typename G>
+__global__ void __launch_bounds__(256) k_strict_scan(active_set_t as, G g, Status want, const int64_t *bsum,
+                                                     int64_t nblocks, int *tile_lo, int64_t tile_cap) {
+  __shared__ int64_t s[33];
+  const int64_t n = as.get_size();
+  const int64_t base = (int64_t)blockIdx.x * STRICT_ITEMS + threadIdx.x * 4;
+  int64_t d[4], loc = 0;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    d[k] = (base + k < n) ? strict_slots<PULL>(as, g, base + k, want) : 0;
+    loc += d[k];
+  }
+  int64_t incl = warp_inclusive_sum(loc);
+  __syncthreads();
+  if (lane_id() == 31) s[warp_id()] = incl;
+  __syncthreads();
+  if (warp_id() == 0) {
+    int64_t y = lane_id() < (int)(blockDim.x >> 5) ? s[lane_id()] : 0;
+    int64_t yi = warp_inclusive_sum(y);
+    if (lane_id() < (int)(blockDim.x >> 5)) s[lane_id()] = yi - y;
+  }
+  __syncthreads();
+  int64_t off = bsum[blockIdx.x] + s[warp_id()] + incl - loc;
+  int64_t *eoff = as.workset.dg_eoff;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const int64_t idx = base + k;
+    if (idx < n) {
+      eoff[idx] = off;
+      for (int64_t t = (off + STRICT_TILE - 1) / STRICT_TILE; t * STRICT_TILE < off + d[k]; ++t) {
+        if (t < tile_cap)
+          tile_lo[t] = (int)idx;
+        else
+          as.raise(DEV_ERR_SCRATCH_OVERFLOW);
+      }
+    }
+    off += d[k];
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    eoff[n] = bsum[nblocks];
+    as.dg_cnt->total_edges = (unsigned long long)bsum[nblocks];
+  }
+}
+
+template <bool FUSED, typename G, typename F>
+__global__ void __launch_bounds__(EXPAND_THREADS) k_push_strict(active_set_t as, G g, F f, config_t conf,
+                                                                const int *tile_lo) {
+  constexpr int T = STRICT_TILE;
+  __shared__ int s_v[T + 2];
+  __shared__ int64_t s_sc[T + 2];
+  __shared__ int64_t s_st[T + 2];
+  const int64_t n = as.get_size();
+  GSW_HALT_IF_EMPTY(n);
+  const Status want = conf.want();
+  const int64_t *eoff = as.workset.dg_eoff;
+  const int64_t total = eoff[n];
+  const int64_t ntiles = (total + T - 1) / T;
+  if (blockIdx.x == 0 && threadIdx.x == 0) account(as, conf, (unsigned long long)(total - n));
+  for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const int64_t lo = tile_lo[t];
+    const int64_t hi = (t + 1 < ntiles) ? tile_lo[t + 1] : n - 1;
+    const int cnt = (int)(hi - lo + 1);
+    for (int j = threadIdx.x; j < cnt; j += blockDim.x) {
+      const int v = as.fetch(lo + j, want);
+      s_v[j] = v;
+      s_sc[j] = eoff[lo + j];
+      s_st[j] = v >= 0 ? __ldg(g.dg_row_off + v) : 0;
+    }
+    if (threadIdx.x == 0) s_sc[cnt] = eoff[hi + 1];
+    __syncthreads();
+    const int64_t t0 = t * T;
+    const int64_t t1 = MIN(total, t0 + T);
+#pragma unroll
+    for (int k = 0; k < T / EXPAND_THREADS; ++k) {
+      const int64_t s = t0 + k * EXPAND_THREADS + threadIdx.x;
+      bool tp = false;
+      int u = -1;
+      if (s < t1) {
+        const int j = upper_bound(s_sc, cnt, s) - 1;
+        const int64_t local = s - s_sc[j];
+        if (local < s_sc[j + 1] - s_sc[j] - 1) {
+          const int64_t ei = s_st[j] + local;
+          u = __ldg(g.dg_adj_list + ei);
+          if (FUSED)
+            tp = push_edge_fused(as, g, f, conf, s_v[j], u, ei);
+          else
+            push_edge_std(as, g, f, conf, s_v[j], u, ei);
+        }
+      }
+      if (FUSED) warp_enqueue(as, tp, u);
+    }
+    __syncthreads();
+  }
+}
+
+// Pull: each thread walks 4 consecutive slots and folds runs of the same
+// candidate before one compAtomic (the "stride mode" of expand_VC_STRICT.cuh:
+// 453-510).
+template <typename G, typename F>
+__global__ void __launch_bounds__(EXPAND_THREADS) k_pull_strict(active_set_t as, G g, F f, config_t conf,
+                                                                const int *tile_lo) {
+  using WA = typename F::wa_t;
+  constexpr int T = STRICT_TILE;
+  constexpr int PER = T / EXPAND_THREADS;
+  __shared__ int s_v[T + 2];
+  __shared__ int64_t s_sc[T + 2];
+  __shared__ int64_t s_st[T + 2];
+  const int64_t n = as.get_size();
+  GSW_HALT_IF_EMPTY(n);
+  const Status want = conf.want();
+  const int64_t *eoff = as.workset.dg_eoff;
+  const int64_t total = eoff[n];
+  const int64_t ntiles = (total + T - 1) / T;
+  if (blockIdx.x == 0 && threadIdx.x == 0) account(as, conf, (unsigned long long)(total - n));
+  for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const int64_t lo = tile_lo[t];
+    const int64_t hi = (t + 1 < ntiles) ? tile_lo[t + 1] : n - 1;
+    const int cnt = (int)(hi - lo + 1);
+    for (int j = threadIdx.x; j < cnt; j += blockDim.x) {
+      const int v = as.fetch(lo + j, want);
+      s_v[j] = v;
+      s_sc[j] = eoff[lo + j];
+      s_st[j] = v >= 0 ? __ldg(g.dgr_row_off + v) : 0;
+    }
+    if (threadIdx.x == 0) s_sc[cnt] = eoff[hi + 1];
+    __syncthreads();
+    const int64_t t0 = t * T + threadIdx.x * PER;
+    const int64_t t1 = MIN(total, t * T + T);
+    int cur = -1;
+    WA acc;
+    bool have = false;
+    for (int k = 0; k < PER; ++k) {
+      const int64_t s = t0 + k;
+      if (s >= t1) break;
+      const int j = upper_bound(s_sc, cnt, s) - 1;
+      const int64_t local = s - s_sc[j];
+      if (local >= s_sc[j + 1] - s_sc[j] - 1) continue;
+      if (j != cur) {
+        if (have) f.compAtomic(f.wa_of(s_v[cur]), acc, g);
+        have = false;
+        cur = j;
+      }
+      const int64_t ei = s_st[j] + local;
+      const int u = __ldg(g.dgr_adj_list + ei);
+      if (conf.conf_fromall || as.bitmap.is_active(u)) {
+        WA x = f.emit(u, g.fetch_edata_r(ei), g);
+        if (have)
+          f.comp(&acc, x, g);
+        else {
+          acc = x;
+          have = true;
+        }
+      }
+    }
+    if (have) f.compAtomic(f.wa_of(s_v[cur]), acc, g);
+    __syncthreads();
+  }
+}
+
+// ===========================================================================
+// TWC: thread / warp / CTA tiers by degree
+// ===========================================================================
+template <bool FUSED, typename G, typename F>
+__global__ void __launch_bounds__(EXPAND_THREADS) k_push_twc(active_set_t as, G g, F f, config_t conf) {
+  constexpr int B = EXPAND_THREADS;
+  __shared__ int s_owner;
+  __shared__ int s_cv;
+  __shared__ int s_cdeg;
+  __shared__ int64_t s_cst;
+  __shared__ int s_scan[B];
+  __shared__ int s_v[B];
+  __shared__ int64_t s_st[B];
+  __shared__ int s_tmp[33];
+  const int64_t n = as.get_size();
+  GSW_HALT_IF_EMPTY(n);
+  const Status want = conf.want();
+  const int lane = lane_id();
+  if (threadIdx.x == 0) s_owner = -1;
+  __syncthreads();
+  for (int64_t tile = blockIdx.x; tile * B < n; tile += gridDim.x) {
+    const int64_t idx = tile * B + threadIdx.x;
+    const int v = idx < n ? as.fetch(idx, want) : -1;
+    int64_t st;
+    int deg;
+    vertex_range(g, false, v, st, deg);
+    // CTA tier
+    for (;;) {
+      if (deg >= B) s_owner = threadIdx.x;
+      __syncthreads();
+      const int owner = s_owner;
+      __syncthreads();  // every thread has read the owner before it is cleared
+      if (owner < 0) break;
+      if ((int)threadIdx.x == owner) {
+        s_cv = v;
+        s_cst = st;
+        s_cdeg = deg;
+        deg = 0;
+        s_owner = -1;
+      }
+      __syncthreads();
+      const int cv = s_cv, cdeg = s_cdeg;
+      const int64_t cst = s_cst;
+      if (threadIdx.x == 0) account(as, conf, (unsigned long long)cdeg);
+      for (int base = 0; base < cdeg; base += B) {
+        const int k = base + threadIdx.x;
+        bool tp = false;
+        int u = -1;
+        if (k < cdeg) {
+          u = __ldg(g.dg_adj_list + cst + k);
+          if (FUSED)
+            tp = push_edge_fused(as, g, f, conf, cv, u, cst + k);
+          else
+            push_edge_std(as, g, f, conf, cv, u, cst + k);
+        }
+        if (FUSED) warp_enqueue(as, tp, u);
+      }
+      __syncthreads();
+    }
+    // warp tier
+    for (;;) {
+      const unsigned m = __ballot_sync(FULL, deg >= 32);
+      if (!m) break;
+      const int leader = __ffs(m) - 1;
+      const int wv = __shfl_sync(FULL, v, leader);
+      const int wdeg = __shfl_sync(FULL, deg, leader);
+      const int64_t wst = __shfl_sync(FULL, st, leader);
+      if (lane == leader) {
+        deg = 0;
+        account(as, conf, (unsigned long long)wdeg);
+      }
+      for (int base = 0; base < wdeg; base += 32) {
+        const int k = base + lane;
+        bool tp = false;
+        int u = -1;
+        if (k < wdeg) {
+          u = __ldg(g.dg_adj_list + wst + k);
+          if (FUSED)
+            tp = push_edge_fused(as, g, f, conf, wv, u, wst + k);
+          else
+            push_edge_std(as, g, f, conf, wv, u, wst + k);
+        }
+        if (FUSED) warp_enqueue(as, tp, u);
+      }
+    }
+    // thread tier: remaining small lists mapped through a CTA scan
+    int total;
+    const int ex = block_exclusive_scan(deg, s_tmp, &total);
+    if (threadIdx.x == 0) account(as, conf, (unsigned long long)total);
+    s_scan[threadIdx.x] = ex;
+    s_v[threadIdx.x] = v;
+    s_st[threadIdx.x] = st;
+    __syncthreads();
+    for (int base = 0; base < total; base += B) {
+      const int i = base + threadIdx.x;
+      bool tp = false;
+      int u = -1;
+      if (i < total) {
+        const int id = upper_bound(s_scan, B, i) - 1;
+        const int64_t ei = s_st[id] + (i - s_scan[id]);
+        u = __ldg(g.dg_adj_list + ei);
+        if (FUSED)
+          tp = push_edge_fused(as, g, f, conf, s_v[id], u, ei);
+        else
+          push_edge_std(as, g, f, conf, s_v[id], u, ei);
+      }
+      if (FUSED) warp_enqueue(as, tp, u);
+    }
+    __syncthreads();
+  }
+}
+
+// TWC pull: candidates with large in-degree are swept by the whole CTA or a
+// warp with a cooperative reduction (and a ballot-driven early exit when the
+// pattern allows pruning); the rest by one thread each.
+template <typename G, typename F>
+__global__ void __launch_bounds__(EXPAND_THREADS) k_pull_twc(active_set_t as, G g, F f, config_t conf) {
+  using WA = typename F::wa_t;
+  constexpr int B = EXPAND_THREADS;
+  constexpr int NW = B / 32;
+  __shared__ int s_owner;
+  __shared__ int s_cv;
+  __shared__ int s_cdeg;
+  __shared__ int64_t s_cst;
+  __shared__ int s_stop;
+  __shared__ WA s_part[NW];
+  __shared__ int s_have[NW];
+  const int64_t n = as.get_size();
+  GSW_HALT_IF_EMPTY(n);
+  const Status want = conf.want();
+  const int lane = lane_id(), w = warp_id();
+  if (threadIdx.x == 0) s_owner = -1;
+  __syncthreads();
+  for (int64_t tile = blockIdx.x; tile * B < n; tile += gridDim.x) {
+    const int64_t idx = tile * B + threadIdx.x;
+    const int v = idx < n ? as.fetch(idx, want) : -1;
+    int64_t st;
+    int deg;
+    vertex_range(g, true, v, st, deg);
+    // CTA tier
+    for (;;) {
+      if (deg >= B) s_owner = threadIdx.x;
+      __syncthreads();
+      const int owner = s_owner;
+      __syncthreads();  // every thread has read the owner before it is cleared
+      if (owner < 0) break;
+      if ((int)threadIdx.x == owner) {
+        s_cv = v;
+        s_cst = st;
+        s_cdeg = deg;
+        deg = 0;
+        s_owner = -1;
+        s_stop = 0;
+      }
+      __syncthreads();
+      const int cv = s_cv, cdeg = s_cdeg;
+      const int64_t cst = s_cst;
+      if (threadIdx.x == 0) account(as, conf, (unsigned long long)cdeg);
+      WA acc;
+      bool have = false;
+      for (int base = 0; base < cdeg; base += B) {
+        const int k = base + threadIdx.x;
+        if (k < cdeg) {
+          const int u = __ldg(g.dgr_adj_list + cst + k);
+          if (conf.conf_fromall || as.bitmap.is_active(u)) {
+            WA x = f.emit(u, g.fetch_edata_r(cst + k), g);
+            if (have)
+              f.comp(&acc, x, g);
+            else {
+              acc = x;
+              have = true;
+            }
+          }
+        }
+        if (conf.conf_pruning) {
+          if (__syncthreads_or(have)) break;
+        }
+      }
+      // warp-level fold of the per-thread partials, then across warps
+#pragma unroll
+      for (int d = 16; d > 0; d >>= 1) {
+        const WA o = shfl_down_any(acc, d);
+        const bool oh = __shfl_down_sync(FULL, have, d);
+        if (oh) {
+          if (have)
+            f.comp(&acc, o, g);
+          else {
+            acc = o;
+            have = true;
+          }
+        }
+      }
+      if (lane == 0) {
+        s_part[w] = acc;
+        s_have[w] = have;
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        WA tot;
+        bool th = false;
+        for (int k = 0; k < NW; ++k)
+          if (s_have[k]) {
+            if (th)
+              f.comp(&tot, s_part[k], g);
+            else {
+              tot = s_part[k];
+              th = true;
+            }
+          }
+        if (th) f.comp(f.wa_of(cv), tot, g);
+      }
+      __syncthreads();
+    }
+    // warp tier
+    for (;;) {
+      const unsigned m = __ballot_sync(FULL, deg >= 32);
+      if (!m) break;
+      const int leader = __ffs(m) - 1;
+      const int wv = __shfl_sync(FULL, v, leader);
+      const int wdeg = __shfl_sync(FULL, deg, leader);
+      const int64_t wst = __shfl_sync(FULL, st, leader);
+      if (lane == leader) {
+        deg = 0;
+        account(as, conf, (unsigned long long)wdeg);
+      }
+      WA acc;
+      bool have = false;
+      for (int base = 0; base < wdeg; base += 32) {
+        const int k = base + lane;
+        if (k < wdeg) {
+          const int u = __ldg(g.dgr_adj_list + wst + k);
+          if (conf.conf_fromall || as.bitmap.is_active(u)) {
+            WA x = f.emit(u, g.fetch_edata_r(wst + k), g);
+            if (have)
+              f.comp(&acc, x, g);
+            else {
+              acc = x;
+              have = true;
+            }
+          }
+        }
+        if (conf.conf_pruning && __any_sync(FULL, have)) break;
+      }
+#pragma unroll
+      for (int d = 16; d > 0; d >>= 1) {
+        const WA o = shfl_down_any(acc, d);
+        const bool oh = __shfl_down_sync(FULL, have, d);
+        if (oh) {
+          if (have)
+            f.comp(&acc, o, g);
+          else {
+            acc = o;
+            have = true;
+          }
+        }
+      }
+      if (lane == 0 && have) f.comp(f.wa_of(wv), acc, g);
+    }
+    // thread tier
+    account(as, conf, (unsigned long long)deg);
+    if (deg > 0) {
+      WA acc;
+      bool have = false;
+      for (int k = 0; k < deg; ++k) {
+        const int u = __ldg(g.dgr_adj_list + st + k);
+        if (conf.conf_fromall || as.bitmap.is_active(u)) {
+          WA x = f.emit(u, g.fetch_edata_r(st + k), g);
+          if (have)
+            f.comp(&acc, x, g);
+          else {
+            acc = x;
+            have = true;
+          }
+          if (conf.conf_pruning) break;
+        }
+      }
+      if (have) f.comp(f.wa_of(v), acc, g);
+    }
+    __syncthreads();
+  }
+}
+
+// ===========================================================================
+// edge-centric, pointer jumping, exit probe, compensation
+// ===========================================================================
+template <typename G, typename F>
+__global__ void __launch_bounds__(512) k_expand_ec(active_set_t as, G g, F f) {
+  const int64_t n = as.get_size();
+  const int64_t STRIDE = (int64_t)blockDim.x * gridDim.x;
+  for (int64_t idx = threadIdx.x + (int64_t)blockIdx.x * blockDim.x; idx < n; idx += STRIDE) {
+    const int e = as.fetch(idx, Active);
+    if (e < 0) continue;
+    const packed_t vv = g.dg_coo[e];
+    f.update((int)(vv >> 32), (int)(vv & 0xffffffffll), (typename G::edge_t *)nullptr);
+  }
+}
+
+// Every vertex is re-pointed at the root of its chain (the fixed point the
+// reference's repeated single jumps reach, src/utils/intrinsics.cuh:328-362);
+// chains only shorten while this runs, and the walk is bounded by n steps.
+__global__ void __launch_bounds__(512) k_pointer_jump(int *wa, int64_t n, unsigned *err) {
+  const int64_t STRIDE = (int64_t)blockDim.x * gridDim.x;
+  for (int64_t v = threadIdx.x + (int64_t)blockIdx.x * blockDim.x; v < n; v += STRIDE) {
+    int r = wa[v];
+    int64_t guard = 0;
+    for (;;) {
+      const int p = ((volatile int *)wa)[r];
+      if (p == r) break;
+      r = p;
+      if (++guard > n) {
+        atomicOr(err, DEV_ERR_BAD_VERTEX);
+        break;
+      }
+    }
+    wa[v] = r;
+  }
+}
+
+template <typename G, typename F>
+__global__ void __launch_bounds__(512) k_exit(G g, F f, int *cnt) {
+  const int64_t STRIDE = (int64_t)blockDim.x * gridDim.x;
+  for (int64_t v = threadIdx.x + (int64_t)blockIdx.x * blockDim.x; v < g.nvertexs; v += STRIDE)
+    if (f.exit((int)v, g)) {
+      *cnt = 1;
+      return;
+    }
+}
+
+template <typename G, typename F>
+__global__ void __launch_bounds__(512) k_filter_all(G g, F f, int64_t n) {
+  const int64_t STRIDE = (int64_t)blockDim.x * gridDim.x;
+  for (int64_t v = threadIdx.x + (int64_t)blockIdx.x * blockDim.x; v < n; v += STRIDE) f.filter((int)v, g);
+}
+
+template <typename G, typename F>
+__global__ void __launch_bounds__(512) k_compensation(active_set_t as, G g, F f) {
+  const int64_t n = as.get_queue_size_hard();
+  const int64_t STRIDE = (int64_t)blockDim.x * gridDim.x;
+  for (int64_t idx = threadIdx.x + (int64_t)blockIdx.x * blockDim.x; idx < n; idx += STRIDE)
+    f.filter(as.fetch_queue(idx), g);
+}
+
+}  // namespace gsw

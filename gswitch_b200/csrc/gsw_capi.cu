@@ -1,0 +1,1191 @@
+// libgsw.so: the C ABI declared in include/gsw.h.
+//
+// Owns contexts (device + stream + reusable workspaces), device graphs
+// (int64 row offsets, int32 columns, int32 degrees, optional weights, lazily
+// built edge list for edge-centric operators) and the level loops of the
+// seven applications, written the way the reference's application mains
+// drive inspector / selector / executor (file:line per runner).
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/gsw.h"
+#include "apps.cuh"
+#include "graphgen.cuh"
+#include "mbfs.cuh"
+
+using namespace gsw;
+
+// ---------------------------------------------------------------------------
+// context and graph objects
+// ---------------------------------------------------------------------------
+struct gsw_graph {
+  gsw_ctx *ctx = nullptr;
+  int64_t n = 0, m = 0;
+  bool directed = false, weighted = false;
+  int64_t *off = nullptr;
+  int *col = nullptr, *odeg = nullptr, *w = nullptr;
+  int64_t *roff = nullptr;
+  int *rcol = nullptr, *rdeg = nullptr, *rw = nullptr;
+  packed_t *coo = nullptr;
+  int64_t ncoo = -1;
+  double attr[6] = {0, 0, 0, 0, 0, 0};
+  double mean_weight = 0;
+
+  template <typename E>
+  device_graph_t<CSR, E> view() const {
+    device_graph_t<CSR, E> g;
+    g.dg_row_off = off;
+    g.dg_adj_list = col;
+    g.dg_odegree = odeg;
+    g.dg_edgedata = (E *)w;
+    g.dgr_row_off = directed ? roff : off;
+    g.dgr_adj_list = directed ? rcol : col;
+    g.dgr_odegree = directed ? rdeg : odeg;
+    g.dgr_edgedata = (E *)(directed ? rw : w);
+    g.nvertexs = (int)n;
+    g.nedges = m;
+    g.level = 0;
+    g.directed = directed;
+    return g;
+  }
+};
+
+struct gsw_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  executor_t executor;
+  std::map<std::pair<int64_t, int>, active_set_t> as_cache;
+  std::map<std::string, std::pair<void *, size_t>> bufs;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+
+  void *buf(const std::string &name, size_t bytes) {
+    auto it = bufs.find(name);
+    if (it != bufs.end() && it->second.second >= bytes) return it->second.first;
+    if (it != bufs.end()) {
+      cudaFree(it->second.first);
+      bufs.erase(it);
+    }
+    void *p = nullptr;
+    if (GSW_CUDA(cudaMalloc(&p, bytes ? bytes : 1))) return nullptr;
+    bufs[name] = {p, bytes};
+    return p;
+  }
+  active_set_t *aset(int64_t size, QueueMode qm) {
+    auto key = std::make_pair(size, (int)qm);
+    auto it = as_cache.find(key);
+    if (it != as_cache.end()) return &it->second;
+    active_set_t as;
+    if (as.build(size, qm)) {
+      as.destroy();
+      return nullptr;
+    }
+    return &(as_cache[key] = as);
+  }
+};
+
+namespace {
+
+thread_local std::string g_last_error;
+
+struct entry_guard {  // binds the context's device and stream for one call
+  explicit entry_guard(gsw_ctx *ctx) {
+    clear_error();
+    if (ctx) {
+      cudaSetDevice(ctx->device);
+      stream() = ctx->stream;
+    }
+  }
+  gsw_status finish() {
+    if (!ok()) g_last_error = err().msg;
+    return err().code;
+  }
+};
+
+gsw_status fail(int code, const char *msg) {
+  set_error(code, "%s", msg);
+  g_last_error = msg;
+  return code;
+}
+
+int grid_for(int64_t n) { return (int)std::min<int64_t>((n + 255) / 256 + 1, (int64_t)sm_count() * 8); }
+
+// degree statistics on the host (same ascending summation order as
+// graph_attr_t::fill, src/utils/fileIO.cuh:35-67)
+void compute_attr(gsw_graph *g) {
+  std::vector<int> deg(g->n);
+  if (GSW_CUDA(cudaMemcpyAsync(deg.data(), g->odeg, sizeof(int) * g->n, cudaMemcpyDeviceToHost, stream()))) return;
+  GSW_CUDA(cudaStreamSynchronize(stream()));
+  int mx = 0;
+  for (int d : deg) mx = std::max(mx, d);
+  std::vector<int64_t> hist((size_t)mx + 1, 0);
+  for (int d : deg) hist[d]++;
+  const double nv = (double)g->n;
+  double avg = 0, sd = 0, sum = 0, gi = 0, her = 0;
+  for (int d = 0; d <= mx; ++d)
+    for (int64_t c = 0; c < hist[d]; ++c) {
+      avg += d;
+      sd += (double)d * d;
+    }
+  sd = std::sqrt((sd - avg * avg / nv) / (nv - 1));
+  avg /= nv;
+  int mn = 0;
+  while (mn < mx && hist[mn] == 0) ++mn;
+  for (int d = 0; d <= mx; ++d)
+    for (int64_t c = 0; c < hist[d]; ++c) sum += d;
+  int64_t i = 1;
+  const double lsum = std::log(sum);
+  for (int d = 0; d <= mx; ++d)
+    for (int64_t c = 0; c < hist[d]; ++c, ++i) {
+      const double du = d;
+      gi += (nv - i + 0.5) * du / nv / sum;
+      if (du != 0) her += du * (lsum - std::log(du)) / sum;
+    }
+  gi = 1 - 2 * gi;
+  her = her / std::log(nv);
+  g->attr[0] = avg;
+  g->attr[1] = sd;
+  g->attr[2] = (double)(mx - mn);
+  g->attr[3] = mx;
+  g->attr[4] = gi;
+  g->attr[5] = her;
+}
+
+__global__ void k_sum_weights(const int *w, int64_t m, unsigned long long *out) {
+  unsigned long long s = 0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < m; i += (int64_t)gridDim.x * blockDim.x) s += w[i];
+  s = warp_sum(s);
+  if (lane_id() == 0 && s) atomicAdd(out, s);
+}
+
+void finalize_graph(gsw_graph *g) {
+  int64_t *off = g->off;
+  if (!g->odeg) {
+    if (GSW_CUDA(cudaMalloc((void **)&g->odeg, sizeof(int) * (g->n + 1)))) return;
+    k_deg_to_i32<<<grid_for(g->n), 256, 0, stream()>>>(off, g->n, g->odeg);
+    GSW_LAUNCHED();
+  }
+  if (g->weighted) {
+    unsigned long long *d = (unsigned long long *)g->ctx->buf("wsum", 8);
+    if (!d) return;
+    GSW_CUDA(cudaMemsetAsync(d, 0, 8, stream()));
+    k_sum_weights<<<grid_for(g->m), 256, 0, stream()>>>(g->w, g->m, d);
+    unsigned long long s = 0;
+    GSW_CUDA(cudaMemcpyAsync(&s, d, 8, cudaMemcpyDeviceToHost, stream()));
+    GSW_CUDA(cudaStreamSynchronize(stream()));
+    g->mean_weight = g->m ? (double)s / (double)g->m : 0;
+  }
+  if (g->n > 1) compute_attr(g);
+}
+
+// CSR from device keys (both directions of every pair, self-loops = ~0)
+int csr_from_keys(gsw_graph *g, uint64_t *keys, int64_t nkeys) {
+  void *tmp = nullptr;
+  size_t tmpb = 0;
+  uint64_t *sorted = nullptr;
+  int *flag = nullptr;
+  int64_t *pos = nullptr;
+  if (GSW_CUDA(cudaMalloc((void **)&sorted, sizeof(uint64_t) * (nkeys + 1)))) return err().code;
+  cub::DeviceRadixSort::SortKeys(nullptr, tmpb, keys, sorted, nkeys, 0, 64, stream());
+  if (GSW_CUDA(cudaMalloc(&tmp, tmpb))) return err().code;
+  GSW_CUDA(cub::DeviceRadixSort::SortKeys(tmp, tmpb, keys, sorted, nkeys, 0, 64, stream()));
+  cudaFree(tmp);
+  tmp = nullptr;
+  // unique: flags -> positions (reuse `keys` as the compacted output)
+  if (GSW_CUDA(cudaMalloc((void **)&flag, sizeof(int) * (nkeys + 1)))) return err().code;
+  if (GSW_CUDA(cudaMalloc((void **)&pos, sizeof(int64_t) * (nkeys + 1)))) return err().code;
+  k_unique_flags<<<grid_for(nkeys), 256, 0, stream()>>>(sorted, nkeys, flag);
+  int *num = (int *)g->ctx->buf("nsel", 8);
+  tmpb = 0;
+  cub::DeviceSelect::Flagged(nullptr, tmpb, sorted, flag, keys, num, nkeys, stream());
+  if (GSW_CUDA(cudaMalloc(&tmp, tmpb))) return err().code;
+  GSW_CUDA(cub::DeviceSelect::Flagged(tmp, tmpb, sorted, flag, keys, num, nkeys, stream()));
+  int m = 0;
+  GSW_CUDA(cudaMemcpyAsync(&m, num, sizeof(int), cudaMemcpyDeviceToHost, stream()));
+  GSW_CUDA(cudaStreamSynchronize(stream()));
+  cudaFree(tmp);
+  cudaFree(sorted);
+  cudaFree(flag);
+  cudaFree(pos);
+  g->m = m;
+  if (GSW_CUDA(cudaMalloc((void **)&g->col, sizeof(int) * ((size_t)m + 1)))) return err().code;
+  if (GSW_CUDA(cudaMalloc((void **)&g->off, sizeof(int64_t) * (g->n + 1)))) return err().code;
+  unsigned long long *deg = (unsigned long long *)g->off;  // count into off[1..n]
+  GSW_CUDA(cudaMemsetAsync(g->off, 0, sizeof(int64_t) * (g->n + 1), stream()));
+  k_split_keys<<<grid_for(m), 256, 0, stream()>>>(keys, m, g->col, deg + 1);
+  tmpb = 0;
+  cub::DeviceScan::InclusiveSum(nullptr, tmpb, g->off + 1, g->off + 1, g->n, stream());
+  if (GSW_CUDA(cudaMalloc(&tmp, tmpb))) return err().code;
+  GSW_CUDA(cub::DeviceScan::InclusiveSum(tmp, tmpb, g->off + 1, g->off + 1, g->n, stream()));
+  GSW_CUDA(cudaStreamSynchronize(stream()));
+  cudaFree(tmp);
+  return err().code;
+}
+
+gsw_graph *new_graph(gsw_ctx *ctx, int64_t n) {
+  gsw_graph *g = new gsw_graph();
+  g->ctx = ctx;
+  g->n = n;
+  return g;
+}
+
+void free_graph(gsw_graph *g) {
+  if (!g) return;
+  cudaFree(g->off);
+  cudaFree(g->col);
+  cudaFree(g->odeg);
+  cudaFree(g->w);
+  cudaFree(g->roff);
+  cudaFree(g->rcol);
+  cudaFree(g->rdeg);
+  cudaFree(g->rw);
+  cudaFree(g->coo);
+  delete g;
+}
+
+int add_weights(gsw_graph *g, int wmax, uint64_t wseed) {
+  if (wmax <= 0) return GSW_OK;
+  if (GSW_CUDA(cudaMalloc((void **)&g->w, sizeof(int) * ((size_t)g->m + 1)))) return err().code;
+  k_weights<<<grid_for(g->n), 256, 0, stream()>>>(g->off, g->col, g->n, stream_key(wseed, ST_W), wmax, g->w);
+  g->weighted = true;
+  return GSW_LAUNCHED();
+}
+
+gsw_status finish_generate(gsw_ctx *ctx, gsw_graph *g, uint64_t *keys, int64_t nkeys, int wmax, uint64_t wseed,
+                           gsw_graph **out, entry_guard &eg) {
+  if (csr_from_keys(g, keys, nkeys) == GSW_OK) add_weights(g, wmax, wseed);
+  cudaFree(keys);
+  if (ok()) finalize_graph(g);
+  if (!ok()) {
+    free_graph(g);
+    return eg.finish();
+  }
+  *out = g;
+  return GSW_OK;
+}
+
+// ---- COO (edge list) for edge-centric operators ---------------------------
+__global__ void k_coo_count(const int64_t *off, const int *col, int64_t n, bool all, int64_t *cnt) {
+  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
+    int64_t c = 0;
+    for (int64_t e = off[v]; e < off[v + 1]; ++e) c += all || col[e] > v;
+    cnt[v] = c;
+  }
+}
+__global__ void k_coo_write(const int64_t *off, const int *col, int64_t n, bool all, const int64_t *pos,
+                            packed_t *coo) {
+  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
+    int64_t p = pos[v];
+    for (int64_t e = off[v]; e < off[v + 1]; ++e)
+      if (all || col[e] > v) coo[p++] = ((packed_t)v << 32) | (uint32_t)col[e];
+  }
+}
+
+int ensure_coo(gsw_graph *g) {
+  if (g->coo) return GSW_OK;
+  int64_t *cnt = (int64_t *)g->ctx->buf("coo_cnt", sizeof(int64_t) * (g->n + 1));
+  if (!cnt) return err().code;
+  const bool all = g->directed;
+  k_coo_count<<<grid_for(g->n), 256, 0, stream()>>>(g->off, g->col, g->n, all, cnt);
+  GSW_CUDA(cudaMemsetAsync(cnt + g->n, 0, sizeof(int64_t), stream()));
+  void *tmp = nullptr;
+  size_t tmpb = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, tmpb, cnt, cnt, g->n + 1, stream());
+  if (GSW_CUDA(cudaMalloc(&tmp, tmpb))) return err().code;
+  GSW_CUDA(cub::DeviceScan::ExclusiveSum(tmp, tmpb, cnt, cnt, g->n + 1, stream()));
+  int64_t total = 0;
+  GSW_CUDA(cudaMemcpyAsync(&total, cnt + g->n, sizeof(int64_t), cudaMemcpyDeviceToHost, stream()));
+  GSW_CUDA(cudaStreamSynchronize(stream()));
+  cudaFree(tmp);
+  if (GSW_CUDA(cudaMalloc((void **)&g->coo, sizeof(packed_t) * (total + 1)))) return err().code;
+  k_coo_write<<<grid_for(g->n), 256, 0, stream()>>>(g->off, g->col, g->n, all, cnt, g->coo);
+  g->ncoo = total;
+  return GSW_LAUNCHED();
+}
+
+// ---------------------------------------------------------------------------
+// run helpers
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void k_fill(T *p, T v, int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) p[i] = v;
+}
+template <typename T>
+__global__ void k_fill_root(T *p, T v, T rootv, int64_t root, int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    p[i] = i == root ? rootv : v;
+}
+template <typename T>
+void fill(T *p, T v, int64_t n) {
+  k_fill<T><<<grid_for(n), 256, 0, stream()>>>(p, v, n);
+}
+template <typename T>
+void fill_root(T *p, T v, T rootv, int64_t root, int64_t n) {
+  k_fill_root<T><<<grid_for(n), 256, 0, stream()>>>(p, v, rootv, root, n);
+}
+
+// Graph500 numerator: sum of degrees of reached vertices, halved
+__global__ void k_reached_edges(const int *lvl_or_dist, int stride_ints, int unreached, const int *odeg, int64_t n,
+                                unsigned long long *out) {
+  unsigned long long s = 0;
+  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
+    const int x = lvl_or_dist[v * stride_ints];
+    if (x != unreached && x >= 0) s += odeg[v];
+  }
+  s = warp_sum(s);
+  if (lane_id() == 0 && s) atomicAdd(out, s);
+}
+
+int64_t reached_edges(gsw_ctx *ctx, gsw_graph *g, const int *vals, int stride, int unreached) {
+  unsigned long long *d = (unsigned long long *)ctx->buf("redges", 8);
+  if (!d) return 0;
+  GSW_CUDA(cudaMemsetAsync(d, 0, 8, stream()));
+  k_reached_edges<<<grid_for(g->n), 256, 0, stream()>>>(vals, stride, unreached, g->odeg, g->n, d);
+  unsigned long long s = 0;
+  GSW_CUDA(cudaMemcpyAsync(&s, d, 8, cudaMemcpyDeviceToHost, stream()));
+  GSW_CUDA(cudaStreamSynchronize(stream()));
+  return (int64_t)(s / 2);
+}
+
+void apply_opts(const gsw_run_opts *o, config_t &conf) {
+  if (!o) return;
+  if (o->direction >= 0) {
+    conf.force.has_direction = true;
+    conf.force.d = o->direction == GSW_PULL ? Pull : Push;
+  }
+  if (o->asfmt >= 0) {
+    conf.force.has_asfmt = true;
+    conf.force.asf = o->asfmt == GSW_BITMAP ? Bitmap : Queue;
+  }
+  if (o->lb >= 0) {
+    conf.force.has_lb = true;
+    conf.force.lb = (LB)o->lb;
+  }
+  if (o->fusion >= 0) {
+    conf.force.has_fusion = true;
+    conf.force.fusion = o->fusion == GSW_FUSED ? Fused : Standalone;
+  }
+  conf.conf_sorted_queue = o->sorted_queue != 0;
+  conf.conf_count_edges = o->account != 0;
+  opts().verbose = o->verbose != 0;
+  opts().timing = o->timing != 0;
+  opts().force_grid = o->expand_grid;
+}
+
+void set_graph_features(feature_t &fets, const gsw_graph *g) {
+  fets.nvertexs = g->n;
+  fets.nedges = g->m;
+  fets.avg_deg = g->attr[0];
+  fets.std_deg = g->attr[1];
+  fets.range = g->attr[2];
+  fets.max_deg = g->attr[3];
+  fets.GI = g->attr[4];
+  fets.Her = g->attr[5];
+  fets.avg_edata = g->mean_weight;
+}
+
+struct loop_trace {
+  gsw_run_stats *st;
+  int64_t cap = 0;
+  int64_t count = 0;
+  int last = -1;
+  std::vector<kernel_marks> pending;  // per traced level, resolved in finish()
+  void level(const config_t &conf, int64_t frontier) {
+    if (cap > 0 && ++count > cap) set_error(GSW_ERR_TIMEOUT, "%s", "level loop did not converge within the level cap");
+    last = -1;
+    if (!st) return;
+    if (st->ntrace < GSW_MAX_TRACE) {
+      last = st->ntrace;
+      st->level_cfg[last] = (conf.conf_dir == Pull) | ((conf.conf_asfmt == Bitmap) << 1) |
+                            ((int)conf.conf_lb << 2) | ((conf.conf_fuse_inspect ? 1 : 0) << 5);
+      st->level_frontier[last] = frontier;
+      st->level_ms[last] = 0;
+      st->level_edges[last] = -1;
+      st->ntrace++;
+    }
+    st->levels++;
+  }
+  // after the expand: edge count now, kernel times once the run is over
+  void done(const stat_t &stats) {
+    if (!st || last < 0) return;
+    st->level_edges[last] = stats.last_scanned;
+    st->level_inspect_ms[last] = 0;
+    if (opts().timing) {
+      if ((int)pending.size() <= last) pending.resize(last + 1);
+      pending[last] = marks();
+    }
+  }
+  // after the final synchronisation of the run
+  void resolve() {
+    if (!st || !opts().timing) return;
+    const event_pool &p = timing_pool();
+    for (int i = 0; i < (int)pending.size() && i < st->ntrace; ++i) {
+      st->level_ms[i] = p.elapsed(pending[i].exp0, pending[i].exp1);
+      st->level_inspect_ms[i] = p.elapsed(pending[i].insp0, pending[i].insp1);
+    }
+    timing_pool().used = 0;
+  }
+};
+
+struct timer {
+  gsw_ctx *ctx;
+  explicit timer(gsw_ctx *c) : ctx(c) {
+    if (!ctx->e0) {
+      cudaEventCreate(&ctx->e0);
+      cudaEventCreate(&ctx->e1);
+    }
+    cudaEventRecord(ctx->e0, stream());
+  }
+  double stop() {
+    cudaEventRecord(ctx->e1, stream());
+    cudaEventSynchronize(ctx->e1);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ctx->e0, ctx->e1);
+    return ms;
+  }
+};
+
+void begin_stats(gsw_run_stats *st) {
+  if (!st) return;
+  st->ms = 0;
+  st->levels = 0;
+  st->edges = 0;
+  st->device_error = 0;
+  st->ntrace = 0;
+  st->launches = 0;
+  launch_count() = 0;
+  timing_pool().used = 0;
+}
+
+unsigned end_checks(active_set_t *as, gsw_run_stats *st) {
+  const unsigned e = as->read_error();
+  if (st) {
+    st->device_error = e;
+    st->launches = launch_count();
+  }
+  if (e & DEV_ERR_QUEUE_OVERFLOW) set_error(GSW_ERR_OVERFLOW, "%s", "frontier queue overflow");
+  if (e & DEV_ERR_SCRATCH_OVERFLOW) set_error(GSW_ERR_OVERFLOW, "%s", "STRICT tile table overflow");
+  if (e & DEV_ERR_BARRIER_TIMEOUT) set_error(GSW_ERR_TIMEOUT, "%s", "grid barrier timed out");
+  if (e & DEV_ERR_BAD_VERTEX) set_error(GSW_ERR_CUDA, "%s", "pointer chain longer than n");
+  GSW_CUDA(cudaMemsetAsync(&as->dg_cnt->err, 0, sizeof(unsigned), stream()));
+  return e;
+}
+
+// level cap of every loop: far above any legitimate run, it turns a loop
+// that cannot converge into an error instead of a hang
+inline int level_cap(int64_t n) { return (int)std::min<int64_t>(std::max<int64_t>(4 * n, 100000), 1 << 30); }
+#define MAX_LEVELS level_cap(gr->n)
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+int gsw_version(void) { return 1; }
+
+const char *gsw_last_error_string(void) { return g_last_error.c_str(); }
+
+void gsw_run_opts_default(gsw_run_opts *o) {
+  if (!o) return;
+  memset(o, 0, sizeof(*o));
+  o->direction = o->asfmt = o->lb = o->fusion = GSW_AUTO;
+  o->sorted_queue = 1;
+  o->max_iters = 0;
+  o->damping = 0.85f;
+  o->eps = 0.01f;
+  o->selector = GSW_SELECT_RULES;
+}
+
+gsw_status gsw_init(int device, gsw_ctx **out) {
+  entry_guard eg(nullptr);
+  if (!out) return fail(GSW_ERR_INVALID_ARG, "gsw_init: out is NULL");
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) return fail(GSW_ERR_NO_DEVICE, "no CUDA device");
+  if (device < 0 || device >= count) return fail(GSW_ERR_INVALID_ARG, "gsw_init: device out of range");
+  if (GSW_CUDA(cudaSetDevice(device))) return eg.finish();
+  gsw_ctx *c = new gsw_ctx();
+  c->device = device;
+  if (GSW_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking))) {
+    delete c;
+    return eg.finish();
+  }
+  *out = c;
+  return GSW_OK;
+}
+
+gsw_status gsw_destroy(gsw_ctx *ctx) {
+  if (!ctx) return GSW_OK;
+  entry_guard eg(ctx);
+  cudaStreamSynchronize(ctx->stream);
+  for (auto &kv : ctx->as_cache) kv.second.destroy();
+  for (auto &kv : ctx->bufs) cudaFree(kv.second.first);
+  ctx->executor.destroy();
+  if (ctx->e0) cudaEventDestroy(ctx->e0);
+  if (ctx->e1) cudaEventDestroy(ctx->e1);
+  cudaStreamDestroy(ctx->stream);
+  stream() = 0;
+  delete ctx;
+  return GSW_OK;
+}
+
+gsw_status gsw_graph_upload(gsw_ctx *ctx, int64_t n, int64_t m, const int64_t *row_off, const int32_t *col,
+                            const int32_t *weights, int directed, gsw_graph **out) {
+  entry_guard eg(ctx);
+  if (!ctx || !out || n <= 0 || m < 0 || !row_off || (m > 0 && !col))
+    return fail(GSW_ERR_INVALID_ARG, "gsw_graph_upload: bad arguments");
+  if (n >= (int64_t)INT32_MAX) return fail(GSW_ERR_UNSUPPORTED, "gsw_graph_upload: n must fit int32");
+  if (row_off[0] != 0 || row_off[n] != m) return fail(GSW_ERR_INVALID_ARG, "gsw_graph_upload: row_off[0] != 0 or row_off[n] != m");
+  gsw_graph *g = new_graph(ctx, n);
+  g->m = m;
+  g->directed = directed != 0;
+  g->weighted = weights != nullptr;
+  auto up = [&](void **dst, const void *src, size_t bytes) {
+    if (GSW_CUDA(cudaMalloc(dst, bytes ? bytes : 1))) return false;
+    if (bytes && GSW_CUDA(cudaMemcpyAsync(*dst, src, bytes, cudaMemcpyHostToDevice, stream()))) return false;
+    return true;
+  };
+  bool okk = up((void **)&g->off, row_off, sizeof(int64_t) * (n + 1)) && up((void **)&g->col, col, sizeof(int) * m);
+  if (okk && weights) okk = up((void **)&g->w, weights, sizeof(int) * m);
+  if (okk && g->directed) {
+    // reverse CSR on the host (counting sort by destination)
+    std::vector<int64_t> roff(n + 1, 0);
+    for (int64_t e = 0; e < m; ++e) roff[(size_t)col[e] + 1]++;
+    for (int64_t v = 0; v < n; ++v) roff[v + 1] += roff[v];
+    std::vector<int> rcol(m), rw(weights ? m : 0);
+    std::vector<int64_t> fillp(roff.begin(), roff.end() - 1);
+    for (int64_t v = 0; v < n; ++v)
+      for (int64_t e = row_off[v]; e < row_off[v + 1]; ++e) {
+        const int64_t p = fillp[col[e]]++;
+        rcol[p] = (int)v;
+        if (weights) rw[p] = weights[e];
+      }
+    okk = up((void **)&g->roff, roff.data(), sizeof(int64_t) * (n + 1)) &&
+          up((void **)&g->rcol, rcol.data(), sizeof(int) * m);
+    if (okk && weights) okk = up((void **)&g->rw, rw.data(), sizeof(int) * m);
+    if (okk) {
+      okk = GSW_CUDA(cudaMalloc((void **)&g->rdeg, sizeof(int) * (n + 1))) == GSW_OK;
+      if (okk) k_deg_to_i32<<<grid_for(n), 256, 0, stream()>>>(g->roff, n, g->rdeg);
+    }
+    GSW_CUDA(cudaStreamSynchronize(stream()));
+  }
+  if (okk) finalize_graph(g);
+  GSW_CUDA(cudaStreamSynchronize(stream()));
+  if (!ok()) {
+    free_graph(g);
+    return eg.finish();
+  }
+  *out = g;
+  return GSW_OK;
+}
+
+gsw_status gsw_graph_generate_rmat(gsw_ctx *ctx, int scale, int edge_factor, double a, double b, double c,
+                                   uint64_t seed, int wmax, uint64_t wseed, gsw_graph **out) {
+  entry_guard eg(ctx);
+  if (!ctx || !out || scale < 1 || scale > 30 || edge_factor < 1)
+    return fail(GSW_ERR_INVALID_ARG, "gsw_graph_generate_rmat: bad arguments");
+  const int64_t npairs = (int64_t)edge_factor << scale;
+  if (2 * npairs >= (int64_t)INT32_MAX * 2) return fail(GSW_ERR_UNSUPPORTED, "rmat: too many arcs");
+  gsw_graph *g = new_graph(ctx, (int64_t)1 << scale);
+  uint64_t *keys = nullptr;
+  if (GSW_CUDA(cudaMalloc((void **)&keys, sizeof(uint64_t) * (2 * npairs + 1)))) {
+    free_graph(g);
+    return eg.finish();
+  }
+  k_rmat_keys<<<grid_for(npairs), 256, 0, stream()>>>(make_rmat(scale, a, b, c, seed), npairs, keys);
+  return finish_generate(ctx, g, keys, 2 * npairs, wmax, wseed, out, eg);
+}
+
+gsw_status gsw_graph_generate_grid(gsw_ctx *ctx, int rows, int cols, int lr_div, uint64_t seed, int wmax,
+                                   uint64_t wseed, gsw_graph **out) {
+  entry_guard eg(ctx);
+  if (!ctx || !out || rows < 1 || cols < 2) return fail(GSW_ERR_INVALID_ARG, "gsw_graph_generate_grid: bad arguments");
+  const int64_t nl = (int64_t)rows * (cols - 1) + (int64_t)(rows - 1) * cols;
+  const int64_t nlr = lr_div > 0 ? nl / lr_div : 0;
+  gsw_graph *g = new_graph(ctx, (int64_t)rows * cols);
+  uint64_t *keys = nullptr;
+  if (GSW_CUDA(cudaMalloc((void **)&keys, sizeof(uint64_t) * (2 * (nl + nlr) + 1)))) {
+    free_graph(g);
+    return eg.finish();
+  }
+  k_grid_keys<<<grid_for(nl + nlr), 256, 0, stream()>>>(rows, cols, nl, nlr, stream_key(seed, ST_GRID), keys);
+  return finish_generate(ctx, g, keys, 2 * (nl + nlr), wmax, wseed, out, eg);
+}
+
+gsw_status gsw_graph_generate_er(gsw_ctx *ctx, int64_t n, int64_t m_pairs, uint64_t seed, int wmax, uint64_t wseed,
+                                 gsw_graph **out) {
+  entry_guard eg(ctx);
+  if (!ctx || !out || n < 2 || m_pairs < 0) return fail(GSW_ERR_INVALID_ARG, "gsw_graph_generate_er: bad arguments");
+  gsw_graph *g = new_graph(ctx, n);
+  uint64_t *keys = nullptr;
+  if (GSW_CUDA(cudaMalloc((void **)&keys, sizeof(uint64_t) * (2 * m_pairs + 1)))) {
+    free_graph(g);
+    return eg.finish();
+  }
+  k_er_keys<<<grid_for(m_pairs), 256, 0, stream()>>>(n, m_pairs, stream_key(seed, ST_ER), keys);
+  return finish_generate(ctx, g, keys, 2 * m_pairs, wmax, wseed, out, eg);
+}
+
+gsw_status gsw_graph_info(const gsw_graph *g, int64_t *n, int64_t *m, int *weighted) {
+  if (!g) return fail(GSW_ERR_INVALID_ARG, "gsw_graph_info: NULL graph");
+  if (n) *n = g->n;
+  if (m) *m = g->m;
+  if (weighted) *weighted = g->weighted;
+  return GSW_OK;
+}
+
+gsw_status gsw_graph_attr(const gsw_graph *g, double *out6) {
+  if (!g || !out6) return fail(GSW_ERR_INVALID_ARG, "gsw_graph_attr: NULL argument");
+  memcpy(out6, g->attr, sizeof(g->attr));
+  return GSW_OK;
+}
+
+gsw_status gsw_graph_download(const gsw_graph *g, int64_t *row_off, int32_t *col, int32_t *weights) {
+  if (!g) return fail(GSW_ERR_INVALID_ARG, "gsw_graph_download: NULL graph");
+  entry_guard eg(g->ctx);
+  if (row_off) GSW_CUDA(cudaMemcpyAsync(row_off, g->off, sizeof(int64_t) * (g->n + 1), cudaMemcpyDeviceToHost, stream()));
+  if (col) GSW_CUDA(cudaMemcpyAsync(col, g->col, sizeof(int) * g->m, cudaMemcpyDeviceToHost, stream()));
+  if (weights && g->w) GSW_CUDA(cudaMemcpyAsync(weights, g->w, sizeof(int) * g->m, cudaMemcpyDeviceToHost, stream()));
+  GSW_CUDA(cudaStreamSynchronize(stream()));
+  return eg.finish();
+}
+
+gsw_status gsw_graph_destroy(gsw_graph *g) {
+  if (!g) return GSW_OK;
+  entry_guard eg(g->ctx);
+  cudaStreamSynchronize(stream());
+  free_graph(g);
+  return eg.finish();
+}
+
+gsw_status gsw_graph_roots(const gsw_graph *g, uint64_t seed, int count, int32_t *roots) {
+  if (!g || !roots || count < 0) return fail(GSW_ERR_INVALID_ARG, "gsw_graph_roots: bad arguments");
+  entry_guard eg(g->ctx);
+  std::vector<int> deg(g->n);
+  GSW_CUDA(cudaMemcpyAsync(deg.data(), g->odeg, sizeof(int) * g->n, cudaMemcpyDeviceToHost, stream()));
+  GSW_CUDA(cudaStreamSynchronize(stream()));
+  if (!ok()) return eg.finish();
+  const uint64_t key = stream_key(seed, ST_ROOT);
+  int got = 0;
+  uint64_t j = 0;
+  const uint64_t budget = 64ull * (uint64_t)g->n + 4096;
+  while (got < count && j < budget) {
+    const int v = (int)(sm64(key + j) % (uint64_t)g->n);
+    ++j;
+    if (deg[v] == 0) continue;
+    bool dup = false;
+    for (int q = 0; q < got; ++q) dup |= roots[q] == v;
+    if (!dup) roots[got++] = v;
+  }
+  for (int64_t v = 0; got < count && v < g->n; ++v) {
+    if (deg[v] == 0) continue;
+    bool dup = false;
+    for (int q = 0; q < got; ++q) dup |= roots[q] == (int)v;
+    if (!dup) roots[got++] = (int)v;
+  }
+  while (got < count) roots[got++] = -1;
+  return eg.finish();
+}
+
+gsw_status gsw_ctx_stream(gsw_ctx *ctx, void **s) {
+  if (!ctx || !s) return fail(GSW_ERR_INVALID_ARG, "gsw_ctx_stream: bad arguments");
+  *s = (void *)ctx->stream;
+  return GSW_OK;
+}
+
+// ---------------------------------------------------------------------------
+// BFS: application/bfs.cu:78-102 (loop) and :104-130 (set-up)
+// ---------------------------------------------------------------------------
+gsw_status gsw_bfs(gsw_ctx *ctx, gsw_graph *gr, int32_t root, const gsw_run_opts *o, int32_t *levels,
+                   gsw_run_stats *st) {
+  entry_guard eg(ctx);
+  if (!ctx || !gr || root < 0 || root >= gr->n) return fail(GSW_ERR_INVALID_ARG, "gsw_bfs: bad arguments");
+  begin_stats(st);
+  auto g = gr->view<Empty>();
+  app::BFS f;
+  f.data.size = gr->n;
+  f.data.dg_wa = (int *)ctx->buf("wa", sizeof(int) * (gr->n + 1));
+  if (!f.data.dg_wa) return eg.finish();
+  fill_root<int>(f.data.dg_wa, -1, 0, root, gr->n);
+  feature_t fets;
+  config_t conf;
+  stat_t stats;
+  inspector_t inspector;
+  selector_t selector;
+  executor_t &executor = ctx->executor;
+  executor.insp = &inspector;
+  fets.centric = VC;
+  fets.pattern = Idem;
+  fets.fromall = false;
+  fets.toall = false;
+  conf.conf_pruning = true;
+  apply_opts(o, conf);
+  set_graph_features(fets, gr);
+  fets.use_root = root;
+  init_conf_impl(stats, fets, conf, g, f, gr->mean_weight, gr->attr[0], false);
+  active_set_t *asp = ctx->aset(gr->n, conf.conf_qmode);
+  if (!asp) return eg.finish();
+  active_set_t &as = *asp;
+  as.reset();
+  as.init(root);
+  loop_trace tr{st, MAX_LEVELS};
+  timer tm(ctx);
+  for (int level = 0; level < MAX_LEVELS && ok(); level++) {
+    inspector.inspect(as, g, f, stats, fets, conf);
+    if (finish(as, g, f, conf)) break;
+    selector.select(stats, fets, conf);
+    executor.filter(as, g, f, stats, fets, conf);
+    g.update_level();
+    tr.level(conf, hints().frontier);
+    executor.expand(as, g, f, stats, fets, conf);
+    tr.done(stats);
+    if (finish(as, g, f, conf)) break;
+  }
+  const double ms = tm.stop();
+  tr.resolve();
+  end_checks(&as, st);
+  stats.destroy();
+  if (st) {
+    st->ms = ms;
+    st->edges = reached_edges(ctx, gr, f.data.dg_wa, 1, -1);
+  }
+  if (levels && ok())
+    GSW_CUDA(cudaMemcpyAsync(levels, f.data.dg_wa, sizeof(int) * gr->n, cudaMemcpyDeviceToHost, stream()));
+  GSW_CUDA(cudaStreamSynchronize(stream()));
+  return eg.finish();
+}
+
+// ---------------------------------------------------------------------------
+// SSSP: application/sssp.cu:106-126 (loop) and :128-160 (set-up)
+// ---------------------------------------------------------------------------
+gsw_status gsw_sssp(gsw_ctx *ctx, gsw_graph *gr, int32_t root, const gsw_run_opts *o, int32_t *dist,
+                    gsw_run_stats *st) {
+  entry_guard eg(ctx);
+  if (!ctx || !gr || root < 0 || root >= gr->n) return fail(GSW_ERR_INVALID_ARG, "gsw_sssp: bad arguments");
+  if (!gr->weighted) return fail(GSW_ERR_INVALID_ARG, "gsw_sssp: graph has no weights");
+  begin_stats(st);
+  auto g = gr->view<int>();
+  app::SSSP f;
+  f.data.size = gr->n;
+  f.data.dg_wa = (int *)ctx->buf("wa", sizeof(int) * (gr->n + 1));
+  f.data.dg_ra = (int *)ctx->buf("ra", sizeof(int) * (gr->n + 1));
+  if (!f.data.dg_wa || !f.data.dg_ra) return eg.finish();
+  fill_root<int>(f.data.dg_wa, INT_MAX, 0, root, gr->n);
+  fill_root<int>(f.data.dg_ra, INT_MAX, 0, root, gr->n);
+  feature_t fets;
+  config_t conf;
+  stat_t stats;
+  inspector_t inspector;
+  selector_t selector;
+  executor_t &executor = ctx->executor;
+  executor.insp = &inspector;
+  fets.centric = VC;
+  fets.pattern = Mono;
+  fets.fromall = false;
+  fets.toall = true;
+  conf.conf_window = true;
+  apply_opts(o, conf);
+  set_graph_features(fets, gr);
+  fets.use_root = root;
+  init_conf_impl(stats, fets, conf, g, f, gr->mean_weight, gr->attr[0], false);
+  active_set_t *asp = ctx->aset(gr->n, conf.conf_qmode);
+  if (!asp) return eg.finish();
+  active_set_t &as = *asp;
+  as.reset();
+  as.init(root);
+  loop_trace tr{st, MAX_LEVELS};
+  timer tm(ctx);
+  for (int level = 0; level < MAX_LEVELS && ok(); level++) {
+    inspector.inspect(as, g, f, stats, fets, conf);
+    selector.select(stats, fets, conf);
+    executor.filter(as, g, f, stats, fets, conf);
+    g.update_level();
+    tr.level(conf, hints().frontier);
+    executor.expand(as, g, f, stats, fets, conf);
+    tr.done(stats);
+    if (finish(as, g, f, conf)) break;
+  }
+  const double ms = tm.stop();
+  tr.resolve();
+  end_checks(&as, st);
+  stats.destroy();
+  if (st) {
+    st->ms = ms;
+    st->edges = reached_edges(ctx, gr, f.data.dg_wa, 1, INT_MAX);
+  }
+  if (dist && ok()) GSW_CUDA(cudaMemcpyAsync(dist, f.data.dg_wa, sizeof(int) * gr->n, cudaMemcpyDeviceToHost, stream()));
+  GSW_CUDA(cudaStreamSynchronize(stream()));
+  return eg.finish();
+}
+
+// ---------------------------------------------------------------------------
+// CC: application/cc.cu:263-289 (loop) and :291-311 (set-up)
+// ---------------------------------------------------------------------------
+__global__ void k_iota(int *p, int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    p[i] = (int)i;
+}
+
+gsw_status gsw_cc(gsw_ctx *ctx, gsw_graph *gr, const gsw_run_opts *o, int32_t *labels, gsw_run_stats *st) {
+  entry_guard eg(ctx);
+  if (!ctx || !gr) return fail(GSW_ERR_INVALID_ARG, "gsw_cc: bad arguments");
+  begin_stats(st);
+  if (ensure_coo(gr)) return eg.finish();
+  device_graph_t<COO, Empty> g;
+  g.dg_coo = gr->coo;
+  g.dg_edgedata = nullptr;
+  g.nvertexs = (int)gr->n;
+  g.nedges = gr->ncoo;
+  g.level = 0;
+  app::CC f;
+  f.data.size = gr->n;
+  f.data.dg_wa = (int *)ctx->buf("wa", sizeof(int) * (gr->n + 1));
+  if (!f.data.dg_wa) return eg.finish();
+  k_iota<<<grid_for(gr->n), 256, 0, stream()>>>(f.data.dg_wa, gr->n);
+  feature_t fets;
+  config_t conf;
+  stat_t stats;
+  inspector_t inspector;
+  selector_t selector;
+  executor_t &executor = ctx->executor;
+  executor.insp = &inspector;
+  fets.centric = EC;
+  fets.pattern = ASSO;
+  apply_opts(o, conf);
+  set_graph_features(fets, gr);
+  init_conf_impl(stats, fets, conf, g, f, 0.0, gr->attr[0], false);
+  active_set_t *asp = ctx->aset(std::max<int64_t>(gr->ncoo, 1), conf.conf_qmode);
+  if (!asp) return eg.finish();
+  active_set_t &as = *asp;
+  as.reset();
+  as.init(ALL_ACTIVE);
+  loop_trace tr{st, MAX_LEVELS};
+  timer tm(ctx);
+  for (int level = 0; level < MAX_LEVELS && ok() && gr->ncoo > 0; level++) {
+    inspector.inspect(as, g, f, stats, fets, conf);
+    if (finish(as, g, f, conf)) break;
+    selector.select(stats, fets, conf);
+    executor.filter(as, g, f, stats, fets, conf);
+    g.update_level();
+    tr.level(conf, hints().frontier);
+    executor.expand(as, g, f, stats, fets, conf);
+    tr.done(stats);
+    p_jump(f, gr->n, as);
+    if (finish(as, g, f, conf)) break;
+  }
+  const double ms = tm.stop();
+  tr.resolve();
+  end_checks(&as, st);
+  stats.destroy();
+  if (st) {
+    st->ms = ms;
+    st->edges = gr->ncoo;
+  }
+  if (labels && ok())
+    GSW_CUDA(cudaMemcpyAsync(labels, f.data.dg_wa, sizeof(int) * gr->n, cudaMemcpyDeviceToHost, stream()));
+  GSW_CUDA(cudaStreamSynchronize(stream()));
+  return eg.finish();
+}
+
+// ---------------------------------------------------------------------------
+// PageRank: application/pagerank.cu:81-103 (loop) and :105-131 (set-up).
+// max_iters > 0 stops after exactly that many Jacobi steps (the filter of
+// inspection k computes pr_k); eps keeps the reference's convergence test.
+// ---------------------------------------------------------------------------
+__global__ void k_pr_init(const int *odeg, int64_t n, float damp, float *ra) {
+  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x)
+    ra[v] = odeg[v] ? (1 - damp) / odeg[v] : (1 - damp);
+}
+
+gsw_status gsw_pagerank(gsw_ctx *ctx, gsw_graph *gr, const gsw_run_opts *o, float *pr_over_od, gsw_run_stats *st) {
+  entry_guard eg(ctx);
+  if (!ctx || !gr) return fail(GSW_ERR_INVALID_ARG, "gsw_pagerank: bad arguments");
+  begin_stats(st);
+  gsw_run_opts def;
+  gsw_run_opts_default(&def);
+  const gsw_run_opts *op = o ? o : &def;
+  auto g = gr->view<Empty>();
+  app::PR f;
+  f.damp = op->damping;
+  f.eps = op->eps;
+  f.data.size = gr->n;
+  f.data.dg_wa = (float *)ctx->buf("wa", sizeof(float) * (gr->n + 1));
+  f.data.dg_ra = (float *)ctx->buf("ra", sizeof(float) * (gr->n + 1));
+  if (!f.data.dg_wa || !f.data.dg_ra) return eg.finish();
+  fill<float>(f.data.dg_wa, 0.0f, gr->n);
+  k_pr_init<<<grid_for(gr->n), 256, 0, stream()>>>(gr->odeg, gr->n, f.damp, f.data.dg_ra);
+  f.data.zero = 0.0f;
+  feature_t fets;
+  config_t conf;
+  stat_t stats;
+  inspector_t inspector;
+  selector_t selector;
+  executor_t &executor = ctx->executor;
+  executor.insp = &inspector;
+  fets.centric = VC;
+  fets.pattern = ASSO;
+  fets.fromall = true;
+  fets.toall = true;
+  apply_opts(op, conf);
+  set_graph_features(fets, gr);
+  init_conf_impl(stats, fets, conf, g, f, 0.0, gr->attr[0], false);
+  active_set_t *asp = ctx->aset(gr->n, conf.conf_qmode);
+  if (!asp) return eg.finish();
+  active_set_t &as = *asp;
+  as.reset();
+  as.init(ALL_ACTIVE);
+  loop_trace tr{st, MAX_LEVELS};
+  timer tm(ctx);
+  int steps = 0;
+  for (int level = 0; level < MAX_LEVELS && ok(); level++) {
+    inspector.inspect(as, g, f, stats, fets, conf);
+    if (op->max_iters > 0 && level == op->max_iters) break;
+    if (finish(as, g, f, conf)) break;
+    selector.select(stats, fets, conf);
+    executor.filter(as, g, f, stats, fets, conf);
+    g.update_level();
+    tr.level(conf, hints().frontier);
+    executor.expand(as, g, f, stats, fets, conf);
+    tr.done(stats);
+    steps++;
+    if (finish(as, g, f, conf)) break;
+  }
+  const double ms = tm.stop();
+  tr.resolve();
+  end_checks(&as, st);
+  stats.destroy();
+  if (st) {
+    st->ms = ms;
+    st->edges = gr->m * (int64_t)steps;
+  }
+  if (pr_over_od && ok())
+    GSW_CUDA(cudaMemcpyAsync(pr_over_od, f.data.dg_ra, sizeof(float) * gr->n, cudaMemcpyDeviceToHost, stream()));
+  GSW_CUDA(cudaStreamSynchronize(stream()));
+  return eg.finish();
+}
+
+// ---------------------------------------------------------------------------
+// BC: application/bc.cu:246-309 (both phases) and :391-431 (set-up).  The
+// cached queue that replays the forward levels backwards is kept for every
+// start (the reference drops to a Normal queue when its fusion tree picks the
+// standalone form, which leaves the deepest level's dependencies unpushed).
+// ---------------------------------------------------------------------------
+__global__ void k_bc_init(app::fwdata_t *wa, int64_t n, int64_t root) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    wa[i] = i == root ? app::fwdata_t{0, 1} : app::fwdata_t{-100, 0};
+}
+__global__ void k_bc_handoff(const app::fwdata_t *fw, int64_t n, int *lvl, app::bwdata_t *bw) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    lvl[i] = fw[i].level;
+    bw[i] = app::bwdata_t{fw[i].nsp, 0.0f};
+  }
+}
+__global__ void k_bc_split(const app::bwdata_t *bw, int64_t n, int *nsp, float *dep) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    nsp[i] = bw[i].nsp;
+    dep[i] = bw[i].dep;
+  }
+}
+
+gsw_status gsw_bc(gsw_ctx *ctx, gsw_graph *gr, int32_t root, const gsw_run_opts *o, int32_t *nsp, float *dep,
+                  gsw_run_stats *st) {
+  entry_guard eg(ctx);
+  if (!ctx || !gr || root < 0 || root >= gr->n) return fail(GSW_ERR_INVALID_ARG, "gsw_bc: bad arguments");
+  begin_stats(st);
+  auto g = gr->view<Empty>();
+  app::BCForward f;
+  app::BCBackward h;
+  f.data.size = h.data.size = gr->n;
+  f.data.dg_wa = (app::fwdata_t *)ctx->buf("wa", sizeof(app::fwdata_t) * (gr->n + 1));
+  h.data.dg_wa = (app::bwdata_t *)ctx->buf("wa2", sizeof(app::bwdata_t) * (gr->n + 1));
+  h.data.dg_ra = (int *)ctx->buf("ra", sizeof(int) * (gr->n + 1));
+  if (!f.data.dg_wa || !h.data.dg_wa || !h.data.dg_ra) return eg.finish();
+  k_bc_init<<<grid_for(gr->n), 256, 0, stream()>>>(f.data.dg_wa, gr->n, root);
+  feature_t fets;
+  config_t conf;
+  stat_t stats;
+  inspector_t inspector;
+  selector_t selector;
+  executor_t &executor = ctx->executor;
+  executor.insp = &inspector;
+  fets.centric = VC;
+  fets.pattern = ASSO;
+  fets.fromall = false;
+  fets.toall = false;
+  conf.conf_fuse_inspect = false;
+  conf.conf_qmode = Cached;
+  apply_opts(o, conf);
+  set_graph_features(fets, gr);
+  fets.use_root = root;
+  init_conf_impl(stats, fets, conf, g, f, 0.0, gr->attr[0], false);
+  conf.conf_qmode = Cached;
+  active_set_t *asp = ctx->aset(gr->n, Cached);
+  if (!asp) return eg.finish();
+  active_set_t &as = *asp;
+  as.reset();
+  as.init(root);
+  loop_trace tr{st, MAX_LEVELS};
+  timer tm(ctx);
+  for (int level = 0; level < MAX_LEVELS && ok(); level++) {
+    inspector.inspect(as, g, f, stats, fets, conf);
+    if (finish(as, g, f, conf)) break;
+    selector.select(stats, fets, conf);
+    executor.filter(as, g, f, stats, fets, conf);
+    g.update_level();
+    tr.level(conf, hints().frontier);
+    executor.expand(as, g, f, stats, fets, conf);
+    tr.done(stats);
+    if (finish(as, g, f, conf)) break;
+  }
+  const int64_t fwd_edges = st ? reached_edges(ctx, gr, (const int *)f.data.dg_wa, 2, -100) : 0;
+  // hand-off (bc.cu:391-395) and backward sweep over the cached levels
+  k_bc_handoff<<<grid_for(gr->n), 256, 0, stream()>>>(f.data.dg_wa, gr->n, h.data.dg_ra, h.data.dg_wa);
+  as.reset(true);
+  conf.reset();
+  stats.reset();
+  conf.conf_compensation = true;
+  g.update_level(-1);
+  if (conf.conf_fuse_inspect) g.update_level(-1);
+  as.init(ALL_INACTIVE);
+  for (int level = 0; level < MAX_LEVELS && ok(); level++) {
+    inspector.inspect(as, g, h, stats, fets, conf);
+    if (finish(as, g, h, conf)) break;
+    selector.select(stats, fets, conf);
+    executor.filter(as, g, h, stats, fets, conf);
+    g.update_level(-1);
+    tr.level(conf, hints().frontier);
+    executor.expand(as, g, h, stats, fets, conf);
+    tr.done(stats);
+    if (finish(as, g, h, conf)) break;
+  }
+  const double ms = tm.stop();
+  tr.resolve();
+  end_checks(&as, st);
+  stats.destroy();
+  if (st) {
+    st->ms = ms;
+    st->edges = fwd_edges;
+  }
+  if ((nsp || dep) && ok()) {
+    int *dn = (int *)ctx->buf("bc_nsp", sizeof(int) * (gr->n + 1));
+    float *dd = (float *)ctx->buf("bc_dep", sizeof(float) * (gr->n + 1));
+    if (dn && dd) {
+      k_bc_split<<<grid_for(gr->n), 256, 0, stream()>>>(h.data.dg_wa, gr->n, dn, dd);
+      if (nsp) GSW_CUDA(cudaMemcpyAsync(nsp, dn, sizeof(int) * gr->n, cudaMemcpyDeviceToHost, stream()));
+      if (dep) GSW_CUDA(cudaMemcpyAsync(dep, dd, sizeof(float) * gr->n, cudaMemcpyDeviceToHost, stream()));
+    }
+  }
+  GSW_CUDA(cudaStreamSynchronize(stream()));
+  return eg.finish();
+}
+
+// ---------------------------------------------------------------------------
+// GC: application/gc.cu:76-99 (loop) and :101-122 (set-up)
+// ---------------------------------------------------------------------------
+gsw_status gsw_gc(gsw_ctx *ctx, gsw_graph *gr, const gsw_run_opts *o, int32_t *colors, gsw_run_stats *st) {
+  entry_guard eg(ctx);
+  if (!ctx || !gr) return fail(GSW_ERR_INVALID_ARG, "gsw_gc: bad arguments");
+  begin_stats(st);
+  auto g = gr->view<Empty>();
+  app::GC f;
+  f.data.size = gr->n;
+  f.data.dg_wa = (int *)ctx->buf("wa", sizeof(int) * (gr->n + 1));
+  f.data.dg_ra = (int *)ctx->buf("ra", sizeof(int) * (gr->n + 1));
+  if (!f.data.dg_wa || !f.data.dg_ra) return eg.finish();
+  fill<int>(f.data.dg_wa, -1, gr->n);
+  fill<int>(f.data.dg_ra, -1, gr->n);
+  feature_t fets;
+  config_t conf;
+  stat_t stats;
+  inspector_t inspector;
+  selector_t selector;
+  executor_t &executor = ctx->executor;
+  executor.insp = &inspector;
+  fets.centric = VC;
+  fets.pattern = ASSO;
+  fets.fromall = true;
+  fets.toall = true;
+  conf.conf_fixed = true;
+  apply_opts(o, conf);
+  set_graph_features(fets, gr);
+  init_conf_impl(stats, fets, conf, g, f, 0.0, gr->attr[0], false);
+  active_set_t *asp = ctx->aset(gr->n, conf.conf_qmode);
+  if (!asp) return eg.finish();
+  active_set_t &as = *asp;
+  as.reset();
+  as.init(ALL_ACTIVE);
+  loop_trace tr{st, MAX_LEVELS};
+  timer tm(ctx);
+  for (int level = 0; level < MAX_LEVELS && ok(); level++) {
+    inspector.inspect(as, g, f, stats, fets, conf);
+    if (finish(as, g, f, conf)) break;
+    selector.select(stats, fets, conf);
+    executor.filter(as, g, f, stats, fets, conf);
+    g.update_level();
+    tr.level(conf, hints().frontier);
+    executor.expand(as, g, f, stats, fets, conf);
+    tr.done(stats);
+    if (finish(as, g, f, conf)) break;
+  }
+  const double ms = tm.stop();
+  tr.resolve();
+  end_checks(&as, st);
+  stats.destroy();
+  if (st) {
+    st->ms = ms;
+    st->edges = gr->m / 2;
+  }
+  if (colors && ok())
+    GSW_CUDA(cudaMemcpyAsync(colors, f.data.dg_ra, sizeof(int) * gr->n, cudaMemcpyDeviceToHost, stream()));
+  GSW_CUDA(cudaStreamSynchronize(stream()));
+  return eg.finish();
+}
+
+// ---------------------------------------------------------------------------
+// MBFS: application/mbfs.cu:222-297 runs the single-source loop per source;
+// the batched form runs 64 sources per bit-sliced word (mbfs.cuh).
+// ---------------------------------------------------------------------------
+gsw_status gsw_mbfs(gsw_ctx *ctx, gsw_graph *gr, int nsrc, const int32_t *roots, int batched, const gsw_run_opts *o,
+                    int32_t *levels, gsw_run_stats *st) {
+  entry_guard eg(ctx);
+  if (!ctx || !gr || nsrc <= 0 || !roots) return fail(GSW_ERR_INVALID_ARG, "gsw_mbfs: bad arguments");
+  for (int s = 0; s < nsrc; ++s)
+    if (roots[s] < 0 || roots[s] >= gr->n) return fail(GSW_ERR_INVALID_ARG, "gsw_mbfs: root out of range");
+  if (!batched) {
+    double tot = 0;
+    int64_t edges = 0;
+    int lv = 0;
+    gsw_run_stats one;
+    for (int s = 0; s < nsrc; ++s) {
+      gsw_status r = gsw_bfs(ctx, gr, roots[s], o, levels ? levels + (int64_t)s * gr->n : nullptr, &one);
+      if (r) return r;
+      tot += one.ms;
+      edges += one.edges;
+      lv += one.levels;
+    }
+    if (st) {
+      begin_stats(st);
+      st->ms = tot;
+      st->edges = edges;
+      st->levels = lv;
+    }
+    return GSW_OK;
+  }
+  begin_stats(st);
+  mbfs_result r = run_mbfs_batched(
+      gr->view<Empty>(), nsrc, roots, [&](const char *name, size_t bytes) { return ctx->buf(name, bytes); }, levels);
+  if (st && ok()) {
+    st->ms = r.ms;
+    st->levels = r.levels;
+    st->edges = r.edges;
+  }
+  return eg.finish();
+}
+
+}  // extern "C"

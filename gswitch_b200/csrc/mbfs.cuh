@@ -1,0 +1,250 @@
+// Batched multi-source BFS with bit-sliced frontiers.
+//
+// The reference's MBFS re-runs the single-source loop per source
+// (application/mbfs.cu:222-297).  Here all sources advance together: bit s
+// of word g stands for source 64*g + s, and each vertex keeps W = ceil(k/64)
+// words of `seen`, `frontier` and `next` stored vertex-major, so one 32-byte
+// sector carries every source's state of a vertex (256 sources).  Levels are
+// level-synchronous and identical to per-source BFS.
+//   push : a warp per frontier vertex ORs (frontier & ~seen[u]) into next[u]
+//   pull : a thread per vertex with unseen bits ORs its neighbours'
+//          frontier words and stops once every unseen bit is covered
+//   update: next & ~seen becomes the new frontier, levels are written for
+//          the new bits, and the counters that pick the next direction
+//          (frontier edges vs. unexplored edges, Beamer's alpha = 14) are
+//          reduced.
+#pragma once
+#include <vector>
+
+#include "engine/executor.cuh"
+
+namespace gsw {
+
+constexpr int MBFS_MAXW = 8;  // up to 512 sources per batch
+
+struct mbfs_result {
+  double ms = 0;
+  int levels = 0;
+  int64_t edges = 0;
+};
+
+struct mbfs_counters {
+  unsigned long long active_v;    // vertices with new bits
+  unsigned long long active_e;    // their degree sum
+  unsigned long long unseen_e;    // degree sum of vertices with unseen bits
+  unsigned long long reached_e;   // sum over vertices of deg * popcount(seen)
+};
+
+template <int W>
+__global__ void __launch_bounds__(256) k_mbfs_push(device_graph_t<CSR, Empty> g, const uint64_t *frontier,
+                                                    const uint64_t *seen, uint64_t *next) {
+  const int64_t n = g.nvertexs;
+  const int lane = lane_id();
+  const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t v = (int64_t)blockIdx.x * (blockDim.x >> 5) + warp_id(); v < n; v += nwarps) {
+    uint64_t f[W];
+    bool any = false;
+#pragma unroll
+    for (int k = 0; k < W; ++k) {
+      f[k] = __ldg(frontier + v * W + k);
+      any |= f[k] != 0;
+    }
+    if (!any) continue;
+    const int64_t st = __ldg(g.dg_row_off + v), en = __ldg(g.dg_row_off + v + 1);
+    for (int64_t e = st + lane; e < en; e += 32) {
+      const int u = __ldg(g.dg_adj_list + e);
+#pragma unroll
+      for (int k = 0; k < W; ++k) {
+        const uint64_t m = f[k] & ~seen[(int64_t)u * W + k];
+        if (m) atomicOr((unsigned long long *)(next + (int64_t)u * W + k), (unsigned long long)m);
+      }
+    }
+  }
+}
+
+template <int W>
+__global__ void __launch_bounds__(256) k_mbfs_pull(device_graph_t<CSR, Empty> g, const uint64_t *frontier,
+                                                    const uint64_t *seen, uint64_t *next, const uint64_t *valid) {
+  const int64_t n = g.nvertexs;
+  const int64_t STRIDE = (int64_t)blockDim.x * gridDim.x;
+  for (int64_t v = threadIdx.x + (int64_t)blockIdx.x * blockDim.x; v < n; v += STRIDE) {
+    uint64_t need[W], acc[W];
+    bool any = false;
+#pragma unroll
+    for (int k = 0; k < W; ++k) {
+      need[k] = valid[k] & ~seen[v * W + k];
+      acc[k] = 0;
+      any |= need[k] != 0;
+    }
+    if (!any) continue;
+    const int64_t st = __ldg(g.dgr_row_off + v), en = __ldg(g.dgr_row_off + v + 1);
+    for (int64_t e = st; e < en; ++e) {
+      const int u = __ldg(g.dgr_adj_list + e);
+      bool done = true;
+#pragma unroll
+      for (int k = 0; k < W; ++k) {
+        acc[k] |= __ldg(frontier + (int64_t)u * W + k);
+        done &= (acc[k] & need[k]) == need[k];
+      }
+      if (done) break;
+    }
+#pragma unroll
+    for (int k = 0; k < W; ++k) next[v * W + k] = acc[k] & need[k];
+  }
+}
+
+template <int W>
+__global__ void __launch_bounds__(256) k_mbfs_update(device_graph_t<CSR, Empty> g, uint64_t *frontier, uint64_t *seen,
+                                                      uint64_t *next, int *levels, int nsrc, int level,
+                                                      const uint64_t *valid, mbfs_counters *cnt) {
+  __shared__ unsigned long long s_red[32];
+  const int64_t n = g.nvertexs;
+  const int64_t STRIDE = (int64_t)blockDim.x * gridDim.x;
+  unsigned long long av = 0, ae = 0, ue = 0;
+  for (int64_t v = threadIdx.x + (int64_t)blockIdx.x * blockDim.x; v < n; v += STRIDE) {
+    const int deg = __ldg(g.dg_odegree + v);
+    bool nb_any = false, unseen = false;
+#pragma unroll
+    for (int k = 0; k < W; ++k) {
+      const uint64_t s = seen[v * W + k];
+      const uint64_t nb = next[v * W + k] & ~s;
+      next[v * W + k] = 0;
+      frontier[v * W + k] = nb;
+      if (nb) {
+        nb_any = true;
+        seen[v * W + k] = s | nb;
+        uint64_t b = nb;
+        while (b) {
+          const int bit = __ffsll((long long)b) - 1;
+          b &= b - 1;
+          const int src = k * 64 + bit;
+          if (src < nsrc) levels[(int64_t)src * n + v] = level;
+        }
+      }
+      unseen |= (valid[k] & ~(s | nb)) != 0;
+    }
+    if (nb_any) {
+      av++;
+      ae += deg;
+    }
+    if (unseen) ue += deg;
+  }
+  unsigned long long r = block_reduce(av, s_red);
+  if (threadIdx.x == 0 && r) atomicAdd(&cnt->active_v, r);
+  r = block_reduce(ae, s_red);
+  if (threadIdx.x == 0 && r) atomicAdd(&cnt->active_e, r);
+  r = block_reduce(ue, s_red);
+  if (threadIdx.x == 0 && r) atomicAdd(&cnt->unseen_e, r);
+}
+
+template <int W>
+__global__ void k_mbfs_seed(uint64_t *frontier, uint64_t *seen, const int *roots, int nsrc, int *levels, int64_t n) {
+  for (int s = threadIdx.x + blockIdx.x * blockDim.x; s < nsrc; s += blockDim.x * gridDim.x) {
+    const int64_t r = roots[s];
+    atomicOr((unsigned long long *)(frontier + r * W + (s >> 6)), 1ull << (s & 63));
+    atomicOr((unsigned long long *)(seen + r * W + (s >> 6)), 1ull << (s & 63));
+    levels[(int64_t)s * n + r] = 0;
+  }
+}
+
+template <int W>
+__global__ void __launch_bounds__(256) k_mbfs_reached(device_graph_t<CSR, Empty> g, const uint64_t *seen,
+                                                       mbfs_counters *cnt) {
+  __shared__ unsigned long long s_red[32];
+  unsigned long long s = 0;
+  for (int64_t v = threadIdx.x + (int64_t)blockIdx.x * blockDim.x; v < g.nvertexs; v += (int64_t)blockDim.x * gridDim.x) {
+    int pc = 0;
+#pragma unroll
+    for (int k = 0; k < W; ++k) pc += __popcll(seen[v * W + k]);
+    s += (unsigned long long)pc * __ldg(g.dg_odegree + v);
+  }
+  s = block_reduce(s, s_red);
+  if (threadIdx.x == 0 && s) atomicAdd(&cnt->reached_e, s);
+}
+
+template <typename T>
+__global__ void k_mbfs_fill(T *p, T v, int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) p[i] = v;
+}
+
+template <int W, typename Buf>
+mbfs_result mbfs_impl(device_graph_t<CSR, Empty> g, int nsrc, const int32_t *roots_host, Buf buf, int32_t *levels_host) {
+  mbfs_result res;
+  const int64_t n = g.nvertexs;
+  const int grid = sm_count() * 8;
+  uint64_t *frontier = (uint64_t *)buf("mb_front", sizeof(uint64_t) * n * W);
+  uint64_t *seen = (uint64_t *)buf("mb_seen", sizeof(uint64_t) * n * W);
+  uint64_t *next = (uint64_t *)buf("mb_next", sizeof(uint64_t) * n * W);
+  int *levels = (int *)buf("mb_levels", sizeof(int) * (size_t)n * nsrc);
+  int *roots = (int *)buf("mb_roots", sizeof(int) * nsrc);
+  uint64_t *valid = (uint64_t *)buf("mb_valid", sizeof(uint64_t) * W);
+  mbfs_counters *cnt = (mbfs_counters *)buf("mb_cnt", sizeof(mbfs_counters));
+  mbfs_counters *hcnt = nullptr;
+  if (!frontier || !seen || !next || !levels || !roots || !valid || !cnt) return res;
+  if (GSW_CUDA(cudaMallocHost((void **)&hcnt, sizeof(mbfs_counters)))) return res;
+  uint64_t hv[W];
+  for (int k = 0; k < W; ++k) {
+    const int lo = k * 64;
+    const int c = nsrc - lo >= 64 ? 64 : (nsrc - lo > 0 ? nsrc - lo : 0);
+    hv[k] = c == 64 ? ~0ull : ((1ull << c) - 1);
+  }
+  cudaStream_t s = stream();
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  GSW_CUDA(cudaMemcpyAsync(valid, hv, sizeof(hv), cudaMemcpyHostToDevice, s));
+  GSW_CUDA(cudaMemcpyAsync(roots, roots_host, sizeof(int) * nsrc, cudaMemcpyHostToDevice, s));
+  GSW_CUDA(cudaMemsetAsync(frontier, 0, sizeof(uint64_t) * n * W, s));
+  GSW_CUDA(cudaMemsetAsync(seen, 0, sizeof(uint64_t) * n * W, s));
+  GSW_CUDA(cudaMemsetAsync(next, 0, sizeof(uint64_t) * n * W, s));
+  k_mbfs_fill<int><<<grid, 256, 0, s>>>(levels, -1, n * (int64_t)nsrc);
+  cudaEventRecord(e0, s);
+  k_mbfs_seed<W><<<1, 256, 0, s>>>(frontier, seen, roots, nsrc, levels, n);
+  // the first level pushes from the sources
+  bool push = true;
+  for (int level = 1; level <= n + 1 && ok(); ++level) {
+    if (push)
+      k_mbfs_push<W><<<grid, 256, 0, s>>>(g, frontier, seen, next);
+    else
+      k_mbfs_pull<W><<<grid, 256, 0, s>>>(g, frontier, seen, next, valid);
+    GSW_CUDA(cudaMemsetAsync(cnt, 0, sizeof(mbfs_counters), s));
+    k_mbfs_update<W><<<grid, 256, 0, s>>>(g, frontier, seen, next, levels, nsrc, level, valid, cnt);
+    GSW_CUDA(cudaMemcpyAsync(hcnt, cnt, sizeof(mbfs_counters), cudaMemcpyDeviceToHost, s));
+    GSW_CUDA(cudaStreamSynchronize(s));
+    res.levels = level;
+    if (hcnt->active_v == 0) break;
+    // Beamer's direction test with alpha = 14
+    push = hcnt->active_e * 14 < hcnt->unseen_e;
+  }
+  cudaEventRecord(e1, s);
+  cudaEventSynchronize(e1);
+  float ms = 0;
+  cudaEventElapsedTime(&ms, e0, e1);
+  res.ms = ms;
+  GSW_CUDA(cudaMemsetAsync(cnt, 0, sizeof(mbfs_counters), s));
+  k_mbfs_reached<W><<<grid, 256, 0, s>>>(g, seen, cnt);
+  GSW_CUDA(cudaMemcpyAsync(hcnt, cnt, sizeof(mbfs_counters), cudaMemcpyDeviceToHost, s));
+  GSW_CUDA(cudaStreamSynchronize(s));
+  res.edges = (int64_t)(hcnt->reached_e / 2);
+  if (levels_host && ok())
+    GSW_CUDA(cudaMemcpyAsync(levels_host, levels, sizeof(int) * (size_t)n * nsrc, cudaMemcpyDeviceToHost, s));
+  GSW_CUDA(cudaStreamSynchronize(s));
+  cudaFreeHost(hcnt);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return res;
+}
+
+template <typename Buf>
+mbfs_result run_mbfs_batched(device_graph_t<CSR, Empty> g, int nsrc, const int32_t *roots, Buf buf,
+                             int32_t *levels_host) {
+  const int w = (nsrc + 63) / 64;
+  if (w <= 1) return mbfs_impl<1>(g, nsrc, roots, buf, levels_host);
+  if (w <= 2) return mbfs_impl<2>(g, nsrc, roots, buf, levels_host);
+  if (w <= 4) return mbfs_impl<4>(g, nsrc, roots, buf, levels_host);
+  if (w <= 8) return mbfs_impl<8>(g, nsrc, roots, buf, levels_host);
+  set_error(GSW_ERR_UNSUPPORTED, "%s", "mbfs: at most 512 sources per batch");
+  return mbfs_result();
+}
+
+}  // namespace gsw

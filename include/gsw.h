@@ -1,0 +1,163 @@
+/*
+ * gswitch-b200 C ABI (libgsw.so).
+ *
+ * The reference (PAA-NCIC/GSWITCH) is a header-only CUDA C++ template API with
+ * no foreign-function interface; its callers are the application mains in
+ * application/*.cu.  This ABI is the flat boundary underneath the
+ * reference-compatible headers: plain pointers and sizes, status codes, no
+ * C++ types.  Each declaration names the reference interface it replaces
+ * (paths inside the PAA-NCIC/GSWITCH tree).
+ *
+ * Conventions
+ *   - every call returns gsw_status (GSW_OK == 0); gsw_last_error_string()
+ *     describes the first failure of the calling thread since its last
+ *     successful call;
+ *   - a context owns one CUDA stream on one device; a context is not
+ *     thread-safe, distinct contexts may run concurrently;
+ *   - host arrays passed in are copied; host arrays passed out are written
+ *     in full before the call returns;
+ *   - graphs are undirected unless `directed` is set; CSR row offsets are
+ *     int64 (n + 1 entries), column ids int32, optional int32 arc weights.
+ */
+#ifndef GSW_H
+#define GSW_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int gsw_status;
+enum {
+  GSW_OK = 0,
+  GSW_ERR_INVALID_ARG = 1,
+  GSW_ERR_OOM = 2,
+  GSW_ERR_CUDA = 3,
+  GSW_ERR_TIMEOUT = 4,
+  GSW_ERR_OVERFLOW = 5,
+  GSW_ERR_UNSUPPORTED = 6,
+  GSW_ERR_NO_DEVICE = 7
+};
+
+typedef struct gsw_ctx gsw_ctx;
+typedef struct gsw_graph gsw_graph;
+
+/* Replaces parse_cmd's cudaSetDevice (src/utils/cmdline.cuh:164-232) and the
+ * global stream helper (src/utils/utils.cuh:238-245). */
+gsw_status gsw_init(int device, gsw_ctx **out);
+gsw_status gsw_destroy(gsw_ctx *ctx);
+/* Replaces the reference's exit()-on-error macros (src/utils/utils.cuh:61-87). */
+const char *gsw_last_error_string(void);
+/* ABI version, for loaders that check it. */
+int gsw_version(void);
+
+/* ---- graphs -------------------------------------------------------------
+ * Replaces build_graph<VC|EC> / device_graph_t<CSR,E>::build
+ * (src/data_structures/graph.cuh:149-215,268-280): upload a host CSR. */
+gsw_status gsw_graph_upload(gsw_ctx *ctx, int64_t n, int64_t m, const int64_t *row_off, const int32_t *col,
+                            const int32_t *weights, int directed, gsw_graph **out);
+/* Device-side generators (the reference reads .mtx files instead,
+ * src/utils/fileIO.cuh:73-146): RMAT (Graph500 a/b/c, no noise), 2D grid with
+ * long-range edges, G(n,m).  wmax > 0 adds symmetric weights in [1, wmax]
+ * drawn from wseed. */
+gsw_status gsw_graph_generate_rmat(gsw_ctx *ctx, int scale, int edge_factor, double a, double b, double c,
+                                   uint64_t seed, int wmax, uint64_t wseed, gsw_graph **out);
+gsw_status gsw_graph_generate_grid(gsw_ctx *ctx, int rows, int cols, int lr_div, uint64_t seed, int wmax,
+                                   uint64_t wseed, gsw_graph **out);
+gsw_status gsw_graph_generate_er(gsw_ctx *ctx, int64_t n, int64_t m_pairs, uint64_t seed, int wmax, uint64_t wseed,
+                                 gsw_graph **out);
+/* n, arcs, weighted flag */
+gsw_status gsw_graph_info(const gsw_graph *g, int64_t *n, int64_t *m, int *weighted);
+/* Degree statistics as graph_attr_t::fill (src/utils/fileIO.cuh:35-67):
+ * out[0..5] = avg, std, range, max, Gini, Hoover-like "Her". */
+gsw_status gsw_graph_attr(const gsw_graph *g, double *out6);
+/* Copy the CSR back to host arrays (weights may be NULL). */
+gsw_status gsw_graph_download(const gsw_graph *g, int64_t *row_off, int32_t *col, int32_t *weights);
+gsw_status gsw_graph_destroy(gsw_graph *g);
+/* `count` distinct seeded non-isolated vertices, the rule the reference's
+ * random_root follows (src/utils/fileIO.cuh:389-397) with a counter-based
+ * hash of (seed, draw) instead of random(). */
+gsw_status gsw_graph_roots(const gsw_graph *g, uint64_t seed, int count, int32_t *roots);
+/* The context's CUDA stream (cudaStream_t), for callers that time or order
+ * work around the library's launches. */
+gsw_status gsw_ctx_stream(gsw_ctx *ctx, void **stream);
+
+/* ---- level-loop configuration --------------------------------------------
+ * Replaces the -c Dir-Fmt-LB-Fusion override of src/utils/cmdline.cuh:51-94
+ * (any field may be left to the selector with -1). */
+enum { GSW_AUTO = -1 };
+enum { GSW_PUSH = 0, GSW_PULL = 1 };
+enum { GSW_QUEUE = 0, GSW_BITMAP = 1 };
+enum { GSW_LB_TM = 0, GSW_LB_WM = 1, GSW_LB_CM = 2, GSW_LB_STRICT = 3, GSW_LB_TWOD = 4, GSW_LB_TWC = 6 };
+enum { GSW_FUSED = 0, GSW_STANDALONE = 1 };
+enum { GSW_SELECT_RULES = 0, GSW_SELECT_MLP = 1 };
+
+typedef struct gsw_run_opts {
+  int direction;     /* GSW_AUTO / GSW_PUSH / GSW_PULL */
+  int asfmt;         /* GSW_AUTO / GSW_QUEUE / GSW_BITMAP */
+  int lb;            /* GSW_AUTO / GSW_LB_* */
+  int fusion;        /* GSW_AUTO / GSW_FUSED / GSW_STANDALONE */
+  int sorted_queue;  /* 1: bitmap->queue in vertex order, 0: atomic append */
+  int max_iters;     /* PageRank: iterations (0 = until the eps test passes) */
+  float damping;     /* PageRank damping (0.85) */
+  float eps;         /* PageRank per-vertex relative change threshold */
+  int selector;      /* GSW_SELECT_RULES or GSW_SELECT_MLP */
+  int verbose;       /* per-level trace on stdout */
+  int timing;        /* per-level device times into gsw_run_stats (CUDA
+                        events around each inspect / expand, resolved after
+                        the run: no extra synchronisation) */
+  int expand_grid;   /* >0: fixed expand grid (autotuner) */
+  int account;       /* 1: count the edges each expand touches (with timing,
+                        for roofline accounting; adds one atomic per thread) */
+  int reserved[7];
+} gsw_run_opts;
+
+void gsw_run_opts_default(gsw_run_opts *o);
+
+#define GSW_MAX_TRACE 4096
+typedef struct gsw_run_stats {
+  double ms;               /* device time of the whole level loop */
+  int levels;              /* expand steps executed */
+  int64_t edges;           /* Graph500 traversed-edge count where defined */
+  unsigned device_error;   /* DEV_ERR bits seen by kernels (0 = clean) */
+  int64_t launches;        /* kernels launched by the run */
+  int ntrace;              /* entries in the per-level trace below */
+  /* per level: dir | fmt<<1 | lb<<2 | fused<<5 | persistent<<6 */
+  int32_t level_cfg[GSW_MAX_TRACE];
+  int64_t level_frontier[GSW_MAX_TRACE];
+  float level_ms[GSW_MAX_TRACE];         /* expand time, with opts.timing */
+  float level_inspect_ms[GSW_MAX_TRACE]; /* inspection time, with opts.timing */
+  int64_t level_edges[GSW_MAX_TRACE];    /* edges touched, with opts.account */
+} gsw_run_stats;
+
+/* ---- applications ----------------------------------------------------------
+ * Each runs the inspect -> select -> filter -> expand loop of the reference
+ * application with the same operator semantics and returns the result to a
+ * host array (NULL: leave it on the device).
+ *   BFS  application/bfs.cu:16-102     levels (-1 unreached)
+ *   SSSP application/sssp.cu:17-126    distances (INT32_MAX unreached)
+ *   CC   application/cc.cu:15-289      component labels (min vertex id)
+ *   PR   application/pagerank.cu:18-103 pr/out-degree (pr for sinks)
+ *   BC   application/bc.cu:31-309      path counts and dependencies
+ *   GC   application/gc.cu:15-99       colours
+ *   MBFS application/mbfs.cu:16-246    levels per source (row-major)  */
+gsw_status gsw_bfs(gsw_ctx *ctx, gsw_graph *g, int32_t root, const gsw_run_opts *o, int32_t *levels,
+                   gsw_run_stats *st);
+gsw_status gsw_sssp(gsw_ctx *ctx, gsw_graph *g, int32_t root, const gsw_run_opts *o, int32_t *dist,
+                    gsw_run_stats *st);
+gsw_status gsw_cc(gsw_ctx *ctx, gsw_graph *g, const gsw_run_opts *o, int32_t *labels, gsw_run_stats *st);
+gsw_status gsw_pagerank(gsw_ctx *ctx, gsw_graph *g, const gsw_run_opts *o, float *pr_over_od, gsw_run_stats *st);
+gsw_status gsw_bc(gsw_ctx *ctx, gsw_graph *g, int32_t root, const gsw_run_opts *o, int32_t *nsp, float *dep,
+                  gsw_run_stats *st);
+gsw_status gsw_gc(gsw_ctx *ctx, gsw_graph *g, const gsw_run_opts *o, int32_t *colors, gsw_run_stats *st);
+/* Multi-source BFS.  batched = 0 runs the single-source loop per source
+ * (as application/mbfs.cu does); batched = 1 runs all sources together with
+ * bit-sliced frontiers (64 sources per word) in one launch sequence. */
+gsw_status gsw_mbfs(gsw_ctx *ctx, gsw_graph *g, int nsrc, const int32_t *roots, int batched, const gsw_run_opts *o,
+                    int32_t *levels, gsw_run_stats *st);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GSW_H */

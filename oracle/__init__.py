@@ -72,6 +72,7 @@ def lib():
     L.or_pagerank_check.argtypes = [i64, I64P, I32P, F32P, C.c_float, C.c_float]
     L.or_gc_check.restype = i64
     L.or_gc_check.argtypes = [i64, I64P, I32P, I32P]
+    L.or_gc_levels.argtypes = [i64, I64P, I32P, I32P]
     L.or_mbfs.argtypes = [i64, I64P, I32P, C.c_int, I32P, I32P]
     L.or_degree_attr.argtypes = [i64, I64P, F64P]
     L.or_traversed_edges.restype = i64
@@ -208,6 +209,12 @@ def pagerank_check(g: Csr, pr_over_od, damp=0.85, eps=0.01) -> int:
 def gc_check(g: Csr, color) -> int:
     col = np.ascontiguousarray(color, dtype=np.int32)
     return int(lib().or_gc_check(g.n, g.off, g.col, col))
+
+
+def gc_levels(g: Csr):
+    out = np.empty(g.n, dtype=np.int32)
+    lib().or_gc_levels(g.n, g.off, g.col, out)
+    return out
 
 
 def mbfs(g: Csr, srcs):

@@ -9,8 +9,50 @@
 
 #include <limits.h>
 #include <math.h>
+#include <pthread.h>
 #include <stdlib.h>
 #include <string.h>
+#include <unistd.h>
+
+/* ------------------------------------------------------------------------ */
+/* minimal parallel-for over [0, n) in chunks (pthreads; the generators and  */
+/* the CSR build use it, the validators stay sequential like the reference)  */
+/* ------------------------------------------------------------------------ */
+typedef void (*range_fn)(int64_t lo, int64_t hi, void *arg);
+typedef struct {
+  range_fn fn;
+  void *arg;
+  int64_t n, chunk;
+  int64_t next;
+} pfor_t;
+
+static void *pfor_worker(void *p) {
+  pfor_t *w = (pfor_t *)p;
+  for (;;) {
+    int64_t lo = __atomic_fetch_add(&w->next, w->chunk, __ATOMIC_RELAXED);
+    if (lo >= w->n) break;
+    int64_t hi = lo + w->chunk < w->n ? lo + w->chunk : w->n;
+    w->fn(lo, hi, w->arg);
+  }
+  return NULL;
+}
+
+static void parallel_for(int64_t n, int64_t chunk, range_fn fn, void *arg) {
+  long nt = sysconf(_SC_NPROCESSORS_ONLN);
+  if (nt < 1) nt = 1;
+  if (nt > 256) nt = 256;
+  if (n <= chunk || nt == 1) {
+    fn(0, n, arg);
+    return;
+  }
+  pfor_t w = {fn, arg, n, chunk, 0};
+  pthread_t th[256];
+  long started = 0;
+  for (long t = 1; t < nt; ++t)
+    if (pthread_create(&th[started], NULL, pfor_worker, &w) == 0) ++started;
+  pfor_worker(&w);
+  for (long t = 0; t < started; ++t) pthread_join(th[t], NULL);
+}
 
 /* ------------------------------------------------------------------------ */
 /* counter-based hashing (SplitMix64 finaliser, Steele/Lea/Flood 2014)        */
@@ -30,22 +72,20 @@ enum { ST_RMAT = 1, ST_W = 2, ST_GRID = 3, ST_ER = 4, ST_ERB = 5, ST_ROOT = 7 };
 
 void or_free(void *p) { free(p); }
 
-/* Graph500-style recursive quadrant choice, no noise, no permutation.
- * Level l fixes bit (scale-1-l) of (src, dst); 32 random bits per level,
- * compared against integer thresholds so every platform picks the same
- * quadrant. */
-void or_rmat_edges(int scale, int ef, double a, double b, double c,
-                   uint64_t seed, uint32_t *src, uint32_t *dst) {
-  const uint64_t key = or_stream_key(seed, ST_RMAT);
-  const uint32_t ta = (uint32_t)(a * 4294967296.0);
-  const uint32_t tab = (uint32_t)((a + b) * 4294967296.0);
-  const uint32_t tabc = (uint32_t)((a + b + c) * 4294967296.0);
-  const int64_t ne = (int64_t)ef << scale;
-  for (int64_t i = 0; i < ne; ++i) {
-    uint64_t base = or_sm64(key + (uint64_t)i);
+typedef struct {
+  int scale;
+  uint64_t key;
+  uint32_t ta, tab, tabc;
+  uint32_t *src, *dst;
+} rmat_job;
+
+static void rmat_range(int64_t lo, int64_t hi, void *p) {
+  const rmat_job *j = (const rmat_job *)p;
+  for (int64_t i = lo; i < hi; ++i) {
+    uint64_t base = or_sm64(j->key + (uint64_t)i);
     uint32_t s = 0, d = 0;
     uint64_t h = 0;
-    for (int l = 0; l < scale; ++l) {
+    for (int l = 0; l < j->scale; ++l) {
       uint32_t r;
       if ((l & 1) == 0) {
         h = or_sm64(base + (uint64_t)(l >> 1));
@@ -53,20 +93,37 @@ void or_rmat_edges(int scale, int ef, double a, double b, double c,
       } else {
         r = (uint32_t)(h >> 32);
       }
-      const uint32_t bit = 1u << (scale - 1 - l);
-      if (r < ta) {
-      } else if (r < tab) {
+      const uint32_t bit = 1u << (j->scale - 1 - l);
+      if (r < j->ta) {
+      } else if (r < j->tab) {
         d |= bit;
-      } else if (r < tabc) {
+      } else if (r < j->tabc) {
         s |= bit;
       } else {
         s |= bit;
         d |= bit;
       }
     }
-    src[i] = s;
-    dst[i] = d;
+    j->src[i] = s;
+    j->dst[i] = d;
   }
+}
+
+/* Graph500-style recursive quadrant choice, no noise, no permutation.
+ * Level l fixes bit (scale-1-l) of (src, dst); 32 random bits per level,
+ * compared against integer thresholds so every platform picks the same
+ * quadrant. */
+void or_rmat_edges(int scale, int ef, double a, double b, double c,
+                   uint64_t seed, uint32_t *src, uint32_t *dst) {
+  rmat_job j;
+  j.scale = scale;
+  j.key = or_stream_key(seed, ST_RMAT);
+  j.ta = (uint32_t)(a * 4294967296.0);
+  j.tab = (uint32_t)((a + b) * 4294967296.0);
+  j.tabc = (uint32_t)((a + b + c) * 4294967296.0);
+  j.src = src;
+  j.dst = dst;
+  parallel_for((int64_t)ef << scale, 1 << 16, rmat_range, &j);
 }
 
 int64_t or_grid_nedges(int rows, int cols, int lr_div) {
@@ -130,55 +187,81 @@ void or_er_batch_params(uint64_t seed, int64_t i, int64_t nlo, int64_t nhi,
   *iseed = or_sm64(key + 3 * (uint64_t)i + 2);
 }
 
-/* LSD radix sort of 64-bit keys, 16-bit digits, constant digits skipped. */
-static void radix_sort_u64(uint64_t *a, uint64_t *tmp, int64_t len) {
-  int64_t *cnt = (int64_t *)malloc(sizeof(int64_t) * 65536);
-  for (int pass = 0; pass < 4; ++pass) {
-    const int sh = pass * 16;
-    memset(cnt, 0, sizeof(int64_t) * 65536);
-    for (int64_t i = 0; i < len; ++i) cnt[(a[i] >> sh) & 0xFFFF]++;
-    int nonzero = 0;
-    for (int d = 0; d < 65536; ++d) nonzero += cnt[d] != 0;
-    if (nonzero <= 1) continue;
-    int64_t s = 0;
-    for (int d = 0; d < 65536; ++d) {
-      int64_t t = cnt[d];
-      cnt[d] = s;
-      s += t;
-    }
-    for (int64_t i = 0; i < len; ++i) tmp[cnt[(a[i] >> sh) & 0xFFFF]++] = a[i];
-    memcpy(a, tmp, sizeof(uint64_t) * (size_t)len);
-  }
-  free(cnt);
+static int cmp_i32(const void *a, const void *b) {
+  int32_t x = *(const int32_t *)a, y = *(const int32_t *)b;
+  return (x > y) - (x < y);
 }
 
+typedef struct {
+  const uint32_t *src, *dst;
+  int64_t *cnt, *cur, *uniq, *off;
+  int32_t *tmp, *col;
+} csr_job;
+
+static void csr_count(int64_t lo, int64_t hi, void *p) {
+  csr_job *j = (csr_job *)p;
+  for (int64_t i = lo; i < hi; ++i) {
+    if (j->src[i] == j->dst[i]) continue;
+    __atomic_fetch_add(&j->cnt[j->src[i] + 1], 1, __ATOMIC_RELAXED);
+    __atomic_fetch_add(&j->cnt[j->dst[i] + 1], 1, __ATOMIC_RELAXED);
+  }
+}
+static void csr_scatter(int64_t lo, int64_t hi, void *p) {
+  csr_job *j = (csr_job *)p;
+  for (int64_t i = lo; i < hi; ++i) {
+    if (j->src[i] == j->dst[i]) continue;
+    j->tmp[__atomic_fetch_add(&j->cur[j->src[i]], 1, __ATOMIC_RELAXED)] = (int32_t)j->dst[i];
+    j->tmp[__atomic_fetch_add(&j->cur[j->dst[i]], 1, __ATOMIC_RELAXED)] = (int32_t)j->src[i];
+  }
+}
+static void csr_sort(int64_t lo, int64_t hi, void *p) {
+  csr_job *j = (csr_job *)p;
+  for (int64_t v = lo; v < hi; ++v) {
+    int32_t *a = j->tmp + j->cnt[v];
+    const int64_t len = j->cnt[v + 1] - j->cnt[v];
+    if (len > 1) qsort(a, (size_t)len, sizeof(int32_t), cmp_i32);
+    int64_t u = 0;
+    for (int64_t k = 0; k < len; ++k)
+      if (k == 0 || a[k] != a[k - 1]) a[u++] = a[k];
+    j->uniq[v] = u;
+  }
+}
+static void csr_compact(int64_t lo, int64_t hi, void *p) {
+  csr_job *j = (csr_job *)p;
+  for (int64_t v = lo; v < hi; ++v)
+    memcpy(j->col + j->off[v], j->tmp + j->cnt[v], sizeof(int32_t) * (size_t)j->uniq[v]);
+}
+
+/* Counting build, parallel over pairs and vertices, deterministic: scatter
+ * both directions of every non-loop pair, sort and de-duplicate each
+ * adjacency, compact. */
 int64_t or_csr_build(int64_t n, int64_t npairs, const uint32_t *src,
                      const uint32_t *dst, int64_t **off_out,
                      int32_t **col_out) {
-  uint64_t *keys = (uint64_t *)malloc(sizeof(uint64_t) * (size_t)(2 * npairs + 1));
-  int64_t k = 0;
-  for (int64_t i = 0; i < npairs; ++i) {
-    uint64_t s = src[i], d = dst[i];
-    if (s == d) continue;
-    keys[k++] = (s << 32) | d;
-    keys[k++] = (d << 32) | s;
-  }
-  uint64_t *tmp = (uint64_t *)malloc(sizeof(uint64_t) * (size_t)(k + 1));
-  radix_sort_u64(keys, tmp, k);
-  free(tmp);
-  int64_t m = 0;
-  for (int64_t i = 0; i < k; ++i)
-    if (i == 0 || keys[i] != keys[i - 1]) keys[m++] = keys[i];
-  int64_t *off = (int64_t *)calloc((size_t)n + 1, sizeof(int64_t));
-  int32_t *col = (int32_t *)malloc(sizeof(int32_t) * (size_t)(m + 1));
-  for (int64_t i = 0; i < m; ++i) {
-    off[(keys[i] >> 32) + 1]++;
-    col[i] = (int32_t)(keys[i] & 0xFFFFFFFFu);
-  }
-  for (int64_t v = 0; v < n; ++v) off[v + 1] += off[v];
-  free(keys);
-  *off_out = off;
-  *col_out = col;
+  csr_job j;
+  j.src = src;
+  j.dst = dst;
+  j.cnt = (int64_t *)calloc((size_t)n + 1, sizeof(int64_t));
+  parallel_for(npairs, 1 << 16, csr_count, &j);
+  for (int64_t v = 0; v < n; ++v) j.cnt[v + 1] += j.cnt[v];
+  const int64_t k = j.cnt[n];
+  j.tmp = (int32_t *)malloc(sizeof(int32_t) * (size_t)(k + 1));
+  j.cur = (int64_t *)malloc(sizeof(int64_t) * (size_t)(n + 1));
+  memcpy(j.cur, j.cnt, sizeof(int64_t) * (size_t)(n + 1));
+  parallel_for(npairs, 1 << 16, csr_scatter, &j);
+  j.uniq = j.cur; /* reused */
+  parallel_for(n, 1024, csr_sort, &j);
+  j.off = (int64_t *)malloc(sizeof(int64_t) * (size_t)(n + 1));
+  j.off[0] = 0;
+  for (int64_t v = 0; v < n; ++v) j.off[v + 1] = j.off[v] + j.uniq[v];
+  const int64_t m = j.off[n];
+  j.col = (int32_t *)malloc(sizeof(int32_t) * (size_t)(m + 1));
+  parallel_for(n, 1024, csr_compact, &j);
+  free(j.tmp);
+  free(j.cur);
+  free(j.cnt);
+  *off_out = j.off;
+  *col_out = j.col;
   return m;
 }
 
@@ -478,6 +561,41 @@ int64_t or_gc_check(int64_t n, const int64_t *off, const int32_t *col,
     }
   }
   return -1;
+}
+
+/* The colouring application/gc.cu:15-43 computes when its functor runs in the
+ * level loop: in the first expand every vertex sends its id to every
+ * neighbour; at level L an uncoloured vertex whose id exceeds the largest
+ * id it received takes colour L, the others clear their maximum and send
+ * their id again.  Deterministic, so GPU colours compare bit for bit. */
+void or_gc_levels(int64_t n, const int64_t *off, const int32_t *col, int32_t *color) {
+  int32_t *maxid = (int32_t *)malloc(sizeof(int32_t) * (size_t)n);
+  char *active = (char *)malloc((size_t)n);
+  for (int64_t v = 0; v < n; ++v) { color[v] = -1; maxid[v] = -1; }
+  for (int64_t v = 0; v < n; ++v)
+    for (int64_t j = off[v]; j < off[v + 1]; ++j)
+      if ((int32_t)v > maxid[col[j]]) maxid[col[j]] = (int32_t)v;
+  for (int32_t level = 1;; ++level) {
+    int any = 0;
+    for (int64_t v = 0; v < n; ++v) {
+      active[v] = 0;
+      if (color[v] != -1) continue;
+      if (maxid[v] < v) {
+        color[v] = level;
+      } else {
+        maxid[v] = -1;
+        active[v] = 1;
+        any = 1;
+      }
+    }
+    if (!any) break;
+    for (int64_t v = 0; v < n; ++v)
+      if (active[v])
+        for (int64_t j = off[v]; j < off[v + 1]; ++j)
+          if ((int32_t)v > maxid[col[j]]) maxid[col[j]] = (int32_t)v;
+  }
+  free(maxid);
+  free(active);
 }
 
 void or_mbfs(int64_t n, const int64_t *off, const int32_t *col, int nsrc,

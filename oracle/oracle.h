@@ -81,6 +81,7 @@ int64_t or_pagerank_check(int64_t n, const int64_t *off, const int32_t *col,
                           const float *pr_over_od, float damp, float eps);
 int64_t or_gc_check(int64_t n, const int64_t *off, const int32_t *col,
                     const int32_t *color);
+void or_gc_levels(int64_t n, const int64_t *off, const int32_t *col, int32_t *color);
 void or_mbfs(int64_t n, const int64_t *off, const int32_t *col, int nsrc,
              const int32_t *roots, int32_t *lvl /* nsrc*n */);
 /* degree statistics as graph_attr_t::fill: out[0..5] = avg, std, range,

@@ -10,7 +10,9 @@
 // int64 off[n+1], int32 col[m], int32 w[m] if has_w.  The arcs are fed to the
 // reference's edgelist_t/host_graph_t as a directed list in CSR order with
 // quiet=true, so its host CSR is exactly the file's CSR (no rinse/renumber).
+#include <chrono>
 #include <cstdint>
+#include <string>
 #include <cstdio>
 #include <cstdlib>
 #include <vector>
@@ -104,6 +106,27 @@ int main(int argc, char **argv) {
   edgelist_t<Empty> el = gsw_to_edgelist<Empty>(fg);
   host_graph_t<CSR, Empty> hg;
   hg.build(el, true);
+  if (argc > 4 && std::string(argv[3]) == "--bench") {
+    // timed mode: the reference's bfs_cpu from every root in argv[4]
+    // (int32 list); one line per root: root, milliseconds, traversed edges
+    std::vector<int> roots;
+    FILE *rf = fopen(argv[4], "rb");
+    int r;
+    while (rf && fread(&r, 4, 1, rf) == 1) roots.push_back(r);
+    if (rf) fclose(rf);
+    for (int root : roots) {
+      auto t0 = std::chrono::steady_clock::now();
+      int *lv = bfs_cpu(hg, root);
+      auto t1 = std::chrono::steady_clock::now();
+      long long te = 0;
+      for (int64_t v = 0; v < fg.n; ++v)
+        if (lv[v] >= 0) te += fg.off[v + 1] - fg.off[v];
+      printf("%d %.6f %lld\n", root, std::chrono::duration<double, std::milli>(t1 - t0).count(), te / 2);
+      fflush(stdout);
+      free(lv);
+    }
+    return 0;
+  }
   int *lvl = bfs_cpu(hg, fg.root);
   gsw_write(argv[2], lvl, fg.n);
   // graph statistics the selector features are built from
