@@ -176,13 +176,23 @@ class Context:
     """One device and one stream (gsw_init / gsw_destroy)."""
 
     def __init__(self, device: int = 0):
+        import weakref
+
         self._h = C.c_void_p()
+        self._graphs = weakref.WeakSet()
         _check(lib().gsw_init(device, C.byref(self._h)))
 
     def close(self):
+        # graphs belong to the context: release them first
+        for g in list(self._graphs):
+            g.close()
         if self._h:
             lib().gsw_destroy(self._h)
             self._h = C.c_void_p()
+
+    @property
+    def alive(self) -> bool:
+        return bool(self._h)
 
     def stream_ptr(self) -> int:
         s = C.c_void_p()
@@ -225,14 +235,15 @@ class Graph:
 
     def __init__(self, ctx: Context, h):
         self.ctx, self._h = ctx, h
+        ctx._graphs.add(self)
         n, m, wt = C.c_int64(), C.c_int64(), C.c_int()
         _check(lib().gsw_graph_info(h, C.byref(n), C.byref(m), C.byref(wt)))
         self.n, self.m, self.weighted = n.value, m.value, bool(wt.value)
 
     def close(self):
-        if self._h:
+        if self._h and self.ctx.alive:
             lib().gsw_graph_destroy(self._h)
-            self._h = None
+        self._h = None
 
     def __del__(self):
         try:

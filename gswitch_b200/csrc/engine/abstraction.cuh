@@ -296,7 +296,7 @@ struct stat_t {
   int level = 0;
   int64_t last_scanned = 0;  // edges the last expand touched (accounting)
 
-  void build(int _size = 8) {
+  void build(int _size = gsw::STAT_SLOTS) {
     if (dg_runtime_info) return;
     size = _size;
     GSW_CUDA(cudaMalloc((void **)&dg_runtime_info, size * sizeof(unsigned long long)));
@@ -439,8 +439,12 @@ struct feature_t {
 
   void architecture_features(int device = -1) {
     if (device < 0) cudaGetDevice(&device);
-    cudaDeviceProp prop;
-    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return;
+    static thread_local int cached_dev = -1;
+    static thread_local cudaDeviceProp prop;
+    if (cached_dev != device) {
+      if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return;
+      cached_dev = device;
+    }
     cap = prop.minor;
     while (cap > 1) cap /= 10;
     cap += prop.major;

@@ -58,6 +58,10 @@ namespace gsw {
 
 // status codes are the C ABI's (GSW_OK, GSW_ERR_*), include/gsw.h
 
+// slots of the inspector's statistics block (six counters, a completion
+// counter, a spare, and 2 x 256 per-virtual-block partial sums)
+constexpr int STAT_SLOTS = 8 + 2 * 256;
+
 // Device error word bits, written by kernels and read by the host.
 enum device_error_bits : unsigned {
   DEV_ERR_QUEUE_OVERFLOW = 1u,

@@ -148,7 +148,7 @@ struct inspector_t {
     }
     marks().insp0 = marks().insp1 = -1;
     if (opts().timing) marks().insp0 = timing_pool().record();
-    k_inspect_ec<<<INSPECT_CTAS, INSPECT_THREADS, 0, stream()>>>(as, g, f, stat.dg_runtime_info);
+    k_inspect_ec<<<EC_INSPECT_CTAS, EC_INSPECT_THREADS, 0, stream()>>>(as, g, f, stat.dg_runtime_info);
     GSW_LAUNCHED();
     if (opts().timing) marks().insp1 = timing_pool().record();
     set_fets(as, stat, fets, conf, g.nvertexs, g.nedges);
@@ -720,14 +720,16 @@ int64_t root_degree(const device_graph_t<COO, E> &, int) {
 
 template <typename G, typename F>
 void init_conf_impl(stat_t &stats, feature_t &fets, config_t &conf, G &dg, F &f, double mean_weight,
-                    double avg_deg_attr, bool reset_only) {
+                    double avg_deg_attr, bool reset_only, int64_t known_root_degree = -1) {
   if (reset_only)
     conf.reset();
   else
     stats.build();
   fets.architecture_features();
   conf.conf_inherit = false;
-  if (fets.use_root >= 0) fets.first_workload = (double)root_degree(dg, fets.use_root);
+  if (fets.use_root >= 0)
+    fets.first_workload =
+        (double)(known_root_degree >= 0 ? known_root_degree : root_degree(dg, fets.use_root));
   if (fets.centric == VC) {
     fets.flatten();
     double v[5];

@@ -137,6 +137,7 @@ struct queue_t {
   // reserve cnt consecutive slots (warp-aggregated enqueue); returns -1 on
   // overflow after recording it
   __device__ __forceinline__ int64_t reserve(int cnt) {
+    if (mode == Cached && traceback) return -1;
     int idx = atomicAdd(output_size(), cnt);
     if ((int64_t)idx + cnt > output_cap()) {
       atomicOr(dg_err, DEV_ERR_QUEUE_OVERFLOW);
@@ -176,9 +177,16 @@ struct queue_t {
       clean_size(cursor);
       cursor ^= 1;
     } else if (traceback) {
-      cursor--;
-      offset_in -= get_qsize_host();
+      if (cursor > 0) {
+        cursor--;
+        offset_in -= get_qsize_host();
+      }
     } else {
+      // one size slot per level; a chain of n vertices has n levels
+      if (cursor + 2 >= subqueue[1].max_size) {
+        set_error(GSW_ERR_OVERFLOW, "%s", "cached queue: more levels than size slots");
+        return;
+      }
       cursor++;
       offset_in = offset_out;
       offset_out += get_qsize_host();
@@ -279,13 +287,15 @@ inline int active_set_t::build(int64_t _size, QueueMode qmode) {
   }
   queue.mode = qmode;
   queue.dg_err = &dg_cnt->err;
+  // Cached mode keeps the per-level sizes in subqueue[1]: levels <= n, plus
+  // the empty level that ends the loop, plus headroom
   for (int i = 0; i < 2; ++i) {
-    queue.subqueue[i].max_size = size + 1;
-    if (alloc((void **)&queue.subqueue[i].dg_queue, sizeof(int) * (size + 1))) return err().code;
+    queue.subqueue[i].max_size = size + 8;
+    if (alloc((void **)&queue.subqueue[i].dg_queue, sizeof(int) * (size + 8))) return err().code;
     queue.subqueue[i].dg_qsize = &dg_cnt->qsize[i];
   }
   if (qmode == Cached)
-    GSW_CUDA(cudaMemsetAsync(queue.subqueue[1].dg_queue, 0, sizeof(int) * (size + 1), stream()));
+    GSW_CUDA(cudaMemsetAsync(queue.subqueue[1].dg_queue, 0, sizeof(int) * (size + 8), stream()));
   workset.cap = size + 1;
   if (alloc((void **)&workset.dg_eoff, sizeof(int64_t) * (size + 2))) return err().code;
   workset.bsum_cap = (size + 1) / 1024 + 4096;

@@ -61,6 +61,7 @@ __device__ __forceinline__ bool push_edge_fused(active_set_t &as, const G &g, F 
 
 // full-warp aggregated enqueue; every lane of the warp must call it
 __device__ __forceinline__ void warp_enqueue(active_set_t &as, bool tp, int u) {
+  if (as.queue.mode == Cached && as.queue.traceback) return;  // replay: nothing is enqueued
   const unsigned m = __ballot_sync(FULL, tp);
   if (!m) return;
   const int leader = __ffs(m) - 1;

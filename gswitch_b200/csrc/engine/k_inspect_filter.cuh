@@ -18,44 +18,71 @@
 
 namespace gsw {
 
-constexpr int INSPECT_CTAS = 256;
-constexpr int INSPECT_THREADS = 512;
+// The statistics block: [0..5] the counters above, [6] blocks finished,
+// [8..8+256) and [264..264+256) the per-virtual-block sums of the two
+// max-degree counters.
+constexpr int INSPECT_VTHREADS = 256 * 512;  // the reference's grid, one virtual thread each
+constexpr int INSPECT_VBLOCK = 512;          // virtual threads per virtual block
+constexpr int INSPECT_THREADS = 128;         // physical block: a quarter virtual block
+constexpr int INSPECT_CTAS = INSPECT_VTHREADS / INSPECT_THREADS;
+constexpr int INSPECT_UNROLL = 4;
+static_assert(STAT_SLOTS == 8 + 2 * (INSPECT_VTHREADS / INSPECT_VBLOCK), "statistics block layout");
+constexpr int EC_INSPECT_CTAS = 256;
+constexpr int EC_INSPECT_THREADS = 512;
 
+// Virtual thread t (0 <= t < 131072) visits vertices t, t + 131072, ...
+// exactly as thread t of the reference's 256 x 512 grid-stride launch, so the
+// max-degree counters are the reference's.  Physical blocks of 128 threads
+// (a quarter of a virtual block) fill all SMs evenly, each thread keeps four
+// vertices in flight, and the last block to finish folds the per-virtual-
+// block sums (max over blocks for push, sum for pull).
 template <typename G, typename F>
 __global__ void __launch_bounds__(INSPECT_THREADS) k_inspect_vc(active_set_t as, G g, F f,
                                                                  unsigned long long *info) {
   __shared__ unsigned long long s_red[32];
-  const int64_t STRIDE = (int64_t)blockDim.x * gridDim.x;
-  const int64_t gtid = threadIdx.x + (int64_t)blockIdx.x * blockDim.x;
+  __shared__ bool s_last;
+  const int64_t S = INSPECT_VTHREADS;
+  const int64_t t = threadIdx.x + (int64_t)blockIdx.x * blockDim.x;
   const int lane = lane_id();
   const int64_t n = as.size;
   unsigned long long active_num = 0, inactive_num = 0, push_wl = 0, pull_wl = 0;
   unsigned long long max_push = 0, max_pull = 0;
-  for (int64_t idx = gtid; idx - lane < n; idx += STRIDE) {
-    const bool valid = idx < n;
-    Status s = Inactive;
-    int od = 0;
-    if (valid) {
-      od = __ldg(g.dg_odegree + idx);
-      s = f.filter((int)idx, g);
+  for (int64_t base = t; base - lane < n; base += INSPECT_UNROLL * S) {
+    Status st[INSPECT_UNROLL];
+    int od[INSPECT_UNROLL];
+#pragma unroll
+    for (int k = 0; k < INSPECT_UNROLL; ++k) {
+      const int64_t idx = base + k * S;
+      od[k] = idx < n ? __ldg(g.dg_odegree + idx) : 0;
     }
-    const bool tag_active = valid && s == Active;
-    const bool tag_inactive = valid && s != Inactive;  // 0 only for Inactive
-    const unsigned aw = __ballot_sync(FULL, tag_active);
-    const unsigned iw = __ballot_sync(FULL, tag_inactive);
-    if (lane == 0) {
-      as.bitmap.active.dg_bits[idx >> 5] = aw;
-      as.bitmap.inactive.dg_bits[idx >> 5] = iw;
+#pragma unroll
+    for (int k = 0; k < INSPECT_UNROLL; ++k) {
+      const int64_t idx = base + k * S;
+      st[k] = idx < n ? f.filter((int)idx, g) : Inactive;
     }
-    if (tag_active) {
-      active_num++;
-      push_wl += od;
-      max_push = MAX(max_push, (unsigned long long)od);
-    }
-    if (valid && !tag_inactive) {
-      inactive_num++;
-      pull_wl += od;
-      max_pull = MAX(max_pull, (unsigned long long)od);
+#pragma unroll
+    for (int k = 0; k < INSPECT_UNROLL; ++k) {
+      const int64_t idx = base + k * S;
+      if (idx - lane >= n) break;  // warp-uniform
+      const bool valid = idx < n;
+      const bool tag_active = valid && st[k] == Active;
+      const bool tag_inactive = valid && st[k] != Inactive;  // 0 only for Inactive
+      const unsigned aw = __ballot_sync(FULL, tag_active);
+      const unsigned iw = __ballot_sync(FULL, tag_inactive);
+      if (lane == 0) {
+        as.bitmap.active.dg_bits[idx >> 5] = aw;
+        as.bitmap.inactive.dg_bits[idx >> 5] = iw;
+      }
+      if (tag_active) {
+        active_num++;
+        push_wl += od[k];
+        max_push = MAX(max_push, (unsigned long long)od[k]);
+      }
+      if (valid && !tag_inactive) {
+        inactive_num++;
+        pull_wl += od[k];
+        max_pull = MAX(max_pull, (unsigned long long)od[k]);
+      }
     }
   }
   unsigned long long r;
@@ -67,16 +94,38 @@ __global__ void __launch_bounds__(INSPECT_THREADS) k_inspect_vc(active_set_t as,
   if (threadIdx.x == 0 && r) atomicAdd(info + 2, r);
   r = block_reduce(pull_wl, s_red);
   if (threadIdx.x == 0 && r) atomicAdd(info + 3, r);
+  const int vb = (int)(t / INSPECT_VBLOCK);
+  const int NVB = INSPECT_VTHREADS / INSPECT_VBLOCK;
   r = block_reduce(max_push, s_red);
-  if (threadIdx.x == 0) atomicMax(info + 4, r);
+  if (threadIdx.x == 0 && r) atomicAdd(info + 8 + vb, r);
   r = block_reduce(max_pull, s_red);
-  if (threadIdx.x == 0 && r) atomicAdd(info + 5, r);
+  if (threadIdx.x == 0 && r) atomicAdd(info + 8 + NVB + vb, r);
+  if (threadIdx.x == 0) {
+    __threadfence();
+    s_last = atomicAdd(info + 6, 1ull) == (unsigned long long)gridDim.x - 1;
+  }
+  __syncthreads();
+  if (s_last) {  // last block: fold the virtual-block sums
+    __threadfence();
+    unsigned long long mp = 0, sp = 0;
+    for (int i = threadIdx.x; i < NVB; i += blockDim.x) {
+      const unsigned long long a = ((volatile unsigned long long *)info)[8 + i];
+      mp = MAX(mp, a);
+      sp += ((volatile unsigned long long *)info)[8 + NVB + i];
+    }
+    mp = block_reduce<unsigned long long, true>(mp, s_red);
+    sp = block_reduce(sp, s_red);
+    if (threadIdx.x == 0) {
+      info[4] = mp;
+      info[5] = sp;
+    }
+  }
 }
 
 // EC: the active set ranges over edges (inspector.cuh:10-37).  An edge stays
 // active while it was active and f.filter still reports Active.
 template <typename G, typename F>
-__global__ void __launch_bounds__(INSPECT_THREADS) k_inspect_ec(active_set_t as, G g, F f,
+__global__ void __launch_bounds__(EC_INSPECT_THREADS) k_inspect_ec(active_set_t as, G g, F f,
                                                                  unsigned long long *info) {
   __shared__ unsigned long long s_red[32];
   const int64_t STRIDE = (int64_t)blockDim.x * gridDim.x;

@@ -36,6 +36,7 @@ struct gsw_graph {
   int64_t ncoo = -1;
   double attr[6] = {0, 0, 0, 0, 0, 0};
   double mean_weight = 0;
+  std::vector<int> hdeg;  // host copy of the out-degrees (root features, roots)
 
   template <typename E>
   device_graph_t<CSR, E> view() const {
@@ -63,6 +64,7 @@ struct gsw_ctx {
   std::map<std::pair<int64_t, int>, active_set_t> as_cache;
   std::map<std::string, std::pair<void *, size_t>> bufs;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
+  stat_t stats;  // inspector counters, reused by every run of the context
 
   void *buf(const std::string &name, size_t bytes) {
     auto it = bufs.find(name);
@@ -118,9 +120,11 @@ int grid_for(int64_t n) { return (int)std::min<int64_t>((n + 255) / 256 + 1, (in
 // degree statistics on the host (same ascending summation order as
 // graph_attr_t::fill, src/utils/fileIO.cuh:35-67)
 void compute_attr(gsw_graph *g) {
-  std::vector<int> deg(g->n);
+  std::vector<int> &deg = g->hdeg;
+  deg.resize(g->n);
   if (GSW_CUDA(cudaMemcpyAsync(deg.data(), g->odeg, sizeof(int) * g->n, cudaMemcpyDeviceToHost, stream()))) return;
   GSW_CUDA(cudaStreamSynchronize(stream()));
+  if (g->n < 2) return;
   int mx = 0;
   for (int d : deg) mx = std::max(mx, d);
   std::vector<int64_t> hist((size_t)mx + 1, 0);
@@ -180,7 +184,7 @@ void finalize_graph(gsw_graph *g) {
     GSW_CUDA(cudaStreamSynchronize(stream()));
     g->mean_weight = g->m ? (double)s / (double)g->m : 0;
   }
-  if (g->n > 1) compute_attr(g);
+  compute_attr(g);
 }
 
 // CSR from device keys (both directions of every pair, self-loops = ~0)
@@ -225,6 +229,10 @@ int csr_from_keys(gsw_graph *g, uint64_t *keys, int64_t nkeys) {
   GSW_CUDA(cudaStreamSynchronize(stream()));
   cudaFree(tmp);
   return err().code;
+}
+
+int64_t root_deg(const gsw_graph *g, int64_t root) {
+  return root >= 0 && root < (int64_t)g->hdeg.size() ? g->hdeg[root] : -1;
 }
 
 gsw_graph *new_graph(gsw_ctx *ctx, int64_t n) {
@@ -527,6 +535,7 @@ gsw_status gsw_destroy(gsw_ctx *ctx) {
   for (auto &kv : ctx->as_cache) kv.second.destroy();
   for (auto &kv : ctx->bufs) cudaFree(kv.second.first);
   ctx->executor.destroy();
+  ctx->stats.destroy();
   if (ctx->e0) cudaEventDestroy(ctx->e0);
   if (ctx->e1) cudaEventDestroy(ctx->e1);
   cudaStreamDestroy(ctx->stream);
@@ -667,10 +676,8 @@ gsw_status gsw_graph_destroy(gsw_graph *g) {
 gsw_status gsw_graph_roots(const gsw_graph *g, uint64_t seed, int count, int32_t *roots) {
   if (!g || !roots || count < 0) return fail(GSW_ERR_INVALID_ARG, "gsw_graph_roots: bad arguments");
   entry_guard eg(g->ctx);
-  std::vector<int> deg(g->n);
-  GSW_CUDA(cudaMemcpyAsync(deg.data(), g->odeg, sizeof(int) * g->n, cudaMemcpyDeviceToHost, stream()));
-  GSW_CUDA(cudaStreamSynchronize(stream()));
-  if (!ok()) return eg.finish();
+  const std::vector<int> &deg = g->hdeg;
+  if ((int64_t)deg.size() != g->n) return fail(GSW_ERR_INVALID_ARG, "gsw_graph_roots: graph has no degree table");
   const uint64_t key = stream_key(seed, ST_ROOT);
   int got = 0;
   uint64_t j = 0;
@@ -715,7 +722,8 @@ gsw_status gsw_bfs(gsw_ctx *ctx, gsw_graph *gr, int32_t root, const gsw_run_opts
   fill_root<int>(f.data.dg_wa, -1, 0, root, gr->n);
   feature_t fets;
   config_t conf;
-  stat_t stats;
+  stat_t &stats = ctx->stats;
+  stats.clean();
   inspector_t inspector;
   selector_t selector;
   executor_t &executor = ctx->executor;
@@ -728,7 +736,7 @@ gsw_status gsw_bfs(gsw_ctx *ctx, gsw_graph *gr, int32_t root, const gsw_run_opts
   apply_opts(o, conf);
   set_graph_features(fets, gr);
   fets.use_root = root;
-  init_conf_impl(stats, fets, conf, g, f, gr->mean_weight, gr->attr[0], false);
+  init_conf_impl(stats, fets, conf, g, f, gr->mean_weight, gr->attr[0], false, root_deg(gr, root));
   active_set_t *asp = ctx->aset(gr->n, conf.conf_qmode);
   if (!asp) return eg.finish();
   active_set_t &as = *asp;
@@ -750,7 +758,6 @@ gsw_status gsw_bfs(gsw_ctx *ctx, gsw_graph *gr, int32_t root, const gsw_run_opts
   const double ms = tm.stop();
   tr.resolve();
   end_checks(&as, st);
-  stats.destroy();
   if (st) {
     st->ms = ms;
     st->edges = reached_edges(ctx, gr, f.data.dg_wa, 1, -1);
@@ -780,7 +787,8 @@ gsw_status gsw_sssp(gsw_ctx *ctx, gsw_graph *gr, int32_t root, const gsw_run_opt
   fill_root<int>(f.data.dg_ra, INT_MAX, 0, root, gr->n);
   feature_t fets;
   config_t conf;
-  stat_t stats;
+  stat_t &stats = ctx->stats;
+  stats.clean();
   inspector_t inspector;
   selector_t selector;
   executor_t &executor = ctx->executor;
@@ -793,7 +801,7 @@ gsw_status gsw_sssp(gsw_ctx *ctx, gsw_graph *gr, int32_t root, const gsw_run_opt
   apply_opts(o, conf);
   set_graph_features(fets, gr);
   fets.use_root = root;
-  init_conf_impl(stats, fets, conf, g, f, gr->mean_weight, gr->attr[0], false);
+  init_conf_impl(stats, fets, conf, g, f, gr->mean_weight, gr->attr[0], false, root_deg(gr, root));
   active_set_t *asp = ctx->aset(gr->n, conf.conf_qmode);
   if (!asp) return eg.finish();
   active_set_t &as = *asp;
@@ -814,7 +822,6 @@ gsw_status gsw_sssp(gsw_ctx *ctx, gsw_graph *gr, int32_t root, const gsw_run_opt
   const double ms = tm.stop();
   tr.resolve();
   end_checks(&as, st);
-  stats.destroy();
   if (st) {
     st->ms = ms;
     st->edges = reached_edges(ctx, gr, f.data.dg_wa, 1, INT_MAX);
@@ -850,7 +857,8 @@ gsw_status gsw_cc(gsw_ctx *ctx, gsw_graph *gr, const gsw_run_opts *o, int32_t *l
   k_iota<<<grid_for(gr->n), 256, 0, stream()>>>(f.data.dg_wa, gr->n);
   feature_t fets;
   config_t conf;
-  stat_t stats;
+  stat_t &stats = ctx->stats;
+  stats.clean();
   inspector_t inspector;
   selector_t selector;
   executor_t &executor = ctx->executor;
@@ -882,7 +890,6 @@ gsw_status gsw_cc(gsw_ctx *ctx, gsw_graph *gr, const gsw_run_opts *o, int32_t *l
   const double ms = tm.stop();
   tr.resolve();
   end_checks(&as, st);
-  stats.destroy();
   if (st) {
     st->ms = ms;
     st->edges = gr->ncoo;
@@ -923,7 +930,8 @@ gsw_status gsw_pagerank(gsw_ctx *ctx, gsw_graph *gr, const gsw_run_opts *o, floa
   f.data.zero = 0.0f;
   feature_t fets;
   config_t conf;
-  stat_t stats;
+  stat_t &stats = ctx->stats;
+  stats.clean();
   inspector_t inspector;
   selector_t selector;
   executor_t &executor = ctx->executor;
@@ -959,7 +967,6 @@ gsw_status gsw_pagerank(gsw_ctx *ctx, gsw_graph *gr, const gsw_run_opts *o, floa
   const double ms = tm.stop();
   tr.resolve();
   end_checks(&as, st);
-  stats.destroy();
   if (st) {
     st->ms = ms;
     st->edges = gr->m * (int64_t)steps;
@@ -993,6 +1000,26 @@ __global__ void k_bc_split(const app::bwdata_t *bw, int64_t n, int *nsp, float *
   }
 }
 
+__global__ void k_max_int(const int *a, int64_t n, int *out) {
+  int m = INT_MIN;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    m = a[i] > m ? a[i] : m;
+  m = warp_max(m);
+  if (lane_id() == 0) atomicMax(out, m);
+}
+
+int max_level(gsw_ctx *ctx, const int *a, int64_t n) {
+  int *d = (int *)ctx->buf("maxlvl", sizeof(int));
+  if (!d) return 0;
+  const int init = INT_MIN;
+  GSW_CUDA(cudaMemcpyAsync(d, &init, sizeof(int), cudaMemcpyHostToDevice, stream()));
+  k_max_int<<<grid_for(n), 256, 0, stream()>>>(a, n, d);
+  int r = 0;
+  GSW_CUDA(cudaMemcpyAsync(&r, d, sizeof(int), cudaMemcpyDeviceToHost, stream()));
+  GSW_CUDA(cudaStreamSynchronize(stream()));
+  return r;
+}
+
 gsw_status gsw_bc(gsw_ctx *ctx, gsw_graph *gr, int32_t root, const gsw_run_opts *o, int32_t *nsp, float *dep,
                   gsw_run_stats *st) {
   entry_guard eg(ctx);
@@ -1009,7 +1036,8 @@ gsw_status gsw_bc(gsw_ctx *ctx, gsw_graph *gr, int32_t root, const gsw_run_opts 
   k_bc_init<<<grid_for(gr->n), 256, 0, stream()>>>(f.data.dg_wa, gr->n, root);
   feature_t fets;
   config_t conf;
-  stat_t stats;
+  stat_t &stats = ctx->stats;
+  stats.clean();
   inspector_t inspector;
   selector_t selector;
   executor_t &executor = ctx->executor;
@@ -1023,9 +1051,14 @@ gsw_status gsw_bc(gsw_ctx *ctx, gsw_graph *gr, int32_t root, const gsw_run_opts 
   apply_opts(o, conf);
   set_graph_features(fets, gr);
   fets.use_root = root;
-  init_conf_impl(stats, fets, conf, g, f, 0.0, gr->attr[0], false);
-  conf.conf_qmode = Cached;
-  active_set_t *asp = ctx->aset(gr->n, Cached);
+  init_conf_impl(stats, fets, conf, g, f, 0.0, gr->attr[0], false, root_deg(gr, root));
+  // The backward sweep replays the forward frontiers from the cached queue
+  // only when every forward level enqueued its frontier, i.e. when the levels
+  // run fused (always Push + Queue).  Otherwise each backward level inspects
+  // the forward levels instead, which holds for every direction and format.
+  const bool replay = conf.conf_fusion;
+  conf.conf_qmode = replay ? Cached : Normal;
+  active_set_t *asp = ctx->aset(gr->n, conf.conf_qmode);
   if (!asp) return eg.finish();
   active_set_t &as = *asp;
   as.reset();
@@ -1044,14 +1077,15 @@ gsw_status gsw_bc(gsw_ctx *ctx, gsw_graph *gr, int32_t root, const gsw_run_opts 
     if (finish(as, g, f, conf)) break;
   }
   const int64_t fwd_edges = st ? reached_edges(ctx, gr, (const int *)f.data.dg_wa, 2, -100) : 0;
-  // hand-off (bc.cu:391-395) and backward sweep over the cached levels
+  // hand-off (bc.cu:391-395); the sweep starts at the deepest forward level
   k_bc_handoff<<<grid_for(gr->n), 256, 0, stream()>>>(f.data.dg_wa, gr->n, h.data.dg_ra, h.data.dg_wa);
-  as.reset(true);
+  const int lmax = max_level(ctx, h.data.dg_ra, gr->n);
+  as.reset(replay);
   conf.reset();
   stats.reset();
   conf.conf_compensation = true;
-  g.update_level(-1);
-  if (conf.conf_fuse_inspect) g.update_level(-1);
+  g.level = lmax;
+  if (!replay) conf.conf_first_round = false;  // inspect the deepest level too
   as.init(ALL_INACTIVE);
   for (int level = 0; level < MAX_LEVELS && ok(); level++) {
     inspector.inspect(as, g, h, stats, fets, conf);
@@ -1067,7 +1101,6 @@ gsw_status gsw_bc(gsw_ctx *ctx, gsw_graph *gr, int32_t root, const gsw_run_opts 
   const double ms = tm.stop();
   tr.resolve();
   end_checks(&as, st);
-  stats.destroy();
   if (st) {
     st->ms = ms;
     st->edges = fwd_edges;
@@ -1102,7 +1135,8 @@ gsw_status gsw_gc(gsw_ctx *ctx, gsw_graph *gr, const gsw_run_opts *o, int32_t *c
   fill<int>(f.data.dg_ra, -1, gr->n);
   feature_t fets;
   config_t conf;
-  stat_t stats;
+  stat_t &stats = ctx->stats;
+  stats.clean();
   inspector_t inspector;
   selector_t selector;
   executor_t &executor = ctx->executor;
@@ -1136,7 +1170,6 @@ gsw_status gsw_gc(gsw_ctx *ctx, gsw_graph *gr, const gsw_run_opts *o, int32_t *c
   const double ms = tm.stop();
   tr.resolve();
   end_checks(&as, st);
-  stats.destroy();
   if (st) {
     st->ms = ms;
     st->edges = gr->m / 2;

@@ -74,6 +74,8 @@ gsw_status gsw_graph_info(const gsw_graph *g, int64_t *n, int64_t *m, int *weigh
 gsw_status gsw_graph_attr(const gsw_graph *g, double *out6);
 /* Copy the CSR back to host arrays (weights may be NULL). */
 gsw_status gsw_graph_download(const gsw_graph *g, int64_t *row_off, int32_t *col, int32_t *weights);
+/* A graph belongs to the context that made it: destroy it before the
+ * context. */
 gsw_status gsw_graph_destroy(gsw_graph *g);
 /* `count` distinct seeded non-isolated vertices, the rule the reference's
  * random_root follows (src/utils/fileIO.cuh:389-397) with a counter-based
