@@ -36,7 +36,7 @@ ABI_SYMBOLS = (
     "gsw_graph_upload", "gsw_graph_generate_rmat", "gsw_graph_generate_grid",
     "gsw_graph_generate_er", "gsw_graph_info", "gsw_graph_attr", "gsw_graph_download",
     "gsw_graph_destroy", "gsw_graph_roots", "gsw_ctx_stream", "gsw_run_opts_default", "gsw_bfs", "gsw_sssp", "gsw_cc",
-    "gsw_pagerank", "gsw_bc", "gsw_gc", "gsw_mbfs",
+    "gsw_pagerank", "gsw_bc", "gsw_gc", "gsw_mbfs", "gsw_bfs_strict_noalloc",
 )
 
 
@@ -98,6 +98,7 @@ def lib():
     L.gsw_bc.argtypes = [vp, vp, i32, po, vp, vp, ps]
     L.gsw_gc.argtypes = [vp, vp, po, vp, ps]
     L.gsw_mbfs.argtypes = [vp, vp, C.c_int, vp, C.c_int, po, vp, ps]
+    L.gsw_bfs_strict_noalloc.argtypes = [i64, i64, vp, vp, i32, vp, vp]
     _LIB = L
     return L
 

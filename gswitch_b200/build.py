@@ -29,7 +29,8 @@ def stale(target: str) -> bool:
 
 def build(force: bool = False, verbose: bool = False) -> str:
     if force or stale(SO):
-        cmd = [NVCC, *ARCH, *FLAGS, "-o", SO + ".tmp", os.path.join(HERE, "csrc", "gsw_capi.cu")]
+        cmd = [NVCC, *ARCH, *FLAGS, "-o", SO + ".tmp", os.path.join(HERE, "csrc", "gsw_capi.cu"),
+               os.path.join(HERE, "csrc", "gsw_noalloc.cu")]
         if verbose:
             print(" ".join(cmd), file=sys.stderr)
         subprocess.check_call(cmd)

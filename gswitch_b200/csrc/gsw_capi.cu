@@ -91,9 +91,13 @@ struct gsw_ctx {
   }
 };
 
-namespace {
-
+namespace gsw {
+// text of the calling thread's last failed ABI call (also set by the
+// allocation-free entry point in gsw_noalloc.cu)
 thread_local std::string g_last_error;
+}  // namespace gsw
+
+namespace {
 
 struct entry_guard {  // binds the context's device and stream for one call
   explicit entry_guard(gsw_ctx *ctx) {

@@ -159,6 +159,24 @@ gsw_status gsw_gc(gsw_ctx *ctx, gsw_graph *g, const gsw_run_opts *o, int32_t *co
 gsw_status gsw_mbfs(gsw_ctx *ctx, gsw_graph *g, int nsrc, const int32_t *roots, int batched, const gsw_run_opts *o,
                     int32_t *levels, gsw_run_stats *st);
 
+/* No counterpart in the reference.  BFS levels (-1 unreached) computed with
+ * the edge-balanced push expand, for callers that cannot allocate device
+ * memory: code inside a host framework whose memory pool already owns the
+ * device memory, or latency-critical code that cannot take the device-wide
+ * synchronisation of cudaMalloc / cudaFree.  The caller passes its own device
+ * CSR (d_row_off: n + 1 int64, d_col: m int32) and its own device output
+ * (d_levels: n int32); the call allocates nothing and keeps its working
+ * memory in one fixed array of about 5 MiB per GPU, held until the process
+ * exits.  Limits: n <= 2^18 vertices, m <= 2^28 arcs (GSW_ERR_UNSUPPORTED
+ * beyond).  The first call on a device looks up that array's address; make
+ * it before any stream capture.  Calls share the array: calls that overlap
+ * on the GPU race and must be serialised by the caller.  stream may be NULL
+ * (the legacy default stream). */
+#define GSW_NOALLOC_MAX_VERTICES (1 << 18)
+#define GSW_NOALLOC_MAX_ARCS (1 << 28)
+gsw_status gsw_bfs_strict_noalloc(int64_t n, int64_t m, const int64_t *d_row_off, const int32_t *d_col, int32_t root,
+                                  int32_t *d_levels, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
