@@ -50,7 +50,8 @@ class _Opts(C.Structure):
     _fields_ = [("direction", C.c_int), ("asfmt", C.c_int), ("lb", C.c_int), ("fusion", C.c_int),
                 ("sorted_queue", C.c_int), ("max_iters", C.c_int), ("damping", C.c_float),
                 ("eps", C.c_float), ("selector", C.c_int), ("verbose", C.c_int), ("timing", C.c_int),
-                ("expand_grid", C.c_int), ("account", C.c_int), ("reserved", C.c_int * 7)]
+                ("expand_grid", C.c_int), ("account", C.c_int), ("persistent", C.c_int), ("barrier_test", C.c_int),
+                ("reserved", C.c_int * 5)]
 
 
 class _Stats(C.Structure):
@@ -117,11 +118,13 @@ class RunOpts:
 
     def __init__(self, direction=None, asfmt=None, lb=None, fusion=None, sorted_queue=True,
                  max_iters=0, damping=0.85, eps=0.01, verbose=False, timing=False, expand_grid=0,
-                 account=False):
+                 account=False, persistent=None, barrier_test=False):
         self.direction, self.asfmt, self.lb, self.fusion = direction, asfmt, lb, fusion
         self.sorted_queue, self.max_iters, self.damping, self.eps = sorted_queue, max_iters, damping, eps
         self.verbose, self.timing, self.expand_grid = verbose, timing, expand_grid
         self.account = account
+        self.persistent = persistent
+        self.barrier_test = barrier_test
 
     @classmethod
     def from_config(cls, cfg: str, **kw):
@@ -144,6 +147,8 @@ class RunOpts:
         o.damping, o.eps = float(self.damping), float(self.eps)
         o.verbose, o.timing, o.expand_grid = int(self.verbose), int(self.timing), int(self.expand_grid)
         o.account = int(self.account)
+        o.persistent = AUTO if self.persistent is None else int(bool(self.persistent))
+        o.barrier_test = int(self.barrier_test)
         return o
 
 

@@ -19,7 +19,8 @@
 #include <chrono>
 #include <unordered_map>
 
-#include "k_expand.cuh"
+#include "k_persistent.cuh"
+#include "k_twod.cuh"
 
 namespace gsw {
 
@@ -61,6 +62,7 @@ struct engine_opts_t {
   bool verbose = false;
   bool timing = false;        // per-level CUDA-event timing into the stats
   int force_grid = 0;         // autotuner: fixed expand grid (0 = derive)
+  bool barrier_leave_test = false;  // failure-path test of the level barrier
 };
 inline engine_opts_t &opts() {
   static thread_local engine_opts_t o;
@@ -395,6 +397,11 @@ struct selector_t {
 // ===========================================================================
 struct executor_t {
   int *dg_tile = nullptr;  // STRICT tile owners
+  twod_layout twod;                 // 2D-partition layout of the current graph
+  int64_t persistent_levels = 0;    // levels run inside persistent launches
+  int64_t persistent_launches = 0;  // persistent launches
+  bool last_persistent = false;     // the last expand was a persistent launch
+  Computation pattern = Idem;       // pattern of the run being expanded
   int64_t tile_cap = 0;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   inspector_t *insp = nullptr;  // source of the host-known frontier sizes
@@ -420,6 +427,8 @@ struct executor_t {
       k_scan_single_block<<<1, 1024, 0, stream()>>>(as.workset.dg_bsum, nb);
       k_filter_write<<<(unsigned)nb, FILTER_WORDS, 0, stream()>>>(as, target, as.workset.dg_bsum, nb);
     } else {
+      // the append builder starts from an empty output whatever ran before
+      GSW_CUDA(cudaMemsetAsync(as.queue.output_size_ptr(), 0, sizeof(int), stream()));
       const int grid = clamp_grid((nwords + 255) / 256, resident_grid(k_filter_unsorted, 256));
       k_filter_unsorted<<<grid, 256, 0, stream()>>>(as, target);
     }
@@ -537,6 +546,14 @@ struct executor_t {
     auto _k = kern;                                               \
     _k<<<grid_for(_k, want), B, 0, stream()>>>(__VA_ARGS__);      \
   } while (0)
+    if (conf.conf_lb == TWOD) {
+      launch_twod(g, f, conf);
+      return;
+    }
+    if (conf.conf_dir == Push && fused && conf.conf_persistent && as.queue.mode == Normal) {
+      launch_persistent(as, g, f, conf);
+      return;
+    }
     if (conf.conf_dir == Push) {
       switch (conf.conf_lb) {
         case TM:
@@ -585,6 +602,85 @@ struct executor_t {
     GSW_LAUNCHED();
   }
 
+  // Consecutive fused levels in one cooperative launch (k_persistent.cuh).
+  // Afterwards the host state looks as if the levels had run one by one:
+  // g.level is advanced, the last output queue sits where the next swap
+  // expects it, an empty frontier halts the loop, and a frontier that grew
+  // past the limit returns the loop to the inspected (standalone) form so the
+  // selector can pick direction and format again.
+  template <typename E, typename F>
+  void launch_persistent(active_set_t &as, device_graph_t<CSR, E> &g, F &f, config_t &conf) {
+    using G = device_graph_t<CSR, E>;
+    auto kern = k_fused_persistent<G, F>;
+    const int grid = resident_grid(kern, EXPAND_THREADS);
+    as_counters_t *c = as.dg_cnt;
+    const int cur = as.queue.cursor;
+    k_persist_prep<<<1, 1, 0, stream()>>>(c, cur);
+    persist_state ps;
+    ps.q[0] = as.queue.subqueue[cur].dg_queue;
+    ps.q[1] = as.queue.subqueue[cur ^ 1].dg_queue;
+    ps.cnt = c->pq;
+    ps.cap = as.queue.subqueue[0].max_size;
+    // only Idem patterns leave fused mode when the frontier grows (the
+    // selector keeps Mono / ASSO patterns fused level after level)
+    ps.grow_limit = pattern == Idem ? (int)MAX((int64_t)4096, as.size / 64) : INT32_MAX;
+    ps.max_levels = (int)MIN(as.size + 2, (int64_t)(1 << 24));  // a BFS-like frontier runs at most n levels
+    ps.budget_ns = opts().barrier_leave_test ? 20000000ull : 2000000000ull;  // per barrier wait
+    ps.leave_block = opts().barrier_leave_test ? 0 : -1;
+    ps.levels_done = &c->plevels;
+    ps.exit_reason = &c->preason;
+    void *args[] = {(void *)&as, (void *)&g, (void *)&f, (void *)&conf, (void *)&ps};
+    if (GSW_CUDA(cudaLaunchCooperativeKernel((const void *)kern, grid, EXPAND_THREADS, args, 0, stream()))) return;
+    GSW_LAUNCHED();
+    int res[2] = {0, -1};
+    GSW_CUDA(cudaMemcpyAsync(res, &c->plevels, sizeof(res), cudaMemcpyDeviceToHost, stream()));
+    GSW_CUDA(cudaStreamSynchronize(stream()));
+    const int L = res[0], reason = res[1];
+    persistent_levels += L;
+    persistent_launches++;
+    last_persistent = true;
+    if (reason == 3 || reason < 0) {
+      set_error(GSW_ERR_TIMEOUT, "%s", "persistent fused levels: grid barrier timed out");
+      return;
+    }
+    if (L > 0) g.level += L - 1;
+    // the next input is the last output: q[L & 1], size pq[L % 3]
+    const int out_idx = cur ^ (L & 1);
+    if (out_idx == cur) as.queue.cursor ^= 1;
+    k_persist_finish<<<1, 1, 0, stream()>>>(c, out_idx, as.queue.cursor, L % 3);
+    GSW_LAUNCHED();
+    if (reason == 0) as.halt_host();
+    if (reason == 1) {
+      // back to inspected levels: the queue is rebuilt from the bitmaps
+      conf.conf_fuse_inspect = false;
+      as.queue.clean_size(0);
+      as.queue.clean_size(1);
+    }
+  }
+
+  // 2D-partition expand (k_twod.cuh): all sources to all destinations, so
+  // only for from-all / to-all patterns, unweighted, 4-byte messages
+  template <typename E, typename F>
+  void launch_twod(device_graph_t<CSR, E> &g, F &f, config_t &conf) {
+    using G = device_graph_t<CSR, E>;
+    using WA = typename F::wa_t;
+    if constexpr (sizeof(WA) <= 4 && std::is_same<E, Empty>::value) {
+      if (!conf.conf_fromall || !conf.conf_toall) {
+        set_error(GSW_ERR_UNSUPPORTED, "%s", "2D-partition expand needs a from-all/to-all pattern");
+        return;
+      }
+      if (!twod.edge) {
+        set_error(GSW_ERR_UNSUPPORTED, "%s", "2D-partition layout not built for this graph");
+        return;
+      }
+      const int grid = (int)MIN(twod.ntiles, (int64_t)resident_grid(k_twod<G, F>, TWOD_THREADS));
+      k_twod<G, F><<<grid, TWOD_THREADS, 0, stream()>>>(g, f, twod);
+      GSW_LAUNCHED();
+    } else {
+      set_error(GSW_ERR_UNSUPPORTED, "%s", "2D-partition expand needs unweighted edges and 4-byte vertex data");
+    }
+  }
+
   template <typename E, typename F>
   void launch_ec(active_set_t &as, device_graph_t<COO, E> &g, F &f) {
     const int grid = resident_grid(k_expand_ec<device_graph_t<COO, E>, F>, 512);
@@ -594,10 +690,6 @@ struct executor_t {
 
   template <typename E, typename F>
   void dispatch(active_set_t &as, device_graph_t<CSR, E> &g, F &f, config_t &conf) {
-    if (conf.conf_lb == TWOD && twod_hook) {
-      twod_hook(this, &as, (void *)&g, (void *)&f, &conf);
-      return;
-    }
     launch_vc(as, g, f, conf);
   }
   template <typename E, typename F>
@@ -615,6 +707,8 @@ struct executor_t {
     if (conf.conf_count_edges) GSW_CUDA(cudaMemsetAsync(&as.dg_cnt->scanned, 0, sizeof(unsigned long long), stream()));
     if (sync_needed) cudaEventRecord(ev[0], stream());
     marks().exp0 = opts().timing ? timing_pool().record() : -1;
+    last_persistent = false;
+    pattern = fets.pattern;
     dispatch(as, g, f, conf);
     marks().exp1 = opts().timing ? timing_pool().record() : -1;
     double e = s;
@@ -641,7 +735,7 @@ struct executor_t {
     // a fused level that is far slower than average goes back to the
     // standalone form (executor.cuh:128-131)
     if (fets.pattern == Idem && fets.avg_expand_time > 0 && fets.last_expand_time > 5 * fets.avg_expand_time &&
-        !conf.force.has_fusion) {
+        !conf.force.has_fusion && !last_persistent) {
       conf.conf_fuse_inspect = false;
       as.queue.swap();
     }
@@ -656,8 +750,6 @@ struct executor_t {
     conf.conf_first_round = false;
   }
 
-  // optional 2D-partition expand, installed by code that owns the tiling
-  void (*twod_hook)(executor_t *, active_set_t *, void *, void *, config_t *) = nullptr;
 };
 
 // ===========================================================================

@@ -50,7 +50,9 @@ struct as_counters_t {
   int cnt;               // __exit / probe counter
   unsigned long long total_edges;  // STRICT: edges in the current frontier
   unsigned long long scanned;      // accounting: edges an expand touched
-  int pad[4];
+  int pq[3];                       // persistent fused levels: rotating sizes
+  int plevels;                     // persistent fused levels: levels done
+  int preason;                     // persistent fused levels: exit reason
 };
 
 struct bits_t {
@@ -157,6 +159,10 @@ struct queue_t {
     return r;
   }
   void clean_size(int which) { GSW_CUDA(cudaMemsetAsync(subqueue[which].dg_qsize, 0, sizeof(int), stream())); }
+  // device address of the size the next builder appends to
+  int *output_size_ptr() const {
+    return mode == Normal ? subqueue[cursor ^ 1].dg_qsize : subqueue[1].dg_queue + cursor + 1;
+  }
   void reset(bool _traceback = false) {
     traceback = _traceback;
     if (mode == Normal) {

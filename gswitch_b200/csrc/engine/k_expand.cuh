@@ -123,41 +123,66 @@ __global__ void __launch_bounds__(EXPAND_THREADS) k_push_tm(active_set_t as, G g
   account(as, conf, cnt);
 }
 
+// Thread per candidate, four candidates per thread: the dependent chain of a
+// candidate (status bit -> offsets -> first in-neighbour -> its frontier bit)
+// is issued for all four before any of them is resolved, so a thread keeps
+// four memory requests in flight instead of one.  Most candidates of a large
+// pull level stop at the first neighbour.
 template <typename G, typename F>
 __global__ void __launch_bounds__(EXPAND_THREADS) k_pull_tm(active_set_t as, G g, F f, config_t conf) {
   using WA = typename F::wa_t;
+  constexpr int K = 4;
   const int64_t n = as.get_size();
   GSW_HALT_IF_EMPTY(n);
   const Status want = conf.want();
   const int64_t STRIDE = (int64_t)blockDim.x * gridDim.x;
   unsigned long long cnt = 0;
-  for (int64_t idx = threadIdx.x + (int64_t)blockIdx.x * blockDim.x; idx < n; idx += STRIDE) {
-    const int v = as.fetch(idx, want);
-    if (v < 0) continue;
-    int64_t st;
-    int deg;
-    vertex_range(g, true, v, st, deg);
-    WA acc;
-    bool have = false;
-    int k = 0;
-    for (; k < deg; ++k) {
-      const int u = __ldg(g.dgr_adj_list + st + k);
-      if (conf.conf_fromall || as.bitmap.is_active(u)) {
-        WA x = f.emit(u, g.fetch_edata_r(st + k), g);
-        if (have)
-          f.comp(&acc, x, g);
-        else {
-          acc = x;
-          have = true;
-        }
-        if (conf.conf_pruning) {
-          ++k;
-          break;
+  for (int64_t base = threadIdx.x + (int64_t)blockIdx.x * blockDim.x; base < n; base += K * STRIDE) {
+    int v[K], deg[K], u0[K];
+    int64_t st[K];
+    bool a0[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const int64_t idx = base + k * STRIDE;
+      v[k] = idx < n ? as.fetch(idx, want) : -1;
+    }
+#pragma unroll
+    for (int k = 0; k < K; ++k) vertex_range(g, true, v[k], st[k], deg[k]);
+#pragma unroll
+    for (int k = 0; k < K; ++k) u0[k] = deg[k] > 0 ? __ldg(g.dgr_adj_list + st[k]) : 0;
+#pragma unroll
+    for (int k = 0; k < K; ++k) a0[k] = deg[k] > 0 && (conf.conf_fromall || as.bitmap.is_active(u0[k]));
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      if (v[k] < 0 || deg[k] == 0) continue;
+      WA acc;
+      bool have = false;
+      int e = 1;
+      if (a0[k]) {
+        acc = f.emit(u0[k], g.fetch_edata_r(st[k]), g);
+        have = true;
+      }
+      if (!(have && conf.conf_pruning)) {
+        for (; e < deg[k]; ++e) {
+          const int u = __ldg(g.dgr_adj_list + st[k] + e);
+          if (conf.conf_fromall || as.bitmap.is_active(u)) {
+            WA x = f.emit(u, g.fetch_edata_r(st[k] + e), g);
+            if (have)
+              f.comp(&acc, x, g);
+            else {
+              acc = x;
+              have = true;
+            }
+            if (conf.conf_pruning) {
+              ++e;
+              break;
+            }
+          }
         }
       }
+      cnt += e;
+      if (have) f.comp(f.wa_of(v[k]), acc, g);
     }
-    cnt += k;
-    if (have) f.comp(f.wa_of(v), acc, g);
   }
   account(as, conf, cnt);
 }

@@ -23,8 +23,10 @@ namespace gsw {
 // max-degree counters.
 constexpr int INSPECT_VTHREADS = 256 * 512;  // the reference's grid, one virtual thread each
 constexpr int INSPECT_VBLOCK = 512;          // virtual threads per virtual block
-constexpr int INSPECT_THREADS = 128;         // physical block: a quarter virtual block
-constexpr int INSPECT_CTAS = INSPECT_VTHREADS / INSPECT_THREADS;
+constexpr int INSPECT_VPB = 128;             // virtual threads per physical block
+constexpr int INSPECT_HALVES = 2;            // physical threads per virtual thread
+constexpr int INSPECT_THREADS = INSPECT_VPB * INSPECT_HALVES;
+constexpr int INSPECT_CTAS = INSPECT_VTHREADS / INSPECT_VPB;
 constexpr int INSPECT_UNROLL = 4;
 static_assert(STAT_SLOTS == 8 + 2 * (INSPECT_VTHREADS / INSPECT_VBLOCK), "statistics block layout");
 constexpr int EC_INSPECT_CTAS = 256;
@@ -32,73 +34,92 @@ constexpr int EC_INSPECT_THREADS = 512;
 
 // Virtual thread t (0 <= t < 131072) visits vertices t, t + 131072, ...
 // exactly as thread t of the reference's 256 x 512 grid-stride launch, so the
-// max-degree counters are the reference's.  Physical blocks of 128 threads
-// (a quarter of a virtual block) fill all SMs evenly, each thread keeps four
-// vertices in flight, and the last block to finish folds the per-virtual-
-// block sums (max over blocks for push, sum for pull).
+// max-degree counters are the reference's.  Two physical threads share one
+// virtual thread (even / odd steps of its sequence) and merge their maxima
+// in shared memory; a physical block holds 128 virtual threads (a quarter
+// virtual block), each thread keeps four vertices in flight, vertex counts
+// are taken per warp from the ballots, and the last block to finish folds the
+// per-virtual-block sums (max over blocks for push, sum for pull).
 template <typename G, typename F>
-__global__ void __launch_bounds__(INSPECT_THREADS) k_inspect_vc(active_set_t as, G g, F f,
+__global__ void __launch_bounds__(INSPECT_THREADS, 7) k_inspect_vc(active_set_t as, G g, F f,
                                                                  unsigned long long *info) {
   __shared__ unsigned long long s_red[32];
+  __shared__ unsigned s_mp[INSPECT_VPB], s_ml[INSPECT_VPB];
   __shared__ bool s_last;
-  const int64_t S = INSPECT_VTHREADS;
-  const int64_t t = threadIdx.x + (int64_t)blockIdx.x * blockDim.x;
+  const int S = INSPECT_VTHREADS;
+  const int half = threadIdx.x / INSPECT_VPB;
+  const int vt_local = threadIdx.x % INSPECT_VPB;
+  const int t = blockIdx.x * INSPECT_VPB + vt_local;
   const int lane = lane_id();
-  const int64_t n = as.size;
-  unsigned long long active_num = 0, inactive_num = 0, push_wl = 0, pull_wl = 0;
-  unsigned long long max_push = 0, max_pull = 0;
-  for (int64_t base = t; base - lane < n; base += INSPECT_UNROLL * S) {
+  const int n = (int)as.size;
+  unsigned active_num = 0, inactive_num = 0;  // per warp, kept by lane 0
+  unsigned long long push_wl = 0, pull_wl = 0;
+  unsigned max_push = 0, max_pull = 0;
+  const long long step = (long long)INSPECT_HALVES * S;
+  for (long long base = t + (long long)half * S; base - lane < n; base += INSPECT_UNROLL * step) {
     Status st[INSPECT_UNROLL];
     int od[INSPECT_UNROLL];
 #pragma unroll
     for (int k = 0; k < INSPECT_UNROLL; ++k) {
-      const int64_t idx = base + k * S;
+      const long long idx = base + k * step;
       od[k] = idx < n ? __ldg(g.dg_odegree + idx) : 0;
     }
 #pragma unroll
     for (int k = 0; k < INSPECT_UNROLL; ++k) {
-      const int64_t idx = base + k * S;
+      const long long idx = base + k * step;
       st[k] = idx < n ? f.filter((int)idx, g) : Inactive;
     }
 #pragma unroll
     for (int k = 0; k < INSPECT_UNROLL; ++k) {
-      const int64_t idx = base + k * S;
-      if (idx - lane >= n) break;  // warp-uniform
+      const long long idx = base + k * step;
+      const long long wbase = idx - lane;
+      if (wbase >= n) break;  // warp-uniform
       const bool valid = idx < n;
       const bool tag_active = valid && st[k] == Active;
       const bool tag_inactive = valid && st[k] != Inactive;  // 0 only for Inactive
       const unsigned aw = __ballot_sync(FULL, tag_active);
       const unsigned iw = __ballot_sync(FULL, tag_inactive);
       if (lane == 0) {
-        as.bitmap.active.dg_bits[idx >> 5] = aw;
-        as.bitmap.inactive.dg_bits[idx >> 5] = iw;
+        as.bitmap.active.dg_bits[wbase >> 5] = aw;
+        as.bitmap.inactive.dg_bits[wbase >> 5] = iw;
+        const long long rem = n - wbase;
+        const unsigned nvalid = rem >= 32 ? 32u : (unsigned)rem;
+        active_num += __popc(aw);
+        inactive_num += nvalid - __popc(iw);
       }
-      if (tag_active) {
-        active_num++;
-        push_wl += od[k];
-        max_push = MAX(max_push, (unsigned long long)od[k]);
-      }
-      if (valid && !tag_inactive) {
-        inactive_num++;
-        pull_wl += od[k];
-        max_pull = MAX(max_pull, (unsigned long long)od[k]);
-      }
+      const unsigned oa = tag_active ? (unsigned)od[k] : 0u;
+      const unsigned oi = (valid && !tag_inactive) ? (unsigned)od[k] : 0u;
+      push_wl += oa;
+      pull_wl += oi;
+      max_push = max_push > oa ? max_push : oa;
+      max_pull = max_pull > oi ? max_pull : oi;
     }
   }
+  // merge the two halves of every virtual thread
+  if (half == 1) {
+    s_mp[vt_local] = max_push;
+    s_ml[vt_local] = max_pull;
+  }
+  __syncthreads();
+  unsigned long long vmp = 0, vml = 0;
+  if (half == 0) {
+    vmp = MAX(max_push, s_mp[vt_local]);
+    vml = MAX(max_pull, s_ml[vt_local]);
+  }
   unsigned long long r;
-  r = block_reduce(active_num, s_red);
+  r = block_reduce((unsigned long long)active_num, s_red);
   if (threadIdx.x == 0 && r) atomicAdd(info + 0, r);
-  r = block_reduce(inactive_num, s_red);
+  r = block_reduce((unsigned long long)inactive_num, s_red);
   if (threadIdx.x == 0 && r) atomicAdd(info + 1, r);
   r = block_reduce(push_wl, s_red);
   if (threadIdx.x == 0 && r) atomicAdd(info + 2, r);
   r = block_reduce(pull_wl, s_red);
   if (threadIdx.x == 0 && r) atomicAdd(info + 3, r);
-  const int vb = (int)(t / INSPECT_VBLOCK);
+  const int vb = t / INSPECT_VBLOCK;
   const int NVB = INSPECT_VTHREADS / INSPECT_VBLOCK;
-  r = block_reduce(max_push, s_red);
+  r = block_reduce(vmp, s_red);
   if (threadIdx.x == 0 && r) atomicAdd(info + 8 + vb, r);
-  r = block_reduce(max_pull, s_red);
+  r = block_reduce(vml, s_red);
   if (threadIdx.x == 0 && r) atomicAdd(info + 8 + NVB + vb, r);
   if (threadIdx.x == 0) {
     __threadfence();

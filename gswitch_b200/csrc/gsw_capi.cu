@@ -37,6 +37,12 @@ struct gsw_graph {
   double attr[6] = {0, 0, 0, 0, 0, 0};
   double mean_weight = 0;
   std::vector<int> hdeg;  // host copy of the out-degrees (root features, roots)
+  struct twod_store {
+    uint64_t *edge = nullptr;
+    int64_t *tile_off = nullptr, *heavy_off = nullptr, *heavy_beg = nullptr, *heavy_end = nullptr;
+    int *heavy_src = nullptr;
+    twod_layout L;
+  } *twod = nullptr;  // 2D-partition layout, built on first use
 
   template <typename E>
   device_graph_t<CSR, E> view() const {
@@ -121,47 +127,93 @@ gsw_status fail(int code, const char *msg) {
 
 int grid_for(int64_t n) { return (int)std::min<int64_t>((n + 255) / 256 + 1, (int64_t)sm_count() * 8); }
 
-// degree statistics on the host (same ascending summation order as
-// graph_attr_t::fill, src/utils/fileIO.cuh:35-67)
+// Degree statistics of graph_attr_t::fill (src/utils/fileIO.cuh:35-67) from a
+// device histogram of the degrees: the integer sums (average, deviation,
+// range, maximum) come out exactly as the reference's ascending double sums;
+// the Gini and Hoover-like terms are summed per run of equal degrees in
+// closed form (equal to the per-vertex sums up to rounding).
+__global__ void k_deg_max(const int *odeg, int64_t n, int *out) {
+  int m = 0;
+  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x)
+    m = odeg[v] > m ? odeg[v] : m;
+  m = warp_max(m);
+  if (lane_id() == 0) atomicMax(out, m);
+}
+constexpr int HIST_SMEM = 2048;
+__global__ void __launch_bounds__(256) k_deg_hist(const int *odeg, int64_t n, unsigned long long *hist) {
+  __shared__ unsigned s_h[HIST_SMEM];
+  for (int i = threadIdx.x; i < HIST_SMEM; i += blockDim.x) s_h[i] = 0;
+  __syncthreads();
+  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
+    const int d = odeg[v];
+    if (d < HIST_SMEM)
+      atomicAdd(&s_h[d], 1u);
+    else
+      atomicAdd(hist + d, 1ull);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < HIST_SMEM; i += blockDim.x)
+    if (s_h[i]) atomicAdd(hist + i, (unsigned long long)s_h[i]);
+}
+
 void compute_attr(gsw_graph *g) {
-  std::vector<int> &deg = g->hdeg;
-  deg.resize(g->n);
-  if (GSW_CUDA(cudaMemcpyAsync(deg.data(), g->odeg, sizeof(int) * g->n, cudaMemcpyDeviceToHost, stream()))) return;
-  GSW_CUDA(cudaStreamSynchronize(stream()));
   if (g->n < 2) return;
+  int *dmax = (int *)g->ctx->buf("attr_max", sizeof(int));
+  if (!dmax) return;
+  GSW_CUDA(cudaMemsetAsync(dmax, 0, sizeof(int), stream()));
+  k_deg_max<<<grid_for(g->n), 256, 0, stream()>>>(g->odeg, g->n, dmax);
   int mx = 0;
-  for (int d : deg) mx = std::max(mx, d);
-  std::vector<int64_t> hist((size_t)mx + 1, 0);
-  for (int d : deg) hist[d]++;
+  GSW_CUDA(cudaMemcpyAsync(&mx, dmax, sizeof(int), cudaMemcpyDeviceToHost, stream()));
+  GSW_CUDA(cudaStreamSynchronize(stream()));
+  const size_t bins = (size_t)MAX(mx + 1, HIST_SMEM);
+  unsigned long long *dh = (unsigned long long *)g->ctx->buf("attr_hist", sizeof(unsigned long long) * bins);
+  if (!dh || !ok()) return;
+  GSW_CUDA(cudaMemsetAsync(dh, 0, sizeof(unsigned long long) * bins, stream()));
+  k_deg_hist<<<grid_for(g->n), 256, 0, stream()>>>(g->odeg, g->n, dh);
+  std::vector<unsigned long long> hist(bins);
+  GSW_CUDA(cudaMemcpyAsync(hist.data(), dh, sizeof(unsigned long long) * bins, cudaMemcpyDeviceToHost, stream()));
+  GSW_CUDA(cudaStreamSynchronize(stream()));
+  if (!ok()) return;
   const double nv = (double)g->n;
-  double avg = 0, sd = 0, sum = 0, gi = 0, her = 0;
-  for (int d = 0; d <= mx; ++d)
-    for (int64_t c = 0; c < hist[d]; ++c) {
-      avg += d;
-      sd += (double)d * d;
-    }
+  double avg = 0, sd = 0;
+  int mn = -1;
+  for (int d = 0; d <= mx; ++d) {
+    if (!hist[d]) continue;
+    if (mn < 0) mn = d;
+    avg += (double)hist[d] * d;  // integer-valued: exact in any order
+    sd += (double)hist[d] * ((double)d * d);
+  }
+  const double sum = avg;
   sd = std::sqrt((sd - avg * avg / nv) / (nv - 1));
   avg /= nv;
-  int mn = 0;
-  while (mn < mx && hist[mn] == 0) ++mn;
-  for (int d = 0; d <= mx; ++d)
-    for (int64_t c = 0; c < hist[d]; ++c) sum += d;
-  int64_t i = 1;
+  double gi = 0, her = 0, i0 = 0;
   const double lsum = std::log(sum);
-  for (int d = 0; d <= mx; ++d)
-    for (int64_t c = 0; c < hist[d]; ++c, ++i) {
-      const double du = d;
-      gi += (nv - i + 0.5) * du / nv / sum;
-      if (du != 0) her += du * (lsum - std::log(du)) / sum;
-    }
+  for (int d = 0; d <= mx; ++d) {
+    const double c = (double)hist[d];
+    if (c == 0) continue;
+    // sum over positions i0+1 .. i0+c of (n - i + 0.5) * d / n / sum
+    gi += (c * (nv + 0.5) - (c * i0 + c * (c + 1) / 2)) * d / nv / sum;
+    if (d != 0) her += c * d * (lsum - std::log((double)d)) / sum;
+    i0 += c;
+  }
   gi = 1 - 2 * gi;
   her = her / std::log(nv);
   g->attr[0] = avg;
   g->attr[1] = sd;
-  g->attr[2] = (double)(mx - mn);
+  g->attr[2] = (double)(mx - (mn < 0 ? 0 : mn));
   g->attr[3] = mx;
   g->attr[4] = gi;
   g->attr[5] = her;
+}
+
+// host copy of the degrees, fetched once when a caller needs it
+const std::vector<int> &host_degrees(gsw_graph *g) {
+  if ((int64_t)g->hdeg.size() != g->n) {
+    g->hdeg.resize(g->n);
+    GSW_CUDA(cudaMemcpyAsync(g->hdeg.data(), g->odeg, sizeof(int) * g->n, cudaMemcpyDeviceToHost, stream()));
+    GSW_CUDA(cudaStreamSynchronize(stream()));
+  }
+  return g->hdeg;
 }
 
 __global__ void k_sum_weights(const int *w, int64_t m, unsigned long long *out) {
@@ -236,7 +288,12 @@ int csr_from_keys(gsw_graph *g, uint64_t *keys, int64_t nkeys) {
 }
 
 int64_t root_deg(const gsw_graph *g, int64_t root) {
-  return root >= 0 && root < (int64_t)g->hdeg.size() ? g->hdeg[root] : -1;
+  if (root < 0 || root >= g->n) return -1;
+  if ((int64_t)g->hdeg.size() == g->n) return g->hdeg[root];
+  int d = 0;  // one value instead of the whole table
+  GSW_CUDA(cudaMemcpyAsync(&d, g->odeg + root, sizeof(int), cudaMemcpyDeviceToHost, stream()));
+  GSW_CUDA(cudaStreamSynchronize(stream()));
+  return d;
 }
 
 gsw_graph *new_graph(gsw_ctx *ctx, int64_t n) {
@@ -257,6 +314,15 @@ void free_graph(gsw_graph *g) {
   cudaFree(g->rdeg);
   cudaFree(g->rw);
   cudaFree(g->coo);
+  if (g->twod) {
+    cudaFree(g->twod->edge);
+    cudaFree(g->twod->tile_off);
+    cudaFree(g->twod->heavy_off);
+    cudaFree(g->twod->heavy_beg);
+    cudaFree(g->twod->heavy_end);
+    cudaFree(g->twod->heavy_src);
+    delete g->twod;
+  }
   delete g;
 }
 
@@ -320,6 +386,105 @@ int ensure_coo(gsw_graph *g) {
   return GSW_LAUNCHED();
 }
 
+// ---- 2D-partition layout (k_twod.cuh) ---------------------------------------
+__global__ void k_twod_count(const int64_t *off, const int *col, int64_t n, int64_t ntiles, int *cnt) {
+  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t row = (v >> TWOD_TILE_BITS) * ntiles;
+    for (int64_t e = off[v]; e < off[v + 1]; ++e) atomicAdd(cnt + row + (col[e] >> TWOD_TILE_BITS), 1);
+  }
+}
+__global__ void k_twod_keys(const int64_t *off, const int *col, int64_t n, int64_t ntiles, const int *cnt,
+                            uint64_t *keys) {
+  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
+    const uint64_t dt = (uint64_t)v >> TWOD_TILE_BITS, dl = (uint64_t)v & (TWOD_TILE - 1);
+    for (int64_t e = off[v]; e < off[v + 1]; ++e) {
+      const uint64_t u = (uint64_t)col[e];
+      const uint64_t st = u >> TWOD_TILE_BITS;
+      const uint64_t light = cnt[dt * ntiles + st] < TWOD_HEAVY ? 1 : 0;
+      keys[e] = twod_key(dt, light, st, dl, u & (TWOD_TILE - 1));
+    }
+  }
+}
+
+// in-edges of every destination, keyed and sorted; heavy block table on the
+// host from the per-pair counts
+int ensure_twod(gsw_graph *g) {
+  if (g->twod) return GSW_OK;
+  const int64_t n = g->n, m = g->m;
+  const int64_t ntiles = (n + TWOD_TILE - 1) / TWOD_TILE;
+  if (ntiles >= (1 << 19)) return set_error(GSW_ERR_UNSUPPORTED, "%s", "2D partition: too many tiles");
+  const int64_t *roff = g->directed ? g->roff : g->off;
+  const int *rcol = g->directed ? g->rcol : g->col;
+  int *cnt = nullptr;
+  uint64_t *keys = nullptr, *sorted = nullptr;
+  void *tmp = nullptr;
+  size_t tmpb = 0;
+  auto cleanup = [&]() {
+    cudaFree(cnt);
+    cudaFree(keys);
+    cudaFree(tmp);
+  };
+  if (GSW_CUDA(cudaMalloc((void **)&cnt, sizeof(int) * ntiles * ntiles))) return cleanup(), err().code;
+  GSW_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int) * ntiles * ntiles, stream()));
+  k_twod_count<<<grid_for(n), 256, 0, stream()>>>(roff, rcol, n, ntiles, cnt);
+  if (GSW_CUDA(cudaMalloc((void **)&keys, sizeof(uint64_t) * (m + 1)))) return cleanup(), err().code;
+  if (GSW_CUDA(cudaMalloc((void **)&sorted, sizeof(uint64_t) * (m + 1)))) return cleanup(), err().code;
+  k_twod_keys<<<grid_for(n), 256, 0, stream()>>>(roff, rcol, n, ntiles, cnt, keys);
+  cub::DeviceRadixSort::SortKeys(nullptr, tmpb, keys, sorted, m, 0, 64, stream());
+  if (GSW_CUDA(cudaMalloc(&tmp, tmpb))) return cudaFree(sorted), cleanup(), err().code;
+  GSW_CUDA(cub::DeviceRadixSort::SortKeys(tmp, tmpb, keys, sorted, m, 0, 64, stream()));
+  std::vector<int> hc((size_t)(ntiles * ntiles));
+  GSW_CUDA(cudaMemcpyAsync(hc.data(), cnt, sizeof(int) * hc.size(), cudaMemcpyDeviceToHost, stream()));
+  GSW_CUDA(cudaStreamSynchronize(stream()));
+  cleanup();
+  if (!ok()) {
+    cudaFree(sorted);
+    return err().code;
+  }
+  std::vector<int64_t> tile_off(ntiles + 1, 0), heavy_off(ntiles + 1, 0), hbeg, hend;
+  std::vector<int> hsrc;
+  for (int64_t dt = 0; dt < ntiles; ++dt) {
+    int64_t pos = tile_off[dt];
+    heavy_off[dt] = (int64_t)hsrc.size();
+    int64_t tot = 0;
+    for (int64_t st = 0; st < ntiles; ++st) {
+      const int c = hc[dt * ntiles + st];
+      tot += c;
+      if (c >= TWOD_HEAVY) {
+        hsrc.push_back((int)st);
+        hbeg.push_back(pos);
+        hend.push_back(pos + c);
+        pos += c;
+      }
+    }
+    tile_off[dt + 1] = tile_off[dt] + tot;
+  }
+  heavy_off[ntiles] = (int64_t)hsrc.size();
+  auto *t = new gsw_graph::twod_store();
+  t->edge = sorted;
+  auto up = [&](void **dst, const void *src, size_t bytes) {
+    if (GSW_CUDA(cudaMalloc(dst, bytes ? bytes : 8))) return;
+    if (bytes) GSW_CUDA(cudaMemcpyAsync(*dst, src, bytes, cudaMemcpyHostToDevice, stream()));
+  };
+  up((void **)&t->tile_off, tile_off.data(), sizeof(int64_t) * tile_off.size());
+  up((void **)&t->heavy_off, heavy_off.data(), sizeof(int64_t) * heavy_off.size());
+  up((void **)&t->heavy_beg, hbeg.data(), sizeof(int64_t) * hbeg.size());
+  up((void **)&t->heavy_end, hend.data(), sizeof(int64_t) * hend.size());
+  up((void **)&t->heavy_src, hsrc.data(), sizeof(int) * hsrc.size());
+  GSW_CUDA(cudaStreamSynchronize(stream()));
+  t->L.edge = t->edge;
+  t->L.tile_off = t->tile_off;
+  t->L.heavy_off = t->heavy_off;
+  t->L.heavy_beg = t->heavy_beg;
+  t->L.heavy_end = t->heavy_end;
+  t->L.heavy_src = t->heavy_src;
+  t->L.ntiles = ntiles;
+  t->L.nheavy = (int64_t)hsrc.size();
+  t->L.m = m;
+  g->twod = t;
+  return err().code;
+}
+
 // ---------------------------------------------------------------------------
 // run helpers
 // ---------------------------------------------------------------------------
@@ -345,9 +510,27 @@ void fill_root(T *p, T v, T rootv, int64_t root, int64_t n) {
 __global__ void k_reached_edges(const int *lvl_or_dist, int stride_ints, int unreached, const int *odeg, int64_t n,
                                 unsigned long long *out) {
   unsigned long long s = 0;
-  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
-    const int x = lvl_or_dist[v * stride_ints];
-    if (x != unreached && x >= 0) s += odeg[v];
+  const int64_t T = (int64_t)gridDim.x * blockDim.x;
+  const int64_t gt = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (stride_ints == 1) {  // four vertices per 16-byte load
+    const int64_t n4 = n / 4;
+    for (int64_t q = gt; q < n4; q += T) {
+      const int4 x = __ldg((const int4 *)lvl_or_dist + q);
+      const int4 d = __ldg((const int4 *)odeg + q);
+      s += (x.x != unreached && x.x >= 0) ? d.x : 0;
+      s += (x.y != unreached && x.y >= 0) ? d.y : 0;
+      s += (x.z != unreached && x.z >= 0) ? d.z : 0;
+      s += (x.w != unreached && x.w >= 0) ? d.w : 0;
+    }
+    for (int64_t v = 4 * n4 + gt; v < n; v += T) {
+      const int x = lvl_or_dist[v];
+      if (x != unreached && x >= 0) s += odeg[v];
+    }
+  } else {
+    for (int64_t v = gt; v < n; v += T) {
+      const int x = lvl_or_dist[v * stride_ints];
+      if (x != unreached && x >= 0) s += odeg[v];
+    }
   }
   s = warp_sum(s);
   if (lane_id() == 0 && s) atomicAdd(out, s);
@@ -365,6 +548,8 @@ int64_t reached_edges(gsw_ctx *ctx, gsw_graph *g, const int *vals, int stride, i
 }
 
 void apply_opts(const gsw_run_opts *o, config_t &conf) {
+  conf.conf_persistent = true;
+  opts().barrier_leave_test = false;
   if (!o) return;
   if (o->direction >= 0) {
     conf.force.has_direction = true;
@@ -384,6 +569,8 @@ void apply_opts(const gsw_run_opts *o, config_t &conf) {
   }
   conf.conf_sorted_queue = o->sorted_queue != 0;
   conf.conf_count_edges = o->account != 0;
+  conf.conf_persistent = o->persistent != 0;
+  opts().barrier_leave_test = o->barrier_test != 0;
   opts().verbose = o->verbose != 0;
   opts().timing = o->timing != 0;
   opts().force_grid = o->expand_grid;
@@ -474,6 +661,11 @@ void begin_stats(gsw_run_stats *st) {
   timing_pool().used = 0;
 }
 
+// levels of persistent launches count one each in the loop; report real levels
+void add_persistent_levels(gsw_run_stats *st, executor_t &ex, int64_t lv0, int64_t ln0) {
+  if (st) st->levels += (int)((ex.persistent_levels - lv0) - (ex.persistent_launches - ln0));
+}
+
 unsigned end_checks(active_set_t *as, gsw_run_stats *st) {
   const unsigned e = as->read_error();
   if (st) {
@@ -513,6 +705,7 @@ void gsw_run_opts_default(gsw_run_opts *o) {
   o->damping = 0.85f;
   o->eps = 0.01f;
   o->selector = GSW_SELECT_RULES;
+  o->persistent = GSW_AUTO;
 }
 
 gsw_status gsw_init(int device, gsw_ctx **out) {
@@ -680,8 +873,8 @@ gsw_status gsw_graph_destroy(gsw_graph *g) {
 gsw_status gsw_graph_roots(const gsw_graph *g, uint64_t seed, int count, int32_t *roots) {
   if (!g || !roots || count < 0) return fail(GSW_ERR_INVALID_ARG, "gsw_graph_roots: bad arguments");
   entry_guard eg(g->ctx);
-  const std::vector<int> &deg = g->hdeg;
-  if ((int64_t)deg.size() != g->n) return fail(GSW_ERR_INVALID_ARG, "gsw_graph_roots: graph has no degree table");
+  const std::vector<int> &deg = host_degrees(const_cast<gsw_graph *>(g));
+  if (!ok()) return eg.finish();
   const uint64_t key = stream_key(seed, ST_ROOT);
   int got = 0;
   uint64_t j = 0;
@@ -732,6 +925,8 @@ gsw_status gsw_bfs(gsw_ctx *ctx, gsw_graph *gr, int32_t root, const gsw_run_opts
   selector_t selector;
   executor_t &executor = ctx->executor;
   executor.insp = &inspector;
+  executor.twod = twod_layout();
+  const int64_t plv0 = executor.persistent_levels, pln0 = executor.persistent_launches;
   fets.centric = VC;
   fets.pattern = Idem;
   fets.fromall = false;
@@ -748,7 +943,7 @@ gsw_status gsw_bfs(gsw_ctx *ctx, gsw_graph *gr, int32_t root, const gsw_run_opts
   as.init(root);
   loop_trace tr{st, MAX_LEVELS};
   timer tm(ctx);
-  for (int level = 0; level < MAX_LEVELS && ok(); level++) {
+  for (int level = 0; ok(); level++) {
     inspector.inspect(as, g, f, stats, fets, conf);
     if (finish(as, g, f, conf)) break;
     selector.select(stats, fets, conf);
@@ -762,6 +957,7 @@ gsw_status gsw_bfs(gsw_ctx *ctx, gsw_graph *gr, int32_t root, const gsw_run_opts
   const double ms = tm.stop();
   tr.resolve();
   end_checks(&as, st);
+  add_persistent_levels(st, executor, plv0, pln0);
   if (st) {
     st->ms = ms;
     st->edges = reached_edges(ctx, gr, f.data.dg_wa, 1, -1);
@@ -797,6 +993,8 @@ gsw_status gsw_sssp(gsw_ctx *ctx, gsw_graph *gr, int32_t root, const gsw_run_opt
   selector_t selector;
   executor_t &executor = ctx->executor;
   executor.insp = &inspector;
+  executor.twod = twod_layout();
+  const int64_t plv0 = executor.persistent_levels, pln0 = executor.persistent_launches;
   fets.centric = VC;
   fets.pattern = Mono;
   fets.fromall = false;
@@ -813,7 +1011,7 @@ gsw_status gsw_sssp(gsw_ctx *ctx, gsw_graph *gr, int32_t root, const gsw_run_opt
   as.init(root);
   loop_trace tr{st, MAX_LEVELS};
   timer tm(ctx);
-  for (int level = 0; level < MAX_LEVELS && ok(); level++) {
+  for (int level = 0; ok(); level++) {
     inspector.inspect(as, g, f, stats, fets, conf);
     selector.select(stats, fets, conf);
     executor.filter(as, g, f, stats, fets, conf);
@@ -826,6 +1024,7 @@ gsw_status gsw_sssp(gsw_ctx *ctx, gsw_graph *gr, int32_t root, const gsw_run_opt
   const double ms = tm.stop();
   tr.resolve();
   end_checks(&as, st);
+  add_persistent_levels(st, executor, plv0, pln0);
   if (st) {
     st->ms = ms;
     st->edges = reached_edges(ctx, gr, f.data.dg_wa, 1, INT_MAX);
@@ -867,6 +1066,8 @@ gsw_status gsw_cc(gsw_ctx *ctx, gsw_graph *gr, const gsw_run_opts *o, int32_t *l
   selector_t selector;
   executor_t &executor = ctx->executor;
   executor.insp = &inspector;
+  executor.twod = twod_layout();
+  const int64_t plv0 = executor.persistent_levels, pln0 = executor.persistent_launches;
   fets.centric = EC;
   fets.pattern = ASSO;
   apply_opts(o, conf);
@@ -879,7 +1080,7 @@ gsw_status gsw_cc(gsw_ctx *ctx, gsw_graph *gr, const gsw_run_opts *o, int32_t *l
   as.init(ALL_ACTIVE);
   loop_trace tr{st, MAX_LEVELS};
   timer tm(ctx);
-  for (int level = 0; level < MAX_LEVELS && ok() && gr->ncoo > 0; level++) {
+  for (int level = 0; ok() && gr->ncoo > 0; level++) {
     inspector.inspect(as, g, f, stats, fets, conf);
     if (finish(as, g, f, conf)) break;
     selector.select(stats, fets, conf);
@@ -894,6 +1095,7 @@ gsw_status gsw_cc(gsw_ctx *ctx, gsw_graph *gr, const gsw_run_opts *o, int32_t *l
   const double ms = tm.stop();
   tr.resolve();
   end_checks(&as, st);
+  add_persistent_levels(st, executor, plv0, pln0);
   if (st) {
     st->ms = ms;
     st->edges = gr->ncoo;
@@ -940,11 +1142,17 @@ gsw_status gsw_pagerank(gsw_ctx *ctx, gsw_graph *gr, const gsw_run_opts *o, floa
   selector_t selector;
   executor_t &executor = ctx->executor;
   executor.insp = &inspector;
+  executor.twod = twod_layout();
+  const int64_t plv0 = executor.persistent_levels, pln0 = executor.persistent_launches;
   fets.centric = VC;
   fets.pattern = ASSO;
   fets.fromall = true;
   fets.toall = true;
   apply_opts(op, conf);
+  if (conf.force.has_lb && conf.force.lb == TWOD) {
+    if (ensure_twod(gr)) return eg.finish();
+    executor.twod = gr->twod->L;
+  }
   set_graph_features(fets, gr);
   init_conf_impl(stats, fets, conf, g, f, 0.0, gr->attr[0], false);
   active_set_t *asp = ctx->aset(gr->n, conf.conf_qmode);
@@ -955,7 +1163,7 @@ gsw_status gsw_pagerank(gsw_ctx *ctx, gsw_graph *gr, const gsw_run_opts *o, floa
   loop_trace tr{st, MAX_LEVELS};
   timer tm(ctx);
   int steps = 0;
-  for (int level = 0; level < MAX_LEVELS && ok(); level++) {
+  for (int level = 0; ok(); level++) {
     inspector.inspect(as, g, f, stats, fets, conf);
     if (op->max_iters > 0 && level == op->max_iters) break;
     if (finish(as, g, f, conf)) break;
@@ -971,6 +1179,7 @@ gsw_status gsw_pagerank(gsw_ctx *ctx, gsw_graph *gr, const gsw_run_opts *o, floa
   const double ms = tm.stop();
   tr.resolve();
   end_checks(&as, st);
+  add_persistent_levels(st, executor, plv0, pln0);
   if (st) {
     st->ms = ms;
     st->edges = gr->m * (int64_t)steps;
@@ -1046,6 +1255,8 @@ gsw_status gsw_bc(gsw_ctx *ctx, gsw_graph *gr, int32_t root, const gsw_run_opts 
   selector_t selector;
   executor_t &executor = ctx->executor;
   executor.insp = &inspector;
+  executor.twod = twod_layout();
+  const int64_t plv0 = executor.persistent_levels, pln0 = executor.persistent_launches;
   fets.centric = VC;
   fets.pattern = ASSO;
   fets.fromall = false;
@@ -1069,7 +1280,7 @@ gsw_status gsw_bc(gsw_ctx *ctx, gsw_graph *gr, int32_t root, const gsw_run_opts 
   as.init(root);
   loop_trace tr{st, MAX_LEVELS};
   timer tm(ctx);
-  for (int level = 0; level < MAX_LEVELS && ok(); level++) {
+  for (int level = 0; ok(); level++) {
     inspector.inspect(as, g, f, stats, fets, conf);
     if (finish(as, g, f, conf)) break;
     selector.select(stats, fets, conf);
@@ -1091,7 +1302,7 @@ gsw_status gsw_bc(gsw_ctx *ctx, gsw_graph *gr, int32_t root, const gsw_run_opts 
   g.level = lmax;
   if (!replay) conf.conf_first_round = false;  // inspect the deepest level too
   as.init(ALL_INACTIVE);
-  for (int level = 0; level < MAX_LEVELS && ok(); level++) {
+  for (int level = 0; ok(); level++) {
     inspector.inspect(as, g, h, stats, fets, conf);
     if (finish(as, g, h, conf)) break;
     selector.select(stats, fets, conf);
@@ -1105,6 +1316,7 @@ gsw_status gsw_bc(gsw_ctx *ctx, gsw_graph *gr, int32_t root, const gsw_run_opts 
   const double ms = tm.stop();
   tr.resolve();
   end_checks(&as, st);
+  add_persistent_levels(st, executor, plv0, pln0);
   if (st) {
     st->ms = ms;
     st->edges = fwd_edges;
@@ -1137,6 +1349,7 @@ gsw_status gsw_gc(gsw_ctx *ctx, gsw_graph *gr, const gsw_run_opts *o, int32_t *c
   if (!f.data.dg_wa || !f.data.dg_ra) return eg.finish();
   fill<int>(f.data.dg_wa, -1, gr->n);
   fill<int>(f.data.dg_ra, -1, gr->n);
+  f.data.set_zero(-1);  // identity of the max the colouring accumulates
   feature_t fets;
   config_t conf;
   stat_t &stats = ctx->stats;
@@ -1145,12 +1358,18 @@ gsw_status gsw_gc(gsw_ctx *ctx, gsw_graph *gr, const gsw_run_opts *o, int32_t *c
   selector_t selector;
   executor_t &executor = ctx->executor;
   executor.insp = &inspector;
+  executor.twod = twod_layout();
+  const int64_t plv0 = executor.persistent_levels, pln0 = executor.persistent_launches;
   fets.centric = VC;
   fets.pattern = ASSO;
   fets.fromall = true;
   fets.toall = true;
   conf.conf_fixed = true;
   apply_opts(o, conf);
+  if (conf.force.has_lb && conf.force.lb == TWOD) {
+    if (ensure_twod(gr)) return eg.finish();
+    executor.twod = gr->twod->L;
+  }
   set_graph_features(fets, gr);
   init_conf_impl(stats, fets, conf, g, f, 0.0, gr->attr[0], false);
   active_set_t *asp = ctx->aset(gr->n, conf.conf_qmode);
@@ -1160,7 +1379,7 @@ gsw_status gsw_gc(gsw_ctx *ctx, gsw_graph *gr, const gsw_run_opts *o, int32_t *c
   as.init(ALL_ACTIVE);
   loop_trace tr{st, MAX_LEVELS};
   timer tm(ctx);
-  for (int level = 0; level < MAX_LEVELS && ok(); level++) {
+  for (int level = 0; ok(); level++) {
     inspector.inspect(as, g, f, stats, fets, conf);
     if (finish(as, g, f, conf)) break;
     selector.select(stats, fets, conf);
@@ -1174,6 +1393,7 @@ gsw_status gsw_gc(gsw_ctx *ctx, gsw_graph *gr, const gsw_run_opts *o, int32_t *c
   const double ms = tm.stop();
   tr.resolve();
   end_checks(&as, st);
+  add_persistent_levels(st, executor, plv0, pln0);
   if (st) {
     st->ms = ms;
     st->edges = gr->m / 2;

@@ -112,7 +112,13 @@ typedef struct gsw_run_opts {
   int expand_grid;   /* >0: fixed expand grid (autotuner) */
   int account;       /* 1: count the edges each expand touches (with timing,
                         for roofline accounting; adds one atomic per thread) */
-  int reserved[7];
+  int persistent;    /* fused levels in one grid-wide launch: GSW_AUTO (on),
+                        0 off (one launch per level), 1 on */
+  int barrier_test;  /* failure-path test only: in a grid-wide launch one
+                        block leaves without reaching the level barrier, the
+                        others' wait (bounded to 20 ms) expires and the call
+                        returns GSW_ERR_TIMEOUT */
+  int reserved[5];
 } gsw_run_opts;
 
 void gsw_run_opts_default(gsw_run_opts *o);
