@@ -51,7 +51,7 @@ class _Opts(C.Structure):
                 ("sorted_queue", C.c_int), ("max_iters", C.c_int), ("damping", C.c_float),
                 ("eps", C.c_float), ("selector", C.c_int), ("verbose", C.c_int), ("timing", C.c_int),
                 ("expand_grid", C.c_int), ("account", C.c_int), ("persistent", C.c_int), ("barrier_test", C.c_int),
-                ("reserved", C.c_int * 5)]
+                ("captured", C.c_int), ("reserved", C.c_int * 4)]
 
 
 class _Stats(C.Structure):
@@ -118,13 +118,14 @@ class RunOpts:
 
     def __init__(self, direction=None, asfmt=None, lb=None, fusion=None, sorted_queue=True,
                  max_iters=0, damping=0.85, eps=0.01, verbose=False, timing=False, expand_grid=0,
-                 account=False, persistent=None, barrier_test=False):
+                 account=False, persistent=None, barrier_test=False, captured=False):
         self.direction, self.asfmt, self.lb, self.fusion = direction, asfmt, lb, fusion
         self.sorted_queue, self.max_iters, self.damping, self.eps = sorted_queue, max_iters, damping, eps
         self.verbose, self.timing, self.expand_grid = verbose, timing, expand_grid
         self.account = account
         self.persistent = persistent
         self.barrier_test = barrier_test
+        self.captured = captured
 
     @classmethod
     def from_config(cls, cfg: str, **kw):
@@ -149,6 +150,7 @@ class RunOpts:
         o.account = int(self.account)
         o.persistent = AUTO if self.persistent is None else int(bool(self.persistent))
         o.barrier_test = int(self.barrier_test)
+        o.captured = int(bool(self.captured))
         return o
 
 

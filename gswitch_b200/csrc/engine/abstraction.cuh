@@ -21,13 +21,38 @@
 
 namespace gsw {
 
-inline int eval_tree(const tree_node *t, const double *fv) {
+__host__ __device__ inline int eval_tree(const tree_node *t, const double *fv) {
   int i = 0;
   for (int guard = 0; guard < 4096 && t[i].feat >= 0; ++guard)
     i = fv[t[i].feat] <= t[i].thr ? t[i].left : t[i].right;
   return t[i].left;
 }
 inline int eval_tree(const tree_node *t, const std::vector<double> &fv) { return eval_tree(t, fv.data()); }
+
+// The selector's trees: the host tables of selector_trees.h, or their copy in
+// device memory for the in-stream selector of the captured level loop.
+struct tree_set {
+  const tree_node *dir_idem, *dir_asso, *dir_asso_backup, *fmt, *fusion, *lb_idem, *lb_asso_forward,
+      *lb_asso_backward, *lb_asso_backward_backup;
+};
+inline const tree_set &host_tree_set() {
+  static const tree_set t = {select_dir_idem_tree, select_dir_asso_tree, select_dir_asso_backup_tree,
+                             select_fmt_tree,      select_fusion_tree,   select_lb_idem_tree,
+                             select_lb_asso_forward_tree, select_lb_asso_backward_tree,
+                             select_lb_asso_backward_backup_tree};
+  return t;
+}
+
+// Products in decision arithmetic are rounded on their own (never fused into
+// a multiply-add), so the device selector reproduces the host's doubles bit
+// for bit.
+__host__ __device__ __forceinline__ double mul_unfused(double a, double b) {
+#ifdef __CUDA_ARCH__
+  return __dmul_rn(a, b);
+#else
+  return a * b;
+#endif
+}
 
 }  // namespace gsw
 
@@ -366,7 +391,7 @@ struct feature_t {
 
   void reset() {}
 
-  void flatten() {
+  __host__ __device__ void flatten() {
     fv[0] = (double)nvertexs;
     fv[1] = (double)nedges;
     fv[2] = avg_deg;
@@ -393,9 +418,12 @@ struct feature_t {
 
   // from-all patterns see every vertex as a source, to-all patterns every
   // vertex as a target: fold the other side's workload in (features.cuh:46-84)
-  void cross() {
+  __host__ __device__ void cross() {
     const double av = active_vertex, uv = unactive_vertex;
-    const double mixed = (av + uv == 0) ? 0 : ((cur_avg_deg_active * av + cur_avg_deg_unactive * uv) / (av + uv));
+    const double mixed = (av + uv == 0) ? 0
+                                        : ((gsw::mul_unfused(cur_avg_deg_active, av) +
+                                            gsw::mul_unfused(cur_avg_deg_unactive, uv)) /
+                                           (av + uv));
     if (fromall) {
       fv[7] += unactive_vertex;
       fv[9] += pull_workload;

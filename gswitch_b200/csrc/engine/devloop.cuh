@@ -1,0 +1,412 @@
+// Captured level loop: the whole inspect -> select -> filter -> expand loop of
+// a vertex-centric run as ONE CUDA graph that runs to convergence without the
+// host.  The reference drives every level from the host and synchronises
+// four times per level (src/abstraction/inspector.cuh:39-110, selector.cuh:
+// 22-76, executor.cuh:17-151, application/bfs.cu:104-153); here the host
+// launches the graph once and reads the result.
+//
+//   WHILE (loop) {
+//     k_dl_select            one CTA: consumes the last inspection's counters,
+//                            runs the selector on the device (the same trees
+//                            and arithmetic as the host loop), advances the
+//                            level and the queue cursor and picks the bodies
+//     SWITCH (filter) {...}  bitmap -> queue builders, one body per
+//                            (sorted, target, input cursor), or visited reset
+//     SWITCH (expand) {...}  one body per (direction, format, load balance,
+//                            fusion) x queue cursor; each is the host loop's
+//                            own launch sequence, captured once
+//     IF (inspect) {...}     the next level's inspection (skipped on fused
+//                            levels and when the expand found no input)
+//   }
+//
+// The select kernel writes every conditional handle at every iteration (an
+// out-of-range switch value runs no body): a body graph's handles keep their
+// last value from one iteration to the next.  Kernels read the level through
+// device_graph_t::dlevel and the queue cursor is baked per body, so no kernel
+// parameter changes between levels.  Differences from the host loop: fused
+// levels run one launch per level (never the cooperative multi-level kernel,
+// whose early exit needs a host decision), and the wall-clock rule that
+// returns a slow fused level to the standalone form (executor.cuh:128-131)
+// does not apply.
+#pragma once
+#include <vector>
+
+#include "executor.cuh"
+
+namespace gsw {
+
+constexpr int DL_VARIANTS = 64;       // lb (3 bits) | bitmap << 3 | pull << 4 | fused << 5
+constexpr int DL_FILTER_BODIES = 13;  // 12 builders (sorted x target x cursor) + visited reset
+constexpr int DL_FILTER_CLEAR = 12;
+constexpr int DL_MAX_TREE_NODES = 1344;  // all selector trees (1,323 nodes) fit shared memory
+
+__host__ __device__ inline int dl_variant(Direction d, ASFmt a, LB lb, bool fused) {
+  return ((int)lb & 7) | ((a == Bitmap) << 3) | ((d == Pull) << 4) | ((fused ? 1 : 0) << 5);
+}
+__host__ __device__ inline int dl_target_index(Status t) { return t == Active ? 0 : (t == Inactive ? 1 : 2); }
+__host__ __device__ inline int dl_filter_body(bool sorted, Status target, int cursor) {
+  return ((sorted ? 3 : 0) + dl_target_index(target)) * 2 + cursor;
+}
+
+enum dl_status_t { DL_RUNNING = 0, DL_DONE = 1, DL_LEVEL_CAP = 2, DL_NO_BODY = 3, DL_NOT_INSPECTED = 4 };
+
+// Device state of one captured loop (lives in device memory; the host writes
+// the initial image before each launch and reads it back afterwards).
+struct dloop_t {
+  feature_t fets;
+  config_t conf;
+  tree_set trees;               // device copies of the selector's trees
+  const tree_node *tree_base;   // the one allocation `trees` points into
+  int tree_nodes;
+  level_counts raw;             // counters of the last inspection (frontier hints)
+  int level;                    // the level kernels read
+  int cursor;                   // Normal queue: input subqueue
+  int halt;                     // set by an expand whose input is empty
+  int inspected;                // the previous iteration ran the inspection
+  int iter;                     // iterations (levels) so far
+  int max_iters;                // > 0: stop at this iteration, after its inspection
+  int iter_cap;                 // iterations before the loop gives up
+  int sorted;                   // sorted bitmap -> queue builder
+  int status;                   // dl_status_t
+  int ntrace, trace_cap;
+  int *trace_cfg;
+  long long *trace_frontier;
+  long long *trace_edges;
+  unsigned long long *info;     // the inspector's statistics block
+  unsigned long long *scanned;  // accounting counter (null: not counting)
+  int *qsize;                   // the Normal queue's two size words
+  long long nvertexs, nedges, as_size;
+  long long launches;           // kernels the loop ran
+  int variant_body[DL_VARIANTS];  // variant -> expand body (-1: none)
+  int expand_kernels[2 * DL_VARIANTS];
+  int filter_kernels[DL_FILTER_BODIES];
+  int inspect_kernels;
+  int n_expand_bodies;
+  cudaGraphConditionalHandle h_loop, h_filter, h_expand, h_inspect;
+};
+
+// one level's decisions: the host loop's inspect-finish-select-filter-update
+// sequence (gsw_capi.cu runners) on device state, by one thread
+__device__ inline void dl_step(dloop_t &d, const level_counts &c, unsigned long long scanned) {
+  auto stop = [&](int status) {
+    d.status = status;
+    cudaGraphSetConditional(d.h_loop, 0);
+    cudaGraphSetConditional(d.h_filter, DL_FILTER_BODIES);
+    cudaGraphSetConditional(d.h_expand, 2 * DL_VARIANTS);
+    cudaGraphSetConditional(d.h_inspect, 0);
+  };
+  if (d.ntrace > 0 && d.ntrace <= d.trace_cap) d.trace_edges[d.ntrace - 1] = (long long)scanned;
+  if (d.halt) return stop(DL_DONE);  // the last expand found an empty input
+  feature_t &fets = d.fets;
+  config_t &conf = d.conf;
+  fets_level_init(fets, d.level, d.nvertexs, d.nedges);
+  bool need = !conf.conf_fuse_inspect;
+  bool done = false;
+  if (need && conf.conf_first_round) {
+    d.raw = fets_first(fets, d.nvertexs, d.nedges);
+    need = false;
+  }
+  if (need) {
+    if (!d.inspected) return stop(DL_NOT_INSPECTED);
+    d.raw = c;
+    done = fets_from_counts(fets, c, d.nvertexs, d.nedges);
+  }
+  fets.flatten();
+  if (d.max_iters > 0 && d.iter == d.max_iters) return stop(DL_DONE);
+  if (done) return stop(DL_DONE);
+  if (d.iter >= d.iter_cap) return stop(DL_LEVEL_CAP);
+  selector_t sel;
+  sel.trees = &d.trees;
+  sel.decide(fets, conf);
+  // filter: queue build (or visited reset) from the pre-swap cursor, then swap
+  int fbody = DL_FILTER_BODIES;  // none
+  if (conf.conf_asfmt == Queue) {
+    if (level_builds_queue(conf))
+      fbody = dl_filter_body(d.sorted != 0, conf.conf_target, d.cursor);
+    else if (!conf.conf_pruning)
+      fbody = DL_FILTER_CLEAR;
+    d.qsize[d.cursor] = 0;
+    d.cursor ^= 1;
+  }
+  level_grid_bookkeeping(fets, conf);
+  long long fr;
+  if (conf.conf_asfmt == Bitmap) {
+    fr = d.as_size;
+  } else if (!conf.conf_fuse_inspect) {
+    const Status t = conf.conf_target;
+    fr = t == Active ? d.raw.active : (t == Inactive ? d.raw.inactive : d.raw.active + d.raw.inactive);
+  } else {
+    fr = -1;
+  }
+  if (fr < 0 || fr > d.as_size) fr = -1;
+  d.level += 1;  // g.update_level()
+  const int v = dl_variant(conf.conf_dir, conf.conf_asfmt, conf.conf_lb, conf.conf_fuse_inspect);
+  const int vb = d.variant_body[v];
+  if (vb < 0) return stop(DL_NO_BODY);
+  const int ebody = vb * 2 + (conf.conf_asfmt == Queue ? d.cursor : 0);
+  if (d.ntrace < d.trace_cap) {
+    d.trace_cfg[d.ntrace] = (conf.conf_dir == Pull) | ((conf.conf_asfmt == Bitmap) << 1) | ((int)conf.conf_lb << 2) |
+                            ((conf.conf_fuse_inspect ? 1 : 0) << 5);
+    d.trace_frontier[d.ntrace] = fr;
+    d.trace_edges[d.ntrace] = 0;
+  }
+  d.ntrace++;
+  conf.conf_first_round = false;
+  d.iter++;
+  d.inspected = !conf.conf_fuse_inspect;
+  d.launches += 1 + (fbody < DL_FILTER_BODIES ? d.filter_kernels[fbody] : 0) + d.expand_kernels[ebody] +
+                (d.inspected ? d.inspect_kernels : 0);
+  cudaGraphSetConditional(d.h_filter, fbody);
+  cudaGraphSetConditional(d.h_expand, ebody);
+  cudaGraphSetConditional(d.h_inspect, d.inspected ? 1 : 0);
+}
+
+// The decision thread works on a shared-memory copy of the loop state and of
+// the trees (a tree walk is a chain of dependent loads; from shared memory it
+// takes nanoseconds per node instead of an L2 round trip), and the block
+// writes the state back at the end.
+__global__ void __launch_bounds__(256) k_dl_select(dloop_t *d) {
+  constexpr int WORDS = (int)(sizeof(dloop_t) / 8);
+  static_assert(sizeof(dloop_t) % 8 == 0, "loop state is copied in 8-byte words");
+  static_assert(sizeof(tree_node) % 8 == 0, "tree nodes are copied in 8-byte words");
+  __shared__ __align__(16) unsigned long long s_state[WORDS];
+  __shared__ __align__(16) unsigned long long s_tree[DL_MAX_TREE_NODES * sizeof(tree_node) / 8];
+  __shared__ level_counts s_c;
+  __shared__ unsigned long long s_scanned;
+  dloop_t &sd = *reinterpret_cast<dloop_t *>(s_state);
+  const unsigned long long *src = reinterpret_cast<const unsigned long long *>(d);
+  for (int i = threadIdx.x; i < WORDS; i += blockDim.x) s_state[i] = src[i];
+  if (threadIdx.x == 0) {
+    const unsigned long long *info = d->info;
+    s_c.active = (int64_t)info[0];
+    s_c.inactive = (int64_t)info[1];
+    s_c.push = (int64_t)info[2];
+    s_c.pull = (int64_t)info[3];
+    s_c.max_push = (int64_t)info[4];
+    s_c.max_pull = (int64_t)info[5];
+    s_scanned = d->scanned ? *d->scanned : 0ull;
+  }
+  __syncthreads();
+  const int tree_words = min(sd.tree_nodes, DL_MAX_TREE_NODES) * (int)(sizeof(tree_node) / 8);
+  const unsigned long long *tsrc = reinterpret_cast<const unsigned long long *>(sd.tree_base);
+  for (int i = threadIdx.x; i < tree_words; i += blockDim.x) s_tree[i] = __ldg(tsrc + i);
+  // the counters start from zero for the next inspection
+  for (int i = threadIdx.x; i < STAT_SLOTS; i += blockDim.x) sd.info[i] = 0;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    if (sd.scanned) *sd.scanned = 0;
+    const tree_set dev = sd.trees;
+    const tree_node *base = sd.tree_base, *sh = reinterpret_cast<const tree_node *>(s_tree);
+    sd.trees = tree_set{sh + (dev.dir_idem - base),        sh + (dev.dir_asso - base),
+                        sh + (dev.dir_asso_backup - base), sh + (dev.fmt - base),
+                        sh + (dev.fusion - base),          sh + (dev.lb_idem - base),
+                        sh + (dev.lb_asso_forward - base), sh + (dev.lb_asso_backward - base),
+                        sh + (dev.lb_asso_backward_backup - base)};
+    dl_step(sd, s_c, s_scanned);
+    sd.trees = dev;
+  }
+  __syncthreads();
+  unsigned long long *dst = reinterpret_cast<unsigned long long *>(d);
+  for (int i = threadIdx.x; i < WORDS; i += blockDim.x) dst[i] = s_state[i];
+}
+
+// ---------------------------------------------------------------------------
+// graph construction
+// ---------------------------------------------------------------------------
+
+// adds a conditional node at the current capture position of `s`
+inline bool dl_add_conditional(cudaStream_t s, cudaGraphConditionalHandle h, cudaGraphConditionalNodeType type,
+                               unsigned size, std::vector<cudaGraph_t> &bodies) {
+  cudaStreamCaptureStatus st;
+  cudaGraph_t g = nullptr;
+  const cudaGraphNode_t *deps = nullptr;
+  size_t nd = 0;
+  if (GSW_CUDA(cudaStreamGetCaptureInfo(s, &st, nullptr, &g, &deps, &nd))) return false;
+  cudaGraphNodeParams p = {};
+  p.type = cudaGraphNodeTypeConditional;
+  p.conditional.handle = h;
+  p.conditional.type = type;
+  p.conditional.size = size;
+  cudaGraphNode_t node;
+  if (GSW_CUDA(cudaGraphAddNode(&node, g, deps, nd, &p))) return false;
+  bodies.assign(p.conditional.phGraph_out, p.conditional.phGraph_out + size);
+  return !GSW_CUDA(cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies));
+}
+
+inline int dl_count_nodes(cudaGraph_t g) {
+  size_t n = 0;
+  cudaGraphGetNodes(g, nullptr, &n);
+  return (int)n;
+}
+
+// captures whatever `launch` issues on the context stream into `body`
+template <typename L>
+inline bool dl_capture(cudaGraph_t body, L &&launch) {
+  if (GSW_CUDA(cudaStreamBeginCaptureToGraph(stream(), body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed)))
+    return false;
+  launch();
+  cudaGraph_t out = nullptr;
+  const bool good = !GSW_CUDA(cudaStreamEndCapture(stream(), &out));
+  return good && ok();
+}
+
+// A built loop: the executable graph plus what the host needs to drive it.
+struct dloop_graph {
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  std::vector<unsigned long long> key;
+  dloop_t image;  // handles and body tables; the per-run fields are filled at launch
+  void destroy() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    exec = nullptr;
+    graph = nullptr;
+    key.clear();
+  }
+};
+
+// Builds the captured loop of a CSR (vertex-centric) run.  `as`, `g`, `f`
+// and `conf` are the run's own objects after init_conf; `d` is the device
+// address of the loop state.  Every body is captured through the executor's
+// ordinary launch code with the grid derived from resident occupancy.
+template <typename E, typename F>
+bool dl_build(dloop_graph &L, executor_t &ex, dloop_t *d, active_set_t as, device_graph_t<CSR, E> g, F f,
+              config_t conf, const feature_t &fets, unsigned long long *info) {
+  using G = device_graph_t<CSR, E>;
+  L.destroy();
+  g.dlevel = &d->level;
+  as.nt.dg_tag = &d->halt;
+  as.nt.already = false;
+  as.queue.traceback = false;
+  conf.conf_persistent = false;
+  const bool saved_timing = opts().timing;
+  opts().timing = false;
+  const long long launches0 = launch_count();
+  const hints_t saved_hints = hints();
+  hints().frontier = -1;
+  hints().edges = -1;
+  ex.ensure_tiles(g.nedges + as.size + 1);
+  dloop_t &im = L.image;
+  im = dloop_t();
+  for (int &b : im.variant_body) b = -1;
+  bool good = ok();
+  // the variants this run can reach
+  struct vdesc {
+    Direction d;
+    ASFmt a;
+    LB lb;
+    bool fused;
+  };
+  std::vector<vdesc> vs;
+  const LB lbs[5] = {TM, WM, CM, STRICT, TWC};
+  for (LB lb : lbs) {
+    vs.push_back({Push, Queue, lb, false});
+    vs.push_back({Push, Queue, lb, true});
+    vs.push_back({Push, Bitmap, lb, false});
+    vs.push_back({Pull, Queue, lb, false});
+    vs.push_back({Pull, Bitmap, lb, false});
+  }
+  const bool twod_ok = fets.fromall && fets.toall && ex.twod.edge;
+  if (twod_ok) vs.push_back({Push, Bitmap, TWOD, false});
+  for (size_t i = 0; i < vs.size(); ++i) {
+    const vdesc &v = vs[i];
+    if (v.lb == TWOD) {
+      for (Direction dd : {Push, Pull})
+        for (ASFmt aa : {Queue, Bitmap}) im.variant_body[dl_variant(dd, aa, TWOD, false)] = (int)i;
+    } else {
+      im.variant_body[dl_variant(v.d, v.a, v.lb, v.fused)] = (int)i;
+    }
+  }
+  im.n_expand_bodies = (int)vs.size();
+
+  cudaGraph_t top = nullptr;
+  good = good && !GSW_CUDA(cudaGraphCreate(&top, 0));
+  L.graph = top;
+  cudaGraphConditionalHandle hl = 0, hf = 0, he = 0, hi = 0;
+  std::vector<cudaGraph_t> wbody, fbodies, ebodies, ibody;
+  if (good) good = !GSW_CUDA(cudaGraphConditionalHandleCreate(&hl, top, 1, cudaGraphCondAssignDefault));
+  if (good) {
+    cudaGraphNodeParams p = {};
+    p.type = cudaGraphNodeTypeConditional;
+    p.conditional.handle = hl;
+    p.conditional.type = cudaGraphCondTypeWhile;
+    p.conditional.size = 1;
+    cudaGraphNode_t wn;
+    good = !GSW_CUDA(cudaGraphAddNode(&wn, top, nullptr, 0, &p));
+    if (good) wbody.assign(p.conditional.phGraph_out, p.conditional.phGraph_out + 1);
+  }
+  const unsigned nexp = 2u * (unsigned)vs.size();
+  if (good) {
+    cudaGraph_t B = wbody[0];
+    good = !GSW_CUDA(cudaGraphConditionalHandleCreate(&hf, B, DL_FILTER_BODIES, 0)) &&
+           !GSW_CUDA(cudaGraphConditionalHandleCreate(&he, B, 2 * DL_VARIANTS, 0)) &&
+           !GSW_CUDA(cudaGraphConditionalHandleCreate(&hi, B, 0, 0));
+    if (good)
+      good = dl_capture(B, [&] {
+        k_dl_select<<<1, 256, 0, stream()>>>(d);
+        if (dl_add_conditional(stream(), hf, cudaGraphCondTypeSwitch, DL_FILTER_BODIES, fbodies) &&
+            dl_add_conditional(stream(), he, cudaGraphCondTypeSwitch, nexp, ebodies))
+          dl_add_conditional(stream(), hi, cudaGraphCondTypeIf, 1, ibody);
+      });
+    good = good && fbodies.size() == DL_FILTER_BODIES && ebodies.size() == nexp && ibody.size() == 1;
+  }
+  // filter bodies
+  for (int sorted = 0; good && sorted < 2; ++sorted)
+    for (Status t : {Active, Inactive, All})
+      for (int cur = 0; good && cur < 2; ++cur) {
+        const int b = dl_filter_body(sorted != 0, t, cur);
+        active_set_t a = as;
+        a.fmt = Queue;
+        a.queue.cursor = cur;
+        good = dl_capture(fbodies[b], [&] { ex.build_queue(a, t, sorted != 0); });
+        im.filter_kernels[b] = dl_count_nodes(fbodies[b]);
+      }
+  if (good) {
+    good = dl_capture(fbodies[DL_FILTER_CLEAR],
+                      [&] { fill_u32(as.bitmap.visited.dg_bits, 0, as.bitmap.visited.n_words); });
+    im.filter_kernels[DL_FILTER_CLEAR] = dl_count_nodes(fbodies[DL_FILTER_CLEAR]);
+  }
+  // expand bodies
+  for (size_t i = 0; good && i < vs.size(); ++i)
+    for (int cur = 0; good && cur < 2; ++cur) {
+      const vdesc &v = vs[i];
+      config_t c = conf;
+      c.conf_dir = v.d;
+      c.conf_asfmt = v.a;
+      c.conf_lb = v.lb;
+      c.conf_fuse_inspect = v.fused;
+      c.conf_fromall = fets.fromall;
+      c.conf_toall = fets.toall;
+      c.conf_centric = fets.centric;
+      selector_t::set_target(c);
+      active_set_t a = as;
+      a.fmt = v.a;
+      a.queue.cursor = cur;
+      G gg = g;
+      const int b = (int)i * 2 + cur;
+      good = dl_capture(ebodies[b], [&] { ex.launch_vc(a, gg, f, c); });
+      im.expand_kernels[b] = dl_count_nodes(ebodies[b]);
+    }
+  // inspection body
+  if (good) {
+    good = dl_capture(ibody[0], [&] {
+      k_inspect_vc<<<INSPECT_CTAS, INSPECT_THREADS, 0, stream()>>>(as, g, f, info, &d->halt);
+    });
+    im.inspect_kernels = 1;
+  }
+  if (good) good = !GSW_CUDA(cudaGraphInstantiate(&L.exec, top, 0));
+  im.h_loop = hl;
+  im.h_filter = hf;
+  im.h_expand = he;
+  im.h_inspect = hi;
+  opts().timing = saved_timing;
+  launch_count() = launches0;
+  hints() = saved_hints;
+  if (!good) {
+    L.destroy();
+    if (ok()) set_error(GSW_ERR_CUDA, "%s", "captured level loop: graph construction failed");
+  }
+  return good;
+}
+
+}  // namespace gsw

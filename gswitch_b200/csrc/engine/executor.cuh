@@ -113,6 +113,109 @@ inline kernel_marks &marks() {
 }
 
 // ===========================================================================
+// Per-level decision arithmetic shared by the host loop and the in-stream
+// (captured) loop, so both take the same decisions from the same counters.
+// ===========================================================================
+struct level_counts {  // statistics block [0..5] of one inspection
+  int64_t active, inactive, push, pull, max_push, max_pull;
+};
+
+// inspector_t::init_fets (inspector.cuh:115-130)
+__host__ __device__ inline void fets_level_init(feature_t &fets, int level, int64_t nvertexs, int64_t edges) {
+  fets.level = level;
+  fets.active_vertex = 0;
+  fets.active_vertex_ratio = 0;
+  fets.unactive_vertex = (double)nvertexs;
+  fets.unactive_vertex_ratio = 1;
+  fets.growing_rate = fets.push_workload;
+  fets.push_workload = 0;
+  fets.pull_workload = (double)edges;
+  fets.push_workload_ratio = 0;
+  fets.pull_workload_ratio = 1;
+  fets.cur_avg_deg_active = 0;
+  fets.cur_avg_deg_unactive = fets.avg_deg;
+}
+
+// inspector_t::set_first_fets (inspector.cuh:180-204): the first level is
+// known without inspecting (one root, or every vertex)
+__host__ __device__ inline level_counts fets_first(feature_t &fets, int64_t nvertexs, int64_t nedges) {
+  if (fets.use_root < 0) {
+    fets.active_vertex = (double)nvertexs;
+    fets.unactive_vertex = 0;
+    fets.push_workload = (double)nedges;
+    fets.pull_workload = 0;
+  } else {
+    fets.active_vertex = 1;
+    fets.unactive_vertex = (double)(nvertexs - 1);
+    fets.push_workload = fets.first_workload;
+    fets.pull_workload = nedges - fets.first_workload;
+  }
+  fets.active_vertex_ratio = fets.active_vertex / nvertexs;
+  fets.unactive_vertex_ratio = fets.unactive_vertex / nvertexs;
+  fets.push_workload_ratio = fets.push_workload / nedges;
+  fets.pull_workload_ratio = fets.pull_workload / nedges;
+  fets.cur_avg_deg_active = DIV(fets.push_workload, fets.active_vertex);
+  fets.cur_avg_deg_unactive = DIV(fets.pull_workload, fets.unactive_vertex);
+  fets.cur_max_deg_active = fets.push_workload;
+  fets.cur_max_deg_unactive = fets.avg_deg;
+  level_counts c;
+  c.active = (int64_t)fets.active_vertex;
+  c.inactive = (int64_t)fets.unactive_vertex;
+  c.push = (int64_t)fets.push_workload;
+  c.pull = (int64_t)fets.pull_workload;
+  c.max_push = c.max_pull = 0;
+  return c;
+}
+
+// inspector_t::set_fets (inspector.cuh:206-241); returns true when the loop
+// is done (no active vertex, or an Idem pattern with nothing left to reach)
+__host__ __device__ inline bool fets_from_counts(feature_t &fets, const level_counts &c, int64_t nvertexs,
+                                                 int64_t nedges) {
+  fets.active_vertex = (double)c.active;
+  fets.unactive_vertex = (double)c.inactive;
+  fets.active_vertex_ratio = (double)c.active / nvertexs;
+  fets.unactive_vertex_ratio = (double)c.inactive / nvertexs;
+  bool done = fets.active_vertex <= 0;
+  if (fets.pattern == Idem && fets.unactive_vertex <= 0) done = true;
+  fets.growing_rate = (0.0 + c.push) / fets.growing_rate;
+  fets.push_workload = (double)c.push;
+  fets.pull_workload = (double)c.pull;
+  fets.push_workload_ratio = (double)c.push / nedges;
+  fets.pull_workload_ratio = (double)c.pull / nedges;
+  fets.cur_avg_deg_active = DIV(fets.push_workload, fets.active_vertex);
+  fets.cur_avg_deg_unactive = DIV(fets.pull_workload, fets.unactive_vertex);
+  fets.cur_max_deg_active = (double)c.max_push;
+  fets.cur_max_deg_unactive = (double)c.max_pull;
+  return done;
+}
+
+// executor_t::filter (executor.cuh:21-29): does a Queue level rebuild its
+// queue from the bitmaps?
+__host__ __device__ inline bool level_builds_queue(config_t &conf) {
+  bool tofilter = !conf.conf_fuse_inspect;
+  if (conf.conf_switch_to_fusion) {
+    tofilter = true;
+    conf.conf_switch_to_fusion = false;
+  }
+  if (conf.conf_first_round) tofilter = true;
+  return tofilter;
+}
+
+// grid bookkeeping of executor_t::filter (executor.cuh:30-52): idle levels
+// feed trigger_fusion, tiny STRICT levels fall back to CM
+__host__ __device__ inline void level_grid_bookkeeping(const feature_t &fets, config_t &conf) {
+  conf.thdnum = THDNUM_EXPAND;
+  if (conf.conf_fuse_inspect) {
+    conf.ctanum = 32;
+  } else {
+    const double workloads = conf.conf_dir == Push ? fets.push_workload : fets.pull_workload;
+    conf.ctanum = (int)MIN((double)CTANUM_EXPAND, workloads / conf.thdnum / 2 + 1);
+    conf.conf_idle = conf.ctanum < 4 ? conf.conf_idle + 1 : 0;
+    if (conf.ctanum < 5 && conf.conf_lb == STRICT && !conf.force.has_lb) conf.conf_lb = CM;
+  }
+}
+
+// ===========================================================================
 // inspector_t
 // ===========================================================================
 struct inspector_t {
@@ -158,73 +261,30 @@ struct inspector_t {
   }
 
   void init_fets(stat_t &stat, feature_t &fets, int64_t nvertexs, int64_t edges) {
-    fets.level = stat.level;
-    fets.active_vertex = 0;
-    fets.active_vertex_ratio = 0;
-    fets.unactive_vertex = (double)nvertexs;
-    fets.unactive_vertex_ratio = 1;
-    fets.growing_rate = fets.push_workload;
-    fets.push_workload = 0;
-    fets.pull_workload = (double)edges;
-    fets.push_workload_ratio = 0;
-    fets.pull_workload_ratio = 1;
-    fets.cur_avg_deg_active = 0;
-    fets.cur_avg_deg_unactive = fets.avg_deg;
+    fets_level_init(fets, stat.level, nvertexs, edges);
   }
 
   void set_first_fets(feature_t &fets, int64_t nvertexs, int64_t nedges) {
-    if (fets.use_root < 0) {
-      fets.active_vertex = (double)nvertexs;
-      fets.unactive_vertex = 0;
-      fets.push_workload = (double)nedges;
-      fets.pull_workload = 0;
-    } else {
-      fets.active_vertex = 1;
-      fets.unactive_vertex = (double)(nvertexs - 1);
-      fets.push_workload = fets.first_workload;
-      fets.pull_workload = nedges - fets.first_workload;
-    }
-    fets.active_vertex_ratio = fets.active_vertex / nvertexs;
-    fets.unactive_vertex_ratio = fets.unactive_vertex / nvertexs;
-    fets.push_workload_ratio = fets.push_workload / nedges;
-    fets.pull_workload_ratio = fets.pull_workload / nedges;
-    fets.cur_avg_deg_active = DIV(fets.push_workload, fets.active_vertex);
-    fets.cur_avg_deg_unactive = DIV(fets.pull_workload, fets.unactive_vertex);
-    fets.cur_max_deg_active = fets.push_workload;
-    fets.cur_max_deg_unactive = fets.avg_deg;
-    raw_frontier = (int64_t)fets.active_vertex;
-    raw_inactive = (int64_t)fets.unactive_vertex;
-    raw_push = (int64_t)fets.push_workload;
-    raw_pull = (int64_t)fets.pull_workload;
+    keep(fets_first(fets, nvertexs, nedges));
   }
 
   void set_fets(active_set_t &as, stat_t &stat, feature_t &fets, const config_t &conf, int64_t nvertexs,
                 int64_t nedges) {
     stat.collect(6);  // the one synchronisation of a standalone level
     stat.clean();
-    raw_frontier = stat.active_num();
-    raw_inactive = stat.unactive_num();
-    raw_push = stat.push_workload();
-    raw_pull = stat.pull_workload();
-    fets.active_vertex = (double)stat.active_num();
-    fets.unactive_vertex = (double)stat.unactive_num();
-    fets.active_vertex_ratio = (double)stat.active_num() / nvertexs;
-    fets.unactive_vertex_ratio = (double)stat.unactive_num() / nvertexs;
-    bool done = fets.active_vertex <= 0;
-    if (fets.pattern == Idem && fets.unactive_vertex <= 0) done = true;
-    if (done) {
+    const level_counts c = {stat.active_num(),    stat.unactive_num(),   stat.push_workload(),
+                            stat.pull_workload(), stat.max_deg_active(), stat.max_deg_unactive()};
+    keep(c);
+    if (fets_from_counts(fets, c, nvertexs, nedges)) {
       if (conf.conf_qmode == Cached) as.queue.swap();
       as.halt_host();
     }
-    fets.growing_rate = (0.0 + stat.push_workload()) / fets.growing_rate;
-    fets.push_workload = (double)stat.push_workload();
-    fets.pull_workload = (double)stat.pull_workload();
-    fets.push_workload_ratio = (double)stat.push_workload() / nedges;
-    fets.pull_workload_ratio = (double)stat.pull_workload() / nedges;
-    fets.cur_avg_deg_active = DIV(fets.push_workload, fets.active_vertex);
-    fets.cur_avg_deg_unactive = DIV(fets.pull_workload, fets.unactive_vertex);
-    fets.cur_max_deg_active = (double)stat.max_deg_active();
-    fets.cur_max_deg_unactive = (double)stat.max_deg_unactive();
+  }
+  void keep(const level_counts &c) {
+    raw_frontier = c.active;
+    raw_inactive = c.inactive;
+    raw_push = c.push;
+    raw_pull = c.pull;
   }
 
   // raw counters of the last inspection (before cross() folding)
@@ -234,12 +294,23 @@ struct inspector_t {
 // ===========================================================================
 // selector_t
 // ===========================================================================
-inline LB lb_from_class(int l) { return l == 0 ? WM : (l == 1 ? CM : STRICT); }
+__host__ __device__ inline LB lb_from_class(int l) { return l == 0 ? WM : (l == 1 ? CM : STRICT); }
 
 struct selector_t {
+  // null: the host tables; the in-stream selector points this at a copy of
+  // the trees on the device
+  const tree_set *trees = nullptr;
+  __host__ __device__ const tree_set &T() const {
+#ifdef __CUDA_ARCH__
+    return *trees;
+#else
+    return trees ? *trees : host_tree_set();
+#endif
+  }
+
   void select(stat_t &stats, feature_t &fets, config_t &conf) { select_based_on_model(stats, fets, conf); }
 
-  void trigger_fusion(const feature_t &fets, config_t &conf) {
+  __host__ __device__ void trigger_fusion(const feature_t &fets, config_t &conf) {
     if (conf.force.has_fusion) return;
     if (!conf.conf_fuse_inspect) {
       const double potential = fets.push_workload_ratio + fets.pull_workload_ratio;
@@ -256,7 +327,7 @@ struct selector_t {
     }
   }
 
-  void fusion(const feature_t &fets, config_t &conf) {
+  __host__ __device__ void fusion(const feature_t &fets, config_t &conf) {
     conf.conf_dir = Push;
     conf.conf_asfmt = Queue;
     conf.conf_cm = Interleave;
@@ -268,14 +339,14 @@ struct selector_t {
     set_target(conf);
   }
 
-  static void set_target(config_t &conf) {
+  __host__ __device__ static void set_target(config_t &conf) {
     if (conf.conf_dir == Push)
       conf.conf_target = conf.conf_fromall ? All : Active;
     else
       conf.conf_target = (conf.conf_toall && conf.conf_dir == Pull) ? All : Inactive;
   }
 
-  static void dir_ratios(const feature_t &fets, double *v) {
+  __host__ __device__ static void dir_ratios(const feature_t &fets, double *v) {
     const double *fv = fets.fv;
     v[0] = fv[8] / (fv[7] + 0.1);
     v[1] = fv[10] / (fv[9] + 0.1);
@@ -287,17 +358,17 @@ struct selector_t {
     v[7] = fv[10] / (fv[18] + 0.1);
   }
 
-  void select_idem(feature_t &fets, config_t &conf) {
+  __host__ __device__ void select_idem(feature_t &fets, config_t &conf) {
     double v[16];
     dir_ratios(fets, v);
-    conf.conf_dir = eval_tree(select_dir_idem_tree, v) == 1 ? Pull : Push;
+    conf.conf_dir = eval_tree(T().dir_idem, v) == 1 ? Pull : Push;
     if (fets.push_workload_ratio * 5 < fets.pull_workload_ratio) conf.conf_dir = Push;
     if (conf.force.has_direction) conf.conf_dir = conf.force.d;
     if (conf.conf_dir == Pull) {
       conf.conf_asfmt = fets.fv[12] < 0.01 ? Queue : Bitmap;
     } else {
       v[0] = fets.fv[11];
-      conf.conf_asfmt = eval_tree(select_fmt_tree, v) ? Bitmap : Queue;
+      conf.conf_asfmt = eval_tree(T().fmt, v) ? Bitmap : Queue;
     }
     if (conf.force.has_asfmt) conf.conf_asfmt = conf.force.asf;
     if (conf.conf_dir == Pull) {
@@ -306,23 +377,23 @@ struct selector_t {
       int k = 0;
       for (int i = 0; i < 7; ++i) v[k++] = fets.fv[i];
       for (int i = 7; i < 18; i += 2) v[k++] = fets.fv[i];
-      conf.conf_lb = lb_from_class(eval_tree(select_lb_idem_tree, v));
+      conf.conf_lb = lb_from_class(eval_tree(T().lb_idem, v));
     }
     if (conf.force.has_lb) conf.conf_lb = conf.force.lb;
   }
 
-  void select_ASSO(feature_t &fets, config_t &conf) {
+  __host__ __device__ void select_ASSO(feature_t &fets, config_t &conf) {
     double v[24];
     dir_ratios(fets, v);
-    conf.conf_dir = eval_tree(select_dir_asso_tree, v) == 1 ? Pull : Push;
+    conf.conf_dir = eval_tree(T().dir_asso, v) == 1 ? Pull : Push;
     if (conf.force.has_direction) conf.conf_dir = conf.force.d;
     if (conf.conf_fromall && conf.conf_toall) {
       for (int i = 0; i < 7; ++i) v[i] = fets.fv[i];
-      conf.conf_dir = eval_tree(select_dir_asso_backup_tree, v) ? Pull : Push;
+      conf.conf_dir = eval_tree(T().dir_asso_backup, v) ? Pull : Push;
       if (conf.force.has_direction) conf.conf_dir = conf.force.d;
     }
     v[0] = conf.conf_dir == Push ? fets.fv[11] : fets.fv[12];
-    conf.conf_asfmt = eval_tree(select_fmt_tree, v) ? Bitmap : Queue;
+    conf.conf_asfmt = eval_tree(T().fmt, v) ? Bitmap : Queue;
     if (fets.fromall && fets.toall && !conf.conf_fixed) conf.conf_asfmt = Bitmap;
     if (conf.force.has_asfmt) conf.conf_asfmt = conf.force.asf;
     int k = 0;
@@ -331,35 +402,38 @@ struct selector_t {
     const bool all2all = conf.conf_fromall && conf.conf_toall && !conf.conf_fixed;
     if (conf.conf_dir == Pull) {
       if (all2all) {
-        l = eval_tree(select_lb_asso_backward_backup_tree, v);
+        l = eval_tree(T().lb_asso_backward_backup, v);
       } else {
         for (int i = 8; i <= 18; i += 2) v[k++] = fets.fv[i];
-        l = eval_tree(select_lb_asso_backward_tree, v);
+        l = eval_tree(T().lb_asso_backward, v);
       }
     } else {
       if (all2all) {
-        l = eval_tree(select_lb_asso_backward_backup_tree, v);
+        l = eval_tree(T().lb_asso_backward_backup, v);
       } else {
         for (int i = 7; i < 18; i += 2) v[k++] = fets.fv[i];
-        l = eval_tree(select_lb_asso_forward_tree, v);
+        l = eval_tree(T().lb_asso_forward, v);
       }
     }
     conf.conf_lb = lb_from_class(l);
     if (conf.force.has_lb) conf.conf_lb = conf.force.lb;
   }
 
-  void select_Mono(feature_t &fets, config_t &conf) {
+  __host__ __device__ void select_Mono(feature_t &fets, config_t &conf) {
     conf.conf_dir = conf.force.has_direction ? conf.force.d : Push;
     conf.conf_asfmt = conf.force.has_asfmt ? conf.force.asf : Queue;
     double v[16];
     int k = 0;
     for (int i = 0; i < 7; ++i) v[k++] = fets.fv[i];
     for (int i = 7; i < 18; i += 2) v[k++] = fets.fv[i];
-    conf.conf_lb = lb_from_class(eval_tree(select_lb_asso_forward_tree, v));
+    conf.conf_lb = lb_from_class(eval_tree(T().lb_asso_forward, v));
     if (conf.force.has_lb) conf.conf_lb = conf.force.lb;
   }
 
-  void select_based_on_model(stat_t &, feature_t &fets, config_t &conf) {
+  void select_based_on_model(stat_t &, feature_t &fets, config_t &conf) { decide(fets, conf); }
+
+  // selector_t::select_based_on_model (selector.cuh:22-76)
+  __host__ __device__ void decide(feature_t &fets, config_t &conf) {
     if (fets.centric == EC) {
       conf.conf_target = Active;
       conf.conf_asfmt = fets.active_vertex_ratio > 0.8 ? Bitmap : Queue;
@@ -440,13 +514,7 @@ struct executor_t {
     const double s = stat.last_filter_time;
     as.set_fmt(conf.conf_asfmt);
     if (conf.conf_asfmt == Queue) {
-      bool tofilter = !conf.conf_fuse_inspect;
-      if (conf.conf_switch_to_fusion) {
-        tofilter = true;
-        conf.conf_switch_to_fusion = false;
-      }
-      if (conf.conf_first_round) tofilter = true;
-      if (tofilter) {
+      if (level_builds_queue(conf)) {
         if (!(as.queue.mode == Cached && as.queue.traceback)) build_queue(as, conf.conf_target, conf.conf_sorted_queue);
       } else if (!conf.conf_pruning) {
         fill_u32(as.bitmap.visited.dg_bits, 0, as.bitmap.visited.n_words);
@@ -455,15 +523,7 @@ struct executor_t {
     }
     // grid bookkeeping of the reference (executor.cuh:30-52): idle levels
     // feed trigger_fusion, tiny STRICT levels fall back to CM
-    conf.thdnum = THDNUM_EXPAND;
-    if (conf.conf_fuse_inspect) {
-      conf.ctanum = 32;
-    } else {
-      const double workloads = conf.conf_dir == Push ? fets.push_workload : fets.pull_workload;
-      conf.ctanum = (int)MIN((double)CTANUM_EXPAND, workloads / conf.thdnum / 2 + 1);
-      conf.conf_idle = conf.ctanum < 4 ? conf.conf_idle + 1 : 0;
-      if (conf.ctanum < 5 && conf.conf_lb == STRICT && !conf.force.has_lb) conf.conf_lb = CM;
-    }
+    level_grid_bookkeeping(fets, conf);
     set_hints(as, fets, conf);
     if (conf.conf_centric == VC && conf.conf_fuse_inspect && !conf.conf_first_round && conf.conf_compensation &&
         as.fmt == Queue)

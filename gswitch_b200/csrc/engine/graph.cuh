@@ -30,8 +30,16 @@ struct device_graph_t<CSR, E> {
   int64_t nedges;
   int level;
   bool directed;
+  // captured level loops keep the level in device memory (the loop advances
+  // it between levels); null: the by-value member above
+  const int *dlevel = nullptr;
 
-  __host__ __device__ __forceinline__ int get_level() const { return level; }
+  __host__ __device__ __forceinline__ int get_level() const {
+#ifdef __CUDA_ARCH__
+    if (dlevel) return *dlevel;
+#endif
+    return level;
+  }
   __device__ __forceinline__ int get_out_degree(const int v) const { return __ldg(dg_odegree + v); }
   __device__ __forceinline__ int get_in_degree(const int v) const { return __ldg(dgr_odegree + v); }
   __device__ __forceinline__ int64_t get_out_start_pos(const int v) const { return __ldg(dg_row_off + v); }
@@ -57,8 +65,14 @@ struct device_graph_t<COO, E> {
   int nvertexs;
   int64_t nedges;
   int level;
+  const int *dlevel = nullptr;  // as in the CSR view
 
-  __host__ __device__ __forceinline__ int get_level() const { return level; }
+  __host__ __device__ __forceinline__ int get_level() const {
+#ifdef __CUDA_ARCH__
+    if (dlevel) return *dlevel;
+#endif
+    return level;
+  }
   __host__ __device__ __forceinline__ void update_level(int inc = 1) { level += inc; }
   __host__ __device__ __forceinline__ void reset_level(int = 1) { level = 0; }
   __device__ __forceinline__ E *fetch_edata(const int64_t eid) const {

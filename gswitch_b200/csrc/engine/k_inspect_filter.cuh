@@ -42,7 +42,11 @@ constexpr int EC_INSPECT_THREADS = 512;
 // per-virtual-block sums (max over blocks for push, sum for pull).
 template <typename G, typename F>
 __global__ void __launch_bounds__(INSPECT_THREADS, 7) k_inspect_vc(active_set_t as, G g, F f,
-                                                                 unsigned long long *info) {
+                                                                 unsigned long long *info,
+                                                                 const int *skip_if = nullptr) {
+  // captured loops: a level whose expand found an empty input ends the loop
+  // before this inspection (the host loop stops there too)
+  if (skip_if && *(volatile const int *)skip_if) return;
   __shared__ unsigned long long s_red[32];
   __shared__ unsigned s_mp[INSPECT_VPB], s_ml[INSPECT_VPB];
   __shared__ bool s_last;

@@ -16,6 +16,7 @@
 
 #include "../../include/gsw.h"
 #include "apps.cuh"
+#include "engine/devloop.cuh"
 #include "graphgen.cuh"
 #include "mbfs.cuh"
 
@@ -71,6 +72,10 @@ struct gsw_ctx {
   std::map<std::string, std::pair<void *, size_t>> bufs;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   stat_t stats;  // inspector counters, reused by every run of the context
+  tree_node *dtrees = nullptr;  // the selector's trees in device memory
+  int ntree_nodes = 0;
+  tree_set dts{};
+  std::map<int, dloop_graph> dl;  // captured level loops, one per application
 
   void *buf(const std::string &name, size_t bytes) {
     auto it = bufs.find(name);
@@ -685,6 +690,164 @@ unsigned end_checks(active_set_t *as, gsw_run_stats *st) {
 inline int level_cap(int64_t n) { return (int)std::min<int64_t>(std::max<int64_t>(4 * n, 100000), 1 << 30); }
 #define MAX_LEVELS level_cap(gr->n)
 
+// ---------------------------------------------------------------------------
+// captured level loop (engine/devloop.cuh)
+// ---------------------------------------------------------------------------
+enum { DL_APP_BFS = 0, DL_APP_PR = 1 };
+
+const tree_set *device_trees(gsw_ctx *ctx) {
+  if (ctx->dtrees) return &ctx->dts;
+  const tree_node *h[9] = {select_dir_idem_tree,        select_dir_asso_tree,         select_dir_asso_backup_tree,
+                           select_fmt_tree,             select_fusion_tree,           select_lb_idem_tree,
+                           select_lb_asso_forward_tree, select_lb_asso_backward_tree, select_lb_asso_backward_backup_tree};
+  const int sz[9] = {select_dir_idem_tree_size,        select_dir_asso_tree_size,
+                     select_dir_asso_backup_tree_size, select_fmt_tree_size,
+                     select_fusion_tree_size,          select_lb_idem_tree_size,
+                     select_lb_asso_forward_tree_size, select_lb_asso_backward_tree_size,
+                     select_lb_asso_backward_backup_tree_size};
+  int total = 0;
+  for (int x : sz) total += x;
+  if (total > DL_MAX_TREE_NODES) return fail(GSW_ERR_UNSUPPORTED, "selector trees exceed the in-stream copy"), nullptr;
+  std::vector<tree_node> all;
+  all.reserve(total);
+  for (int i = 0; i < 9; ++i) all.insert(all.end(), h[i], h[i] + sz[i]);
+  if (GSW_CUDA(cudaMalloc((void **)&ctx->dtrees, sizeof(tree_node) * total))) return nullptr;
+  if (GSW_CUDA(cudaMemcpy(ctx->dtrees, all.data(), sizeof(tree_node) * total, cudaMemcpyHostToDevice))) return nullptr;
+  ctx->ntree_nodes = total;
+  const tree_node *p[9];
+  int off = 0;
+  for (int i = 0; i < 9; ++i) {
+    p[i] = ctx->dtrees + off;
+    off += sz[i];
+  }
+  ctx->dts = tree_set{p[0], p[1], p[2], p[3], p[4], p[5], p[6], p[7], p[8]};
+  return &ctx->dts;
+}
+
+// the values a captured loop bakes into its kernels: a cached graph is
+// reused only when all of them are unchanged
+struct dl_key {
+  std::vector<unsigned long long> v;
+  template <typename T>
+  dl_key &operator<<(const T &x) {
+    static_assert(sizeof(T) <= 8, "key fields are scalars");
+    unsigned long long w = 0;
+    memcpy(&w, &x, sizeof(T));
+    v.push_back(w);
+    return *this;
+  }
+};
+
+// One prepared run of a captured loop: built (or found in the context's
+// cache) before the timed region, launched inside it, collected after it.
+struct dl_run {
+  gsw_ctx *ctx = nullptr;
+  dloop_graph *L = nullptr;
+  dloop_t *d = nullptr;
+  int *trace_cfg = nullptr;
+  long long *trace_frontier = nullptr, *trace_edges = nullptr;
+  dloop_t image;
+};
+
+template <typename E, typename F>
+bool dl_prepare(dl_run &R, gsw_ctx *ctx, int app, dl_key key, active_set_t &as, device_graph_t<CSR, E> g, F &f,
+                const config_t &conf, const feature_t &fets, int max_iters, int iter_cap) {
+  if (conf.conf_qmode != Normal || conf.conf_window || conf.conf_compensation || fets.centric != VC)
+    return fail(GSW_ERR_UNSUPPORTED, "captured level loop: needs a Normal queue without window or compensation"),
+           false;
+  const tree_set *trees = device_trees(ctx);
+  R.ctx = ctx;
+  R.d = (dloop_t *)ctx->buf("dl_state", sizeof(dloop_t));
+  R.trace_cfg = (int *)ctx->buf("dl_trace_cfg", sizeof(int) * GSW_MAX_TRACE);
+  R.trace_frontier = (long long *)ctx->buf("dl_trace_frontier", sizeof(long long) * GSW_MAX_TRACE);
+  R.trace_edges = (long long *)ctx->buf("dl_trace_edges", sizeof(long long) * GSW_MAX_TRACE);
+  if (!trees || !R.d || !R.trace_cfg || !R.trace_frontier || !R.trace_edges) return false;
+  executor_t &ex = ctx->executor;
+  ex.ensure_tiles(g.nedges + as.size + 1);
+  if (!ok()) return false;
+  key << app << R.d << g.dg_row_off << g.dg_adj_list << g.dg_odegree << g.dg_edgedata << g.dgr_row_off
+      << g.dgr_adj_list << g.dgr_odegree << g.dgr_edgedata << g.nvertexs << g.nedges << g.directed;
+  key << as.size << as.bitmap.visited.dg_bits << as.bitmap.active.dg_bits << as.bitmap.inactive.dg_bits
+      << as.queue.subqueue[0].dg_queue << as.queue.subqueue[1].dg_queue << as.queue.subqueue[0].max_size
+      << as.dg_cnt << as.workset.dg_eoff << as.workset.dg_bsum << as.workset.bsum_cap;
+  key << conf.conf_pruning << conf.conf_count_edges << conf.conf_sorted_queue << fets.fromall << fets.toall
+      << ex.dg_tile << ex.tile_cap << ex.twod.edge << opts().force_grid << ctx->stats.dg_runtime_info;
+  dloop_graph &L = ctx->dl[app];
+  R.L = &L;
+  if (L.key != key.v || !L.exec) {
+    if (!dl_build(L, ex, R.d, as, g, f, conf, fets, ctx->stats.dg_runtime_info)) return false;
+    L.key = key.v;
+  }
+  dloop_t &im = R.image;
+  im = L.image;
+  im.fets = fets;
+  im.conf = conf;
+  im.trees = *trees;
+  im.tree_base = ctx->dtrees;
+  im.tree_nodes = ctx->ntree_nodes;
+  im.raw = level_counts{0, 0, 0, 0, 0, 0};
+  im.level = g.level;
+  im.cursor = as.queue.cursor;
+  im.halt = 0;
+  im.inspected = 0;
+  im.iter = 0;
+  im.max_iters = max_iters;
+  im.iter_cap = iter_cap;
+  im.sorted = conf.conf_sorted_queue ? 1 : 0;
+  im.status = DL_RUNNING;
+  im.ntrace = 0;
+  im.trace_cap = GSW_MAX_TRACE;
+  im.trace_cfg = R.trace_cfg;
+  im.trace_frontier = R.trace_frontier;
+  im.trace_edges = R.trace_edges;
+  im.info = ctx->stats.dg_runtime_info;
+  im.scanned = conf.conf_count_edges ? &as.dg_cnt->scanned : nullptr;
+  im.qsize = as.dg_cnt->qsize;
+  im.nvertexs = g.nvertexs;
+  im.nedges = g.nedges;
+  im.as_size = as.size;
+  im.launches = 0;
+  return ok();
+}
+
+// inside the timed region: state image in, one graph launch
+void dl_launch(dl_run &R) {
+  if (GSW_CUDA(cudaMemcpyAsync(R.d, &R.image, sizeof(dloop_t), cudaMemcpyHostToDevice, stream()))) return;
+  if (R.image.scanned) GSW_CUDA(cudaMemsetAsync(R.image.scanned, 0, sizeof(unsigned long long), stream()));
+  GSW_CUDA(cudaGraphLaunch(R.L->exec, stream()));
+}
+
+// after the timed region: state and trace back into the run statistics
+void dl_collect(dl_run &R, gsw_run_stats *st) {
+  dloop_t out;
+  if (GSW_CUDA(cudaMemcpyAsync(&out, R.d, sizeof(dloop_t), cudaMemcpyDeviceToHost, stream()))) return;
+  if (GSW_CUDA(cudaStreamSynchronize(stream()))) return;
+  launch_count() += out.launches;
+  if (out.status == DL_LEVEL_CAP) set_error(GSW_ERR_TIMEOUT, "%s", "level loop did not converge within the level cap");
+  if (out.status == DL_NO_BODY) set_error(GSW_ERR_UNSUPPORTED, "%s", "captured level loop: variant has no body");
+  if (out.status == DL_NOT_INSPECTED) set_error(GSW_ERR_CUDA, "%s", "captured level loop: inspection missing");
+  if (out.status == DL_RUNNING) set_error(GSW_ERR_CUDA, "%s", "captured level loop did not finish");
+  if (!st) return;
+  st->levels = out.iter;
+  const int nt = std::min(out.ntrace, (int)GSW_MAX_TRACE);
+  st->ntrace = nt;
+  if (nt > 0) {
+    std::vector<int> cfg(nt);
+    std::vector<long long> fr(nt), ed(nt);
+    GSW_CUDA(cudaMemcpyAsync(cfg.data(), R.trace_cfg, sizeof(int) * nt, cudaMemcpyDeviceToHost, stream()));
+    GSW_CUDA(cudaMemcpyAsync(fr.data(), R.trace_frontier, sizeof(long long) * nt, cudaMemcpyDeviceToHost, stream()));
+    GSW_CUDA(cudaMemcpyAsync(ed.data(), R.trace_edges, sizeof(long long) * nt, cudaMemcpyDeviceToHost, stream()));
+    GSW_CUDA(cudaStreamSynchronize(stream()));
+    for (int i = 0; i < nt; ++i) {
+      st->level_cfg[i] = cfg[i];
+      st->level_frontier[i] = fr[i];
+      st->level_edges[i] = ed[i];
+      st->level_ms[i] = 0;
+      st->level_inspect_ms[i] = 0;
+    }
+  }
+}
+
 }  // namespace
 
 // ===========================================================================
@@ -731,6 +894,8 @@ gsw_status gsw_destroy(gsw_ctx *ctx) {
   cudaStreamSynchronize(ctx->stream);
   for (auto &kv : ctx->as_cache) kv.second.destroy();
   for (auto &kv : ctx->bufs) cudaFree(kv.second.first);
+  for (auto &kv : ctx->dl) kv.second.destroy();
+  cudaFree(ctx->dtrees);
   ctx->executor.destroy();
   ctx->stats.destroy();
   if (ctx->e0) cudaEventDestroy(ctx->e0);
@@ -942,8 +1107,13 @@ gsw_status gsw_bfs(gsw_ctx *ctx, gsw_graph *gr, int32_t root, const gsw_run_opts
   as.reset();
   as.init(root);
   loop_trace tr{st, MAX_LEVELS};
+  const bool captured = o && o->captured;
+  dl_run R;
+  if (captured && !dl_prepare(R, ctx, DL_APP_BFS, dl_key() << f.data.dg_wa, as, g, f, conf, fets, 0, MAX_LEVELS))
+    return eg.finish();
   timer tm(ctx);
-  for (int level = 0; ok(); level++) {
+  if (captured) dl_launch(R);
+  for (int level = 0; !captured && ok(); level++) {
     inspector.inspect(as, g, f, stats, fets, conf);
     if (finish(as, g, f, conf)) break;
     selector.select(stats, fets, conf);
@@ -955,6 +1125,7 @@ gsw_status gsw_bfs(gsw_ctx *ctx, gsw_graph *gr, int32_t root, const gsw_run_opts
     if (finish(as, g, f, conf)) break;
   }
   const double ms = tm.stop();
+  if (captured) dl_collect(R, st);
   tr.resolve();
   end_checks(&as, st);
   add_persistent_levels(st, executor, plv0, pln0);
@@ -975,6 +1146,7 @@ gsw_status gsw_sssp(gsw_ctx *ctx, gsw_graph *gr, int32_t root, const gsw_run_opt
                     gsw_run_stats *st) {
   entry_guard eg(ctx);
   if (!ctx || !gr || root < 0 || root >= gr->n) return fail(GSW_ERR_INVALID_ARG, "gsw_sssp: bad arguments");
+  if (o && o->captured) return fail(GSW_ERR_UNSUPPORTED, "gsw_sssp: no captured level loop");
   if (!gr->weighted) return fail(GSW_ERR_INVALID_ARG, "gsw_sssp: graph has no weights");
   begin_stats(st);
   auto g = gr->view<int>();
@@ -1045,6 +1217,7 @@ __global__ void k_iota(int *p, int64_t n) {
 gsw_status gsw_cc(gsw_ctx *ctx, gsw_graph *gr, const gsw_run_opts *o, int32_t *labels, gsw_run_stats *st) {
   entry_guard eg(ctx);
   if (!ctx || !gr) return fail(GSW_ERR_INVALID_ARG, "gsw_cc: bad arguments");
+  if (o && o->captured) return fail(GSW_ERR_UNSUPPORTED, "gsw_cc: no captured level loop");
   begin_stats(st);
   if (ensure_coo(gr)) return eg.finish();
   device_graph_t<COO, Empty> g;
@@ -1161,9 +1334,16 @@ gsw_status gsw_pagerank(gsw_ctx *ctx, gsw_graph *gr, const gsw_run_opts *o, floa
   as.reset();
   as.init(ALL_ACTIVE);
   loop_trace tr{st, MAX_LEVELS};
+  const bool captured = op->captured != 0;
+  dl_run R;
+  if (captured && !dl_prepare(R, ctx, DL_APP_PR,
+                              dl_key() << f.data.dg_wa << f.data.dg_ra << f.damp << f.eps << f.data.zero, as, g, f,
+                              conf, fets, op->max_iters, MAX_LEVELS))
+    return eg.finish();
   timer tm(ctx);
   int steps = 0;
-  for (int level = 0; ok(); level++) {
+  if (captured) dl_launch(R);
+  for (int level = 0; !captured && ok(); level++) {
     inspector.inspect(as, g, f, stats, fets, conf);
     if (op->max_iters > 0 && level == op->max_iters) break;
     if (finish(as, g, f, conf)) break;
@@ -1177,6 +1357,11 @@ gsw_status gsw_pagerank(gsw_ctx *ctx, gsw_graph *gr, const gsw_run_opts *o, floa
     if (finish(as, g, f, conf)) break;
   }
   const double ms = tm.stop();
+  if (captured) {
+    gsw_run_stats tmp;
+    dl_collect(R, st ? st : &tmp);
+    steps = st ? st->levels : tmp.levels;
+  }
   tr.resolve();
   end_checks(&as, st);
   add_persistent_levels(st, executor, plv0, pln0);
@@ -1237,6 +1422,7 @@ gsw_status gsw_bc(gsw_ctx *ctx, gsw_graph *gr, int32_t root, const gsw_run_opts 
                   gsw_run_stats *st) {
   entry_guard eg(ctx);
   if (!ctx || !gr || root < 0 || root >= gr->n) return fail(GSW_ERR_INVALID_ARG, "gsw_bc: bad arguments");
+  if (o && o->captured) return fail(GSW_ERR_UNSUPPORTED, "gsw_bc: no captured level loop");
   begin_stats(st);
   auto g = gr->view<Empty>();
   app::BCForward f;
@@ -1340,6 +1526,7 @@ gsw_status gsw_bc(gsw_ctx *ctx, gsw_graph *gr, int32_t root, const gsw_run_opts 
 gsw_status gsw_gc(gsw_ctx *ctx, gsw_graph *gr, const gsw_run_opts *o, int32_t *colors, gsw_run_stats *st) {
   entry_guard eg(ctx);
   if (!ctx || !gr) return fail(GSW_ERR_INVALID_ARG, "gsw_gc: bad arguments");
+  if (o && o->captured) return fail(GSW_ERR_UNSUPPORTED, "gsw_gc: no captured level loop");
   begin_stats(st);
   auto g = gr->view<Empty>();
   app::GC f;
@@ -1412,6 +1599,7 @@ gsw_status gsw_mbfs(gsw_ctx *ctx, gsw_graph *gr, int nsrc, const int32_t *roots,
                     int32_t *levels, gsw_run_stats *st) {
   entry_guard eg(ctx);
   if (!ctx || !gr || nsrc <= 0 || !roots) return fail(GSW_ERR_INVALID_ARG, "gsw_mbfs: bad arguments");
+  if (o && o->captured) return fail(GSW_ERR_UNSUPPORTED, "gsw_mbfs: no captured level loop");
   for (int s = 0; s < nsrc; ++s)
     if (roots[s] < 0 || roots[s] >= gr->n) return fail(GSW_ERR_INVALID_ARG, "gsw_mbfs: root out of range");
   if (!batched) {

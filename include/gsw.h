@@ -118,7 +118,10 @@ typedef struct gsw_run_opts {
                         block leaves without reaching the level barrier, the
                         others' wait (bounded to 20 ms) expires and the call
                         returns GSW_ERR_TIMEOUT */
-  int reserved[5];
+  int captured;      /* 1: run the whole level loop as one CUDA graph with
+                        device-side selection and termination (BFS, PR;
+                        GSW_ERR_UNSUPPORTED elsewhere); 0: host-driven loop */
+  int reserved[4];
 } gsw_run_opts;
 
 void gsw_run_opts_default(gsw_run_opts *o);

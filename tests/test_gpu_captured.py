@@ -1,0 +1,113 @@
+"""Captured level loop: the whole inspect -> select -> filter -> expand loop
+as one CUDA graph with device-side selection and termination.
+
+Results must be bit-exact with the oracle (BFS) or within the PageRank
+tolerance (L1 of normalised vectors <= 1e-6 after 20 iterations), and the
+device selector must take the host selector's decisions level for level."""
+import numpy as np
+import pytest
+
+import gswitch_b200 as gs
+import oracle
+from conftest import golden_names, load_golden
+from test_gpu_apps import ALL_VARIANTS, STANDALONE_VARIANTS, _pr_l1
+
+pytestmark = pytest.mark.gpu
+
+
+def cap(cfg="", **kw):
+    return gs.RunOpts.from_config(cfg, captured=True, **kw)
+
+
+@pytest.fixture(scope="module")
+def graphs():
+    out = {}
+    for name, g in [("rmat14", oracle.rmat(14, 16, seed=1)), ("grid64", oracle.grid(64, 64, 100, seed=2)),
+                    ("er20k", oracle.er(20000, 80000, seed=3))]:
+        root = 0 if name.startswith("rmat") else int(oracle.roots(g, 9, 1)[0])
+        out[name] = (g, root)
+    return out
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_captured_bfs_goldens_every_variant(ctx, name):
+    d = load_golden(name)
+    g = ctx.upload(d["off"], d["col"])
+    for cfg in ALL_VARIANTS:
+        lv, st = g.bfs(int(d["root"]), cap(cfg))
+        assert np.array_equal(lv, d["lvl"]), (name, cfg)
+        assert st.device_error == 0
+        assert st.levels == len(st.trace)
+
+
+@pytest.mark.parametrize("name", ["rmat14", "grid64", "er20k"])
+def test_captured_bfs_large(ctx, graphs, name):
+    h, root = graphs[name]
+    ref = oracle.bfs(h, root)
+    g = ctx.upload(h.off, h.col)
+    for cfg in ALL_VARIANTS:
+        lv, st = g.bfs(root, cap(cfg, sorted_queue=(len(cfg) % 2 == 0)))
+        assert np.array_equal(lv, ref), (name, cfg)
+        assert st.edges == oracle.traversed_edges(h, ref)
+
+
+@pytest.mark.parametrize("name", ["rmat14", "grid64", "er20k"])
+def test_captured_selector_takes_host_decisions(ctx, graphs, name):
+    """Standalone levels: same variant and frontier size at every level as
+    the host-driven loop (forced standalone keeps the host loop's
+    wall-clock fusion rule out of the comparison)."""
+    h, root = graphs[name]
+    g = ctx.upload(h.off, h.col)
+    for cfg in ["x-x-x-Standalone", "Push-x-x-Standalone", "Pull-x-x-Standalone", "x-Queue-x-Standalone"]:
+        _, host = g.bfs(root, gs.RunOpts.from_config(cfg, persistent=False))
+        _, dev = g.bfs(root, cap(cfg))
+        assert dev.trace == host.trace, (name, cfg)
+        assert dev.levels == host.levels
+
+
+def test_captured_graph_reused_across_roots_and_rebuilt_per_graph(ctx, graphs):
+    for name in ["rmat14", "er20k"]:
+        h, _ = graphs[name]
+        g = ctx.upload(h.off, h.col)
+        for r in oracle.roots(h, 11, 4):
+            lv, _ = g.bfs(int(r), cap())
+            assert np.array_equal(lv, oracle.bfs(h, int(r))), (name, r)
+
+
+def test_captured_bfs_accounting_matches_host(ctx, graphs):
+    h, root = graphs["rmat14"]
+    g = ctx.upload(h.off, h.col)
+    cfg = "Push-Queue-WM-Standalone"
+    _, host = g.bfs(root, gs.RunOpts.from_config(cfg, account=True, persistent=False))
+    _, dev = g.bfs(root, cap(cfg, account=True))
+    assert dev.level_edges == host.level_edges
+    assert sum(dev.level_edges) > 0
+
+
+@pytest.mark.parametrize("name", ["rmat10", "grid24_lr", "er1500", "path10", "twocomp_isolated"])
+def test_captured_pagerank_20_iterations(ctx, name):
+    d = load_golden(name)
+    h = oracle.Csr(d["off"], d["col"])
+    g = ctx.upload(d["off"], d["col"])
+    for cfg in STANDALONE_VARIANTS + ["x-x-TWOD"]:
+        pr, st = g.pagerank(iters=20, eps=0.0, opts=cap(cfg))
+        l1, mrel = _pr_l1(pr, h)
+        assert l1 <= 1e-6, (name, cfg, l1, mrel)
+        assert st.levels == 20
+
+
+def test_captured_pagerank_fixpoint(ctx, graphs):
+    h, _ = graphs["rmat14"]
+    g = ctx.upload(h.off, h.col)
+    pr, st = g.pagerank(iters=0, eps=0.01, opts=cap())
+    assert oracle.pagerank_check(h, pr) < 0
+    assert st.levels > 1
+
+
+def test_captured_rejected_where_unsupported(ctx, graphs):
+    h, root = graphs["er20k"]
+    hw = oracle.add_weights(h, 5, 64)
+    g = ctx.upload(hw.off, hw.col, hw.w)
+    with pytest.raises(gs.GswError) as e:
+        g.sssp(root, cap())
+    assert gs.STATUS[e.value.code] == "UNSUPPORTED"
