@@ -210,6 +210,23 @@ __device__ __forceinline__ int64_t upper_bound64(const T *a, int64_t n, T key) {
 // 4-byte-packed shuffle of an arbitrary value type (the reference's
 // __exshfl_down, src/utils/intrinsics.cuh:293-302).
 template <typename T>
+__device__ __forceinline__ T shfl_up_any(T v, int delta) {
+  static_assert(sizeof(T) % 4 == 0 || sizeof(T) < 4, "4-byte packed type");
+  if (sizeof(T) < 4) {
+    int x = 0;
+    memcpy(&x, &v, sizeof(T));
+    x = __shfl_up_sync(FULL, x, delta);
+    memcpy(&v, &x, sizeof(T));
+    return v;
+  }
+  int x[sizeof(T) / 4 > 0 ? sizeof(T) / 4 : 1];
+  memcpy(x, &v, sizeof(T));
+#pragma unroll
+  for (int i = 0; i < (int)(sizeof(T) / 4); ++i) x[i] = __shfl_up_sync(FULL, x[i], delta);
+  memcpy(&v, x, sizeof(T));
+  return v;
+}
+template <typename T>
 __device__ __forceinline__ T shfl_down_any(T v, int delta) {
   static_assert(sizeof(T) % 4 == 0 || sizeof(T) < 4, "4-byte packed type");
   if (sizeof(T) < 4) {

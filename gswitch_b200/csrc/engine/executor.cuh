@@ -651,6 +651,12 @@ struct executor_t {
           strict_prepare<true>(as, g, conf.want());
           if (!ok()) return;
           const int64_t want = (ed < 0 || fr < 0) ? -1 : (ed + fr) / STRICT_TILE + 1;
+          if constexpr (sizeof(typename F::wa_t) <= 4) {
+            if (conf.conf_fromall) {
+              GSW_GO((k_pull_strict_all<G, F>), want, as, g, f, conf, dg_tile);
+              break;
+            }
+          }
           GSW_GO((k_pull_strict<G, F>), want, as, g, f, conf, dg_tile);
           break;
         }
@@ -733,7 +739,7 @@ struct executor_t {
         set_error(GSW_ERR_UNSUPPORTED, "%s", "2D-partition layout not built for this graph");
         return;
       }
-      const int grid = (int)MIN(twod.ntiles, (int64_t)resident_grid(k_twod<G, F>, TWOD_THREADS));
+      const int grid = (int)MAX((int64_t)1, MIN(twod.nitems, (int64_t)resident_grid(k_twod<G, F>, TWOD_THREADS)));
       k_twod<G, F><<<grid, TWOD_THREADS, 0, stream()>>>(g, f, twod);
       GSW_LAUNCHED();
     } else {

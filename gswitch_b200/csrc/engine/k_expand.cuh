@@ -507,12 +507,20 @@ __global__ void __launch_bounds__(EXPAND_THREADS) k_push_strict(active_set_t as,
 // Pull: each thread walks 4 consecutive slots and folds runs of the same
 // candidate before one compAtomic (the "stride mode" of expand_VC_STRICT.cuh:
 // 453-510).
+// Edge-balanced pull.  A tile's slots are read warp-contiguously (slot
+// t*T + k*B + lane + 32*warp at pass k, so the in-edge loads coalesce), the
+// messages of each warp pass are combined per destination by a segmented
+// shuffle scan, and only the last lane of each run writes: with a plain
+// comp() when the run holds every in-edge of its vertex, with compAtomic()
+// when the vertex's edges continue in another pass or tile.  A hub therefore
+// costs one atomic per 32 edges instead of one per thread.
 template <typename G, typename F>
 __global__ void __launch_bounds__(EXPAND_THREADS) k_pull_strict(active_set_t as, G g, F f, config_t conf,
                                                                 const int *tile_lo) {
   using WA = typename F::wa_t;
   constexpr int T = STRICT_TILE;
-  constexpr int PER = T / EXPAND_THREADS;
+  constexpr int B = EXPAND_THREADS;
+  constexpr int PER = T / B;
   __shared__ int s_v[T + 2];
   __shared__ int64_t s_sc[T + 2];
   __shared__ int64_t s_st[T + 2];
@@ -522,6 +530,7 @@ __global__ void __launch_bounds__(EXPAND_THREADS) k_pull_strict(active_set_t as,
   const int64_t *eoff = as.workset.dg_eoff;
   const int64_t total = eoff[n];
   const int64_t ntiles = (total + T - 1) / T;
+  const int lane = lane_id();
   if (blockIdx.x == 0 && threadIdx.x == 0) account(as, conf, (unsigned long long)(total - n));
   for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const int64_t lo = tile_lo[t];
@@ -535,35 +544,144 @@ __global__ void __launch_bounds__(EXPAND_THREADS) k_pull_strict(active_set_t as,
     }
     if (threadIdx.x == 0) s_sc[cnt] = eoff[hi + 1];
     __syncthreads();
-    const int64_t t0 = t * T + threadIdx.x * PER;
     const int64_t t1 = MIN(total, t * T + T);
-    int cur = -1;
-    WA acc;
-    bool have = false;
     for (int k = 0; k < PER; ++k) {
-      const int64_t s = t0 + k;
-      if (s >= t1) break;
-      const int j = upper_bound(s_sc, cnt, s) - 1;
-      const int64_t local = s - s_sc[j];
-      if (local >= s_sc[j + 1] - s_sc[j] - 1) continue;
-      if (j != cur) {
-        if (have) f.compAtomic(f.wa_of(s_v[cur]), acc, g);
-        have = false;
-        cur = j;
-      }
-      const int64_t ei = s_st[j] + local;
-      const int u = __ldg(g.dgr_adj_list + ei);
-      if (conf.conf_fromall || as.bitmap.is_active(u)) {
-        WA x = f.emit(u, g.fetch_edata_r(ei), g);
-        if (have)
-          f.comp(&acc, x, g);
-        else {
-          acc = x;
-          have = true;
+      const int64_t wbase = t * T + (int64_t)k * B + (threadIdx.x & ~31);
+      if (wbase >= t1) break;  // warp-uniform
+      const int64_t s = wbase + lane;
+      int j = -1;
+      bool have = false;
+      WA x = f.data.zero;
+      if (s < t1) {
+        j = upper_bound(s_sc, cnt, s) - 1;
+        const int64_t local = s - s_sc[j];
+        if (local < s_sc[j + 1] - s_sc[j] - 1) {
+          const int64_t ei = s_st[j] + local;
+          const int u = __ldg(g.dgr_adj_list + ei);
+          if (conf.conf_fromall || as.bitmap.is_active(u)) {
+            x = f.emit(u, g.fetch_edata_r(ei), g);
+            have = true;
+          }
         }
       }
+      // segmented inclusive scan over runs of equal j (j is non-decreasing
+      // across the lanes)
+#pragma unroll
+      for (int d = 1; d < 32; d <<= 1) {
+        const WA ox = shfl_up_any(x, d);
+        const int oj = __shfl_up_sync(FULL, j, d);
+        const bool oh = __shfl_up_sync(FULL, have ? 1 : 0, d) != 0;
+        if (lane >= d && oj == j && oh) {
+          if (have) {
+            f.comp(&x, ox, g);
+          } else {
+            x = ox;
+            have = true;
+          }
+        }
+      }
+      const int nj = __shfl_down_sync(FULL, j, 1);
+      const bool tail = lane == 31 || nj != j;
+      if (tail && have && j >= 0) {
+        const int64_t first = s_sc[j];
+        const int64_t last = s_sc[j + 1] - 2;  // the vertex's last edge slot
+        if (first >= wbase && last <= wbase + 31)
+          f.comp(f.wa_of(s_v[j]), x, g);
+        else
+          f.compAtomic(f.wa_of(s_v[j]), x, g);
+      }
     }
-    if (have) f.compAtomic(f.wa_of(s_v[cur]), acc, g);
+    __syncthreads();
+  }
+}
+
+// Edge-balanced pull for from-all patterns (every in-edge carries a message,
+// e.g. PageRank): each warp reads 128 consecutive slots of the tile as four
+// windows of 32.  The owner of a slot comes from a bitmap of the vertex
+// boundaries that fall inside the window (every vertex holds at least one
+// slot, so boundaries are distinct), not from a per-lane search; messages of
+// a run are combined by a segmented shuffle scan whose run heads come from
+// the same bitmap (f.data.zero fills the slots without a message), the run
+// tails meet in shared memory, and every vertex
+// of the tile is written once: comp() when all its slots lie in the tile,
+// compAtomic() otherwise.
+template <typename G, typename F>
+__global__ void __launch_bounds__(EXPAND_THREADS) k_pull_strict_all(active_set_t as, G g, F f, config_t conf,
+                                                                    const int *tile_lo) {
+  using WA = typename F::wa_t;
+  constexpr int T = STRICT_TILE;
+  constexpr int WSLOTS = T / (EXPAND_THREADS / 32);  // slots per warp
+  __shared__ int s_v[T + 2];
+  __shared__ int64_t s_sc[T + 2];
+  __shared__ int64_t s_st[T + 2];
+  __shared__ WA s_acc[T + 2];
+  const int64_t n = as.get_size();
+  GSW_HALT_IF_EMPTY(n);
+  const Status want = conf.want();
+  const int64_t *eoff = as.workset.dg_eoff;
+  const int64_t total = eoff[n];
+  const int64_t ntiles = (total + T - 1) / T;
+  const int lane = lane_id(), w = warp_id();
+  if (blockIdx.x == 0 && threadIdx.x == 0) account(as, conf, (unsigned long long)(total - n));
+  for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const int64_t lo = tile_lo[t];
+    const int64_t hi = (t + 1 < ntiles) ? tile_lo[t + 1] : n - 1;
+    const int cnt = (int)(hi - lo + 1);
+    for (int j = threadIdx.x; j < cnt; j += blockDim.x) {
+      const int v = as.fetch(lo + j, want);
+      s_v[j] = v;
+      s_sc[j] = eoff[lo + j];
+      s_st[j] = v >= 0 ? __ldg(g.dgr_row_off + v) : 0;
+      s_acc[j] = f.data.zero;
+    }
+    if (threadIdx.x == 0) s_sc[cnt] = eoff[hi + 1];
+    __syncthreads();
+    const int64_t t1 = MIN(total, t * T + T);
+    const int64_t wbeg = t * T + (int64_t)w * WSLOTS;
+    if (wbeg < t1) {
+      int j0 = upper_bound(s_sc, cnt, wbeg) - 1;  // owner of the warp's first slot
+      for (int64_t wb = wbeg; wb < MIN(t1, wbeg + WSLOTS); wb += 32) {
+        const int64_t s = wb + lane;
+        // boundaries (first slots of the next vertices) inside this window
+        const int bj = j0 + 1 + lane;
+        const int64_t bpos = bj <= cnt ? s_sc[bj] : INT64_MAX;
+        const unsigned bm = __reduce_or_sync(FULL, bpos <= wb + 31 ? 1u << (int)(bpos - wb) : 0u);
+        const unsigned upto = bm & (0xffffffffu >> (31 - lane));  // boundaries at or before this lane
+        const int j = j0 + __popc(upto);
+        const int head = upto ? 31 - __clz(upto) : 0;  // first lane of this lane's run
+        WA x = f.data.zero;
+        if (s < t1) {
+          const int64_t local = s - s_sc[j];
+          if (local < s_sc[j + 1] - s_sc[j] - 1) {
+            const int64_t ei = s_st[j] + local;
+            const int u = __ldg(g.dgr_adj_list + ei);
+            x = f.emit(u, g.fetch_edata_r(ei), g);
+          }
+        }
+        // segmented inclusive scan: runs start at the boundary lanes
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+          const WA ox = shfl_up_any(x, d);
+          if (lane - d >= head) f.comp(&x, ox, g);
+        }
+        // a run ends at lane 31, before the next boundary, or at the tile's
+        // last slot (the lanes past it hold the identity)
+        const bool tail = lane == 31 || ((bm >> (lane + 1)) & 1u) || s + 1 == t1;
+        if (tail && s < t1) f.compAtomic(&s_acc[j], x, g);
+        j0 = __shfl_sync(FULL, j, 31);
+        if (j0 + 1 <= cnt && s_sc[j0 + 1] <= wb + 32) ++j0;  // a vertex starting right after the window
+      }
+    }
+    __syncthreads();
+    for (int j = threadIdx.x; j < cnt; j += blockDim.x) {
+      const int v = s_v[j];
+      const int64_t first = s_sc[j], deg = s_sc[j + 1] - s_sc[j] - 1;
+      if (v < 0 || deg <= 0) continue;
+      if (first >= t * T && first + deg <= t * T + T)
+        f.comp(f.wa_of(v), s_acc[j], g);
+      else
+        f.compAtomic(f.wa_of(v), s_acc[j], g);
+    }
     __syncthreads();
   }
 }

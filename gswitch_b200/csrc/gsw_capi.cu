@@ -42,6 +42,8 @@ struct gsw_graph {
     uint64_t *edge = nullptr;
     int64_t *tile_off = nullptr, *heavy_off = nullptr, *heavy_beg = nullptr, *heavy_end = nullptr;
     int *heavy_src = nullptr;
+    int *item_tile = nullptr, *tile_items = nullptr;
+    int64_t *item_beg = nullptr, *item_end = nullptr;
     twod_layout L;
   } *twod = nullptr;  // 2D-partition layout, built on first use
 
@@ -326,6 +328,10 @@ void free_graph(gsw_graph *g) {
     cudaFree(g->twod->heavy_beg);
     cudaFree(g->twod->heavy_end);
     cudaFree(g->twod->heavy_src);
+    cudaFree(g->twod->item_tile);
+    cudaFree(g->twod->tile_items);
+    cudaFree(g->twod->item_beg);
+    cudaFree(g->twod->item_end);
     delete g->twod;
   }
   delete g;
@@ -465,6 +471,21 @@ int ensure_twod(gsw_graph *g) {
     tile_off[dt + 1] = tile_off[dt] + tot;
   }
   heavy_off[ntiles] = (int64_t)hsrc.size();
+  // work items: each tile's edges cut into near-equal pieces of at most
+  // TWOD_ITEM_EDGES
+  std::vector<int> it_tile, tile_items(ntiles);
+  std::vector<int64_t> it_beg, it_end;
+  for (int64_t dt = 0; dt < ntiles; ++dt) {
+    const int64_t a = tile_off[dt], e = tile_off[dt + 1] - a;
+    if (e == 0) continue;
+    const int64_t k = (e + TWOD_ITEM_EDGES - 1) / TWOD_ITEM_EDGES;
+    tile_items[dt] = (int)k;
+    for (int64_t i = 0; i < k; ++i) {
+      it_tile.push_back((int)dt);
+      it_beg.push_back(a + e * i / k);
+      it_end.push_back(a + e * (i + 1) / k);
+    }
+  }
   auto *t = new gsw_graph::twod_store();
   t->edge = sorted;
   auto up = [&](void **dst, const void *src, size_t bytes) {
@@ -476,6 +497,10 @@ int ensure_twod(gsw_graph *g) {
   up((void **)&t->heavy_beg, hbeg.data(), sizeof(int64_t) * hbeg.size());
   up((void **)&t->heavy_end, hend.data(), sizeof(int64_t) * hend.size());
   up((void **)&t->heavy_src, hsrc.data(), sizeof(int) * hsrc.size());
+  up((void **)&t->item_tile, it_tile.data(), sizeof(int) * it_tile.size());
+  up((void **)&t->tile_items, tile_items.data(), sizeof(int) * tile_items.size());
+  up((void **)&t->item_beg, it_beg.data(), sizeof(int64_t) * it_beg.size());
+  up((void **)&t->item_end, it_end.data(), sizeof(int64_t) * it_end.size());
   GSW_CUDA(cudaStreamSynchronize(stream()));
   t->L.edge = t->edge;
   t->L.tile_off = t->tile_off;
@@ -486,6 +511,11 @@ int ensure_twod(gsw_graph *g) {
   t->L.ntiles = ntiles;
   t->L.nheavy = (int64_t)hsrc.size();
   t->L.m = m;
+  t->L.item_tile = t->item_tile;
+  t->L.item_beg = t->item_beg;
+  t->L.item_end = t->item_end;
+  t->L.tile_items = t->tile_items;
+  t->L.nitems = (int64_t)it_tile.size();
   g->twod = t;
   return err().code;
 }
