@@ -37,7 +37,21 @@ ABI_SYMBOLS = (
     "gsw_graph_generate_er", "gsw_graph_info", "gsw_graph_attr", "gsw_graph_download",
     "gsw_graph_destroy", "gsw_graph_roots", "gsw_ctx_stream", "gsw_run_opts_default", "gsw_bfs", "gsw_sssp", "gsw_cc",
     "gsw_pagerank", "gsw_bc", "gsw_gc", "gsw_mbfs", "gsw_bfs_strict_noalloc",
+    "gsw_graph_generate_powerlaw", "gsw_label_levels", "gsw_mlp_train", "gsw_mlp_grad", "gsw_mlp_infer",
+    "gsw_mlp_load",
 )
+
+# learned selector (include/gsw.h): 8 features -> 32 -> 32 -> 20 classes
+MLP_FEATURES, MLP_CLASSES, MLP_NPARAM = 8, 20, 2004
+MLP_MODEL_FLOATS = MLP_NPARAM + 2 * MLP_FEATURES
+APP_BFS, APP_SSSP, APP_PR = 0, 1, 2
+SELECT_RULES, SELECT_MLP = 0, 1
+
+
+def mlp_class_name(k: int) -> str:
+    """Class k of the learned selector as a ``Dir-Fmt-LB`` string."""
+    return "-".join((("Push", "Pull")[k // 10], ("Queue", "Bitmap")[(k // 5) % 2],
+                     ("TM", "WM", "CM", "STRICT", "TWC")[k % 5]))
 
 
 class GswError(RuntimeError):
@@ -100,6 +114,12 @@ def lib():
     L.gsw_gc.argtypes = [vp, vp, po, vp, ps]
     L.gsw_mbfs.argtypes = [vp, vp, C.c_int, vp, C.c_int, po, vp, ps]
     L.gsw_bfs_strict_noalloc.argtypes = [i64, i64, vp, vp, i32, vp, vp]
+    L.gsw_graph_generate_powerlaw.argtypes = [vp, i64, C.c_double, u64, C.c_int, u64, pvp]
+    L.gsw_label_levels.argtypes = [vp, vp, C.c_int, i32, C.c_int, C.c_int, vp, vp, vp, C.POINTER(C.c_int)]
+    L.gsw_mlp_train.argtypes = [vp, vp, vp, i64, C.c_int, C.c_float, C.c_float, u64, vp, vp]
+    L.gsw_mlp_grad.argtypes = [vp, vp, vp, vp, i64, C.c_float, vp, vp]
+    L.gsw_mlp_infer.argtypes = [vp, vp, vp, i64, vp, vp]
+    L.gsw_mlp_load.argtypes = [vp, vp, C.c_float]
     _LIB = L
     return L
 
@@ -118,7 +138,7 @@ class RunOpts:
 
     def __init__(self, direction=None, asfmt=None, lb=None, fusion=None, sorted_queue=True,
                  max_iters=0, damping=0.85, eps=0.01, verbose=False, timing=False, expand_grid=0,
-                 account=False, persistent=None, barrier_test=False, captured=False):
+                 account=False, persistent=None, barrier_test=False, captured=False, selector="rules"):
         self.direction, self.asfmt, self.lb, self.fusion = direction, asfmt, lb, fusion
         self.sorted_queue, self.max_iters, self.damping, self.eps = sorted_queue, max_iters, damping, eps
         self.verbose, self.timing, self.expand_grid = verbose, timing, expand_grid
@@ -126,6 +146,7 @@ class RunOpts:
         self.persistent = persistent
         self.barrier_test = barrier_test
         self.captured = captured
+        self.selector = selector  # "rules" (decision trees) or "mlp" (loaded network, rules as fallback)
 
     @classmethod
     def from_config(cls, cfg: str, **kw):
@@ -151,6 +172,7 @@ class RunOpts:
         o.persistent = AUTO if self.persistent is None else int(bool(self.persistent))
         o.barrier_test = int(self.barrier_test)
         o.captured = int(bool(self.captured))
+        o.selector = SELECT_MLP if self.selector == "mlp" else SELECT_RULES
         return o
 
 
@@ -237,6 +259,44 @@ class Context:
         _check(lib().gsw_graph_generate_er(self._h, n, m_pairs, seed, wmax, wseed, C.byref(h)))
         return Graph(self, h)
 
+    def powerlaw(self, n, gamma, seed=1, wmax=0, wseed=0) -> "Graph":
+        h = C.c_void_p()
+        _check(lib().gsw_graph_generate_powerlaw(self._h, n, float(gamma), seed, wmax, wseed, C.byref(h)))
+        return Graph(self, h)
+
+    # ---- learned selector
+    def mlp_train(self, X, T, epochs=2000, lr=3e-3, tau=0.1, seed=1):
+        """Train on features X [n, 8] and per-variant times T [n, 20]; returns
+        (model [MLP_MODEL_FLOATS], per-epoch loss)."""
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        T = np.ascontiguousarray(T, dtype=np.float32)
+        model = np.zeros(MLP_MODEL_FLOATS, dtype=np.float32)
+        loss = np.zeros(epochs, dtype=np.float32)
+        _check(lib().gsw_mlp_train(self._h, _ptr(X), _ptr(T), len(X), epochs, lr, tau, seed, _ptr(model),
+                                   _ptr(loss)))
+        return model, loss
+
+    def mlp_grad(self, model, X, T, tau=0.1):
+        model = np.ascontiguousarray(model, dtype=np.float32)
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        T = np.ascontiguousarray(T, dtype=np.float32)
+        g = np.zeros(MLP_NPARAM, dtype=np.float32)
+        loss = np.zeros(1, dtype=np.float32)
+        _check(lib().gsw_mlp_grad(self._h, _ptr(model), _ptr(X), _ptr(T), len(X), tau, _ptr(g), _ptr(loss)))
+        return g, float(loss[0])
+
+    def mlp_infer(self, model, X):
+        model = np.ascontiguousarray(model, dtype=np.float32)
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        cls = np.zeros(len(X), dtype=np.int32)
+        prob = np.zeros(len(X), dtype=np.float32)
+        _check(lib().gsw_mlp_infer(self._h, _ptr(model), _ptr(X), len(X), _ptr(cls), _ptr(prob)))
+        return cls, prob
+
+    def mlp_load(self, model=None, min_conf=0.0):
+        m = None if model is None else np.ascontiguousarray(model, dtype=np.float32)
+        _check(lib().gsw_mlp_load(self._h, _ptr(m), min_conf))
+
 
 class Graph:
     """A device-resident graph (gsw_graph)."""
@@ -312,6 +372,19 @@ class Graph:
         pr = np.empty(self.n, dtype=np.float32) if out else None
         st = self._run(lib().gsw_pagerank, outs=[pr], opts=opts)
         return pr, st
+
+    def label(self, app, root=0, max_levels=64, pr_iters=3):
+        """Per-level features [rows, 8], per-variant times in ms [rows, 20] and
+        the rule-based selector's class per level [rows] (gsw_label_levels);
+        app is APP_BFS, APP_SSSP or APP_PR."""
+        X = np.zeros((max_levels, MLP_FEATURES), dtype=np.float32)
+        T = np.zeros((max_levels, MLP_CLASSES), dtype=np.float32)
+        R = np.zeros(max_levels, dtype=np.int32)
+        rows = C.c_int(0)
+        _check(lib().gsw_label_levels(self.ctx._h, self._h, app, root, max_levels, pr_iters, _ptr(X), _ptr(T),
+                                      _ptr(R), C.byref(rows)))
+        r = rows.value
+        return X[:r], T[:r], R[:r]
 
     def bc(self, root, opts=None, out=True):
         nsp = np.empty(self.n, dtype=np.int32) if out else None

@@ -31,7 +31,7 @@
 #pragma once
 #include <vector>
 
-#include "executor.cuh"
+#include "mlp.cuh"
 
 namespace gsw {
 
@@ -58,6 +58,7 @@ struct dloop_t {
   tree_set trees;               // device copies of the selector's trees
   const tree_node *tree_base;   // the one allocation `trees` points into
   int tree_nodes;
+  const mlp_model *mlp;         // learned selector (null: the rules alone)
   level_counts raw;             // counters of the last inspection (frontier hints)
   int level;                    // the level kernels read
   int cursor;                   // Normal queue: input subqueue
@@ -85,15 +86,21 @@ struct dloop_t {
   cudaGraphConditionalHandle h_loop, h_filter, h_expand, h_inspect;
 };
 
-// one level's decisions: the host loop's inspect-finish-select-filter-update
-// sequence (gsw_capi.cu runners) on device state, by one thread
-__device__ inline void dl_step(dloop_t &d, const level_counts &c, unsigned long long scanned) {
+__device__ inline void dl_stop(dloop_t &d, int status) {
+  d.status = status;
+  cudaGraphSetConditional(d.h_loop, 0);
+  cudaGraphSetConditional(d.h_filter, DL_FILTER_BODIES);
+  cudaGraphSetConditional(d.h_expand, 2 * DL_VARIANTS);
+  cudaGraphSetConditional(d.h_inspect, 0);
+}
+
+// One level's decisions: the host loop's inspect-finish-select sequence
+// (gsw_capi.cu runners) on device state, by one thread.  Returns false when
+// the loop stops here.
+__device__ inline bool dl_decide(dloop_t &d, const level_counts &c, unsigned long long scanned) {
   auto stop = [&](int status) {
-    d.status = status;
-    cudaGraphSetConditional(d.h_loop, 0);
-    cudaGraphSetConditional(d.h_filter, DL_FILTER_BODIES);
-    cudaGraphSetConditional(d.h_expand, 2 * DL_VARIANTS);
-    cudaGraphSetConditional(d.h_inspect, 0);
+    dl_stop(d, status);
+    return false;
   };
   if (d.ntrace > 0 && d.ntrace <= d.trace_cap) d.trace_edges[d.ntrace - 1] = (long long)scanned;
   if (d.halt) return stop(DL_DONE);  // the last expand found an empty input
@@ -118,6 +125,15 @@ __device__ inline void dl_step(dloop_t &d, const level_counts &c, unsigned long 
   selector_t sel;
   sel.trees = &d.trees;
   sel.decide(fets, conf);
+  return true;
+}
+
+// the filter-update-trace part of the level, after the selector (and the
+// network, when one is loaded) decided
+__device__ inline void dl_commit(dloop_t &d) {
+  auto stop = [&](int status) { dl_stop(d, status); };
+  feature_t &fets = d.fets;
+  config_t &conf = d.conf;
   // filter: queue build (or visited reset) from the pre-swap cursor, then swap
   int fbody = DL_FILTER_BODIES;  // none
   if (conf.conf_asfmt == Queue) {
@@ -173,6 +189,8 @@ __global__ void __launch_bounds__(256) k_dl_select(dloop_t *d) {
   __shared__ __align__(16) unsigned long long s_tree[DL_MAX_TREE_NODES * sizeof(tree_node) / 8];
   __shared__ level_counts s_c;
   __shared__ unsigned long long s_scanned;
+  __shared__ int s_go, s_mlp;
+  __shared__ float s_x[MLP_IN];
   dloop_t &sd = *reinterpret_cast<dloop_t *>(s_state);
   const unsigned long long *src = reinterpret_cast<const unsigned long long *>(d);
   for (int i = threadIdx.x; i < WORDS; i += blockDim.x) s_state[i] = src[i];
@@ -202,9 +220,20 @@ __global__ void __launch_bounds__(256) k_dl_select(dloop_t *d) {
                         sh + (dev.fusion - base),          sh + (dev.lb_idem - base),
                         sh + (dev.lb_asso_forward - base), sh + (dev.lb_asso_backward - base),
                         sh + (dev.lb_asso_backward_backup - base)};
-    dl_step(sd, s_c, s_scanned);
+    s_go = dl_decide(sd, s_c, s_scanned);
     sd.trees = dev;
+    s_mlp = s_go && sd.mlp && mlp_applicable(*sd.mlp, sd.fets, sd.conf);
+    if (s_mlp) mlp_features(sd.fets, s_x);
   }
+  __syncthreads();
+  // in-stream inference of the learned selector by warp 0
+  if (s_mlp && threadIdx.x < 32) {
+    float pt;
+    const int k = mlp_predict_warp(*sd.mlp, s_x, &pt);
+    if (threadIdx.x == 0 && pt >= sd.mlp->min_conf) mlp_apply(k, sd.conf);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && s_go) dl_commit(sd);
   __syncthreads();
   unsigned long long *dst = reinterpret_cast<unsigned long long *>(d);
   for (int i = threadIdx.x; i < WORDS; i += blockDim.x) dst[i] = s_state[i];

@@ -9,7 +9,9 @@
 //           (src, dst) - Graph500 Kronecker, no noise, no permutation;
 //   grid  : rows x cols 4-neighbour lattice plus (lattice edges / lr_div)
 //           uniform long-range pairs;
-//   G(n,m): m uniform pairs.
+//   G(n,m): m uniform pairs;
+//   power law (configuration model): vertex degrees from P(d) ~ d^-gamma by
+//           inversion, stubs shuffled by sorting on hashed keys and paired.
 // The undirected CSR build drops self-loops, adds both directions, sorts by
 // (src, dst), removes duplicates and derives int64 row offsets - the clean
 // form the reference's rinse() produces (src/utils/fileIO.cuh:399-443) except
@@ -31,7 +33,7 @@ __host__ __device__ __forceinline__ uint64_t sm64(uint64_t x) {
 __host__ __device__ __forceinline__ uint64_t stream_key(uint64_t seed, uint64_t stream) {
   return sm64(seed ^ sm64(stream));
 }
-enum gen_stream : uint64_t { ST_RMAT = 1, ST_W = 2, ST_GRID = 3, ST_ER = 4, ST_ERB = 5, ST_ROOT = 7 };
+enum gen_stream : uint64_t { ST_RMAT = 1, ST_W = 2, ST_GRID = 3, ST_ER = 4, ST_ERB = 5, ST_PL = 6, ST_ROOT = 7 };
 
 struct rmat_params {
   int scale;
@@ -115,6 +117,36 @@ __global__ void k_er_keys(int64_t n, int64_t m, uint64_t key, uint64_t *keys) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < m; i += (int64_t)gridDim.x * blockDim.x) {
     const uint64_t s = sm64(key + 2 * (uint64_t)i) % (uint64_t)n;
     const uint64_t d = sm64(key + 2 * (uint64_t)i + 1) % (uint64_t)n;
+    const bool loop = s == d;
+    keys[2 * i] = loop ? ~0ull : ((s << 32) | d);
+    keys[2 * i + 1] = loop ? ~0ull : ((d << 32) | s);
+  }
+}
+
+// power-law degree of v: floor((1 - u)^(-1 / (gamma - 1))), at least 1, at
+// most cap, with u uniform in [0, 1) from the vertex's hash
+__global__ void k_pl_degrees(int64_t n, double gamma, int64_t cap, uint64_t key, int64_t *deg) {
+  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
+    const double u = (double)(sm64(key + (uint64_t)v) >> 11) * (1.0 / 9007199254740992.0);
+    double d = floor(pow(1.0 - u, -1.0 / (gamma - 1.0)));
+    if (!(d >= 1.0)) d = 1.0;
+    deg[v] = (int64_t)(d > (double)cap ? (double)cap : d);
+  }
+}
+
+// stub i of vertex v (at off[v] + j) gets a random sort key; value = v
+__global__ void k_pl_stubs(int64_t n, const int64_t *off, uint64_t key, uint64_t *skey, int *sval) {
+  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x)
+    for (int64_t i = off[v]; i < off[v + 1]; ++i) {
+      skey[i] = sm64(key + (uint64_t)i);
+      sval[i] = (int)v;
+    }
+}
+
+// consecutive shuffled stubs form an edge (both directions; loops dropped)
+__global__ void k_pl_pairs(const int *sval, int64_t npairs, uint64_t *keys) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < npairs; i += (int64_t)gridDim.x * blockDim.x) {
+    const uint64_t s = (uint64_t)sval[2 * i], d = (uint64_t)sval[2 * i + 1];
     const bool loop = s == d;
     keys[2 * i] = loop ? ~0ull : ((s << 32) | d);
     keys[2 * i + 1] = loop ? ~0ull : ((d << 32) | s);

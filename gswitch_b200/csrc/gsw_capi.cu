@@ -17,6 +17,7 @@
 #include "../../include/gsw.h"
 #include "apps.cuh"
 #include "engine/devloop.cuh"
+#include "engine/mlp.cuh"
 #include "graphgen.cuh"
 #include "mbfs.cuh"
 
@@ -78,6 +79,8 @@ struct gsw_ctx {
   int ntree_nodes = 0;
   tree_set dts{};
   std::map<int, dloop_graph> dl;  // captured level loops, one per application
+  mlp_model mlp{};                // learned selector (valid = 0: none loaded)
+  mlp_model *dmlp = nullptr;      // its device copy (captured loops)
 
   void *buf(const std::string &name, size_t bytes) {
     auto it = bufs.find(name);
@@ -781,7 +784,7 @@ struct dl_run {
 
 template <typename E, typename F>
 bool dl_prepare(dl_run &R, gsw_ctx *ctx, int app, dl_key key, active_set_t &as, device_graph_t<CSR, E> g, F &f,
-                const config_t &conf, const feature_t &fets, int max_iters, int iter_cap) {
+                const config_t &conf, const feature_t &fets, int max_iters, int iter_cap, int selector) {
   if (conf.conf_qmode != Normal || conf.conf_window || conf.conf_compensation || fets.centric != VC)
     return fail(GSW_ERR_UNSUPPORTED, "captured level loop: needs a Normal queue without window or compensation"),
            false;
@@ -815,6 +818,7 @@ bool dl_prepare(dl_run &R, gsw_ctx *ctx, int app, dl_key key, active_set_t &as, 
   im.trees = *trees;
   im.tree_base = ctx->dtrees;
   im.tree_nodes = ctx->ntree_nodes;
+  im.mlp = (selector == GSW_SELECT_MLP && ctx->mlp.valid) ? ctx->dmlp : nullptr;
   im.raw = level_counts{0, 0, 0, 0, 0, 0};
   im.level = g.level;
   im.cursor = as.queue.cursor;
@@ -878,6 +882,121 @@ void dl_collect(dl_run &R, gsw_run_stats *st) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// learned selector in the host-driven loop (engine/mlp.cuh)
+// ---------------------------------------------------------------------------
+bool mlp_override(const mlp_model &m, const feature_t &fets, config_t &conf) {
+  if (!mlp_applicable(m, fets, conf)) return false;
+  float x[MLP_IN], pt = 0;
+  mlp_features(fets, x);
+  const int k = mlp_predict_host(m, x, &pt);
+  if (pt < m.min_conf) return false;
+  mlp_apply(k, conf);
+  return true;
+}
+
+void select_level(gsw_ctx *ctx, const gsw_run_opts *o, selector_t &sel, stat_t &stats, feature_t &fets,
+                  config_t &conf) {
+  sel.select(stats, fets, conf);
+  if (o && o->selector == GSW_SELECT_MLP) mlp_override(ctx->mlp, fets, conf);
+}
+
+// ---------------------------------------------------------------------------
+// per-level labels for the learned selector
+// ---------------------------------------------------------------------------
+struct label_sink {
+  int max_levels = 0, rows = 0, level = 0, every = 8, first = 24, level_limit = 1 << 30;
+  float *X = nullptr, *T = nullptr;
+  int32_t *R = nullptr;
+};
+thread_local label_sink *g_label = nullptr;
+
+// Times every variant for this level from one snapshot of the state the
+// expand touches (vertex data, the visited bits and the counters block), then
+// puts everything back so the run continues exactly as without labelling.
+template <typename G, typename F>
+void label_level(gsw_ctx *ctx, active_set_t &as, G &g, F &f, stat_t &stats, feature_t &fets, config_t &conf) {
+  label_sink *L = g_label;
+  if (!L || !ok()) return;
+  const int lv = L->level++;
+  if (L->rows >= L->max_levels || lv >= L->level_limit || !(lv < L->first || lv % L->every == 0)) return;
+  using WA = typename F::wa_t;
+  using RA = typename F::ra_t;
+  const int64_t n = as.size;
+  const size_t wab = std::is_same<WA, Empty>::value ? 0 : sizeof(WA) * n;
+  const size_t rab = std::is_same<RA, Empty>::value ? 0 : sizeof(RA) * n;
+  const size_t vb = sizeof(uint32_t) * as.bitmap.visited.n_words;
+  char *snap = (char *)ctx->buf("label_snap", wab + rab + vb + sizeof(as_counters_t) + 64);
+  if (!snap) return;
+  char *s_wa = snap, *s_ra = s_wa + wab, *s_vis = s_ra + rab, *s_cnt = s_vis + vb;
+  auto copy_state = [&](bool save) {
+    auto cp = [&](void *dev, char *keep, size_t bytes) {
+      if (bytes)
+        GSW_CUDA(cudaMemcpyAsync(save ? (void *)keep : dev, save ? dev : (void *)keep, bytes, cudaMemcpyDeviceToDevice,
+                                 stream()));
+    };
+    cp(f.data.dg_wa, s_wa, wab);
+    cp(f.data.dg_ra, s_ra, rab);
+    cp(as.bitmap.visited.dg_bits, s_vis, vb);
+    cp(as.dg_cnt, s_cnt, sizeof(as_counters_t));
+  };
+  // a level the inspection already halted (loops that test convergence after
+  // the expand) expands nothing: no label, and the halt must survive
+  if (*as.nt.h_tag) return;
+  copy_state(true);
+  const active_set_t as0 = as;
+  const config_t conf0 = conf;
+  const feature_t fets0 = fets;
+  const int level0 = g.level;
+  const double lt = stats.last_time, at = stats.avg_time, lf = stats.last_filter_time, le = stats.last_expand_time,
+               af = stats.avg_filter_time, ae = stats.avg_expand_time;
+  const int slevel = stats.level;
+  executor_t &ex = ctx->executor;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  float *X = L->X + (size_t)L->rows * MLP_IN, *T = L->T + (size_t)L->rows * MLP_K;
+  mlp_features(fets, X);
+  if (L->R) L->R[L->rows] = conf.conf_fuse_inspect ? -1 : mlp_class(conf.conf_dir, conf.conf_asfmt, conf.conf_lb);
+  for (int k = 0; k < MLP_K; ++k) {
+    Direction d;
+    ASFmt a;
+    LB lb;
+    mlp_variant(k, d, a, lb);
+    conf.conf_dir = d;
+    conf.conf_asfmt = a;
+    conf.conf_lb = lb;
+    conf.conf_fuse_inspect = false;
+    selector_t::set_target(conf);
+    conf.force.has_lb = true;  // no small-level STRICT -> CM fallback while timing STRICT
+    conf.force.lb = lb;
+    cudaEventRecord(e0, stream());
+    ex.filter(as, g, f, stats, fets, conf);
+    g.update_level();
+    ex.expand(as, g, f, stats, fets, conf);
+    cudaEventRecord(e1, stream());
+    float ms = 0;
+    const bool good = ok() && cudaEventSynchronize(e1) == cudaSuccess && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess;
+    const unsigned derr = as.read_error();
+    T[k] = (good && !derr) ? (ms > 0 ? ms : 1e-4f) : 0.f;
+    clear_error();
+    GSW_CUDA(cudaStreamSynchronize(stream()));
+    // back to the snapshot
+    as = as0;
+    conf = conf0;
+    fets = fets0;
+    g.level = level0;
+    stats.last_time = lt, stats.avg_time = at, stats.last_filter_time = lf, stats.last_expand_time = le;
+    stats.avg_filter_time = af, stats.avg_expand_time = ae, stats.level = slevel;
+    copy_state(false);
+    as.nt.reset();  // a trial's empty expand may have raised the halt flag
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  GSW_CUDA(cudaStreamSynchronize(stream()));
+  L->rows++;
+}
+
 }  // namespace
 
 // ===========================================================================
@@ -926,6 +1045,7 @@ gsw_status gsw_destroy(gsw_ctx *ctx) {
   for (auto &kv : ctx->bufs) cudaFree(kv.second.first);
   for (auto &kv : ctx->dl) kv.second.destroy();
   cudaFree(ctx->dtrees);
+  cudaFree(ctx->dmlp);
   ctx->executor.destroy();
   ctx->stats.destroy();
   if (ctx->e0) cudaEventDestroy(ctx->e0);
@@ -1031,6 +1151,63 @@ gsw_status gsw_graph_generate_er(gsw_ctx *ctx, int64_t n, int64_t m_pairs, uint6
   }
   k_er_keys<<<grid_for(m_pairs), 256, 0, stream()>>>(n, m_pairs, stream_key(seed, ST_ER), keys);
   return finish_generate(ctx, g, keys, 2 * m_pairs, wmax, wseed, out, eg);
+}
+
+gsw_status gsw_graph_generate_powerlaw(gsw_ctx *ctx, int64_t n, double gamma, uint64_t seed, int wmax,
+                                       uint64_t wseed, gsw_graph **out) {
+  entry_guard eg(ctx);
+  if (!ctx || !out || n < 2 || !(gamma > 1.0) || n >= (int64_t)INT32_MAX)
+    return fail(GSW_ERR_INVALID_ARG, "gsw_graph_generate_powerlaw: bad arguments");
+  const int64_t cap = std::max<int64_t>(2, (int64_t)std::sqrt((double)n) * 4);
+  int64_t *deg = nullptr, *off = nullptr;
+  uint64_t *skey = nullptr, *skey2 = nullptr, *keys = nullptr;
+  int *sval = nullptr, *sval2 = nullptr;
+  void *tmp = nullptr;
+  auto cleanup = [&]() {
+    cudaFree(deg);
+    cudaFree(off);
+    cudaFree(skey);
+    cudaFree(skey2);
+    cudaFree(sval);
+    cudaFree(sval2);
+    cudaFree(tmp);
+  };
+  if (GSW_CUDA(cudaMalloc((void **)&deg, sizeof(int64_t) * (n + 1))) ||
+      GSW_CUDA(cudaMalloc((void **)&off, sizeof(int64_t) * (n + 1))))
+    return cleanup(), eg.finish();
+  GSW_CUDA(cudaMemsetAsync(deg + n, 0, sizeof(int64_t), stream()));
+  k_pl_degrees<<<grid_for(n), 256, 0, stream()>>>(n, gamma, cap, stream_key(seed, ST_PL), deg);
+  size_t tb = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, tb, deg, off, n + 1, stream());
+  if (GSW_CUDA(cudaMalloc(&tmp, tb))) return cleanup(), eg.finish();
+  GSW_CUDA(cub::DeviceScan::ExclusiveSum(tmp, tb, deg, off, n + 1, stream()));
+  int64_t S = 0;
+  GSW_CUDA(cudaMemcpyAsync(&S, off + n, sizeof(int64_t), cudaMemcpyDeviceToHost, stream()));
+  GSW_CUDA(cudaStreamSynchronize(stream()));
+  cudaFree(tmp);
+  tmp = nullptr;
+  if (!ok()) return cleanup(), eg.finish();
+  const int64_t npairs = S / 2;
+  if (GSW_CUDA(cudaMalloc((void **)&skey, sizeof(uint64_t) * (S + 1))) ||
+      GSW_CUDA(cudaMalloc((void **)&skey2, sizeof(uint64_t) * (S + 1))) ||
+      GSW_CUDA(cudaMalloc((void **)&sval, sizeof(int) * (S + 1))) ||
+      GSW_CUDA(cudaMalloc((void **)&sval2, sizeof(int) * (S + 1))))
+    return cleanup(), eg.finish();
+  k_pl_stubs<<<grid_for(n), 256, 0, stream()>>>(n, off, stream_key(seed, ST_PL + 100), skey, sval);
+  tb = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, tb, skey, skey2, sval, sval2, S, 0, 64, stream());
+  if (GSW_CUDA(cudaMalloc(&tmp, tb))) return cleanup(), eg.finish();
+  GSW_CUDA(cub::DeviceRadixSort::SortPairs(tmp, tb, skey, skey2, sval, sval2, S, 0, 64, stream()));
+  if (GSW_CUDA(cudaMalloc((void **)&keys, sizeof(uint64_t) * (2 * npairs + 1)))) return cleanup(), eg.finish();
+  k_pl_pairs<<<grid_for(npairs), 256, 0, stream()>>>(sval2, npairs, keys);
+  GSW_CUDA(cudaStreamSynchronize(stream()));
+  cleanup();
+  if (!ok()) {
+    cudaFree(keys);
+    return eg.finish();
+  }
+  gsw_graph *g = new_graph(ctx, n);
+  return finish_generate(ctx, g, keys, 2 * npairs, wmax, wseed, out, eg);
 }
 
 gsw_status gsw_graph_info(const gsw_graph *g, int64_t *n, int64_t *m, int *weighted) {
@@ -1139,14 +1316,16 @@ gsw_status gsw_bfs(gsw_ctx *ctx, gsw_graph *gr, int32_t root, const gsw_run_opts
   loop_trace tr{st, MAX_LEVELS};
   const bool captured = o && o->captured;
   dl_run R;
-  if (captured && !dl_prepare(R, ctx, DL_APP_BFS, dl_key() << f.data.dg_wa, as, g, f, conf, fets, 0, MAX_LEVELS))
+  if (captured && !dl_prepare(R, ctx, DL_APP_BFS, dl_key() << f.data.dg_wa, as, g, f, conf, fets, 0, MAX_LEVELS,
+                              o->selector))
     return eg.finish();
   timer tm(ctx);
   if (captured) dl_launch(R);
   for (int level = 0; !captured && ok(); level++) {
     inspector.inspect(as, g, f, stats, fets, conf);
     if (finish(as, g, f, conf)) break;
-    selector.select(stats, fets, conf);
+    select_level(ctx, o, selector, stats, fets, conf);
+    if (g_label) label_level(ctx, as, g, f, stats, fets, conf);
     executor.filter(as, g, f, stats, fets, conf);
     g.update_level();
     tr.level(conf, hints().frontier);
@@ -1215,7 +1394,8 @@ gsw_status gsw_sssp(gsw_ctx *ctx, gsw_graph *gr, int32_t root, const gsw_run_opt
   timer tm(ctx);
   for (int level = 0; ok(); level++) {
     inspector.inspect(as, g, f, stats, fets, conf);
-    selector.select(stats, fets, conf);
+    select_level(ctx, o, selector, stats, fets, conf);
+    if (g_label) label_level(ctx, as, g, f, stats, fets, conf);
     executor.filter(as, g, f, stats, fets, conf);
     g.update_level();
     tr.level(conf, hints().frontier);
@@ -1368,7 +1548,7 @@ gsw_status gsw_pagerank(gsw_ctx *ctx, gsw_graph *gr, const gsw_run_opts *o, floa
   dl_run R;
   if (captured && !dl_prepare(R, ctx, DL_APP_PR,
                               dl_key() << f.data.dg_wa << f.data.dg_ra << f.damp << f.eps << f.data.zero, as, g, f,
-                              conf, fets, op->max_iters, MAX_LEVELS))
+                              conf, fets, op->max_iters, MAX_LEVELS, op->selector))
     return eg.finish();
   timer tm(ctx);
   int steps = 0;
@@ -1377,7 +1557,8 @@ gsw_status gsw_pagerank(gsw_ctx *ctx, gsw_graph *gr, const gsw_run_opts *o, floa
     inspector.inspect(as, g, f, stats, fets, conf);
     if (op->max_iters > 0 && level == op->max_iters) break;
     if (finish(as, g, f, conf)) break;
-    selector.select(stats, fets, conf);
+    select_level(ctx, op, selector, stats, fets, conf);
+    if (g_label) label_level(ctx, as, g, f, stats, fets, conf);
     executor.filter(as, g, f, stats, fets, conf);
     g.update_level();
     tr.level(conf, hints().frontier);
@@ -1660,6 +1841,172 @@ gsw_status gsw_mbfs(gsw_ctx *ctx, gsw_graph *gr, int nsrc, const int32_t *roots,
     st->levels = r.levels;
     st->edges = r.edges;
   }
+  return eg.finish();
+}
+
+// ---------------------------------------------------------------------------
+// learned selector: labels, training, inference, loading (engine/mlp.cuh)
+// ---------------------------------------------------------------------------
+gsw_status gsw_label_levels(gsw_ctx *ctx, gsw_graph *gr, int app, int32_t root, int max_levels, int pr_iters,
+                            float *features, float *times_ms, int32_t *rule_class, int *nlevels) {
+  if (!ctx || !gr || max_levels <= 0 || !features || !times_ms || app < 0 || app > 2)
+    return fail(GSW_ERR_INVALID_ARG, "gsw_label_levels: bad arguments");
+  label_sink L;
+  L.max_levels = max_levels;
+  L.X = features;
+  L.T = times_ms;
+  L.R = rule_class;
+  if (app == GSW_APP_PR) {
+    L.first = pr_iters > 0 ? pr_iters : 3;
+    L.level_limit = L.first;
+  }
+  gsw_run_opts o;
+  gsw_run_opts_default(&o);
+  o.fusion = GSW_STANDALONE;
+  o.persistent = 0;
+  g_label = &L;
+  gsw_status r;
+  if (app == GSW_APP_BFS) {
+    r = gsw_bfs(ctx, gr, root, &o, nullptr, nullptr);
+  } else if (app == GSW_APP_SSSP) {
+    r = gsw_sssp(ctx, gr, root, &o, nullptr, nullptr);
+  } else {
+    o.max_iters = L.first;
+    o.eps = 0.0f;
+    r = gsw_pagerank(ctx, gr, &o, nullptr, nullptr);
+  }
+  g_label = nullptr;
+  if (nlevels) *nlevels = L.rows;
+  return r;
+}
+
+namespace {
+// model floats (parameters, means, inverse deviations) -> device mlp_model
+mlp_model model_from_floats(const float *m, float min_conf) {
+  mlp_model h;
+  memcpy(h.p, m, sizeof(float) * MLP_NPARAM);
+  memcpy(h.mean, m + MLP_NPARAM, sizeof(float) * MLP_IN);
+  memcpy(h.inv_std, m + MLP_NPARAM + MLP_IN, sizeof(float) * MLP_IN);
+  h.min_conf = min_conf;
+  h.valid = 1;
+  return h;
+}
+}  // namespace
+
+gsw_status gsw_mlp_grad(gsw_ctx *ctx, const float *model, const float *X, const float *T, int64_t n, float tau,
+                        float *grad, float *loss) {
+  entry_guard eg(ctx);
+  if (!ctx || !model || !X || !T || n <= 0 || !grad || !(tau > 0)) return fail(GSW_ERR_INVALID_ARG, "gsw_mlp_grad: bad arguments");
+  float *d = (float *)ctx->buf("mlp_work", sizeof(float) * (MLP_NPARAM * 2 + 2 * MLP_IN + 8));
+  float *dX = (float *)ctx->buf("mlp_X", sizeof(float) * n * MLP_IN);
+  float *dT = (float *)ctx->buf("mlp_T", sizeof(float) * n * MLP_K);
+  float *dQ = (float *)ctx->buf("mlp_Q", sizeof(float) * n * MLP_K);
+  if (!d || !dX || !dT || !dQ) return eg.finish();
+  float *dP = d, *dG = d + MLP_NPARAM, *dmean = dG + MLP_NPARAM, *dinv = dmean + MLP_IN, *dloss = dinv + MLP_IN;
+  GSW_CUDA(cudaMemcpyAsync(dP, model, sizeof(float) * (MLP_NPARAM), cudaMemcpyHostToDevice, stream()));
+  GSW_CUDA(cudaMemcpyAsync(dmean, model + MLP_NPARAM, sizeof(float) * 2 * MLP_IN, cudaMemcpyHostToDevice, stream()));
+  GSW_CUDA(cudaMemcpyAsync(dX, X, sizeof(float) * n * MLP_IN, cudaMemcpyHostToDevice, stream()));
+  GSW_CUDA(cudaMemcpyAsync(dT, T, sizeof(float) * n * MLP_K, cudaMemcpyHostToDevice, stream()));
+  GSW_CUDA(cudaMemsetAsync(dG, 0, sizeof(float) * MLP_NPARAM, stream()));
+  GSW_CUDA(cudaMemsetAsync(dloss, 0, sizeof(float), stream()));
+  k_mlp_soft_labels<<<grid_for(n), 256, 0, stream()>>>(dT, n, tau, dQ);
+  const int gb = (int)std::min<int64_t>((n + MLP_TRAIN_THREADS - 1) / MLP_TRAIN_THREADS, 2 * sm_count());
+  k_mlp_grad<<<gb, MLP_TRAIN_THREADS, 0, stream()>>>(dP, dmean, dinv, dX, dQ, n, dG, dloss);
+  GSW_LAUNCHED();
+  GSW_CUDA(cudaMemcpyAsync(grad, dG, sizeof(float) * MLP_NPARAM, cudaMemcpyDeviceToHost, stream()));
+  if (loss) GSW_CUDA(cudaMemcpyAsync(loss, dloss, sizeof(float), cudaMemcpyDeviceToHost, stream()));
+  GSW_CUDA(cudaStreamSynchronize(stream()));
+  return eg.finish();
+}
+
+gsw_status gsw_mlp_train(gsw_ctx *ctx, const float *X, const float *T, int64_t n, int epochs, float lr, float tau,
+                         uint64_t seed, float *model_out, float *loss_out) {
+  entry_guard eg(ctx);
+  if (!ctx || !X || !T || n <= 0 || epochs <= 0 || !model_out || !(lr > 0) || !(tau > 0))
+    return fail(GSW_ERR_INVALID_ARG, "gsw_mlp_train: bad arguments");
+  // feature normalisation of this corpus (host, FP64)
+  std::vector<float> model(MLP_NPARAM + 2 * MLP_IN, 0.f);
+  for (int j = 0; j < MLP_IN; ++j) {
+    double s = 0, s2 = 0;
+    for (int64_t i = 0; i < n; ++i) {
+      s += X[i * MLP_IN + j];
+      s2 += (double)X[i * MLP_IN + j] * X[i * MLP_IN + j];
+    }
+    const double mu = s / n, var = std::max(s2 / n - mu * mu, 0.0);
+    model[MLP_NPARAM + j] = (float)mu;
+    model[MLP_NPARAM + MLP_IN + j] = (float)(1.0 / std::sqrt(var + 1e-6));
+  }
+  // He-uniform initial weights from the seed, zero biases
+  auto init = [&](int off, int fan_out, int fan_in) {
+    const double r = std::sqrt(6.0 / fan_in);
+    for (int i = 0; i < fan_out * fan_in; ++i) {
+      const double u = (double)(sm64(stream_key(seed, 11) + (uint64_t)(off + i)) >> 11) * (1.0 / 9007199254740992.0);
+      model[off + i] = (float)((2 * u - 1) * r);
+    }
+  };
+  init(MLP_W1, MLP_H, MLP_IN);
+  init(MLP_W2, MLP_H, MLP_H);
+  init(MLP_W3, MLP_K, MLP_H);
+  float *d = (float *)ctx->buf("mlp_work", sizeof(float) * (MLP_NPARAM * 4 + 2 * MLP_IN + 8));
+  float *dX = (float *)ctx->buf("mlp_X", sizeof(float) * n * MLP_IN);
+  float *dT = (float *)ctx->buf("mlp_T", sizeof(float) * n * MLP_K);
+  float *dQ = (float *)ctx->buf("mlp_Q", sizeof(float) * n * MLP_K);
+  float *dL = (float *)ctx->buf("mlp_L", sizeof(float) * epochs);
+  if (!d || !dX || !dT || !dQ || !dL) return eg.finish();
+  float *dP = d, *dG = d + MLP_NPARAM, *dM1 = dG + MLP_NPARAM, *dM2 = dM1 + MLP_NPARAM, *dmean = dM2 + MLP_NPARAM,
+        *dinv = dmean + MLP_IN;
+  GSW_CUDA(cudaMemcpyAsync(dP, model.data(), sizeof(float) * MLP_NPARAM, cudaMemcpyHostToDevice, stream()));
+  GSW_CUDA(cudaMemcpyAsync(dmean, model.data() + MLP_NPARAM, sizeof(float) * 2 * MLP_IN, cudaMemcpyHostToDevice,
+                           stream()));
+  GSW_CUDA(cudaMemcpyAsync(dX, X, sizeof(float) * n * MLP_IN, cudaMemcpyHostToDevice, stream()));
+  GSW_CUDA(cudaMemcpyAsync(dT, T, sizeof(float) * n * MLP_K, cudaMemcpyHostToDevice, stream()));
+  GSW_CUDA(cudaMemsetAsync(dM1, 0, sizeof(float) * 2 * MLP_NPARAM, stream()));
+  GSW_CUDA(cudaMemsetAsync(dL, 0, sizeof(float) * epochs, stream()));
+  k_mlp_soft_labels<<<grid_for(n), 256, 0, stream()>>>(dT, n, tau, dQ);
+  const int gb = (int)std::min<int64_t>((n + MLP_TRAIN_THREADS - 1) / MLP_TRAIN_THREADS, 2 * sm_count());
+  for (int e = 0; e < epochs && ok(); ++e) {
+    GSW_CUDA(cudaMemsetAsync(dG, 0, sizeof(float) * MLP_NPARAM, stream()));
+    k_mlp_grad<<<gb, MLP_TRAIN_THREADS, 0, stream()>>>(dP, dmean, dinv, dX, dQ, n, dG, dL + e);
+    k_mlp_adam<<<(MLP_NPARAM + 255) / 256, 256, 0, stream()>>>(dP, dG, dM1, dM2, e + 1, lr, 1e-5f);
+    GSW_LAUNCHED();
+  }
+  GSW_CUDA(cudaMemcpyAsync(model.data(), dP, sizeof(float) * MLP_NPARAM, cudaMemcpyDeviceToHost, stream()));
+  if (loss_out) GSW_CUDA(cudaMemcpyAsync(loss_out, dL, sizeof(float) * epochs, cudaMemcpyDeviceToHost, stream()));
+  GSW_CUDA(cudaStreamSynchronize(stream()));
+  if (ok()) memcpy(model_out, model.data(), sizeof(float) * model.size());
+  return eg.finish();
+}
+
+gsw_status gsw_mlp_infer(gsw_ctx *ctx, const float *model, const float *X, int64_t n, int32_t *cls, float *prob) {
+  entry_guard eg(ctx);
+  if (!ctx || !model || !X || n <= 0 || !cls) return fail(GSW_ERR_INVALID_ARG, "gsw_mlp_infer: bad arguments");
+  const mlp_model h = model_from_floats(model, 0.f);
+  mlp_model *dm = (mlp_model *)ctx->buf("mlp_model_tmp", sizeof(mlp_model));
+  float *dX = (float *)ctx->buf("mlp_X", sizeof(float) * n * MLP_IN);
+  int *dc = (int *)ctx->buf("mlp_cls", sizeof(int) * n);
+  float *dp = (float *)ctx->buf("mlp_prob", sizeof(float) * n);
+  if (!dm || !dX || !dc || !dp) return eg.finish();
+  GSW_CUDA(cudaMemcpyAsync(dm, &h, sizeof(h), cudaMemcpyHostToDevice, stream()));
+  GSW_CUDA(cudaMemcpyAsync(dX, X, sizeof(float) * n * MLP_IN, cudaMemcpyHostToDevice, stream()));
+  k_mlp_infer<<<(unsigned)((n * 32 + 255) / 256), 256, 0, stream()>>>(dm, dX, n, dc, dp);
+  GSW_LAUNCHED();
+  GSW_CUDA(cudaMemcpyAsync(cls, dc, sizeof(int) * n, cudaMemcpyDeviceToHost, stream()));
+  if (prob) GSW_CUDA(cudaMemcpyAsync(prob, dp, sizeof(float) * n, cudaMemcpyDeviceToHost, stream()));
+  GSW_CUDA(cudaStreamSynchronize(stream()));
+  return eg.finish();
+}
+
+gsw_status gsw_mlp_load(gsw_ctx *ctx, const float *model, float min_conf) {
+  entry_guard eg(ctx);
+  if (!ctx) return fail(GSW_ERR_INVALID_ARG, "gsw_mlp_load: NULL context");
+  if (!model) {
+    ctx->mlp.valid = 0;
+  } else {
+    ctx->mlp = model_from_floats(model, min_conf);
+  }
+  if (!ctx->dmlp && GSW_CUDA(cudaMalloc((void **)&ctx->dmlp, sizeof(mlp_model)))) return eg.finish();
+  GSW_CUDA(cudaMemcpyAsync(ctx->dmlp, &ctx->mlp, sizeof(mlp_model), cudaMemcpyHostToDevice, stream()));
+  GSW_CUDA(cudaStreamSynchronize(stream()));
   return eg.finish();
 }
 

@@ -67,6 +67,13 @@ gsw_status gsw_graph_generate_grid(gsw_ctx *ctx, int rows, int cols, int lr_div,
                                    uint64_t wseed, gsw_graph **out);
 gsw_status gsw_graph_generate_er(gsw_ctx *ctx, int64_t n, int64_t m_pairs, uint64_t seed, int wmax, uint64_t wseed,
                                  gsw_graph **out);
+/* No counterpart in the reference (its corpus is downloaded graphs).
+ * Undirected configuration-model graph for the selector corpus: vertex
+ * degrees drawn from a power law P(d) ~ d^-gamma (d >= 1, capped at
+ * sqrt(n * mean_degree)), stubs paired by a seeded shuffle, self-loops and
+ * duplicate edges dropped. */
+gsw_status gsw_graph_generate_powerlaw(gsw_ctx *ctx, int64_t n, double gamma, uint64_t seed, int wmax,
+                                       uint64_t wseed, gsw_graph **out);
 /* n, arcs, weighted flag */
 gsw_status gsw_graph_info(const gsw_graph *g, int64_t *n, int64_t *m, int *weighted);
 /* Degree statistics as graph_attr_t::fill (src/utils/fileIO.cuh:35-67):
@@ -167,6 +174,46 @@ gsw_status gsw_gc(gsw_ctx *ctx, gsw_graph *g, const gsw_run_opts *o, int32_t *co
  * bit-sliced frontiers (64 sources per word) in one launch sequence. */
 gsw_status gsw_mbfs(gsw_ctx *ctx, gsw_graph *g, int nsrc, const int32_t *roots, int batched, const gsw_run_opts *o,
                     int32_t *levels, gsw_run_stats *st);
+
+/* ---- learned selector -------------------------------------------------------
+ * No counterpart in the reference, whose selector is decision trees
+ * (src/abstraction/selector.cuh:22-303).  An FP32 MLP 8 -> 32 -> 32 -> 20
+ * over per-level features; class k is the standalone variant
+ * direction = k / 10 (push, pull), format = (k / 5) % 2 (queue, bitmap),
+ * load balance = k % 5 (TM, WM, CM, STRICT, TWC).
+ * A model is GSW_MLP_MODEL_FLOATS floats: the GSW_MLP_NPARAM parameters
+ * (W1[32][8] b1[32] W2[32][32] b2[32] W3[20][32] b3[20]) followed by the
+ * feature means (8) and inverse standard deviations (8). */
+#define GSW_MLP_FEATURES 8
+#define GSW_MLP_CLASSES 20
+#define GSW_MLP_NPARAM 2004
+#define GSW_MLP_MODEL_FLOATS (GSW_MLP_NPARAM + 2 * GSW_MLP_FEATURES)
+enum { GSW_APP_BFS = 0, GSW_APP_SSSP = 1, GSW_APP_PR = 2 };
+
+/* Labels for training: runs the application with standalone levels and, at
+ * each labelled level (the first 24, then every 8th, at most max_levels; PR:
+ * the first pr_iters iterations), times every one of the 20 variants from the
+ * same snapshot of the level's state (filter + expand, CUDA events).
+ * features: [max_levels][8]; times_ms: [max_levels][20] (0 = the variant
+ * failed); rule_class: [max_levels] the class the rule-based selector chose
+ * (may be NULL); *nlevels = rows written. */
+gsw_status gsw_label_levels(gsw_ctx *ctx, gsw_graph *g, int app, int32_t root, int max_levels, int pr_iters,
+                            float *features, float *times_ms, int32_t *rule_class, int *nlevels);
+/* Trains a model on n samples with the project's forward/backward and Adam
+ * kernels (full batch, soft labels q_k ~ exp(-(t_k / t_min - 1) / tau)).
+ * loss: per-epoch mean loss (may be NULL). */
+gsw_status gsw_mlp_train(gsw_ctx *ctx, const float *features, const float *times_ms, int64_t n, int epochs, float lr,
+                         float tau, uint64_t seed, float *model_out, float *loss);
+/* Loss and gradient (GSW_MLP_NPARAM floats) of a model on n samples. */
+gsw_status gsw_mlp_grad(gsw_ctx *ctx, const float *model, const float *features, const float *times_ms, int64_t n,
+                        float tau, float *grad, float *loss);
+/* Warp-level inference: class and top probability per sample. */
+gsw_status gsw_mlp_infer(gsw_ctx *ctx, const float *model, const float *features, int64_t n, int32_t *cls,
+                         float *prob);
+/* Loads (model != NULL) or unloads the model that runs with
+ * opts.selector = GSW_SELECT_MLP; below min_conf top-class probability the
+ * rules decide. */
+gsw_status gsw_mlp_load(gsw_ctx *ctx, const float *model, float min_conf);
 
 /* No counterpart in the reference.  BFS levels (-1 unreached) computed with
  * the edge-balanced push expand, for callers that cannot allocate device
