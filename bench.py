@@ -12,8 +12,13 @@ Also reported:
                step uploads the host CSR (pinned), runs BFS and reads the
                levels back;
   roofline     the dominant kernel's algorithmic bytes per launch over its
-               average CUDA-event duration in the timed region, against the
-               measured HBM copy bandwidth;
+               average CUDA-event duration (the timed steps repeated with an
+               event pair around every kernel), against the measured HBM copy
+               bandwidth;
+  apps         config C2's four applications on the same graph: the switched
+               form (rule trees, learned selector, captured loop) against
+               every fixed variant; the 256-source batched MBFS and the
+               512-graph G(n, m) batch (config C4) batched vs unbatched;
   cpu_baseline the CPU oracle's restated reference BFS on the same graph,
                one core, bounded sample (rank 0, N=1).
 `--impl reference` times the reference's own bfs_cpu (application/bfs.cu:
@@ -58,14 +63,21 @@ class ClockSampler:
         self.gpu = gpu
         self.proc = None
         self.path = None
+        self.skip = 0
 
     def start(self):
+        """Starts sampling every 20 ms and waits (up to 5 s) for the first
+        sample, so that the timed region that follows is covered."""
         try:
             fd, self.path = tempfile.mkstemp(suffix=".csv")
             os.close(fd)
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
-                 "-lms", "100"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+                 "-lms", "20"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+            t0 = time.time()
+            while time.time() - t0 < 5.0 and os.path.getsize(self.path) == 0:
+                time.sleep(0.02)
+            self.skip = sum(1 for _ in open(self.path))  # samples taken before the timed region
         except Exception:
             self.proc = None
 
@@ -79,7 +91,11 @@ class ClockSampler:
             self.proc.kill()
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in open(self.path):
+        lines = open(self.path).read().splitlines()
+        # keep the samples of the timed region (the last pre-region one too,
+        # when the region was shorter than the sampling period)
+        lines = lines[max(0, self.skip - 1):]
+        for line in lines:
             f = [x.strip() for x in line.split(",")]
             if len(f) < 9:
                 continue
@@ -143,10 +159,15 @@ def roofline_from(runs, n, peak_gbs, peak_kind):
             "avg_launch_ms": round(ms / max(launches, 1), 5), "traffic": None, "time_shares": shares}
 
 
+def run_opts(gs, selector, **kw):
+    return gs.RunOpts(selector=selector, **kw)
+
+
 def run_ours(args):
     import torch
 
     import gswitch_b200 as gs
+    from gswitch_b200.selector_train import load_model
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -164,27 +185,35 @@ def run_ours(args):
             dist.barrier()
 
     ctx = gs.Context(local)
+    selector = args.selector
+    if selector == "mlp":
+        model, min_conf = load_model()
+        if model is None:
+            selector = "rules"
+        else:
+            ctx.mlp_load(model, min_conf)
+    sampler = ClockSampler(local)
+    sampler.start()
     t0 = time.time()
     g = ctx.rmat(args.scale, args.ef, 0.57, 0.19, 0.19, seed=1)
     gen_s = time.time() - t0
     W, K = args.warmup, args.steps
     roots = g.roots(1000 + rank, W + K)
     for r in roots[:W]:
-        g.bfs(int(r), out=False)
+        g.bfs(int(r), run_opts(gs, selector), out=False)
 
     stream = torch.cuda.ExternalStream(ctx.stream_ptr(), device=local)
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
-    sampler = ClockSampler(local)
     timed = []
     barrier()
     torch.cuda.synchronize()
-    sampler.start()
+    sampler.skip = sum(1 for _ in open(sampler.path)) if sampler.proc else 0
     e0.record(stream)
     edges = 0
     launches = 0
     for r in roots[W:W + K]:
-        _, st = g.bfs(int(r), opts=gs.RunOpts(timing=True), out=False)
+        _, st = g.bfs(int(r), opts=run_opts(gs, selector), out=False)
         edges += st.edges
         launches += st.launches
         timed.append(st)
@@ -205,11 +234,15 @@ def run_ours(args):
 
     out = None
     if rank == 0:
-        # accounting pass (untimed): same roots, edges touched per expand
+        # per-kernel pass: the same steps again with a CUDA event pair around
+        # every inspection and expand (kept out of the timed region above,
+        # whose value it would lower by the event records), plus an
+        # accounting pass for the edges each expand touched
         runs = []
-        for r, st in zip(roots[W:W + K], timed):
-            lv, acc = g.bfs(int(r), opts=gs.RunOpts(account=True))
-            runs.append((st, acc, lv))
+        for r in roots[W:W + K]:
+            _, sti = g.bfs(int(r), opts=run_opts(gs, selector, timing=True), out=False)
+            lv, acc = g.bfs(int(r), opts=run_opts(gs, selector, account=True))
+            runs.append((sti, acc, lv))
         peak, kind = peaks()
         roof = roofline_from(runs, g.n, peak, kind)
         trace = [list(t[:4]) + [int(t[4])] for t in timed[0].trace]
@@ -221,13 +254,16 @@ def run_ours(args):
                        "rmat_abcd": [0.57, 0.19, 0.19, 0.05], "seed": 1, "n": g.n, "arcs": g.m,
                        "roots": "seeded non-isolated, one per step, per rank",
                        "l2": "inputs larger than L2 (CSR %.2f GB)" % ((8 * (g.n + 1) + 4 * g.m) / 1e9),
-                       "parallelism": f"replicas x{world}", "selector": "rules (reference trees)",
+                       "parallelism": f"replicas x{world}",
+                       "selector": "learned MLP (rules as fallback)" if selector == "mlp" else "rules (reference trees)",
                        "graph_build_s": round(gen_s, 2)},
             "roofline": roof, "gpu_launches": int(launches), "clocks": clocks,
             "levels_first_step": trace,
         }
+        if world == 1 and not args.no_apps:
+            out["apps"] = app_table(ctx, g, gs, args, roots[W:W + 3], selector)
         if not args.no_e2e:
-            out["e2e"] = e2e(ctx, g, roots[W:W + K], gs, torch)
+            out["e2e"] = e2e(ctx, g, roots[W:W + min(K, 20)], gs, torch, selector)
         if world == 1 and not args.no_cpu:
             out["cpu_baseline"] = cpu_baseline(g, roots, args.cpu_seconds)
     g.close()
@@ -238,7 +274,125 @@ def run_ours(args):
         print(json.dumps(out))
 
 
-def e2e(ctx, g, roots, gs, torch):
+FIXED = ["-".join((d, f, lb, "Standalone")) for d in ("Push", "Pull") for f in ("Queue", "Bitmap")
+         for lb in ("TM", "WM", "CM", "STRICT", "TWC")] + [f"Push-Queue-{lb}-Fused" for lb in
+                                                          ("TM", "WM", "CM", "STRICT", "TWC")]
+
+
+def app_table(ctx, g, gs, args, roots, selector):
+    """BFS, SSSP, CC and PageRank on the same RMAT
+    graph (SSSP on an int32-weighted copy, weights U[1, 64]): the switched
+    form (rules, and the learned selector; host-driven and captured loop)
+    against every fixed variant, GTEPS by each app's definition (BFS / SSSP:
+    Graph500 edges of the reached component; CC: m/2; PageRank: m x
+    iterations).  Plus the batched multi-source BFS (config C4's 256
+    sources) against 256 sequential switched BFS runs."""
+    gw = ctx.rmat(args.scale, args.ef, 0.57, 0.19, 0.19, seed=1, wmax=64, wseed=2)
+    root = int(roots[0])
+    pr_iters = 5
+
+    def once(app, o):
+        if app == "bfs":
+            _, st = g.bfs(root, o, out=False)
+        elif app == "sssp":
+            _, st = gw.sssp(root, o, out=False)
+        elif app == "pr":
+            _, st = g.pagerank(pr_iters, 0.85, 0.0, opts=o, out=False)
+        else:
+            _, st = g.cc(o, out=False)
+        return st.edges / (st.ms * 1e6) if st.ms > 0 else 0.0, st.ms
+
+    def measure(app, o, reps):
+        once(app, o)
+        vals = sorted(once(app, o) for _ in range(reps))
+        return vals[len(vals) // 2]
+
+    table = {}
+    for app in ("bfs", "sssp", "pr", "cc"):
+        row = {"switched_rules": round(measure(app, gs.RunOpts(), 3)[0], 3)}
+        if app != "cc":
+            row["switched_mlp"] = round(measure(app, gs.RunOpts(selector="mlp"), 3)[0], 3)
+        if app in ("bfs", "pr"):
+            row["switched_mlp_captured"] = round(measure(app, gs.RunOpts(selector="mlp", captured=True), 3)[0], 3)
+        fixed = {}
+        if app == "cc":
+            for cfg in ("x-Queue", "x-Bitmap"):
+                fixed[cfg] = round(measure(app, gs.RunOpts.from_config(cfg), 1)[0], 3)
+        else:
+            for cfg in FIXED + (["x-x-TWOD"] if app == "pr" else []):
+                if app == "pr" and cfg.endswith("Fused"):
+                    continue
+                fixed[cfg] = round(measure(app, gs.RunOpts.from_config(cfg), 1)[0], 3)
+        best = max(fixed.items(), key=lambda kv: kv[1])
+        sw = row.get("switched_mlp" if selector == "mlp" and app != "cc" else "switched_rules")
+        row.update({"fixed": fixed, "best_fixed": {"variant": best[0], "gteps": best[1]},
+                    "switched_vs_best_fixed": round(sw / best[1], 3) if best[1] > 0 else None})
+        table[app] = row
+    table["definitions"] = {"bfs": "sum deg(reached)/2 / t", "sssp": "sum deg(reached)/2 / t", "cc": "m/2 / t",
+                            "pr": f"m x {pr_iters} iterations / t", "unit": "GTEPS", "graph": "same RMAT as the headline"}
+    gw.close()
+    # batched multi-source BFS: 256 seeded sources in one bit-sliced run vs
+    # 256 switched single-source runs
+    if args.scale >= 22:
+        gm = ctx.rmat(22, 16, 0.57, 0.19, 0.19, seed=1)
+        src = gm.roots(77, 256)
+        gm.mbfs(src, batched=True, out=False)
+        _, stb = gm.mbfs(src, batched=True, out=False)
+        _, sts = gm.mbfs(src, batched=False, opts=gs.RunOpts(selector=selector), out=False)
+        table["mbfs_rmat22_256src"] = {"batched_gteps": round(stb.edges / (stb.ms * 1e6), 3),
+                                       "sequential_switched_gteps": round(sts.edges / (sts.ms * 1e6), 3),
+                                       "batched_vs_sequential": round(sts.ms / stb.ms, 3)}
+        gm.close()
+    table["er_batch_512"] = er_batch_entry(ctx, gs, selector)
+    return table
+
+
+def er_batch_entry(ctx, gs, selector):
+    """Config C4's batch: 512 G(n, m) graphs, n log-uniform in [1e3, 2e5],
+    mean degree uniform in [4, 32].  Batched: one BFS level loop over the
+    disjoint union from one root per instance (and CC over the union);
+    unbatched: each instance as its own graph, one BFS per graph."""
+    gb, voff = ctx.er_batch(512, seed=7, nlo=1000, nhi=200000, dlo=4.0, dhi=32.0)
+    off, col, _ = gb.download()
+    parts, roots = [], []
+    for i in range(512):
+        a, b = int(voff[i]), int(voff[i + 1])
+        o = off[a:b + 1] - off[a]
+        c = col[off[a]:off[b]] - a
+        h = ctx.upload(o, c)
+        parts.append(h)
+        roots.append(int(h.roots(11 + i, 1)[0]))
+    groots = [int(voff[i]) + r for i, r in enumerate(roots)]
+    o = gs.RunOpts(selector=selector)
+    res = {"instances": 512, "vertices": int(gb.n), "arcs": int(gb.m)}
+    for name, oo in (("batched", o), ("batched_captured", gs.RunOpts(selector=selector, captured=True))):
+        gb.bfs_multi(groots, oo, out=False)
+        _, st = gb.bfs_multi(groots, oo, out=False)
+        res[f"bfs_{name}_ms"] = round(st.ms, 3)
+        res[f"bfs_{name}_gteps"] = round(st.edges / (st.ms * 1e6), 3)
+    tot_ms, tot_e = 0.0, 0
+    for h, r in zip(parts, roots):
+        _, st = h.bfs(r, o, out=False)
+        tot_ms += st.ms
+        tot_e += st.edges
+    res["bfs_unbatched_ms"] = round(tot_ms, 3)
+    res["bfs_unbatched_gteps"] = round(tot_e / (tot_ms * 1e6), 3)
+    res["bfs_batched_vs_unbatched"] = round(tot_ms / res["bfs_batched_ms"], 2)
+    gb.cc(out=False)
+    _, st = gb.cc(out=False)
+    cc_un = 0.0
+    for h in parts:
+        _, s2 = h.cc(out=False)
+        cc_un += s2.ms
+    res.update({"cc_batched_ms": round(st.ms, 3), "cc_unbatched_ms": round(cc_un, 3),
+                "cc_batched_vs_unbatched": round(cc_un / st.ms, 2)})
+    for h in parts:
+        h.close()
+    gb.close()
+    return res
+
+
+def e2e(ctx, g, roots, gs, torch, selector="rules"):
     """BFS through the C ABI with host buffers: upload (pinned CSR) + BFS +
     levels back to host, per step."""
     off, col, _ = g.download()
@@ -252,7 +406,7 @@ def e2e(ctx, g, roots, gs, torch):
     e0.record(stream)
     for r in roots:
         h = ctx.upload(poff, pcol)
-        st = h._run(gs.lib().gsw_bfs, gs.C.c_int32(int(r)), outs=[plev], opts=None)
+        st = h._run(gs.lib().gsw_bfs, gs.C.c_int32(int(r)), outs=[plev], opts=gs.RunOpts(selector=selector))
         edges += st.edges
         h.close()
     e1.record(stream)
@@ -343,7 +497,7 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--scale", type=int, default=24)
@@ -351,6 +505,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--selector", default="mlp", choices=["mlp", "rules"])
+    ap.add_argument("--no-apps", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3

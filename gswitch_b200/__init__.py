@@ -38,7 +38,7 @@ ABI_SYMBOLS = (
     "gsw_graph_destroy", "gsw_graph_roots", "gsw_ctx_stream", "gsw_run_opts_default", "gsw_bfs", "gsw_sssp", "gsw_cc",
     "gsw_pagerank", "gsw_bc", "gsw_gc", "gsw_mbfs", "gsw_bfs_strict_noalloc",
     "gsw_graph_generate_powerlaw", "gsw_label_levels", "gsw_mlp_train", "gsw_mlp_grad", "gsw_mlp_infer",
-    "gsw_mlp_load",
+    "gsw_mlp_load", "gsw_graph_generate_er_batch", "gsw_bfs_multi",
 )
 
 # learned selector (include/gsw.h): 8 features -> 32 -> 32 -> 20 classes
@@ -120,6 +120,9 @@ def lib():
     L.gsw_mlp_grad.argtypes = [vp, vp, vp, vp, i64, C.c_float, vp, vp]
     L.gsw_mlp_infer.argtypes = [vp, vp, vp, i64, vp, vp]
     L.gsw_mlp_load.argtypes = [vp, vp, C.c_float]
+    L.gsw_graph_generate_er_batch.argtypes = [vp, C.c_int, u64, i64, i64, C.c_double, C.c_double, C.c_int, u64, vp,
+                                              pvp]
+    L.gsw_bfs_multi.argtypes = [vp, vp, C.c_int, vp, po, vp, ps]
     _LIB = L
     return L
 
@@ -259,6 +262,15 @@ class Context:
         _check(lib().gsw_graph_generate_er(self._h, n, m_pairs, seed, wmax, wseed, C.byref(h)))
         return Graph(self, h)
 
+    def er_batch(self, count, seed=1, nlo=1000, nhi=200000, dlo=4.0, dhi=32.0, wmax=0, wseed=0):
+        """`count` G(n, m) graphs as one disjoint union; returns (graph,
+        vertex offsets [count + 1])."""
+        h = C.c_void_p()
+        voff = np.zeros(count + 1, dtype=np.int64)
+        _check(lib().gsw_graph_generate_er_batch(self._h, count, seed, nlo, nhi, dlo, dhi, wmax, wseed, _ptr(voff),
+                                                 C.byref(h)))
+        return Graph(self, h), voff
+
     def powerlaw(self, n, gamma, seed=1, wmax=0, wseed=0) -> "Graph":
         h = C.c_void_p()
         _check(lib().gsw_graph_generate_powerlaw(self._h, n, float(gamma), seed, wmax, wseed, C.byref(h)))
@@ -354,6 +366,16 @@ class Graph:
         lv = np.empty(self.n, dtype=np.int32) if out else None
         st = self._run(lib().gsw_bfs, C.c_int32(root), outs=[lv], opts=opts)
         return lv, st
+
+    def bfs_multi(self, roots, opts=None, out=True):
+        """BFS from all `roots` at once (distance to the nearest root)."""
+        roots = np.ascontiguousarray(roots, dtype=np.int32)
+        lv = np.empty(self.n, dtype=np.int32) if out else None
+        st = _Stats()
+        o = self._opts(opts)
+        _check(lib().gsw_bfs_multi(self.ctx._h, self._h, len(roots), _ptr(roots), C.byref(o), _ptr(lv),
+                                   C.byref(st)))
+        return lv, RunStats(st)
 
     def sssp(self, root, opts=None, out=True):
         d = np.empty(self.n, dtype=np.int32) if out else None

@@ -361,6 +361,7 @@ struct feature_t {
   Centric centric = VC;
   Computation pattern = Idem;
   int use_root = -1;
+  double first_active = 1;  // vertices active at the first level when it starts from roots (multi-root runs)
   bool fromall = false;
   bool toall = false;
 

@@ -145,8 +145,8 @@ __host__ __device__ inline level_counts fets_first(feature_t &fets, int64_t nver
     fets.push_workload = (double)nedges;
     fets.pull_workload = 0;
   } else {
-    fets.active_vertex = 1;
-    fets.unactive_vertex = (double)(nvertexs - 1);
+    fets.active_vertex = fets.first_active;
+    fets.unactive_vertex = (double)nvertexs - fets.first_active;
     fets.push_workload = fets.first_workload;
     fets.pull_workload = nedges - fets.first_workload;
   }

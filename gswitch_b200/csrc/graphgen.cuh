@@ -153,6 +153,29 @@ __global__ void k_pl_pairs(const int *sval, int64_t npairs, uint64_t *keys) {
   }
 }
 
+// A batch of G(n_i, m_i) instances as one disjoint union: instance i owns
+// vertices [voff[i], voff[i+1]) and pairs [poff[i], poff[i+1]); its pairs are
+// drawn exactly as k_er_keys draws a standalone instance with key ikey[i],
+// then shifted by voff[i].
+__global__ void k_er_batch_keys(int count, const int64_t *voff, const int64_t *poff, const uint64_t *ikey,
+                                uint64_t *keys) {
+  const int64_t total = poff[count];
+  for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < total; p += (int64_t)gridDim.x * blockDim.x) {
+    int lo = 0, hi = count;  // instance: last i with poff[i] <= p
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (poff[mid] <= p) lo = mid; else hi = mid;
+    }
+    const int64_t j = p - poff[lo];
+    const uint64_t n = (uint64_t)(voff[lo + 1] - voff[lo]), base = (uint64_t)voff[lo];
+    const uint64_t s = sm64(ikey[lo] + 2 * (uint64_t)j) % n + base;
+    const uint64_t d = sm64(ikey[lo] + 2 * (uint64_t)j + 1) % n + base;
+    const bool loop = s == d;
+    keys[2 * p] = loop ? ~0ull : ((s << 32) | d);
+    keys[2 * p + 1] = loop ? ~0ull : ((d << 32) | s);
+  }
+}
+
 // after sorting: keep the first of each run of equal keys, drop sentinels
 __global__ void k_unique_flags(const uint64_t *keys, int64_t len, int *flag) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < len; i += (int64_t)gridDim.x * blockDim.x)

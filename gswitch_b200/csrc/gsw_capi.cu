@@ -544,6 +544,20 @@ void fill_root(T *p, T v, T rootv, int64_t root, int64_t n) {
   k_fill_root<T><<<grid_for(n), 256, 0, stream()>>>(p, v, rootv, root, n);
 }
 
+__global__ void k_set_roots(int *wa, const int *roots, int nroots, int v) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nroots) wa[roots[i]] = v;
+}
+// the roots are Active (and not Inactive) in the first inspection's bitmaps
+__global__ void k_mark_roots(uint32_t *active, uint32_t *inactive, const int *roots, int nroots) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nroots) {
+    const int r = roots[i];
+    atomicOr(active + (r >> 5), 1u << (r & 31));
+    atomicOr(inactive + (r >> 5), 1u << (r & 31));
+  }
+}
+
 // Graph500 numerator: sum of degrees of reached vertices, halved
 __global__ void k_reached_edges(const int *lvl_or_dist, int stride_ints, int unreached, const int *odeg, int64_t n,
                                 unsigned long long *out) {
@@ -1153,6 +1167,53 @@ gsw_status gsw_graph_generate_er(gsw_ctx *ctx, int64_t n, int64_t m_pairs, uint6
   return finish_generate(ctx, g, keys, 2 * m_pairs, wmax, wseed, out, eg);
 }
 
+gsw_status gsw_graph_generate_er_batch(gsw_ctx *ctx, int count, uint64_t seed, int64_t nlo, int64_t nhi, double dlo,
+                                       double dhi, int wmax, uint64_t wseed, int64_t *vertex_offsets,
+                                       gsw_graph **out) {
+  entry_guard eg(ctx);
+  if (!ctx || !out || count <= 0 || nlo < 2 || nhi < nlo || !(dlo > 0) || dhi < dlo)
+    return fail(GSW_ERR_INVALID_ARG, "gsw_graph_generate_er_batch: bad arguments");
+  // instance parameters: n log-uniform in [nlo, nhi], mean degree uniform
+  // in [dlo, dhi], m = floor(n * degree / 2) pairs, its own seed
+  std::vector<int64_t> voff(count + 1, 0), poff(count + 1, 0);
+  std::vector<uint64_t> ikey(count);
+  const uint64_t key = stream_key(seed, ST_ERB);
+  auto unit = [](uint64_t h) { return (double)(h >> 11) * (1.0 / 9007199254740992.0); };
+  for (int i = 0; i < count; ++i) {
+    const double u1 = unit(sm64(key + 3 * (uint64_t)i)), u2 = unit(sm64(key + 3 * (uint64_t)i + 1));
+    int64_t n = (int64_t)std::llround(std::exp(std::log((double)nlo) + u1 * (std::log((double)nhi) - std::log((double)nlo))));
+    n = std::min(std::max(n, nlo), nhi);
+    const double deg = dlo + u2 * (dhi - dlo);
+    voff[i + 1] = voff[i] + n;
+    poff[i + 1] = poff[i] + (int64_t)std::floor((double)n * deg / 2.0);
+    ikey[i] = stream_key(sm64(key + 3 * (uint64_t)i + 2), ST_ER);
+  }
+  const int64_t N = voff[count], P = poff[count];
+  if (N >= (int64_t)INT32_MAX) return fail(GSW_ERR_UNSUPPORTED, "gsw_graph_generate_er_batch: union exceeds int32 ids");
+  int64_t *dv = nullptr, *dp = nullptr;
+  uint64_t *dk = nullptr, *keys = nullptr;
+  auto cleanup = [&]() {
+    cudaFree(dv);
+    cudaFree(dp);
+    cudaFree(dk);
+  };
+  if (GSW_CUDA(cudaMalloc((void **)&dv, sizeof(int64_t) * (count + 1))) ||
+      GSW_CUDA(cudaMalloc((void **)&dp, sizeof(int64_t) * (count + 1))) ||
+      GSW_CUDA(cudaMalloc((void **)&dk, sizeof(uint64_t) * count)) ||
+      GSW_CUDA(cudaMalloc((void **)&keys, sizeof(uint64_t) * (2 * P + 1))))
+    return cleanup(), cudaFree(keys), eg.finish();
+  GSW_CUDA(cudaMemcpyAsync(dv, voff.data(), sizeof(int64_t) * (count + 1), cudaMemcpyHostToDevice, stream()));
+  GSW_CUDA(cudaMemcpyAsync(dp, poff.data(), sizeof(int64_t) * (count + 1), cudaMemcpyHostToDevice, stream()));
+  GSW_CUDA(cudaMemcpyAsync(dk, ikey.data(), sizeof(uint64_t) * count, cudaMemcpyHostToDevice, stream()));
+  k_er_batch_keys<<<grid_for(P), 256, 0, stream()>>>(count, dv, dp, dk, keys);
+  GSW_CUDA(cudaStreamSynchronize(stream()));
+  cleanup();
+  if (!ok()) return cudaFree(keys), eg.finish();
+  if (vertex_offsets) memcpy(vertex_offsets, voff.data(), sizeof(int64_t) * (count + 1));
+  gsw_graph *g = new_graph(ctx, N);
+  return finish_generate(ctx, g, keys, 2 * P, wmax, wseed, out, eg);
+}
+
 gsw_status gsw_graph_generate_powerlaw(gsw_ctx *ctx, int64_t n, double gamma, uint64_t seed, int wmax,
                                        uint64_t wseed, gsw_graph **out) {
   entry_guard eg(ctx);
@@ -1278,17 +1339,31 @@ gsw_status gsw_ctx_stream(gsw_ctx *ctx, void **s) {
 // ---------------------------------------------------------------------------
 // BFS: application/bfs.cu:78-102 (loop) and :104-130 (set-up)
 // ---------------------------------------------------------------------------
-gsw_status gsw_bfs(gsw_ctx *ctx, gsw_graph *gr, int32_t root, const gsw_run_opts *o, int32_t *levels,
-                   gsw_run_stats *st) {
-  entry_guard eg(ctx);
-  if (!ctx || !gr || root < 0 || root >= gr->n) return fail(GSW_ERR_INVALID_ARG, "gsw_bfs: bad arguments");
+// BFS from one root, or from several at once (levels = distance to the
+// nearest root; over a disjoint union of graphs with one root per part this
+// is one BFS per part, all in the same level loop)
+gsw_status bfs_run(gsw_ctx *ctx, gsw_graph *gr, const int32_t *roots, int nroots, const gsw_run_opts *o,
+                   int32_t *levels, gsw_run_stats *st, entry_guard &eg) {
+  const int32_t root = roots[0];
   begin_stats(st);
   auto g = gr->view<Empty>();
   app::BFS f;
   f.data.size = gr->n;
   f.data.dg_wa = (int *)ctx->buf("wa", sizeof(int) * (gr->n + 1));
   if (!f.data.dg_wa) return eg.finish();
-  fill_root<int>(f.data.dg_wa, -1, 0, root, gr->n);
+  int64_t root_degree_sum = 0;
+  if (nroots == 1) {
+    fill_root<int>(f.data.dg_wa, -1, 0, root, gr->n);
+    root_degree_sum = root_deg(gr, root);
+  } else {
+    int *droots = (int *)ctx->buf("bfs_roots", sizeof(int) * nroots);
+    if (!droots) return eg.finish();
+    GSW_CUDA(cudaMemcpyAsync(droots, roots, sizeof(int) * nroots, cudaMemcpyHostToDevice, stream()));
+    fill<int>(f.data.dg_wa, -1, gr->n);
+    k_set_roots<<<(nroots + 255) / 256, 256, 0, stream()>>>(f.data.dg_wa, droots, nroots, 0);
+    host_degrees(gr);
+    for (int i = 0; i < nroots; ++i) root_degree_sum += gr->hdeg[roots[i]];
+  }
   feature_t fets;
   config_t conf;
   stat_t &stats = ctx->stats;
@@ -1307,12 +1382,20 @@ gsw_status gsw_bfs(gsw_ctx *ctx, gsw_graph *gr, int32_t root, const gsw_run_opts
   apply_opts(o, conf);
   set_graph_features(fets, gr);
   fets.use_root = root;
-  init_conf_impl(stats, fets, conf, g, f, gr->mean_weight, gr->attr[0], false, root_deg(gr, root));
+  fets.first_active = nroots;
+  init_conf_impl(stats, fets, conf, g, f, gr->mean_weight, gr->attr[0], false, root_degree_sum);
   active_set_t *asp = ctx->aset(gr->n, conf.conf_qmode);
   if (!asp) return eg.finish();
   active_set_t &as = *asp;
   as.reset();
-  as.init(root);
+  if (nroots == 1) {
+    as.init(root);
+  } else {
+    as.init(ALL_INACTIVE);
+    int *droots = (int *)ctx->buf("bfs_roots", sizeof(int) * nroots);
+    k_mark_roots<<<(nroots + 255) / 256, 256, 0, stream()>>>(as.bitmap.active.dg_bits, as.bitmap.inactive.dg_bits,
+                                                           droots, nroots);
+  }
   loop_trace tr{st, MAX_LEVELS};
   const bool captured = o && o->captured;
   dl_run R;
@@ -1346,6 +1429,22 @@ gsw_status gsw_bfs(gsw_ctx *ctx, gsw_graph *gr, int32_t root, const gsw_run_opts
     GSW_CUDA(cudaMemcpyAsync(levels, f.data.dg_wa, sizeof(int) * gr->n, cudaMemcpyDeviceToHost, stream()));
   GSW_CUDA(cudaStreamSynchronize(stream()));
   return eg.finish();
+}
+
+gsw_status gsw_bfs(gsw_ctx *ctx, gsw_graph *gr, int32_t root, const gsw_run_opts *o, int32_t *levels,
+                   gsw_run_stats *st) {
+  entry_guard eg(ctx);
+  if (!ctx || !gr || root < 0 || root >= gr->n) return fail(GSW_ERR_INVALID_ARG, "gsw_bfs: bad arguments");
+  return bfs_run(ctx, gr, &root, 1, o, levels, st, eg);
+}
+
+gsw_status gsw_bfs_multi(gsw_ctx *ctx, gsw_graph *gr, int nroots, const int32_t *roots, const gsw_run_opts *o,
+                         int32_t *levels, gsw_run_stats *st) {
+  entry_guard eg(ctx);
+  if (!ctx || !gr || nroots <= 0 || !roots) return fail(GSW_ERR_INVALID_ARG, "gsw_bfs_multi: bad arguments");
+  for (int i = 0; i < nroots; ++i)
+    if (roots[i] < 0 || roots[i] >= gr->n) return fail(GSW_ERR_INVALID_ARG, "gsw_bfs_multi: root out of range");
+  return bfs_run(ctx, gr, roots, nroots, o, levels, st, eg);
 }
 
 // ---------------------------------------------------------------------------

@@ -6,15 +6,21 @@
 // words of `seen`, `frontier` and `next` stored vertex-major, so one 32-byte
 // sector carries every source's state of a vertex (256 sources).  Levels are
 // level-synchronous and identical to per-source BFS.
-//   push : a warp per frontier vertex ORs (frontier & ~seen[u]) into next[u]
-//   pull : a thread per vertex with unseen bits ORs its neighbours'
-//          frontier words and stops once every unseen bit is covered
+//   push : a warp per adjacency chunk (at most 1024 edges of one vertex) ORs
+//          (frontier & ~seen[u]) into next[u]
+//   pull : a warp per chunk of a vertex with unseen bits ORs the
+//          neighbours' frontier words and stops once every unseen bit is
+//          covered
 //   update: next & ~seen becomes the new frontier, levels are written for
-//          the new bits, and the counters that pick the next direction
+//          the new bits (vertex-major, so one vertex's writes share its row
+//          of nsrc entries; one tiled transpose gives the source-major
+//          result at the end), and the counters that pick the next direction
 //          (frontier edges vs. unexplored edges, Beamer's alpha = 14) are
 //          reduced.
 #pragma once
 #include <vector>
+
+#include <cub/cub.cuh>
 
 #include "engine/executor.cuh"
 
@@ -35,24 +41,46 @@ struct mbfs_counters {
   unsigned long long reached_e;   // sum over vertices of deg * popcount(seen)
 };
 
+// Adjacency lists cut into pieces of at most MBFS_CHUNK edges, so a hub's
+// edges spread over many warps instead of serialising one.
+constexpr int64_t MBFS_CHUNK = 1024;
+
+__global__ void k_mbfs_chunk_count(const int64_t *off, int64_t n, int64_t *cnt) {
+  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t d = off[v + 1] - off[v];
+    cnt[v] = d == 0 ? 0 : (d + MBFS_CHUNK - 1) / MBFS_CHUNK;
+  }
+}
+__global__ void k_mbfs_chunk_fill(const int64_t *off, int64_t n, const int64_t *coff, int *cv, int64_t *cbeg) {
+  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x)
+    for (int64_t i = coff[v], b = off[v]; i < coff[v + 1]; ++i, b += MBFS_CHUNK) {
+      cv[i] = (int)v;
+      cbeg[i] = b;
+    }
+}
+
+// push, warp per chunk: the chunk's vertex's frontier bits go to every
+// neighbour that has not seen them
 template <int W>
-__global__ void __launch_bounds__(256) k_mbfs_push(device_graph_t<CSR, Empty> g, const uint64_t *frontier,
-                                                    const uint64_t *seen, uint64_t *next) {
-  const int64_t n = g.nvertexs;
+__global__ void __launch_bounds__(256) k_mbfs_push_chunks(device_graph_t<CSR, Empty> g, const int *cv,
+                                                           const int64_t *cbeg, int64_t nchunks,
+                                                           const uint64_t *frontier, const uint64_t *seen,
+                                                           uint64_t *next) {
   const int lane = lane_id();
   const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
-  for (int64_t v = (int64_t)blockIdx.x * (blockDim.x >> 5) + warp_id(); v < n; v += nwarps) {
+  for (int64_t c = (int64_t)blockIdx.x * (blockDim.x >> 5) + warp_id(); c < nchunks; c += nwarps) {
+    const int v = cv[c];
     uint64_t f[W];
     bool any = false;
 #pragma unroll
     for (int k = 0; k < W; ++k) {
-      f[k] = __ldg(frontier + v * W + k);
+      f[k] = __ldg(frontier + (int64_t)v * W + k);
       any |= f[k] != 0;
     }
     if (!any) continue;
-    const int64_t st = __ldg(g.dg_row_off + v), en = __ldg(g.dg_row_off + v + 1);
-    for (int64_t e = st + lane; e < en; e += 32) {
-      const int u = __ldg(g.dg_adj_list + e);
+    const int64_t b = cbeg[c], e = MIN(b + MBFS_CHUNK, __ldg(g.dg_row_off + v + 1));
+    for (int64_t i = b + lane; i < e; i += 32) {
+      const int u = __ldg(g.dg_adj_list + i);
 #pragma unroll
       for (int k = 0; k < W; ++k) {
         const uint64_t m = f[k] & ~seen[(int64_t)u * W + k];
@@ -62,34 +90,63 @@ __global__ void __launch_bounds__(256) k_mbfs_push(device_graph_t<CSR, Empty> g,
   }
 }
 
+// pull, warp per chunk: OR of the in-neighbours' frontier words over the
+// chunk, cut short once every bit the vertex still needs is covered; a vertex
+// with several chunks combines them with atomicOr
 template <int W>
-__global__ void __launch_bounds__(256) k_mbfs_pull(device_graph_t<CSR, Empty> g, const uint64_t *frontier,
-                                                    const uint64_t *seen, uint64_t *next, const uint64_t *valid) {
-  const int64_t n = g.nvertexs;
-  const int64_t STRIDE = (int64_t)blockDim.x * gridDim.x;
-  for (int64_t v = threadIdx.x + (int64_t)blockIdx.x * blockDim.x; v < n; v += STRIDE) {
+__global__ void __launch_bounds__(256) k_mbfs_pull_chunks(device_graph_t<CSR, Empty> g, const int *cv,
+                                                           const int64_t *cbeg, int64_t nchunks,
+                                                           const uint64_t *frontier, const uint64_t *seen,
+                                                           uint64_t *next, const uint64_t *valid) {
+  const int lane = lane_id();
+  const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t c = (int64_t)blockIdx.x * (blockDim.x >> 5) + warp_id(); c < nchunks; c += nwarps) {
+    const int v = cv[c];
     uint64_t need[W], acc[W];
     bool any = false;
 #pragma unroll
     for (int k = 0; k < W; ++k) {
-      need[k] = valid[k] & ~seen[v * W + k];
+      need[k] = valid[k] & ~seen[(int64_t)v * W + k];
       acc[k] = 0;
       any |= need[k] != 0;
     }
     if (!any) continue;
     const int64_t st = __ldg(g.dgr_row_off + v), en = __ldg(g.dgr_row_off + v + 1);
-    for (int64_t e = st; e < en; ++e) {
-      const int u = __ldg(g.dgr_adj_list + e);
-      bool done = true;
+    const int64_t b = cbeg[c], e = MIN(b + MBFS_CHUNK, en);
+    for (int64_t base = b; base < e; base += 32) {
+      const int64_t i = base + lane;
+      if (i < e) {
+        const int u = __ldg(g.dgr_adj_list + i);
+#pragma unroll
+        for (int k = 0; k < W; ++k) acc[k] |= __ldg(frontier + (int64_t)u * W + k);
+      }
+      // every 32 edges: stop when the warp's bits cover what v needs
+      bool covered = true;
 #pragma unroll
       for (int k = 0; k < W; ++k) {
-        acc[k] |= __ldg(frontier + (int64_t)u * W + k);
-        done &= (acc[k] & need[k]) == need[k];
+        const unsigned lo = __reduce_or_sync(FULL, (unsigned)acc[k]);
+        const unsigned hi = __reduce_or_sync(FULL, (unsigned)(acc[k] >> 32));
+        covered &= ((((uint64_t)hi << 32) | lo) & need[k]) == need[k];
       }
-      if (done) break;
+      if (covered) break;
     }
 #pragma unroll
-    for (int k = 0; k < W; ++k) next[v * W + k] = acc[k] & need[k];
+    for (int k = 0; k < W; ++k) {
+      const unsigned lo = __reduce_or_sync(FULL, (unsigned)acc[k]);
+      const unsigned hi = __reduce_or_sync(FULL, (unsigned)(acc[k] >> 32));
+      acc[k] = (((uint64_t)hi << 32) | lo) & need[k];
+    }
+    if (lane < W) {
+      uint64_t mine = 0;
+#pragma unroll
+      for (int k = 0; k < W; ++k)
+        if (k == lane) mine = acc[k];
+      uint64_t *dst = next + (int64_t)v * W + lane;
+      if (e - b == en - st)
+        *dst = mine;  // the only chunk of v
+      else if (mine)
+        atomicOr((unsigned long long *)dst, (unsigned long long)mine);
+    }
   }
 }
 
@@ -118,7 +175,7 @@ __global__ void __launch_bounds__(256) k_mbfs_update(device_graph_t<CSR, Empty> 
           const int bit = __ffsll((long long)b) - 1;
           b &= b - 1;
           const int src = k * 64 + bit;
-          if (src < nsrc) levels[(int64_t)src * n + v] = level;
+          if (src < nsrc) levels[v * nsrc + src] = level;  // vertex-major while running
         }
       }
       unseen |= (valid[k] & ~(s | nb)) != 0;
@@ -143,7 +200,7 @@ __global__ void k_mbfs_seed(uint64_t *frontier, uint64_t *seen, const int *roots
     const int64_t r = roots[s];
     atomicOr((unsigned long long *)(frontier + r * W + (s >> 6)), 1ull << (s & 63));
     atomicOr((unsigned long long *)(seen + r * W + (s >> 6)), 1ull << (s & 63));
-    levels[(int64_t)s * n + r] = 0;
+    levels[r * nsrc + s] = 0;
   }
 }
 
@@ -162,6 +219,30 @@ __global__ void __launch_bounds__(256) k_mbfs_reached(device_graph_t<CSR, Empty>
   if (threadIdx.x == 0 && s) atomicAdd(&cnt->reached_e, s);
 }
 
+// vertex-major [n][nsrc] -> source-major [nsrc][n] through 32 x 32 tiles
+__global__ void __launch_bounds__(256) k_mbfs_transpose(const int *vm, int64_t n, int nsrc, int *sm) {
+  __shared__ int tile[32][33];
+  const int64_t vt = (n + 31) / 32, st = (nsrc + 31) / 32;
+  for (int64_t t = blockIdx.x; t < vt * st; t += gridDim.x) {
+    const int64_t v0 = (t / st) * 32;
+    const int s0 = (int)(t % st) * 32;
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+      const int64_t v = v0 + r;
+      const int s = s0 + threadIdx.x;
+      tile[r][threadIdx.x] = (v < n && s < nsrc) ? vm[v * nsrc + s] : 0;
+    }
+    __syncthreads();
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+      const int s = s0 + r;
+      const int64_t v = v0 + threadIdx.x;
+      if (v < n && s < nsrc) sm[(int64_t)s * n + v] = tile[threadIdx.x][r];
+    }
+    __syncthreads();
+  }
+}
+
+inline int grid_for_n(int64_t n) { return (int)MIN((n + 255) / 256 + 1, (int64_t)sm_count() * 16); }
+
 template <typename T>
 __global__ void k_mbfs_fill(T *p, T v, int64_t n) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) p[i] = v;
@@ -175,12 +256,32 @@ mbfs_result mbfs_impl(device_graph_t<CSR, Empty> g, int nsrc, const int32_t *roo
   uint64_t *frontier = (uint64_t *)buf("mb_front", sizeof(uint64_t) * n * W);
   uint64_t *seen = (uint64_t *)buf("mb_seen", sizeof(uint64_t) * n * W);
   uint64_t *next = (uint64_t *)buf("mb_next", sizeof(uint64_t) * n * W);
-  int *levels = (int *)buf("mb_levels", sizeof(int) * (size_t)n * nsrc);
+  int *levels = (int *)buf("mb_levels_vm", sizeof(int) * (size_t)n * nsrc);  // vertex-major, while running
+  int *levels_sm = (int *)buf("mb_levels", sizeof(int) * (size_t)n * nsrc);   // source-major result
   int *roots = (int *)buf("mb_roots", sizeof(int) * nsrc);
   uint64_t *valid = (uint64_t *)buf("mb_valid", sizeof(uint64_t) * W);
   mbfs_counters *cnt = (mbfs_counters *)buf("mb_cnt", sizeof(mbfs_counters));
   mbfs_counters *hcnt = nullptr;
-  if (!frontier || !seen || !next || !levels || !roots || !valid || !cnt) return res;
+  if (!frontier || !seen || !next || !levels || !levels_sm || !roots || !valid || !cnt) return res;
+  // the chunk list of the adjacency lists (the graph is undirected, so it
+  // serves pushes and pulls alike)
+  int64_t *ccnt = (int64_t *)buf("mb_ccnt", sizeof(int64_t) * (n + 1));
+  int64_t *coff = (int64_t *)buf("mb_coff", sizeof(int64_t) * (n + 1));
+  if (!ccnt || !coff) return res;
+  GSW_CUDA(cudaMemsetAsync(ccnt + n, 0, sizeof(int64_t), stream()));
+  k_mbfs_chunk_count<<<grid_for_n(n), 256, 0, stream()>>>(g.dg_row_off, n, ccnt);
+  size_t tb = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, tb, ccnt, coff, n + 1, stream());
+  void *tmp = buf("mb_scan_tmp", tb);
+  if (!tmp) return res;
+  GSW_CUDA(cub::DeviceScan::ExclusiveSum(tmp, tb, ccnt, coff, n + 1, stream()));
+  int64_t nchunks = 0;
+  GSW_CUDA(cudaMemcpyAsync(&nchunks, coff + n, sizeof(int64_t), cudaMemcpyDeviceToHost, stream()));
+  GSW_CUDA(cudaStreamSynchronize(stream()));
+  int *cv = (int *)buf("mb_cv", sizeof(int) * (nchunks + 1));
+  int64_t *cbeg = (int64_t *)buf("mb_cbeg", sizeof(int64_t) * (nchunks + 1));
+  if (!cv || !cbeg) return res;
+  k_mbfs_chunk_fill<<<grid_for_n(n), 256, 0, stream()>>>(g.dg_row_off, n, coff, cv, cbeg);
   if (GSW_CUDA(cudaMallocHost((void **)&hcnt, sizeof(mbfs_counters)))) return res;
   uint64_t hv[W];
   for (int k = 0; k < W; ++k) {
@@ -204,9 +305,9 @@ mbfs_result mbfs_impl(device_graph_t<CSR, Empty> g, int nsrc, const int32_t *roo
   bool push = true;
   for (int level = 1; level <= n + 1 && ok(); ++level) {
     if (push)
-      k_mbfs_push<W><<<grid, 256, 0, s>>>(g, frontier, seen, next);
+      k_mbfs_push_chunks<W><<<grid, 256, 0, s>>>(g, cv, cbeg, nchunks, frontier, seen, next);
     else
-      k_mbfs_pull<W><<<grid, 256, 0, s>>>(g, frontier, seen, next, valid);
+      k_mbfs_pull_chunks<W><<<grid, 256, 0, s>>>(g, cv, cbeg, nchunks, frontier, seen, next, valid);
     GSW_CUDA(cudaMemsetAsync(cnt, 0, sizeof(mbfs_counters), s));
     k_mbfs_update<W><<<grid, 256, 0, s>>>(g, frontier, seen, next, levels, nsrc, level, valid, cnt);
     GSW_CUDA(cudaMemcpyAsync(hcnt, cnt, sizeof(mbfs_counters), cudaMemcpyDeviceToHost, s));
@@ -216,6 +317,7 @@ mbfs_result mbfs_impl(device_graph_t<CSR, Empty> g, int nsrc, const int32_t *roo
     // Beamer's direction test with alpha = 14
     push = hcnt->active_e * 14 < hcnt->unseen_e;
   }
+  k_mbfs_transpose<<<sm_count() * 8, dim3(32, 8), 0, s>>>(levels, n, nsrc, levels_sm);
   cudaEventRecord(e1, s);
   cudaEventSynchronize(e1);
   float ms = 0;
@@ -227,7 +329,7 @@ mbfs_result mbfs_impl(device_graph_t<CSR, Empty> g, int nsrc, const int32_t *roo
   GSW_CUDA(cudaStreamSynchronize(s));
   res.edges = (int64_t)(hcnt->reached_e / 2);
   if (levels_host && ok())
-    GSW_CUDA(cudaMemcpyAsync(levels_host, levels, sizeof(int) * (size_t)n * nsrc, cudaMemcpyDeviceToHost, s));
+    GSW_CUDA(cudaMemcpyAsync(levels_host, levels_sm, sizeof(int) * (size_t)n * nsrc, cudaMemcpyDeviceToHost, s));
   GSW_CUDA(cudaStreamSynchronize(s));
   cudaFreeHost(hcnt);
   cudaEventDestroy(e0);

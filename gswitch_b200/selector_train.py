@@ -3,7 +3,8 @@ from timing every variant, training on the GPU with the library's own
 kernels, and the regret of the network and of the rule-based selector
 against the exhaustively timed best variant on held-out graphs.
 
-Corpus (one seed per graph): RMAT with 2^14..2^20 vertices (log-uniform),
+Corpus (one seed per graph): RMAT with 2^14..2^20 vertices (log-uniform;
+--big adds graphs with 2^21..2^23),
 edge factor 16, a in [0.45, 0.65], d = 0.05, b = c = (1 - a - d) / 2;
 Erdos-Renyi G(n, m) with n in 2^14..2^20 and mean degree in [4, 32]; square
 2D grids with 1% long-range edges, side 64..1024; power-law configuration
@@ -31,8 +32,9 @@ KINDS = ("rmat", "er", "grid", "powerlaw")
 APPS = ((gs.APP_BFS, "bfs"), (gs.APP_SSSP, "sssp"), (gs.APP_PR, "pr"))
 
 
-def corpus(count: int, seed: int):
-    """`count` graph specifications drawn from one seed."""
+def corpus(count: int, seed: int, lg_min: int = 14, lg_max: int = 20):
+    """`count` graph specifications drawn from one seed, with 2^lg_min ..
+    2^lg_max vertices."""
     rng = np.random.default_rng(seed)
     out = []
     for i in range(count):
@@ -41,16 +43,17 @@ def corpus(count: int, seed: int):
         if kind == "rmat":
             a = float(rng.uniform(0.45, 0.65))
             bc = (1.0 - a - 0.05) / 2
-            out.append({"kind": kind, "scale": int(rng.integers(14, 21)), "a": a, "b": bc, "c": bc, "seed": gseed})
+            out.append({"kind": kind, "scale": int(rng.integers(lg_min, lg_max + 1)), "a": a, "b": bc, "c": bc,
+                        "seed": gseed})
         elif kind == "er":
-            n = int(2 ** rng.uniform(14, 20))
+            n = int(2 ** rng.uniform(lg_min, lg_max))
             deg = float(rng.uniform(4, 32))
             out.append({"kind": kind, "n": n, "m_pairs": int(n * deg / 2), "seed": gseed})
         elif kind == "grid":
-            side = int(2 ** rng.uniform(6, 10))
+            side = int(2 ** rng.uniform(lg_min / 2 - 1, lg_max / 2))
             out.append({"kind": kind, "side": side, "seed": gseed})
         else:
-            out.append({"kind": kind, "n": int(2 ** rng.uniform(14, 20)), "gamma": float(rng.uniform(1.8, 3.0)),
+            out.append({"kind": kind, "n": int(2 ** rng.uniform(lg_min, lg_max)), "gamma": float(rng.uniform(1.8, 3.0)),
                         "seed": gseed})
     return out
 
@@ -120,15 +123,33 @@ def main(argv=None):
     ap.add_argument("--out", default=os.path.join(os.path.dirname(os.path.abspath(__file__)), "models",
                                                   "selector_mlp.json"))
     ap.add_argument("--save-labels", default=None)
+    ap.add_argument("--labels-in", default=None, help="start from labels saved by an earlier run")
+    ap.add_argument("--big", type=int, default=0, help="extra graphs with 2^21..2^23 vertices")
+    ap.add_argument("--big-test", type=int, default=0)
+    ap.add_argument("--big-budget-s", type=float, default=600.0)
     args = ap.parse_args(argv)
     log = lambda m: print(m, file=sys.stderr, flush=True)
     ctx = gs.Context(0)
-    train_specs = corpus(args.train, args.seed)
-    test_specs = corpus(args.test, args.seed + 1)
     t0 = time.time()
-    Xtr, Ttr, Rtr, Gtr, Atr, ntr = label_corpus(ctx, train_specs, args.budget_s, log)
+    if args.labels_in:
+        d = np.load(args.labels_in)
+        Xtr, Ttr, Rtr, Gtr, Atr = d["Xtr"], d["Ttr"], d["Rtr"], d["Gtr"], d["Atr"]
+        Xte, Tte, Rte, Gte, Ate = d["Xte"], d["Tte"], d["Rte"], d["Gte"], d["Ate"]
+        ntr, nte = int(Gtr.max()) + 1 if len(Gtr) else 0, int(Gte.max()) + 1 if len(Gte) else 0
+    else:
+        Xtr, Ttr, Rtr, Gtr, Atr, ntr = label_corpus(ctx, corpus(args.train, args.seed), args.budget_s, log)
+        Xte, Tte, Rte, Gte, Ate, nte = label_corpus(ctx, corpus(args.test, args.seed + 1), args.budget_s / 4, log)
+    if args.big:
+        parts = label_corpus(ctx, corpus(args.big, args.seed + 2, 21, 23), args.big_budget_s, log)
+        Xtr, Ttr, Rtr, Atr = (np.concatenate([a, b]) for a, b in zip((Xtr, Ttr, Rtr, Atr), parts[:2] + parts[2:3] + parts[4:5]))
+        Gtr = np.concatenate([Gtr, parts[3] + ntr])
+        ntr += parts[5]
+    if args.big_test:
+        parts = label_corpus(ctx, corpus(args.big_test, args.seed + 3, 21, 23), args.big_budget_s / 4, log)
+        Xte, Tte, Rte, Ate = (np.concatenate([a, b]) for a, b in zip((Xte, Tte, Rte, Ate), parts[:2] + parts[2:3] + parts[4:5]))
+        Gte = np.concatenate([Gte, parts[3] + nte])
+        nte += parts[5]
     t_lab = time.time() - t0
-    Xte, Tte, Rte, Gte, Ate, nte = label_corpus(ctx, test_specs, args.budget_s / 4, log)
     log(f"labels: train {len(Xtr)} rows / {ntr} graphs, test {len(Xte)} rows / {nte} graphs")
     if args.save_labels:
         np.savez_compressed(args.save_labels, Xtr=Xtr, Ttr=Ttr, Rtr=Rtr, Gtr=Gtr, Atr=Atr, Xte=Xte, Tte=Tte,

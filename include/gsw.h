@@ -67,6 +67,15 @@ gsw_status gsw_graph_generate_grid(gsw_ctx *ctx, int rows, int cols, int lr_div,
                                    uint64_t wseed, gsw_graph **out);
 gsw_status gsw_graph_generate_er(gsw_ctx *ctx, int64_t n, int64_t m_pairs, uint64_t seed, int wmax, uint64_t wseed,
                                  gsw_graph **out);
+/* No counterpart in the reference.  A batch of `count` G(n, m) graphs as one
+ * disjoint union (config C4): instance i has n_i log-uniform in [nlo, nhi],
+ * mean degree uniform in [dlo, dhi] and m_i = floor(n_i * degree / 2) pairs,
+ * drawn from its own seed exactly as gsw_graph_generate_er draws a single
+ * graph; it owns vertices [vertex_offsets[i], vertex_offsets[i + 1])
+ * (vertex_offsets: count + 1 entries, may be NULL). */
+gsw_status gsw_graph_generate_er_batch(gsw_ctx *ctx, int count, uint64_t seed, int64_t nlo, int64_t nhi, double dlo,
+                                       double dhi, int wmax, uint64_t wseed, int64_t *vertex_offsets,
+                                       gsw_graph **out);
 /* No counterpart in the reference (its corpus is downloaded graphs).
  * Undirected configuration-model graph for the selector corpus: vertex
  * degrees drawn from a power law P(d) ~ d^-gamma (d >= 1, capped at
@@ -162,6 +171,11 @@ typedef struct gsw_run_stats {
  *   MBFS application/mbfs.cu:16-246    levels per source (row-major)  */
 gsw_status gsw_bfs(gsw_ctx *ctx, gsw_graph *g, int32_t root, const gsw_run_opts *o, int32_t *levels,
                    gsw_run_stats *st);
+/* BFS from several roots at once: levels are distances to the nearest root.
+ * Over a disjoint union of graphs with one root per part this runs every
+ * part's BFS in one level loop (the batched form of config C4). */
+gsw_status gsw_bfs_multi(gsw_ctx *ctx, gsw_graph *g, int nroots, const int32_t *roots, const gsw_run_opts *o,
+                         int32_t *levels, gsw_run_stats *st);
 gsw_status gsw_sssp(gsw_ctx *ctx, gsw_graph *g, int32_t root, const gsw_run_opts *o, int32_t *dist,
                     gsw_run_stats *st);
 gsw_status gsw_cc(gsw_ctx *ctx, gsw_graph *g, const gsw_run_opts *o, int32_t *labels, gsw_run_stats *st);

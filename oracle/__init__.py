@@ -150,6 +150,16 @@ def er_batch_params(seed, i, nlo=1000, nhi=200000, dlo=4.0, dhi=32.0):
     return n.value, m.value, s.value
 
 
+def er_batch(seed, count, nlo=1000, nhi=200000, dlo=4.0, dhi=32.0):
+    """The instances of a G(n, m) batch, each built on its own (the device
+    builds them as one disjoint union)."""
+    out = []
+    for i in range(count):
+        n, m, s = er_batch_params(seed, i, nlo, nhi, dlo, dhi)
+        out.append(er(n, m, s))
+    return out
+
+
 def roots(g: Csr, seed: int, count: int):
     r = np.empty(count, dtype=np.int32)
     lib().or_roots(seed, g.n, g.off, count, r)

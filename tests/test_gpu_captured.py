@@ -111,3 +111,52 @@ def test_captured_rejected_where_unsupported(ctx, graphs):
     with pytest.raises(gs.GswError) as e:
         g.sssp(root, cap())
     assert gs.STATUS[e.value.code] == "UNSUPPORTED"
+
+
+# ---------------------------------------------------------------------------
+# batched instances: a batch of G(n, m) graphs as one disjoint union, every
+# instance's BFS in one level loop (host-driven, captured) and CC over all
+# ---------------------------------------------------------------------------
+@pytest.fixture(scope="module")
+def er_batch(ctx):
+    g, voff = ctx.er_batch(48, seed=21, nlo=500, nhi=20000, dlo=4.0, dhi=32.0)
+    parts = oracle.er_batch(21, 48, nlo=500, nhi=20000, dlo=4.0, dhi=32.0)
+    yield g, voff, parts
+    g.close()
+
+
+def test_er_batch_union_matches_instances(er_batch):
+    g, voff, parts = er_batch
+    off, col, _ = g.download()
+    assert len(voff) == len(parts) + 1 and voff[-1] == g.n
+    for i, h in enumerate(parts):
+        a, b = voff[i], voff[i + 1]
+        assert b - a == h.n
+        seg = off[a:b + 1] - off[a]
+        assert np.array_equal(seg, h.off), i
+        assert np.array_equal(col[off[a]:off[b]] - a, h.col), i
+
+
+@pytest.mark.parametrize("opts", [dict(), dict(selector="mlp"), dict(captured=True), dict(persistent=False),
+                                  dict(fusion=1)])
+def test_er_batch_bfs_every_instance_in_one_loop(ctx, er_batch, opts):
+    g, voff, parts = er_batch
+    if opts.get("selector") == "mlp":
+        from gswitch_b200.selector_train import load_model
+        model, conf = load_model()
+        ctx.mlp_load(model, conf)
+    roots = [int(voff[i] + oracle.roots(h, 5 + i, 1)[0]) for i, h in enumerate(parts)]
+    lv, st = g.bfs_multi(roots, gs.RunOpts(**opts))
+    for i, h in enumerate(parts):
+        ref = oracle.bfs(h, roots[i] - int(voff[i]))
+        assert np.array_equal(lv[voff[i]:voff[i + 1]], ref), (i, opts)
+    assert st.edges == sum(oracle.traversed_edges(h, oracle.bfs(h, roots[i] - int(voff[i])))
+                           for i, h in enumerate(parts))
+    ctx.mlp_load(None)
+
+
+def test_er_batch_cc_labels_per_instance(er_batch):
+    g, voff, parts = er_batch
+    lab, _ = g.cc()
+    for i, h in enumerate(parts):
+        assert np.array_equal(lab[voff[i]:voff[i + 1]] - voff[i], oracle.cc(h)), i
