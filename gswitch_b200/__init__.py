@@ -38,7 +38,7 @@ ABI_SYMBOLS = (
     "gsw_graph_destroy", "gsw_graph_roots", "gsw_ctx_stream", "gsw_run_opts_default", "gsw_bfs", "gsw_sssp", "gsw_cc",
     "gsw_pagerank", "gsw_bc", "gsw_gc", "gsw_mbfs", "gsw_bfs_strict_noalloc",
     "gsw_graph_generate_powerlaw", "gsw_label_levels", "gsw_mlp_train", "gsw_mlp_grad", "gsw_mlp_infer",
-    "gsw_mlp_load", "gsw_graph_generate_er_batch", "gsw_bfs_multi",
+    "gsw_mlp_load", "gsw_graph_generate_er_batch", "gsw_bfs_multi", "gsw_bfs_inspect",
 )
 
 # learned selector (include/gsw.h): 8 features -> 32 -> 32 -> 20 classes
@@ -123,6 +123,7 @@ def lib():
     L.gsw_graph_generate_er_batch.argtypes = [vp, C.c_int, u64, i64, i64, C.c_double, C.c_double, C.c_int, u64, vp,
                                               pvp]
     L.gsw_bfs_multi.argtypes = [vp, vp, C.c_int, vp, po, vp, ps]
+    L.gsw_bfs_inspect.argtypes = [vp, vp, vp, i32, vp]
     _LIB = L
     return L
 
@@ -366,6 +367,13 @@ class Graph:
         lv = np.empty(self.n, dtype=np.int32) if out else None
         st = self._run(lib().gsw_bfs, C.c_int32(root), outs=[lv], opts=opts)
         return lv, st
+
+    def bfs_inspect(self, levels, level):
+        """The inspector's six counters for a BFS state (gsw_bfs_inspect)."""
+        lv = np.ascontiguousarray(levels, dtype=np.int32)
+        out = np.zeros(6, dtype=np.uint64)
+        _check(lib().gsw_bfs_inspect(self.ctx._h, self._h, _ptr(lv), level, _ptr(out)))
+        return out
 
     def bfs_multi(self, roots, opts=None, out=True):
         """BFS from all `roots` at once (distance to the nearest root)."""

@@ -23,93 +23,124 @@ namespace gsw {
 // max-degree counters.
 constexpr int INSPECT_VTHREADS = 256 * 512;  // the reference's grid, one virtual thread each
 constexpr int INSPECT_VBLOCK = 512;          // virtual threads per virtual block
-constexpr int INSPECT_VPB = 128;             // virtual threads per physical block
-constexpr int INSPECT_HALVES = 2;            // physical threads per virtual thread
-constexpr int INSPECT_THREADS = INSPECT_VPB * INSPECT_HALVES;
-constexpr int INSPECT_CTAS = INSPECT_VTHREADS / INSPECT_VPB;
-constexpr int INSPECT_UNROLL = 4;
+constexpr int INSPECT_SPAN = 4;              // consecutive vertices a physical thread takes per step
+constexpr int INSPECT_OWNERS = INSPECT_VBLOCK / INSPECT_SPAN;  // 128 threads own one virtual block
+constexpr int INSPECT_HALVES = 4;            // physical threads sharing those virtual threads
+constexpr int INSPECT_THREADS = INSPECT_OWNERS * INSPECT_HALVES;
+constexpr int INSPECT_CTAS = INSPECT_VTHREADS / INSPECT_VBLOCK;  // one CTA per virtual block
+constexpr int INSPECT_UNROLL = 2;
 static_assert(STAT_SLOTS == 8 + 2 * (INSPECT_VTHREADS / INSPECT_VBLOCK), "statistics block layout");
 constexpr int EC_INSPECT_CTAS = 256;
 constexpr int EC_INSPECT_THREADS = 512;
 
 // Virtual thread t (0 <= t < 131072) visits vertices t, t + 131072, ...
 // exactly as thread t of the reference's 256 x 512 grid-stride launch, so the
-// max-degree counters are the reference's.  Two physical threads share one
-// virtual thread (even / odd steps of its sequence) and merge their maxima
-// in shared memory; a physical block holds 128 virtual threads (a quarter
-// virtual block), each thread keeps four vertices in flight, vertex counts
-// are taken per warp from the ballots, and the last block to finish folds the
-// per-virtual-block sums (max over blocks for push, sum for pull).
+// max-degree counters are the reference's.  Vertex 4q + i + k * 131072 (i < 4)
+// always belongs to virtual thread 4q + i, so a physical thread owns the
+// four virtual threads 4q .. 4q+3 and reads four consecutive vertices per
+// step (a warp covers 128 consecutive vertices: four bitmap words, built
+// with shuffles), and the 128 owners 4q .. 4q+3 of one CTA are exactly one
+// virtual block of the reference.  Four quarters of the CTA take turns at the
+// steps and merge their maxima in shared memory; the last CTA to finish
+// folds the per-virtual-block sums (max over blocks for push, sum for pull).
 template <typename G, typename F>
-__global__ void __launch_bounds__(INSPECT_THREADS, 7) k_inspect_vc(active_set_t as, G g, F f,
-                                                                 unsigned long long *info,
-                                                                 const int *skip_if = nullptr) {
+__global__ void __launch_bounds__(INSPECT_THREADS, 2) k_inspect_vc(active_set_t as, G g, F f, unsigned long long *info,
+                                                               const int *skip_if = nullptr) {
   // captured loops: a level whose expand found an empty input ends the loop
   // before this inspection (the host loop stops there too)
   if (skip_if && *(volatile const int *)skip_if) return;
   __shared__ unsigned long long s_red[32];
-  __shared__ unsigned s_mp[INSPECT_VPB], s_ml[INSPECT_VPB];
+  __shared__ unsigned s_mp[INSPECT_OWNERS][INSPECT_SPAN], s_ml[INSPECT_OWNERS][INSPECT_SPAN];
   __shared__ bool s_last;
-  const int S = INSPECT_VTHREADS;
-  const int half = threadIdx.x / INSPECT_VPB;
-  const int vt_local = threadIdx.x % INSPECT_VPB;
-  const int t = blockIdx.x * INSPECT_VPB + vt_local;
-  const int lane = lane_id();
-  const int n = (int)as.size;
-  unsigned active_num = 0, inactive_num = 0;  // per warp, kept by lane 0
-  unsigned long long push_wl = 0, pull_wl = 0;
-  unsigned max_push = 0, max_pull = 0;
-  const long long step = (long long)INSPECT_HALVES * S;
-  for (long long base = t + (long long)half * S; base - lane < n; base += INSPECT_UNROLL * step) {
-    Status st[INSPECT_UNROLL];
-    int od[INSPECT_UNROLL];
-#pragma unroll
-    for (int k = 0; k < INSPECT_UNROLL; ++k) {
-      const long long idx = base + k * step;
-      od[k] = idx < n ? __ldg(g.dg_odegree + idx) : 0;
-    }
-#pragma unroll
-    for (int k = 0; k < INSPECT_UNROLL; ++k) {
-      const long long idx = base + k * step;
-      st[k] = idx < n ? f.filter((int)idx, g) : Inactive;
-    }
-#pragma unroll
-    for (int k = 0; k < INSPECT_UNROLL; ++k) {
-      const long long idx = base + k * step;
-      const long long wbase = idx - lane;
-      if (wbase >= n) break;  // warp-uniform
-      const bool valid = idx < n;
-      const bool tag_active = valid && st[k] == Active;
-      const bool tag_inactive = valid && st[k] != Inactive;  // 0 only for Inactive
-      const unsigned aw = __ballot_sync(FULL, tag_active);
-      const unsigned iw = __ballot_sync(FULL, tag_inactive);
-      if (lane == 0) {
-        as.bitmap.active.dg_bits[wbase >> 5] = aw;
-        as.bitmap.inactive.dg_bits[wbase >> 5] = iw;
-        const long long rem = n - wbase;
-        const unsigned nvalid = rem >= 32 ? 32u : (unsigned)rem;
-        active_num += __popc(aw);
-        inactive_num += nvalid - __popc(iw);
-      }
-      const unsigned oa = tag_active ? (unsigned)od[k] : 0u;
-      const unsigned oi = (valid && !tag_inactive) ? (unsigned)od[k] : 0u;
-      push_wl += oa;
-      pull_wl += oi;
-      max_push = max_push > oa ? max_push : oa;
-      max_pull = max_pull > oi ? max_pull : oi;
-    }
-  }
-  // merge the two halves of every virtual thread
-  if (half == 1) {
-    s_mp[vt_local] = max_push;
-    s_ml[vt_local] = max_pull;
+  for (int i = threadIdx.x; i < INSPECT_OWNERS * INSPECT_SPAN; i += blockDim.x) {
+    (&s_mp[0][0])[i] = 0;
+    (&s_ml[0][0])[i] = 0;
   }
   __syncthreads();
-  unsigned long long vmp = 0, vml = 0;
-  if (half == 0) {
-    vmp = MAX(max_push, s_mp[vt_local]);
-    vml = MAX(max_pull, s_ml[vt_local]);
+  constexpr long long S = INSPECT_VTHREADS;
+  const int half = threadIdx.x / INSPECT_OWNERS;
+  const int q_local = threadIdx.x % INSPECT_OWNERS;
+  const long long first = 4ll * (blockIdx.x * INSPECT_OWNERS + q_local);  // virtual threads first .. first+3
+  const int lane = lane_id();
+  const long long n = as.size;
+  unsigned active_num = 0, inactive_num = 0;
+  unsigned long long push_wl = 0, pull_wl = 0;
+  unsigned mp[INSPECT_SPAN] = {0, 0, 0, 0}, ml[INSPECT_SPAN] = {0, 0, 0, 0};
+  const long long step = INSPECT_HALVES * S;
+  // the warp's first vertex is first - 4 * lane: a multiple of 128
+  for (long long base = first + half * S; base - 4ll * lane < n; base += INSPECT_UNROLL * step) {
+    int od[INSPECT_UNROLL][INSPECT_SPAN];
+    Status st[INSPECT_UNROLL][INSPECT_SPAN];
+#pragma unroll
+    for (int u = 0; u < INSPECT_UNROLL; ++u) {
+      const long long v = base + u * step;  // a multiple of 4: 16-byte aligned
+      if (v + 3 < n) {
+        const int4 d4 = __ldg(reinterpret_cast<const int4 *>(g.dg_odegree + v));
+        od[u][0] = d4.x, od[u][1] = d4.y, od[u][2] = d4.z, od[u][3] = d4.w;
+      } else {
+#pragma unroll
+        for (int i = 0; i < INSPECT_SPAN; ++i) od[u][i] = v + i < n ? __ldg(g.dg_odegree + v + i) : 0;
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < INSPECT_UNROLL; ++u)
+#pragma unroll
+      for (int i = 0; i < INSPECT_SPAN; ++i) {
+        const long long v = base + u * step + i;
+        st[u][i] = v < n ? f.filter((int)v, g) : Inactive;
+      }
+#pragma unroll
+    for (int u = 0; u < INSPECT_UNROLL; ++u) {
+      const long long v0 = base + u * step;
+      if (v0 - 4ll * lane >= n) break;  // warp-uniform
+      unsigned na = 0, ni = 0, nvalid = 0;
+#pragma unroll
+      for (int i = 0; i < INSPECT_SPAN; ++i) {
+        const bool valid = v0 + i < n;
+        const bool tag_active = valid && st[u][i] == Active;
+        const bool tag_inactive = valid && st[u][i] != Inactive;  // 0 only for Inactive
+        na |= (unsigned)tag_active << i;
+        ni |= (unsigned)tag_inactive << i;
+        nvalid += valid;
+        const unsigned oa = tag_active ? (unsigned)od[u][i] : 0u;
+        const unsigned oi = (valid && !tag_inactive) ? (unsigned)od[u][i] : 0u;
+        push_wl += oa;
+        pull_wl += oi;
+        mp[i] = mp[i] > oa ? mp[i] : oa;
+        ml[i] = ml[i] > oi ? ml[i] : oi;
+      }
+      active_num += __popc(na);
+      inactive_num += nvalid - __popc(ni);
+      // lanes 8j .. 8j+7 hold the 32 vertices of bitmap word j of the warp
+      unsigned wa = na << (4 * (lane & 7)), wi = ni << (4 * (lane & 7));
+#pragma unroll
+      for (int d = 1; d < 8; d <<= 1) {
+        wa |= __shfl_xor_sync(FULL, wa, d);
+        wi |= __shfl_xor_sync(FULL, wi, d);
+      }
+      if ((lane & 7) == 0 && v0 < n) {
+        as.bitmap.active.dg_bits[v0 >> 5] = wa;
+        as.bitmap.inactive.dg_bits[v0 >> 5] = wi;
+      }
+    }
   }
+  // merge the halves of every virtual thread
+  for (int h = 1; h < INSPECT_HALVES; ++h) {
+    if (half == h)
+#pragma unroll
+      for (int i = 0; i < INSPECT_SPAN; ++i) {
+        s_mp[q_local][i] = MAX(s_mp[q_local][i], mp[i]);
+        s_ml[q_local][i] = MAX(s_ml[q_local][i], ml[i]);
+      }
+    __syncthreads();
+  }
+  unsigned long long vmp = 0, vml = 0;  // sums over this thread's four virtual threads
+  if (half == 0)
+#pragma unroll
+    for (int i = 0; i < INSPECT_SPAN; ++i) {
+      vmp += MAX(mp[i], s_mp[q_local][i]);
+      vml += MAX(ml[i], s_ml[q_local][i]);
+    }
   unsigned long long r;
   r = block_reduce((unsigned long long)active_num, s_red);
   if (threadIdx.x == 0 && r) atomicAdd(info + 0, r);
@@ -119,7 +150,7 @@ __global__ void __launch_bounds__(INSPECT_THREADS, 7) k_inspect_vc(active_set_t 
   if (threadIdx.x == 0 && r) atomicAdd(info + 2, r);
   r = block_reduce(pull_wl, s_red);
   if (threadIdx.x == 0 && r) atomicAdd(info + 3, r);
-  const int vb = t / INSPECT_VBLOCK;
+  const int vb = blockIdx.x;  // this CTA's virtual block
   const int NVB = INSPECT_VTHREADS / INSPECT_VBLOCK;
   r = block_reduce(vmp, s_red);
   if (threadIdx.x == 0 && r) atomicAdd(info + 8 + vb, r);
@@ -132,16 +163,16 @@ __global__ void __launch_bounds__(INSPECT_THREADS, 7) k_inspect_vc(active_set_t 
   __syncthreads();
   if (s_last) {  // last block: fold the virtual-block sums
     __threadfence();
-    unsigned long long mp = 0, sp = 0;
+    unsigned long long mpx = 0, sp = 0;
     for (int i = threadIdx.x; i < NVB; i += blockDim.x) {
       const unsigned long long a = ((volatile unsigned long long *)info)[8 + i];
-      mp = MAX(mp, a);
+      mpx = MAX(mpx, a);
       sp += ((volatile unsigned long long *)info)[8 + NVB + i];
     }
-    mp = block_reduce<unsigned long long, true>(mp, s_red);
+    mpx = block_reduce<unsigned long long, true>(mpx, s_red);
     sp = block_reduce(sp, s_red);
     if (threadIdx.x == 0) {
-      info[4] = mp;
+      info[4] = mpx;
       info[5] = sp;
     }
   }

@@ -1438,6 +1438,29 @@ gsw_status gsw_bfs(gsw_ctx *ctx, gsw_graph *gr, int32_t root, const gsw_run_opts
   return bfs_run(ctx, gr, &root, 1, o, levels, st, eg);
 }
 
+gsw_status gsw_bfs_inspect(gsw_ctx *ctx, gsw_graph *gr, const int32_t *levels, int32_t level, uint64_t *out6) {
+  entry_guard eg(ctx);
+  if (!ctx || !gr || !levels || !out6) return fail(GSW_ERR_INVALID_ARG, "gsw_bfs_inspect: bad arguments");
+  auto g = gr->view<Empty>();
+  g.level = level;
+  app::BFS f;
+  f.data.size = gr->n;
+  f.data.dg_wa = (int *)ctx->buf("wa", sizeof(int) * (gr->n + 1));
+  if (!f.data.dg_wa) return eg.finish();
+  GSW_CUDA(cudaMemcpyAsync(f.data.dg_wa, levels, sizeof(int) * gr->n, cudaMemcpyHostToDevice, stream()));
+  active_set_t *asp = ctx->aset(gr->n, Normal);
+  if (!asp) return eg.finish();
+  stat_t &stats = ctx->stats;
+  stats.build();
+  stats.clean();
+  k_inspect_vc<<<INSPECT_CTAS, INSPECT_THREADS, 0, stream()>>>(*asp, g, f, stats.dg_runtime_info);
+  GSW_LAUNCHED();
+  stats.collect(6);
+  stats.clean();
+  for (int i = 0; i < 6; ++i) out6[i] = stats.h_runtime_info[i];
+  return eg.finish();
+}
+
 gsw_status gsw_bfs_multi(gsw_ctx *ctx, gsw_graph *gr, int nroots, const int32_t *roots, const gsw_run_opts *o,
                          int32_t *levels, gsw_run_stats *st) {
   entry_guard eg(ctx);

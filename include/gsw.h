@@ -176,6 +176,11 @@ gsw_status gsw_bfs(gsw_ctx *ctx, gsw_graph *g, int32_t root, const gsw_run_opts 
  * part's BFS in one level loop (the batched form of config C4). */
 gsw_status gsw_bfs_multi(gsw_ctx *ctx, gsw_graph *g, int nroots, const int32_t *roots, const gsw_run_opts *o,
                          int32_t *levels, gsw_run_stats *st);
+/* Test hook: the six counters one inspection of the BFS state `levels` at
+ * `level` produces (src/abstraction/inspector.cuh:39-110): active and
+ * inactive vertices, their degree sums, and the reference's per-block sums
+ * of per-thread maximum degrees (max over blocks, sum over blocks). */
+gsw_status gsw_bfs_inspect(gsw_ctx *ctx, gsw_graph *g, const int32_t *levels, int32_t level, uint64_t *out6);
 gsw_status gsw_sssp(gsw_ctx *ctx, gsw_graph *g, int32_t root, const gsw_run_opts *o, int32_t *dist,
                     gsw_run_stats *st);
 gsw_status gsw_cc(gsw_ctx *ctx, gsw_graph *g, const gsw_run_opts *o, int32_t *labels, gsw_run_stats *st);

@@ -77,6 +77,7 @@ def lib():
     L.or_degree_attr.argtypes = [i64, I64P, F64P]
     L.or_traversed_edges.restype = i64
     L.or_traversed_edges.argtypes = [i64, I64P, I32P]
+    L.or_inspect_bfs.argtypes = [i64, I64P, I32P, i32, np.ctypeslib.ndpointer(np.uint64, flags="C")]
     _LIB = L
     return L
 
@@ -157,6 +158,13 @@ def er_batch(seed, count, nlo=1000, nhi=200000, dlo=4.0, dhi=32.0):
     for i in range(count):
         n, m, s = er_batch_params(seed, i, nlo, nhi, dlo, dhi)
         out.append(er(n, m, s))
+    return out
+
+
+def inspect_bfs(g: Csr, lvl, level):
+    """The inspector's six counters for a BFS state (inspector.cuh:39-110)."""
+    out = np.zeros(6, dtype=np.uint64)
+    lib().or_inspect_bfs(g.n, g.off, np.ascontiguousarray(lvl, dtype=np.int32), level, out)
     return out
 
 

@@ -638,3 +638,44 @@ int64_t or_traversed_edges(int64_t n, const int64_t *off, const int32_t *lvl) {
     if (lvl[v] >= 0) s += off[v + 1] - off[v];
   return s / 2;
 }
+
+/* The six counters of one vertex-centric inspection of a BFS state
+ * (src/abstraction/inspector.cuh:39-110): thread t of the 256 x 512 launch
+ * visits vertices t, t + 131072, ...; Active = level, Inactive = unreached;
+ * [0] active vertices, [1] inactive vertices, [2] their out-degree sum,
+ * [3] the inactive out-degree sum, [4] max over blocks of the sum of the
+ * threads' largest active degree, [5] sum over blocks of the sum of the
+ * threads' largest inactive degree.  Sums are 64-bit here (int32 in the
+ * reference). */
+void or_inspect_bfs(int64_t n, const int64_t *off, const int32_t *lvl, int32_t level, uint64_t *out) {
+  const int64_t S = 256 * 512;
+  uint64_t c[4] = {0, 0, 0, 0}, bmax = 0, bsum_l = 0;
+  for (int64_t b = 0; b < 256; ++b) {
+    uint64_t sp = 0, sl = 0;
+    for (int64_t t = b * 512; t < (b + 1) * 512; ++t) {
+      uint64_t mp = 0, ml = 0;
+      for (int64_t v = t; v < n; v += S) {
+        const uint64_t od = (uint64_t)(off[v + 1] - off[v]);
+        if (lvl[v] == level) {
+          c[0]++;
+          c[2] += od;
+          if (od > mp) mp = od;
+        } else if (lvl[v] < 0) {
+          c[1]++;
+          c[3] += od;
+          if (od > ml) ml = od;
+        }
+      }
+      sp += mp;
+      sl += ml;
+    }
+    if (sp > bmax) bmax = sp;
+    bsum_l += sl;
+  }
+  out[0] = c[0];
+  out[1] = c[1];
+  out[2] = c[2];
+  out[3] = c[3];
+  out[4] = bmax;
+  out[5] = bsum_l;
+}

@@ -90,6 +90,7 @@ void or_degree_attr(int64_t n, const int64_t *off, double *out);
 /* Graph500 traversed-edge count: (sum of degrees of reached vertices)/2 */
 int64_t or_traversed_edges(int64_t n, const int64_t *off, const int32_t *lvl);
 
+void or_inspect_bfs(int64_t n, const int64_t *off, const int32_t *lvl, int32_t level, uint64_t *out);
 #ifdef __cplusplus
 }
 #endif

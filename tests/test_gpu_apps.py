@@ -283,3 +283,31 @@ def test_twod_heavy_blocks_on_dense_tiles(ctx):
     pr, _ = g.pagerank(iters=20, eps=0.0, opts="x-x-TWOD")
     l1, _ = _pr_l1(pr, h)
     assert l1 <= 1e-6, l1
+
+
+@pytest.mark.parametrize("name", ["rmat14", "grid64", "er20k"])
+def test_inspection_counters_match_reference_definition(ctx, big, name):
+    """The six counters of one inspection, including the reference's
+    per-block sums of per-thread maximum degrees (inspector.cuh:39-110), for
+    every level of a BFS and for random states, against the oracle."""
+    h, _, root = big[name]
+    g = ctx.upload(h.off, h.col)
+    lv = oracle.bfs(h, root)
+    for level in range(0, int(lv.max()) + 2):
+        assert np.array_equal(g.bfs_inspect(lv, level), oracle.inspect_bfs(h, lv, level)), (name, level)
+    rng = np.random.default_rng(4)
+    for _ in range(3):
+        st = rng.integers(-1, 3, h.n).astype(np.int32)
+        assert np.array_equal(g.bfs_inspect(st, 1), oracle.inspect_bfs(h, st, 1))
+
+
+def test_inspection_counters_on_multi_step_sizes(ctx):
+    """Sizes where every virtual thread takes several steps (both halves of a
+    CTA, a ragged last word): RMAT 2^19 and G(n, m) with n = 700,001."""
+    for h in (oracle.rmat(19, 8, seed=3), oracle.er(700001, 2000000, seed=5)):
+        g = ctx.upload(h.off, h.col)
+        root = int(oracle.roots(h, 2, 1)[0])
+        lv = oracle.bfs(h, root)
+        for level in (0, 1, 2, 3, 5):
+            assert np.array_equal(g.bfs_inspect(lv, level), oracle.inspect_bfs(h, lv, level)), (h.n, level)
+        g.close()
