@@ -861,6 +861,11 @@ bool finish(active_set_t &as, G &g, F &f, config_t &conf) {
   return converged && window_exit(as, g, f, conf);
 }
 
+template <typename G, typename F, typename C>
+bool active_set_t::finish(G &g, F &f, C &conf) {
+  return gsw::finish(*this, g, f, conf);
+}
+
 // ===========================================================================
 // init_conf / reset_conf (src/gswitch.h:19-108)
 // ===========================================================================

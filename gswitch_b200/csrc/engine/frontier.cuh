@@ -259,6 +259,11 @@ struct active_set_t {
   __device__ __forceinline__ void raise(unsigned bits) const { atomicOr(&dg_cnt->err, bits); }
 
   // ---- host
+  // the reference's as.finish(g, f, conf) (active_set.cuh:37-43): true when
+  // the level loop is over; defined beside the engine's finish() in
+  // executor.cuh
+  template <typename G, typename F, typename C>
+  bool finish(G &g, F &f, C &conf);
   int build(int64_t _size, QueueMode qmode);
   void destroy();
   void reset(bool traceback = false);
