@@ -185,6 +185,9 @@ def run_ours(args):
             dist.barrier()
 
     ctx = gs.Context(local)
+    from gswitch_b200.autotune import load_table
+
+    ctx.tune_load(load_table())  # autotuned expand grids (defaults when absent)
     selector = args.selector
     if selector == "mlp":
         model, min_conf = load_model()

@@ -38,8 +38,10 @@ ABI_SYMBOLS = (
     "gsw_graph_destroy", "gsw_graph_roots", "gsw_ctx_stream", "gsw_run_opts_default", "gsw_bfs", "gsw_sssp", "gsw_cc",
     "gsw_pagerank", "gsw_bc", "gsw_gc", "gsw_mbfs", "gsw_bfs_strict_noalloc",
     "gsw_graph_generate_powerlaw", "gsw_label_levels", "gsw_mlp_train", "gsw_mlp_grad", "gsw_mlp_infer",
-    "gsw_mlp_load", "gsw_graph_generate_er_batch", "gsw_bfs_multi", "gsw_bfs_inspect",
+    "gsw_mlp_load", "gsw_graph_generate_er_batch", "gsw_bfs_multi", "gsw_bfs_inspect", "gsw_tune_load",
+    "gsw_tune_save",
 )
+TUNE_ENTRIES = 64
 
 # learned selector (include/gsw.h): 8 features -> 32 -> 32 -> 20 classes
 MLP_FEATURES, MLP_CLASSES, MLP_NPARAM = 8, 20, 2004
@@ -124,6 +126,8 @@ def lib():
                                               pvp]
     L.gsw_bfs_multi.argtypes = [vp, vp, C.c_int, vp, po, vp, ps]
     L.gsw_bfs_inspect.argtypes = [vp, vp, vp, i32, vp]
+    L.gsw_tune_load.argtypes = [vp, vp]
+    L.gsw_tune_save.argtypes = [vp, vp]
     _LIB = L
     return L
 
@@ -305,6 +309,23 @@ class Context:
         prob = np.zeros(len(X), dtype=np.float32)
         _check(lib().gsw_mlp_infer(self._h, _ptr(model), _ptr(X), len(X), _ptr(cls), _ptr(prob)))
         return cls, prob
+
+    @staticmethod
+    def tune_index(direction, fmt, lb, fused=False):
+        """Entry of (``"Push"|"Pull"``, ``"Queue"|"Bitmap"``, LB name, fused)."""
+        return (((direction == "Pull") * 2 + (fmt == "Bitmap")) * 8 + LB[lb]) * 2 + int(bool(fused))
+
+    def tune_load(self, quarters=None):
+        """Expand grid caps in quarters of the resident grid (None: defaults)."""
+        q = None if quarters is None else np.ascontiguousarray(quarters, dtype=np.int32)
+        if q is not None and q.shape != (TUNE_ENTRIES,):
+            raise ValueError(f"tune table has {TUNE_ENTRIES} entries")
+        _check(lib().gsw_tune_load(self._h, _ptr(q)))
+
+    def tune_save(self):
+        q = np.zeros(TUNE_ENTRIES, dtype=np.int32)
+        _check(lib().gsw_tune_save(self._h, _ptr(q)))
+        return q
 
     def mlp_load(self, model=None, min_conf=0.0):
         m = None if model is None else np.ascontiguousarray(model, dtype=np.float32)

@@ -471,6 +471,11 @@ struct selector_t {
 // ===========================================================================
 struct executor_t {
   int *dg_tile = nullptr;  // STRICT tile owners
+  // Autotuned expand grids: for (pull, bitmap, load balance, fused) the grid
+  // cap in quarters of the kernel's resident grid (0: the resident grid).
+  struct tune_t {
+    int quarters[2][2][8][2] = {};
+  } tune;
   twod_layout twod;                 // 2D-partition layout of the current graph
   int64_t persistent_levels = 0;    // levels run inside persistent launches
   int64_t persistent_launches = 0;  // persistent launches
@@ -596,9 +601,12 @@ struct executor_t {
     const int64_t ed = hints().edges;
     const int B = EXPAND_THREADS;
     const int fg = opts().force_grid;
+    // autotuned grid of this variant: quarters of the resident grid
+    const int tq = tune.quarters[conf.conf_dir == Pull][as.fmt == Bitmap][(int)conf.conf_lb & 7][fused ? 1 : 0];
     auto grid_for = [&](auto kern, int64_t want) {
-      const int cap = resident_grid(kern, B);
+      const int res = resident_grid(kern, B);
       if (fg > 0) return fg;
+      const int cap = tq > 0 ? (int)MAX((int64_t)1, (int64_t)res * tq / 4) : res;
       return want < 0 ? cap : clamp_grid(want, cap);
     };
 #define GSW_GO(kern, want, ...)                                   \

@@ -819,6 +819,13 @@ bool dl_prepare(dl_run &R, gsw_ctx *ctx, int app, dl_key key, active_set_t &as, 
       << as.dg_cnt << as.workset.dg_eoff << as.workset.dg_bsum << as.workset.bsum_cap;
   key << conf.conf_pruning << conf.conf_count_edges << conf.conf_sorted_queue << fets.fromall << fets.toall
       << ex.dg_tile << ex.tile_cap << ex.twod.edge << opts().force_grid << ctx->stats.dg_runtime_info;
+  for (int q : ex.tune.quarters[0][0][0]) key << q;  // first row: cheap change detector
+  {
+    const int *flat = &ex.tune.quarters[0][0][0][0];
+    unsigned long long h = 1469598103934665603ull;  // FNV-1a over the whole table
+    for (size_t i = 0; i < sizeof(ex.tune.quarters) / sizeof(int); ++i) h = (h ^ (unsigned)flat[i]) * 1099511628211ull;
+    key << h;
+  }
   dloop_graph &L = ctx->dl[app];
   R.L = &L;
   if (L.key != key.v || !L.exec) {
@@ -2116,6 +2123,27 @@ gsw_status gsw_mlp_infer(gsw_ctx *ctx, const float *model, const float *X, int64
   if (prob) GSW_CUDA(cudaMemcpyAsync(prob, dp, sizeof(float) * n, cudaMemcpyDeviceToHost, stream()));
   GSW_CUDA(cudaStreamSynchronize(stream()));
   return eg.finish();
+}
+
+gsw_status gsw_tune_load(gsw_ctx *ctx, const int32_t *quarters) {
+  entry_guard eg(ctx);
+  if (!ctx) return fail(GSW_ERR_INVALID_ARG, "gsw_tune_load: NULL context");
+  auto &q = ctx->executor.tune.quarters;
+  int *flat = &q[0][0][0][0];
+  const int count = (int)(sizeof(q) / sizeof(int));
+  for (int i = 0; i < count; ++i) {
+    const int v = quarters ? quarters[i] : 0;
+    if (v < 0 || v > 64) return fail(GSW_ERR_INVALID_ARG, "gsw_tune_load: entries are 0..64 quarters");
+    flat[i] = v;
+  }
+  return GSW_OK;
+}
+
+gsw_status gsw_tune_save(gsw_ctx *ctx, int32_t *quarters) {
+  if (!ctx || !quarters) return fail(GSW_ERR_INVALID_ARG, "gsw_tune_save: bad arguments");
+  const auto &q = ctx->executor.tune.quarters;
+  memcpy(quarters, &q[0][0][0][0], sizeof(q));
+  return GSW_OK;
 }
 
 gsw_status gsw_mlp_load(gsw_ctx *ctx, const float *model, float min_conf) {

@@ -234,6 +234,16 @@ gsw_status gsw_mlp_infer(gsw_ctx *ctx, const float *model, const float *features
  * rules decide. */
 gsw_status gsw_mlp_load(gsw_ctx *ctx, const float *model, float min_conf);
 
+/* ---- autotuned launch geometry ----------------------------------------------
+ * No counterpart in the reference (its grids are fixed per kernel).  The
+ * expand grid of every variant, as GSW_TUNE_ENTRIES int32 entries indexed
+ * [pull][bitmap][load balance (GSW_LB_*)][fused]: the grid cap in quarters of
+ * the kernel's resident grid (SMs x resident CTAs), 0 = the resident grid,
+ * at most 64.  gswitch_b200/autotune.py measures and writes the table. */
+#define GSW_TUNE_ENTRIES 64
+gsw_status gsw_tune_load(gsw_ctx *ctx, const int32_t *quarters); /* NULL: defaults */
+gsw_status gsw_tune_save(gsw_ctx *ctx, int32_t *quarters);
+
 /* No counterpart in the reference.  BFS levels (-1 unreached) computed with
  * the edge-balanced push expand, for callers that cannot allocate device
  * memory: code inside a host framework whose memory pool already owns the
