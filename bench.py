@@ -126,6 +126,13 @@ def level_bytes(kind, n, A, U, D, E):
     return work + 16 * U + 4.125 * E + 4 * D
 
 
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per vertex of
+# one inspection launch, from the ncu capture summarised in
+# profiles/bfs_rmat22_inspect_pulltm.md (33.60 MB over 4,194,304 vertices);
+# the inspection streams every vertex once, so a launch's traffic scales with n
+INSPECT_TRAFFIC_PER_VERTEX = 33.60e6 / 4194304
+
+
 def roofline_from(runs, n, peak_gbs, peak_kind):
     """runs: list of (timed RunStats, accounting RunStats, levels array)."""
     per = {}
@@ -156,7 +163,11 @@ def roofline_from(runs, n, peak_gbs, peak_kind):
     return {"bound": "hbm", "kernel": name, "achieved": round(achieved, 1), "peak": peak_gbs,
             "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak_gbs, 4),
             "bytes_per_launch": round(byt / max(launches, 1)), "launches": launches,
-            "avg_launch_ms": round(ms / max(launches, 1), 5), "traffic": None, "time_shares": shares}
+            "avg_launch_ms": round(ms / max(launches, 1), 5),
+            "traffic": round(INSPECT_TRAFFIC_PER_VERTEX * n) if name == "inspect" else None,
+            "traffic_note": ("ncu DRAM bytes of one inspection at scale 22 scaled by vertices"
+                             if name == "inspect" else "no per-launch ncu figure for this kernel's level mix"),
+            "time_shares": shares}
 
 
 def run_opts(gs, selector, **kw):
