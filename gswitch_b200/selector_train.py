@@ -4,7 +4,8 @@ kernels, and the regret of the network and of the rule-based selector
 against the exhaustively timed best variant on held-out graphs.
 
 Corpus (one seed per graph): RMAT with 2^14..2^20 vertices (log-uniform;
---big adds graphs with 2^21..2^23),
+--big adds graphs with 2^21..2^23, --huge RMAT graphs with 2^24 for BFS and
+PageRank),
 edge factor 16, a in [0.45, 0.65], d = 0.05, b = c = (1 - a - d) / 2;
 Erdos-Renyi G(n, m) with n in 2^14..2^20 and mean degree in [4, 32]; square
 2D grids with 1% long-range edges, side 64..1024; power-law configuration
@@ -70,7 +71,7 @@ def build(ctx, spec, wmax=64):
     return ctx.powerlaw(spec["n"], spec["gamma"], seed=spec["seed"], wmax=wmax, wseed=spec["seed"] + 1)
 
 
-def label_corpus(ctx, specs, budget_s: float, log=None):
+def label_corpus(ctx, specs, budget_s: float, log=None, apps=APPS):
     """Labels every graph (until the time budget runs out); returns rows
     X [r, 8], T [r, 20], R (rule class) [r], G (graph index) [r], A (app) [r]."""
     Xs, Ts, Rs, Gs, As = [], [], [], [], []
@@ -81,7 +82,7 @@ def label_corpus(ctx, specs, budget_s: float, log=None):
             break
         g = build(ctx, spec)
         root = int(g.roots(spec["seed"] % 1000 + 3, 1)[0])
-        for app, _ in APPS:
+        for app, _ in apps:
             X, T, R = g.label(app, root, max_levels=48, pr_iters=2)
             Xs.append(X)
             Ts.append(T)
@@ -127,6 +128,8 @@ def main(argv=None):
     ap.add_argument("--big", type=int, default=0, help="extra graphs with 2^21..2^23 vertices")
     ap.add_argument("--big-test", type=int, default=0)
     ap.add_argument("--big-budget-s", type=float, default=600.0)
+    ap.add_argument("--huge", type=int, default=0, help="extra RMAT graphs with 2^24 vertices (BFS, PageRank)")
+    ap.add_argument("--huge-test", type=int, default=0)
     args = ap.parse_args(argv)
     log = lambda m: print(m, file=sys.stderr, flush=True)
     ctx = gs.Context(0)
@@ -149,6 +152,25 @@ def main(argv=None):
         Xte, Tte, Rte, Ate = (np.concatenate([a, b]) for a, b in zip((Xte, Tte, Rte, Ate), parts[:2] + parts[2:3] + parts[4:5]))
         Gte = np.concatenate([Gte, parts[3] + nte])
         nte += parts[5]
+    for count, seed, test in ((args.huge, args.seed + 4, False), (args.huge_test, args.seed + 5, True)):
+        if not count:
+            continue
+        rng = np.random.default_rng(seed)
+        specs = []
+        for _ in range(count):
+            a = float(rng.uniform(0.5, 0.62))
+            bc = (1.0 - a - 0.05) / 2
+            specs.append({"kind": "rmat", "scale": 24, "a": a, "b": bc, "c": bc,
+                          "seed": int(rng.integers(1000, 2**62))})
+        parts = label_corpus(ctx, specs, args.big_budget_s, log, apps=((gs.APP_BFS, "bfs"), (gs.APP_PR, "pr")))
+        if test:
+            Xte, Tte, Rte, Ate = (np.concatenate([a, b]) for a, b in zip((Xte, Tte, Rte, Ate), parts[:3] + parts[4:5]))
+            Gte = np.concatenate([Gte, parts[3] + nte])
+            nte += parts[5]
+        else:
+            Xtr, Ttr, Rtr, Atr = (np.concatenate([a, b]) for a, b in zip((Xtr, Ttr, Rtr, Atr), parts[:3] + parts[4:5]))
+            Gtr = np.concatenate([Gtr, parts[3] + ntr])
+            ntr += parts[5]
     t_lab = time.time() - t0
     log(f"labels: train {len(Xtr)} rows / {ntr} graphs, test {len(Xte)} rows / {nte} graphs")
     if args.save_labels:
