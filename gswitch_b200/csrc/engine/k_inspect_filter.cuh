@@ -28,7 +28,13 @@ constexpr int INSPECT_OWNERS = INSPECT_VBLOCK / INSPECT_SPAN;  // 128 threads ow
 constexpr int INSPECT_HALVES = 4;            // physical threads sharing those virtual threads
 constexpr int INSPECT_THREADS = INSPECT_OWNERS * INSPECT_HALVES;
 constexpr int INSPECT_CTAS = INSPECT_VTHREADS / INSPECT_VBLOCK;  // one CTA per virtual block
-constexpr int INSPECT_UNROLL = 2;
+#ifndef GSW_INSPECT_UNROLL
+#define GSW_INSPECT_UNROLL 2
+#endif
+#ifndef GSW_INSPECT_MINBLOCKS
+#define GSW_INSPECT_MINBLOCKS 2
+#endif
+constexpr int INSPECT_UNROLL = GSW_INSPECT_UNROLL;
 static_assert(STAT_SLOTS == 8 + 2 * (INSPECT_VTHREADS / INSPECT_VBLOCK), "statistics block layout");
 constexpr int EC_INSPECT_CTAS = 256;
 constexpr int EC_INSPECT_THREADS = 512;
@@ -44,7 +50,7 @@ constexpr int EC_INSPECT_THREADS = 512;
 // steps and merge their maxima in shared memory; the last CTA to finish
 // folds the per-virtual-block sums (max over blocks for push, sum for pull).
 template <typename G, typename F>
-__global__ void __launch_bounds__(INSPECT_THREADS, 2) k_inspect_vc(active_set_t as, G g, F f, unsigned long long *info,
+__global__ void __launch_bounds__(INSPECT_THREADS, GSW_INSPECT_MINBLOCKS) k_inspect_vc(active_set_t as, G g, F f, unsigned long long *info,
                                                                const int *skip_if = nullptr) {
   // captured loops: a level whose expand found an empty input ends the loop
   // before this inspection (the host loop stops there too)
@@ -93,24 +99,28 @@ __global__ void __launch_bounds__(INSPECT_THREADS, 2) k_inspect_vc(active_set_t 
     for (int u = 0; u < INSPECT_UNROLL; ++u) {
       const long long v0 = base + u * step;
       if (v0 - 4ll * lane >= n) break;  // warp-uniform
-      unsigned na = 0, ni = 0, nvalid = 0;
+      unsigned na = 0, ni = 0, nvalid = INSPECT_SPAN;
+      unsigned long long pw = 0, lw = 0;
+      // out-of-range vertices were given status Inactive and degree 0 above,
+      // so only the count of valid vertices needs the bound
+      if (v0 + INSPECT_SPAN > n) nvalid = v0 < n ? (unsigned)(n - v0) : 0u;
 #pragma unroll
       for (int i = 0; i < INSPECT_SPAN; ++i) {
-        const bool valid = v0 + i < n;
-        const bool tag_active = valid && st[u][i] == Active;
-        const bool tag_inactive = valid && st[u][i] != Inactive;  // 0 only for Inactive
+        const bool tag_active = st[u][i] == Active;
+        const bool tag_inactive = st[u][i] != Inactive;  // 0 only for Inactive
         na |= (unsigned)tag_active << i;
         ni |= (unsigned)tag_inactive << i;
-        nvalid += valid;
         const unsigned oa = tag_active ? (unsigned)od[u][i] : 0u;
-        const unsigned oi = (valid && !tag_inactive) ? (unsigned)od[u][i] : 0u;
-        push_wl += oa;
-        pull_wl += oi;
-        mp[i] = mp[i] > oa ? mp[i] : oa;
-        ml[i] = ml[i] > oi ? ml[i] : oi;
+        const unsigned oi = tag_inactive ? 0u : (unsigned)od[u][i];
+        pw += oa;
+        lw += oi;
+        mp[i] = max(mp[i], oa);
+        ml[i] = max(ml[i], oi);
       }
+      push_wl += pw;
+      pull_wl += lw;
       active_num += __popc(na);
-      inactive_num += nvalid - __popc(ni);
+      inactive_num += nvalid - (unsigned)__popc(ni & ((1u << nvalid) - 1u));
       // lanes 8j .. 8j+7 hold the 32 vertices of bitmap word j of the warp
       unsigned wa = na << (4 * (lane & 7)), wi = ni << (4 * (lane & 7));
 #pragma unroll
