@@ -201,11 +201,16 @@ def run_ours(args):
     ctx.tune_load(load_table())  # autotuned expand grids (defaults when absent)
     selector = args.selector
     if selector == "mlp":
+        from gswitch_b200.selector_train import load_fusion_model
+
         model, min_conf = load_model()
         if model is None:
             selector = "rules"
         else:
             ctx.mlp_load(model, min_conf)
+            fmodel, fconf = load_fusion_model()
+            if fmodel is not None:
+                ctx.mlp_load_fusion(fmodel, fconf)
     sampler = ClockSampler(local)
     sampler.start()
     t0 = time.time()
@@ -359,6 +364,68 @@ def app_table(ctx, g, gs, args, roots, selector):
         gm.close()
     table["er_batch_512"] = er_batch_entry(ctx, gs, selector)
     return table
+
+
+def run_c3(args):
+    import gswitch_b200 as gs
+    from gswitch_b200.autotune import load_table
+    from gswitch_b200.selector_train import load_model
+
+    ctx = gs.Context(0)
+    ctx.tune_load(load_table())
+    selector = "rules"
+    model, min_conf = load_model()
+    if args.selector == "mlp" and model is not None:
+        from gswitch_b200.selector_train import load_fusion_model
+
+        ctx.mlp_load(model, min_conf)
+        fmodel, fconf = load_fusion_model()
+        if fmodel is not None:
+            ctx.mlp_load_fusion(fmodel, fconf)
+        selector = "mlp"
+    print(json.dumps({"config": "C3", "selector": selector, "c3": c3_table(ctx, gs, selector)}))
+    ctx.close()
+
+
+def c3_table(ctx, gs, selector):
+    """Config C3 (separate run, `--c3`): the 4096 x 4096 grid with 1%
+    long-range edges (weights U[1, 1000]) for BFS, SSSP and BC, and RMAT
+    scale 26 for BFS: the switched form against the fixed variants."""
+    out = {}
+    grid = ctx.grid(4096, 4096, 100, seed=1, wmax=1000, wseed=5)
+    r26 = ctx.rmat(26, 16, 0.57, 0.19, 0.19, seed=1)
+
+    def run(g, app, root, o):
+        if app == "bfs":
+            _, st = g.bfs(root, o, out=False)
+        elif app == "sssp":
+            _, st = g.sssp(root, o, out=False)
+        else:
+            _, _, st = g.bc(root, o, out=False)
+        return st
+
+    def measure(g, app, root, o):
+        run(g, app, root, o)
+        st = run(g, app, root, o)
+        return {"ms": round(st.ms, 3), "gteps": round(st.edges / (st.ms * 1e6), 3), "levels": st.levels}
+
+    for gname, g, apps in (("grid4096_lr100", grid, ("bfs", "sssp", "bc")), ("rmat26_ef16", r26, ("bfs",))):
+        root = int(g.roots(1000, 1)[0])
+        for app in apps:
+            row = {"switched_rules": measure(g, app, root, gs.RunOpts()),
+                   "switched_mlp": measure(g, app, root, gs.RunOpts(selector=selector))}
+            fixed = {}
+            for cfg in FIXED:
+                fixed[cfg] = measure(g, app, root, gs.RunOpts.from_config(cfg))
+            best = max(fixed.items(), key=lambda kv: kv[1]["gteps"])
+            row.update({"fixed": {k: v["gteps"] for k, v in fixed.items()},
+                        "best_fixed": {"variant": best[0], **best[1]},
+                        "switched_vs_best_fixed": round(row["switched_mlp"]["gteps"] / best[1]["gteps"], 3)})
+            out[f"{app}_{gname}"] = row
+    out["definitions"] = {"bfs/sssp/bc": "sum deg(reached)/2 / t (BC: both phases timed)", "unit": "GTEPS"}
+    grid.close()
+    r26.close()
+    return out
 
 
 def er_batch_entry(ctx, gs, selector):
@@ -521,11 +588,14 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--selector", default="mlp", choices=["mlp", "rules"])
     ap.add_argument("--no-apps", action="store_true")
+    ap.add_argument("--c3", action="store_true", help="print config C3's switched-vs-fixed table instead")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
+    elif args.c3:
+        run_c3(args)
     else:
         run_ours(args)
 

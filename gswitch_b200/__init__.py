@@ -39,7 +39,7 @@ ABI_SYMBOLS = (
     "gsw_pagerank", "gsw_bc", "gsw_gc", "gsw_mbfs", "gsw_bfs_strict_noalloc",
     "gsw_graph_generate_powerlaw", "gsw_label_levels", "gsw_mlp_train", "gsw_mlp_grad", "gsw_mlp_infer",
     "gsw_mlp_load", "gsw_graph_generate_er_batch", "gsw_bfs_multi", "gsw_bfs_inspect", "gsw_tune_load",
-    "gsw_tune_save",
+    "gsw_tune_save", "gsw_mlp_load_fusion",
 )
 TUNE_ENTRIES = 64
 
@@ -127,6 +127,7 @@ def lib():
     L.gsw_bfs_multi.argtypes = [vp, vp, C.c_int, vp, po, vp, ps]
     L.gsw_bfs_inspect.argtypes = [vp, vp, vp, i32, vp]
     L.gsw_tune_load.argtypes = [vp, vp]
+    L.gsw_mlp_load_fusion.argtypes = [vp, vp, C.c_float]
     L.gsw_tune_save.argtypes = [vp, vp]
     _LIB = L
     return L
@@ -326,6 +327,10 @@ class Context:
         q = np.zeros(TUNE_ENTRIES, dtype=np.int32)
         _check(lib().gsw_tune_save(self._h, _ptr(q)))
         return q
+
+    def mlp_load_fusion(self, model=None, min_conf=0.0):
+        m = None if model is None else np.ascontiguousarray(model, dtype=np.float32)
+        _check(lib().gsw_mlp_load_fusion(self._h, _ptr(m), min_conf))
 
     def mlp_load(self, model=None, min_conf=0.0):
         m = None if model is None else np.ascontiguousarray(model, dtype=np.float32)

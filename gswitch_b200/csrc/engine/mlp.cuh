@@ -93,6 +93,20 @@ __host__ __device__ inline void mlp_apply(int k, config_t &conf) {
   selector_t::set_target(conf);
 }
 
+// Graph-level features for the fusion decision of a run (the quantities the
+// reference's select_fusion tree reads, log-scaled, plus size and pattern).
+// Class 0 = standalone levels, class 1 = fused levels.
+__host__ __device__ inline void mlp_fusion_features(const feature_t &f, float *x) {
+  x[0] = mlp_log2p1(f.avg_deg);
+  x[1] = mlp_log2p1(f.std_deg);
+  x[2] = mlp_log2p1(f.range);
+  x[3] = (float)f.GI;
+  x[4] = (float)f.Her;
+  x[5] = mlp_log2p1((double)f.nvertexs);
+  x[6] = mlp_log2p1((double)f.nedges);
+  x[7] = f.pattern == Idem ? 0.f : (f.pattern == Mono ? 0.5f : 1.f);
+}
+
 // forward pass on the host (the device warp version below computes the same
 // sums in the same order)
 inline int mlp_predict_host(const mlp_model &m, const float *xin, float *prob_top) {

@@ -80,6 +80,7 @@ struct gsw_ctx {
   tree_set dts{};
   std::map<int, dloop_graph> dl;  // captured level loops, one per application
   mlp_model mlp{};                // learned selector (valid = 0: none loaded)
+  mlp_model mlp_fusion{};         // learned fusion decision of Mono-pattern runs
   mlp_model *dmlp = nullptr;      // its device copy (captured loops)
 
   void *buf(const std::string &name, size_t bytes) {
@@ -916,6 +917,23 @@ bool mlp_override(const mlp_model &m, const feature_t &fets, config_t &conf) {
   return true;
 }
 
+// Mono-pattern runs (SSSP) keep one fusion mode for the whole run (the
+// reference's select_fusion tree, src/model/select_fusion.h); with the
+// learned selector a second network over graph features takes that
+// decision.  Forced fusion wins.
+void mlp_fusion_override(gsw_ctx *ctx, const gsw_run_opts *o, const feature_t &fets, config_t &conf) {
+  const mlp_model &m = ctx->mlp_fusion;
+  if (!o || o->selector != GSW_SELECT_MLP || !m.valid || conf.force.has_fusion || fets.centric != VC ||
+      fets.pattern != Mono)
+    return;
+  float x[MLP_IN], pt = 0;
+  mlp_fusion_features(fets, x);
+  const int k = mlp_predict_host(m, x, &pt);
+  if (pt < m.min_conf || k > 1) return;
+  conf.conf_fuse_inspect = conf.conf_fusion = (k == 1);
+  if (!conf.conf_fuse_inspect) conf.conf_qmode = Normal;
+}
+
 void select_level(gsw_ctx *ctx, const gsw_run_opts *o, selector_t &sel, stat_t &stats, feature_t &fets,
                   config_t &conf) {
   sel.select(stats, fets, conf);
@@ -1514,6 +1532,7 @@ gsw_status gsw_sssp(gsw_ctx *ctx, gsw_graph *gr, int32_t root, const gsw_run_opt
   set_graph_features(fets, gr);
   fets.use_root = root;
   init_conf_impl(stats, fets, conf, g, f, gr->mean_weight, gr->attr[0], false, root_deg(gr, root));
+  mlp_fusion_override(ctx, o, fets, conf);
   active_set_t *asp = ctx->aset(gr->n, conf.conf_qmode);
   if (!asp) return eg.finish();
   active_set_t &as = *asp;
@@ -2143,6 +2162,16 @@ gsw_status gsw_tune_save(gsw_ctx *ctx, int32_t *quarters) {
   if (!ctx || !quarters) return fail(GSW_ERR_INVALID_ARG, "gsw_tune_save: bad arguments");
   const auto &q = ctx->executor.tune.quarters;
   memcpy(quarters, &q[0][0][0][0], sizeof(q));
+  return GSW_OK;
+}
+
+gsw_status gsw_mlp_load_fusion(gsw_ctx *ctx, const float *model, float min_conf) {
+  entry_guard eg(ctx);
+  if (!ctx) return fail(GSW_ERR_INVALID_ARG, "gsw_mlp_load_fusion: NULL context");
+  if (!model)
+    ctx->mlp_fusion.valid = 0;
+  else
+    ctx->mlp_fusion = model_from_floats(model, min_conf);
   return GSW_OK;
 }
 

@@ -14,6 +14,7 @@ graphs with gamma in [1.8, 3.0].  Each graph is labelled for BFS, SSSP
 
     python -m gswitch_b200.selector_train --train 2000 --test 200 \\
         --out gswitch_b200/models/selector_mlp.json
+    python -m gswitch_b200.selector_train fusion     # SSSP fused vs standalone
 """
 from __future__ import annotations
 
@@ -198,6 +199,91 @@ def main(argv=None):
     ctx.close()
 
 
+# ---------------------------------------------------------------------------
+# the fusion decision of SSSP (Mono pattern) runs
+# ---------------------------------------------------------------------------
+FUSION_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "models", "fusion_mlp.json")
+
+
+def fusion_features(g):
+    """The graph-level features of engine/mlp.cuh mlp_fusion_features (SSSP)."""
+    a = g.attr()  # avg, std, range, max degree, Gini, entropy
+    lg = lambda x: float(np.log2(1.0 + max(x, 0.0)))
+    return np.array([lg(a[0]), lg(a[1]), lg(a[2]), a[4], a[5], lg(g.n), lg(g.m), 0.5], dtype=np.float32)
+
+
+def fusion_corpus(count, seed):
+    """Graphs for the fusion decision: the selector corpus shapes up to 2^22
+    vertices, plus large grids (side up to 3,000)."""
+    specs = corpus(count, seed, 14, 22)
+    rng = np.random.default_rng(seed + 7)
+    for s in specs:
+        if s["kind"] == "grid" and rng.random() < 0.5:
+            s["side"] = int(rng.uniform(1024, 3000))
+    return specs
+
+
+def label_fusion(ctx, specs, log=None, wmax_grid=1000):
+    """Per graph: features, and SSSP device time with standalone (class 0) and
+    fused (class 1) levels, the learned variant selector deciding the rest."""
+    X, T, R = [], [], []
+    for i, spec in enumerate(specs):
+        g = build(ctx, spec, wmax=wmax_grid if spec["kind"] == "grid" else 64)
+        root = int(g.roots(spec["seed"] % 1000 + 3, 1)[0])
+        t = np.zeros(gs.MLP_CLASSES, dtype=np.float32)
+        for k, fu in ((0, gs.STANDALONE), (1, gs.FUSED)):
+            o = gs.RunOpts(selector="mlp", fusion=fu)
+            g.sssp(root, o, out=False)
+            t[k] = min(g.sssp(root, o, out=False)[1].ms for _ in range(2))
+        _, st = g.sssp(root, gs.RunOpts(), out=False)  # the rule tree's decision
+        X.append(fusion_features(g))
+        T.append(t)
+        R.append(1 if st.trace and st.trace[-1][3] == "Fused" else 0)
+        g.close()
+        if log and (i + 1) % 50 == 0:
+            log(f"fusion labels: {i + 1} graphs")
+    return np.array(X), np.array(T), np.array(R, dtype=np.int32)
+
+
+def train_fusion(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--train", type=int, default=400)
+    ap.add_argument("--test", type=int, default=80)
+    ap.add_argument("--seed", type=int, default=3030)
+    ap.add_argument("--epochs", type=int, default=2000)
+    ap.add_argument("--out", default=FUSION_PATH)
+    args = ap.parse_args(argv)
+    log = lambda m: print(m, file=sys.stderr, flush=True)
+    ctx = gs.Context(0)
+    model, conf = load_model()
+    ctx.mlp_load(model, conf)
+    Xtr, Ttr, _ = label_fusion(ctx, fusion_corpus(args.train, args.seed), log)
+    Xte, Tte, Rte = label_fusion(ctx, fusion_corpus(args.test, args.seed + 1), log)
+    fmodel, loss = ctx.mlp_train(Xtr, Ttr, epochs=args.epochs, lr=3e-3, tau=0.05, seed=args.seed)
+    cls, _ = ctx.mlp_infer(fmodel, Xte)
+    cls = np.minimum(cls, 1)
+    report = {"train_graphs": len(Xtr), "test_graphs": len(Xte), "final_loss": float(loss[-1]),
+              "sssp_ms_test": {"mlp": float(Tte[np.arange(len(Tte)), cls].sum()),
+                               "tree": float(Tte[np.arange(len(Tte)), Rte].sum()),
+                               "always_standalone": float(Tte[:, 0].sum()),
+                               "always_fused": float(Tte[:, 1].sum()),
+                               "best": float(Tte[:, :2].min(axis=1).sum())}}
+    with open(args.out, "w") as f:
+        json.dump({"format": "gswitch_b200 fusion MLP 8-32-32-20 fp32 (classes 0 standalone, 1 fused)",
+                   "model": [float(x) for x in fmodel], "min_conf": 0.0, "corpus_seed": args.seed,
+                   "report": report}, f)
+    print(json.dumps(report))
+    ctx.close()
+
+
+def load_fusion_model(path=None):
+    path = path or FUSION_PATH
+    if not os.path.exists(path):
+        return None, 0.0
+    d = json.load(open(path))
+    return np.asarray(d["model"], dtype=np.float32), float(d.get("min_conf", 0.0))
+
+
 def load_model(path=None):
     """The committed model as a float32 array, or None when absent."""
     path = path or os.path.join(os.path.dirname(os.path.abspath(__file__)), "models", "selector_mlp.json")
@@ -208,4 +294,7 @@ def load_model(path=None):
 
 
 if __name__ == "__main__":
-    main()
+    if len(sys.argv) > 1 and sys.argv[1] == "fusion":
+        train_fusion(sys.argv[2:])
+    else:
+        main()

@@ -233,6 +233,11 @@ gsw_status gsw_mlp_infer(gsw_ctx *ctx, const float *model, const float *features
  * opts.selector = GSW_SELECT_MLP; below min_conf top-class probability the
  * rules decide. */
 gsw_status gsw_mlp_load(gsw_ctx *ctx, const float *model, float min_conf);
+/* The second network: whether a Mono-pattern run (SSSP) runs fused or
+ * standalone levels, from graph features (avg, std and range of degree, Gini,
+ * entropy, log n, log m, pattern); class 0 standalone, 1 fused.  Used with
+ * opts.selector = GSW_SELECT_MLP; NULL unloads (the reference's tree decides). */
+gsw_status gsw_mlp_load_fusion(gsw_ctx *ctx, const float *model, float min_conf);
 
 /* ---- autotuned launch geometry ----------------------------------------------
  * No counterpart in the reference (its grids are fixed per kernel).  The

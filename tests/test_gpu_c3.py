@@ -12,7 +12,7 @@ import pytest
 
 import gswitch_b200 as gs
 import oracle
-from gswitch_b200.selector_train import load_model
+from gswitch_b200.selector_train import load_fusion_model, load_model
 
 pytestmark = pytest.mark.gpu
 
@@ -54,6 +54,15 @@ def test_c3_grid_sssp(ctx, c3grid):
     for cfg in ("", "Push-Queue-STRICT", "Push-Queue-WM-Fused"):
         d, _ = g.sssp(root, cfg)
         assert np.array_equal(d, ref), cfg
+    # the learned level selector and fused/standalone decision
+    model, conf = load_model()
+    fmodel, fconf = load_fusion_model()
+    ctx.mlp_load(model, conf)
+    ctx.mlp_load_fusion(fmodel, fconf)
+    d, _ = g.sssp(root, gs.RunOpts(selector="mlp"))
+    assert np.array_equal(d, ref)
+    ctx.mlp_load_fusion(None)
+    ctx.mlp_load(None)
 
 
 def test_c3_grid_bc(ctx, c3grid):

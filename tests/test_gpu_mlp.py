@@ -203,3 +203,58 @@ def test_committed_model_speeds_up_pagerank(ctx):
         times[sel] = st.ms
     ctx.mlp_load(None)
     assert times["mlp"] < times["rules"], times
+
+
+def _biased_model(cls):
+    """A network whose output is the constant class `cls`."""
+    m = np.zeros(gs.MLP_MODEL_FLOATS, dtype=np.float32)
+    m[gs.MLP_NPARAM - gs.MLP_CLASSES + cls] = 10.0  # b3[cls]
+    m[gs.MLP_NPARAM + gs.MLP_FEATURES:] = 1.0
+    return m
+
+
+def test_sssp_exact_under_both_fusion_decisions(ctx):
+    h = oracle.er(30000, 150000, seed=8)
+    hw = oracle.add_weights(h, 9, 64)
+    root = int(oracle.roots(h, 2, 1)[0])
+    ref = oracle.sssp_dijkstra(hw, root)
+    g = ctx.upload(hw.off, hw.col, hw.w)
+    model, conf = load_model()
+    ctx.mlp_load(model, conf)
+    for cls in (0, 1):
+        ctx.mlp_load_fusion(_biased_model(cls), 0.0)
+        d, st = g.sssp(root, gs.RunOpts(selector="mlp"))
+        assert np.array_equal(d, ref), cls
+        assert ({t[3] for t in st.trace} == {"Fused"}) == (cls == 1)
+    ctx.mlp_load_fusion(None)
+    ctx.mlp_load(None)
+
+
+def test_committed_fusion_model_beats_the_tree_on_fresh_graphs(ctx):
+    """SSSP on graphs the fusion corpus never saw: total device time with the
+    learned fused/standalone decision is below the reference tree's."""
+    from gswitch_b200.selector_train import load_fusion_model
+
+    fm, fc = load_fusion_model()
+    assert fm is not None, "gswitch_b200/models/fusion_mlp.json is missing"
+    model, conf = load_model()
+    ctx.mlp_load(model, conf)
+    ctx.mlp_load_fusion(fm, fc)
+    graphs = [ctx.er(1 << 19, 4 << 19, seed=91001, wmax=64, wseed=3),
+              ctx.grid(2900, 2900, 100, seed=91002, wmax=1000, wseed=3),
+              ctx.rmat(19, 16, 0.55, 0.2, 0.2, seed=91003, wmax=64, wseed=3)]
+    t_mlp = t_tree = 0.0
+    for g in graphs:
+        root = int(g.roots(8, 1)[0])
+        for sel in ("mlp", "rules"):
+            o = gs.RunOpts(selector=sel)
+            g.sssp(root, o, out=False)
+            ms = min(g.sssp(root, o, out=False)[1].ms for _ in range(2))
+            if sel == "mlp":
+                t_mlp += ms
+            else:
+                t_tree += ms
+        g.close()
+    ctx.mlp_load_fusion(None)
+    ctx.mlp_load(None)
+    assert t_mlp < t_tree, (t_mlp, t_tree)

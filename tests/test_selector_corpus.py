@@ -58,3 +58,15 @@ def test_class_names_cover_the_standalone_variants():
     names = {gs.mlp_class_name(k) for k in range(gs.MLP_CLASSES)}
     assert len(names) == 20
     assert "Push-Queue-TM" in names and "Pull-Bitmap-TWC" in names
+
+
+def test_committed_fusion_model_layout():
+    from gswitch_b200.selector_train import load_fusion_model
+
+    model, _ = load_fusion_model()
+    assert model is not None
+    assert model.shape == (gs.MLP_MODEL_FLOATS,) and np.all(np.isfinite(model))
+    d = json.load(open(os.path.join(ROOT, "gswitch_b200", "models", "fusion_mlp.json")))
+    t = d["report"]["sssp_ms_test"]
+    assert d["report"]["test_graphs"] >= 50
+    assert t["mlp"] < t["tree"] and t["mlp"] <= 1.05 * t["best"]
