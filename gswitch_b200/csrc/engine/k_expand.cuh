@@ -24,8 +24,8 @@
 //           sweeps for degree >= 256, warp sweeps for degree >= 32, and a
 //           CTA-scan mapping for the rest (the intent recorded in
 //           src/kernel_libs/expand_VC_TWC.cuh:11-63).
-// Loops that enqueue run with warp-uniform trip counts so the enqueue can be
-// aggregated with a full-warp ballot (one atomic per warp).
+// Loops that enqueue run with warp-uniform trip counts so a warp can stage its
+// appends in shared memory and reserve queue space once per STAGE_SLOTS.
 #pragma once
 #include "k_inspect_filter.cuh"
 
@@ -59,17 +59,60 @@ __device__ __forceinline__ bool push_edge_fused(active_set_t &as, const G &g, F 
   return tp;
 }
 
-// full-warp aggregated enqueue; every lane of the warp must call it
-__device__ __forceinline__ void warp_enqueue(active_set_t &as, bool tp, int u) {
-  if (as.queue.mode == Cached && as.queue.traceback) return;  // replay: nothing is enqueued
-  const unsigned m = __ballot_sync(FULL, tp);
-  if (!m) return;
-  const int leader = __ffs(m) - 1;
-  int64_t base = 0;
-  if (lane_id() == leader) base = as.queue.reserve(__popc(m));
-  base = __shfl_sync(FULL, base, leader);
-  if (tp && base >= 0) as.queue.output_base()[base + __popc(m & ((1u << lane_id()) - 1u))] = u;
-}
+// Fused levels append the vertices they activate to the output queue.  A warp
+// stages its appends in shared memory and reserves queue space once per
+// STAGE_SLOTS entries (and once when it is done), not once per 32-edge round:
+// on a large fused level every warp of the grid would otherwise hit the one
+// queue counter each round, and those same-address atomics serialise at the
+// L2 (4M-vertex SSSP levels ran at 9 G edges/s instead of 30+).  The order of
+// a level's queue is unspecified either way.
+constexpr int STAGE_SLOTS = 128;
+
+struct warp_stage_t {
+  int *buf;       // this warp's STAGE_SLOTS slots in shared memory
+  int n = 0;      // staged entries, warp-uniform
+  int *out;       // nullptr: appends are dropped (Cached replay)
+  int *cnt;
+  int64_t cap;
+  unsigned *err;
+
+  __device__ __forceinline__ warp_stage_t(int *smem, int *o, int *c, int64_t cp, unsigned *e)
+      : buf(smem), out(o), cnt(c), cap(cp), err(e) {}
+  __device__ __forceinline__ warp_stage_t(int *smem, const active_set_t &as)
+      : buf(smem),
+        out(as.queue.mode == Cached && as.queue.traceback ? nullptr : as.queue.output_base()),
+        cnt(as.queue.output_size()),
+        cap(as.queue.output_cap()),
+        err(as.queue.dg_err) {}
+
+  // every lane of the warp calls it
+  __device__ __forceinline__ void flush() {
+    if (n == 0) return;
+    __syncwarp();
+    int base = 0;
+    if (lane_id() == 0) {
+      base = atomicAdd(cnt, n);
+      if ((int64_t)base + n > cap) {
+        atomicOr(err, DEV_ERR_QUEUE_OVERFLOW);
+        base = -1;
+      }
+    }
+    base = __shfl_sync(FULL, base, 0);
+    if (base >= 0)
+      for (int i = lane_id(); i < n; i += 32) out[base + i] = buf[i];
+    n = 0;
+    __syncwarp();
+  }
+  // every lane of the warp calls it; lanes with tp append u
+  __device__ __forceinline__ void push(bool tp, int u) {
+    const unsigned m = __ballot_sync(FULL, tp && out != nullptr);
+    if (!m) return;
+    const int c = __popc(m);
+    if (n + c > STAGE_SLOTS) flush();
+    if (tp) buf[n + __popc(m & ((1u << lane_id()) - 1u))] = u;
+    n += c;
+  }
+};
 
 template <typename G>
 __device__ __forceinline__ void vertex_range(const G &g, bool pull, int v, int64_t &st, int &deg) {
@@ -104,20 +147,38 @@ __global__ void __launch_bounds__(EXPAND_THREADS) k_push_tm(active_set_t as, G g
   const Status want = conf.want();
   const int64_t STRIDE = (int64_t)blockDim.x * gridDim.x;
   unsigned long long cnt = 0;
-  for (int64_t idx = threadIdx.x + (int64_t)blockIdx.x * blockDim.x; idx < n; idx += STRIDE) {
-    const int v = as.fetch(idx, want);
-    if (v < 0) continue;
-    int64_t st;
-    int deg;
-    vertex_range(g, false, v, st, deg);
-    cnt += deg;
-    for (int k = 0; k < deg; ++k) {
-      const int u = __ldg(g.dg_adj_list + st + k);
-      if (FUSED) {
-        if (push_edge_fused(as, g, f, conf, v, u, st + k)) as.queue.push(u);
-      } else {
-        push_edge_std(as, g, f, conf, v, u, st + k);
+  if constexpr (FUSED) {
+    // warp-uniform trip counts, so the warp stages its appends together
+    __shared__ int s_stage[EXPAND_THREADS / 32][STAGE_SLOTS];
+    warp_stage_t stage(s_stage[warp_id()], as);
+    for (int64_t w0 = (threadIdx.x & ~31u) + (int64_t)blockIdx.x * blockDim.x; w0 < n; w0 += STRIDE) {
+      const int64_t idx = w0 + lane_id();
+      const int v = idx < n ? as.fetch(idx, want) : -1;
+      int64_t st;
+      int deg;
+      vertex_range(g, false, v, st, deg);
+      cnt += deg;
+      const int rounds = (int)__reduce_max_sync(FULL, (unsigned)deg);
+      for (int k = 0; k < rounds; ++k) {
+        bool tp = false;
+        int u = -1;
+        if (k < deg) {
+          u = __ldg(g.dg_adj_list + st + k);
+          tp = push_edge_fused(as, g, f, conf, v, u, st + k);
+        }
+        stage.push(tp, u);
       }
+    }
+    stage.flush();
+  } else {
+    for (int64_t idx = threadIdx.x + (int64_t)blockIdx.x * blockDim.x; idx < n; idx += STRIDE) {
+      const int v = as.fetch(idx, want);
+      if (v < 0) continue;
+      int64_t st;
+      int deg;
+      vertex_range(g, false, v, st, deg);
+      cnt += deg;
+      for (int k = 0; k < deg; ++k) push_edge_std(as, g, f, conf, v, __ldg(g.dg_adj_list + st + k), st + k);
     }
   }
   account(as, conf, cnt);
@@ -196,10 +257,12 @@ __global__ void __launch_bounds__(EXPAND_THREADS) k_push_wm(active_set_t as, G g
   __shared__ int s_scan[W][32];
   __shared__ int s_v[W][32];
   __shared__ int64_t s_st[W][32];
+  __shared__ int s_stage[FUSED ? W : 1][FUSED ? STAGE_SLOTS : 1];
   const int64_t n = as.get_size();
   GSW_HALT_IF_EMPTY(n);
   const Status want = conf.want();
   const int lane = lane_id(), w = warp_id();
+  warp_stage_t stage(s_stage[FUSED ? w : 0], as);
   const int64_t nwarps = (int64_t)gridDim.x * W;
   for (int64_t tile = (int64_t)blockIdx.x * W + w; tile * 32 < n; tile += nwarps) {
     const int64_t idx = tile * 32 + lane;
@@ -227,10 +290,11 @@ __global__ void __launch_bounds__(EXPAND_THREADS) k_push_wm(active_set_t as, G g
         else
           push_edge_std(as, g, f, conf, s_v[w][id], u, ei);
       }
-      if (FUSED) warp_enqueue(as, tp, u);
+      if (FUSED) stage.push(tp, u);
     }
     __syncwarp();
   }
+  if (FUSED) stage.flush();
 }
 
 template <typename G, typename F>
@@ -308,9 +372,11 @@ __global__ void __launch_bounds__(EXPAND_THREADS) k_push_cm(active_set_t as, G g
   __shared__ int s_v[B];
   __shared__ int64_t s_st[B];
   __shared__ int s_tmp[33];
+  __shared__ int s_stage[FUSED ? B / 32 : 1][FUSED ? STAGE_SLOTS : 1];
   const int64_t n = as.get_size();
   GSW_HALT_IF_EMPTY(n);
   const Status want = conf.want();
+  warp_stage_t stage(s_stage[FUSED ? warp_id() : 0], as);
   for (int64_t tile = blockIdx.x; tile * B < n; tile += gridDim.x) {
     const int64_t idx = tile * B + threadIdx.x;
     const int v = idx < n ? as.fetch(idx, want) : -1;
@@ -337,10 +403,11 @@ __global__ void __launch_bounds__(EXPAND_THREADS) k_push_cm(active_set_t as, G g
         else
           push_edge_std(as, g, f, conf, s_v[id], u, ei);
       }
-      if (FUSED) warp_enqueue(as, tp, u);
+      if (FUSED) stage.push(tp, u);
     }
     __syncthreads();
   }
+  if (FUSED) stage.flush();
 }
 
 template <typename G, typename F>
@@ -460,9 +527,11 @@ __global__ void __launch_bounds__(EXPAND_THREADS) k_push_strict(active_set_t as,
   __shared__ int s_v[T + 2];
   __shared__ int64_t s_sc[T + 2];
   __shared__ int64_t s_st[T + 2];
+  __shared__ int s_stage[FUSED ? EXPAND_THREADS / 32 : 1][FUSED ? STAGE_SLOTS : 1];
   const int64_t n = as.get_size();
   GSW_HALT_IF_EMPTY(n);
   const Status want = conf.want();
+  warp_stage_t stage(s_stage[FUSED ? warp_id() : 0], as);
   const int64_t *eoff = as.workset.dg_eoff;
   const int64_t total = eoff[n];
   const int64_t ntiles = (total + T - 1) / T;
@@ -498,10 +567,11 @@ __global__ void __launch_bounds__(EXPAND_THREADS) k_push_strict(active_set_t as,
             push_edge_std(as, g, f, conf, s_v[j], u, ei);
         }
       }
-      if (FUSED) warp_enqueue(as, tp, u);
+      if (FUSED) stage.push(tp, u);
     }
     __syncthreads();
   }
+  if (FUSED) stage.flush();
 }
 
 // Pull: each thread walks 4 consecutive slots and folds runs of the same
@@ -700,10 +770,12 @@ __global__ void __launch_bounds__(EXPAND_THREADS) k_push_twc(active_set_t as, G 
   __shared__ int s_v[B];
   __shared__ int64_t s_st[B];
   __shared__ int s_tmp[33];
+  __shared__ int s_stage[FUSED ? B / 32 : 1][FUSED ? STAGE_SLOTS : 1];
   const int64_t n = as.get_size();
   GSW_HALT_IF_EMPTY(n);
   const Status want = conf.want();
   const int lane = lane_id();
+  warp_stage_t stage(s_stage[FUSED ? warp_id() : 0], as);
   if (threadIdx.x == 0) s_owner = -1;
   __syncthreads();
   for (int64_t tile = blockIdx.x; tile * B < n; tile += gridDim.x) {
@@ -741,7 +813,7 @@ __global__ void __launch_bounds__(EXPAND_THREADS) k_push_twc(active_set_t as, G 
           else
             push_edge_std(as, g, f, conf, cv, u, cst + k);
         }
-        if (FUSED) warp_enqueue(as, tp, u);
+        if (FUSED) stage.push(tp, u);
       }
       __syncthreads();
     }
@@ -768,7 +840,7 @@ __global__ void __launch_bounds__(EXPAND_THREADS) k_push_twc(active_set_t as, G 
           else
             push_edge_std(as, g, f, conf, wv, u, wst + k);
         }
-        if (FUSED) warp_enqueue(as, tp, u);
+        if (FUSED) stage.push(tp, u);
       }
     }
     // thread tier: remaining small lists mapped through a CTA scan
@@ -792,10 +864,11 @@ __global__ void __launch_bounds__(EXPAND_THREADS) k_push_twc(active_set_t as, G 
         else
           push_edge_std(as, g, f, conf, s_v[id], u, ei);
       }
-      if (FUSED) warp_enqueue(as, tp, u);
+      if (FUSED) stage.push(tp, u);
     }
     __syncthreads();
   }
+  if (FUSED) stage.flush();
 }
 
 // TWC pull: candidates with large in-degree are swept by the whole CTA or a

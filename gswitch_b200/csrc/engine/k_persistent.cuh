@@ -85,7 +85,9 @@ __device__ __forceinline__ void persist_wm_level(active_set_t &as, const G &g, F
   __shared__ int s_scan[W][32];
   __shared__ int s_v[W][32];
   __shared__ int64_t s_st[W][32];
+  __shared__ int s_stage[W][STAGE_SLOTS];
   const int lane = lane_id(), w = warp_id();
+  warp_stage_t stage(s_stage[w], out, out_cnt, cap, &as.dg_cnt->err);
   const int64_t nwarps = (int64_t)gridDim.x * W;
   for (int64_t tile = (int64_t)blockIdx.x * W + w; tile * 32 < n; tile += nwarps) {
     const int64_t idx = tile * 32 + lane;
@@ -110,23 +112,11 @@ __device__ __forceinline__ void persist_wm_level(active_set_t &as, const G &g, F
         u = __ldg(g.dg_adj_list + ei);
         tp = push_edge_fused(as, g, f, conf, s_v[w][id], u, ei);
       }
-      const unsigned m = __ballot_sync(FULL, tp);
-      if (m) {
-        const int leader = __ffs(m) - 1;
-        int pos = 0;
-        if (lane == leader) pos = atomicAdd(out_cnt, __popc(m));
-        pos = __shfl_sync(FULL, pos, leader);
-        const int64_t mine = (int64_t)pos + __popc(m & ((1u << lane) - 1u));
-        if (tp) {
-          if (mine < cap)
-            out[mine] = u;
-          else
-            as.raise(DEV_ERR_QUEUE_OVERFLOW);
-        }
-      }
+      stage.push(tp, u);
     }
     __syncwarp();
   }
+  stage.flush();
 }
 
 template <typename G, typename F>
