@@ -324,10 +324,13 @@ struct stat_t {
   void build(int _size = gsw::STAT_SLOTS) {
     if (dg_runtime_info) return;
     size = _size;
-    GSW_CUDA(cudaMalloc((void **)&dg_runtime_info, size * sizeof(unsigned long long)));
+    // the inspection's merge scratch follows the counters; only the
+    // counters are cleared per level
+    const size_t bytes = (size + gsw::STAT_SCRATCH) * sizeof(unsigned long long);
+    GSW_CUDA(cudaMalloc((void **)&dg_runtime_info, bytes));
+    GSW_CUDA(cudaMemsetAsync(dg_runtime_info, 0, bytes, gsw::stream()));
     GSW_CUDA(cudaMallocHost((void **)&h_runtime_info, size * sizeof(unsigned long long)));
     memset(h_runtime_info, 0, size * sizeof(unsigned long long));
-    clean();
   }
   void destroy() {
     cudaFree(dg_runtime_info);

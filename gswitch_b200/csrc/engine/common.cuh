@@ -61,6 +61,10 @@ namespace gsw {
 // slots of the inspector's statistics block (six counters, a completion
 // counter, a spare, and 2 x 256 per-virtual-block partial sums)
 constexpr int STAT_SLOTS = 8 + 2 * 256;
+// behind it, in u64 words: the VC inspection's merge scratch (two u32 maxima
+// per virtual thread of the 256 x 512 grid, one u32 step counter per virtual
+// block), zeroed once at allocation and left zeroed by every inspection
+constexpr int STAT_SCRATCH = (2 * 256 * 512 + 256 + 1) / 2;
 
 // Device error word bits, written by kernels and read by the host.
 enum device_error_bits : unsigned {

@@ -419,7 +419,7 @@ bool dl_build(dloop_graph &L, executor_t &ex, dloop_t *d, active_set_t as, devic
   // inspection body
   if (good) {
     good = dl_capture(ibody[0], [&] {
-      k_inspect_vc<<<INSPECT_CTAS, INSPECT_THREADS, 0, stream()>>>(as, g, f, info, &d->halt);
+      launch_inspect_vc(as, g, f, info, &d->halt);
     });
     im.inspect_kernels = 1;
   }

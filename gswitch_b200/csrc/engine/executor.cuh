@@ -53,6 +53,14 @@ inline int clamp_grid(int64_t want, int cap) {
   return (int)MIN(want, (int64_t)cap);
 }
 
+// the VC inspection on one wave of resident CTAs (no more CTAs than units)
+template <typename G, typename F>
+inline void launch_inspect_vc(const active_set_t &as, const G &g, const F &f, unsigned long long *info,
+                              const int *skip_if = nullptr) {
+  const int grid = clamp_grid(inspect_units(as.size), resident_grid(k_inspect_vc<G, F>, INSPECT_THREADS));
+  k_inspect_vc<G, F><<<grid, INSPECT_THREADS, 0, stream()>>>(as, g, f, info, skip_if);
+}
+
 inline double now_ms() {
   return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
@@ -232,7 +240,7 @@ struct inspector_t {
     marks().insp0 = marks().insp1 = -1;
     if (need_inspect) {
       if (opts().timing) marks().insp0 = timing_pool().record();
-      k_inspect_vc<<<INSPECT_CTAS, INSPECT_THREADS, 0, stream()>>>(as, g, f, stat.dg_runtime_info);
+      launch_inspect_vc(as, g, f, stat.dg_runtime_info);
       GSW_LAUNCHED();
       if (opts().timing) marks().insp1 = timing_pool().record();
       set_fets(as, stat, fets, conf, g.nvertexs, g.nedges);

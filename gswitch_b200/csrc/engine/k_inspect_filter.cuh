@@ -20,137 +20,197 @@ namespace gsw {
 
 // The statistics block: [0..5] the counters above, [6] blocks finished,
 // [8..8+256) and [264..264+256) the per-virtual-block sums of the two
-// max-degree counters.
+// max-degree counters.  Behind it (never cleared by the host) the inspection
+// keeps its merge scratch: per-virtual-thread maxima for push and pull and a
+// per-virtual-block count of finished steps, all zero between launches.
 constexpr int INSPECT_VTHREADS = 256 * 512;  // the reference's grid, one virtual thread each
 constexpr int INSPECT_VBLOCK = 512;          // virtual threads per virtual block
+constexpr int INSPECT_NVB = INSPECT_VTHREADS / INSPECT_VBLOCK;
 constexpr int INSPECT_SPAN = 4;              // consecutive vertices a physical thread takes per step
-constexpr int INSPECT_OWNERS = INSPECT_VBLOCK / INSPECT_SPAN;  // 128 threads own one virtual block
-constexpr int INSPECT_HALVES = 4;            // physical threads sharing those virtual threads
-constexpr int INSPECT_THREADS = INSPECT_OWNERS * INSPECT_HALVES;
-constexpr int INSPECT_CTAS = INSPECT_VTHREADS / INSPECT_VBLOCK;  // one CTA per virtual block
+constexpr int INSPECT_OWNERS = INSPECT_VBLOCK / INSPECT_SPAN;  // 128 threads cover one virtual block
+constexpr int INSPECT_PARTS = 2;             // thread groups of a CTA taking alternate steps
+constexpr int INSPECT_THREADS = INSPECT_OWNERS * INSPECT_PARTS;
+constexpr int INSPECT_SCRATCH_U32 = 2 * INSPECT_VTHREADS + INSPECT_NVB;
+constexpr int INSPECT_SCRATCH_U64 = (INSPECT_SCRATCH_U32 + 1) / 2;
 #ifndef GSW_INSPECT_UNROLL
 #define GSW_INSPECT_UNROLL 2
 #endif
 #ifndef GSW_INSPECT_MINBLOCKS
-#define GSW_INSPECT_MINBLOCKS 2
+#define GSW_INSPECT_MINBLOCKS 4
 #endif
 constexpr int INSPECT_UNROLL = GSW_INSPECT_UNROLL;
-static_assert(STAT_SLOTS == 8 + 2 * (INSPECT_VTHREADS / INSPECT_VBLOCK), "statistics block layout");
+static_assert(STAT_SLOTS == 8 + 2 * INSPECT_NVB, "statistics block layout");
+static_assert(STAT_SCRATCH == INSPECT_SCRATCH_U64, "inspection scratch layout");
 constexpr int EC_INSPECT_CTAS = 256;
 constexpr int EC_INSPECT_THREADS = 512;
 
+// steps of the reference's grid-stride loop: virtual thread t visits
+// t + k * 131072 for k < inspect_steps(n)
+__host__ __device__ __forceinline__ unsigned inspect_steps(int64_t n) {
+  const int64_t k = (n + INSPECT_VTHREADS - 1) / INSPECT_VTHREADS;
+  return k > 0 ? (unsigned)k : 1u;
+}
+// work units (virtual block, step): 512 consecutive vertices each
+__host__ __device__ __forceinline__ int64_t inspect_units(int64_t n) { return (int64_t)INSPECT_NVB * inspect_steps(n); }
+
 // Virtual thread t (0 <= t < 131072) visits vertices t, t + 131072, ...
 // exactly as thread t of the reference's 256 x 512 grid-stride launch, so the
-// max-degree counters are the reference's.  Vertex 4q + i + k * 131072 (i < 4)
-// always belongs to virtual thread 4q + i, so a physical thread owns the
-// four virtual threads 4q .. 4q+3 and reads four consecutive vertices per
-// step (a warp covers 128 consecutive vertices: four bitmap words, built
-// with shuffles), and the 128 owners 4q .. 4q+3 of one CTA are exactly one
-// virtual block of the reference.  Four quarters of the CTA take turns at the
-// steps and merge their maxima in shared memory; the last CTA to finish
-// folds the per-virtual-block sums (max over blocks for push, sum for pull).
+// max-degree counters are the reference's.  The work is cut into units
+// (virtual block b, step k) = vertices b*512 + k*131072 + [0, 512); CTA c of
+// the (resident-sized) grid takes units [c*U/G, (c+1)*U/G) in b-major order,
+// so every SM gets the same share whatever the graph size.  Inside a unit,
+// owner thread q reads vertices 4q .. 4q+3 (virtual threads 4q .. 4q+3 of b;
+// a warp covers 128 consecutive vertices: four bitmap words, built with
+// shuffles) and the CTA's two thread groups take alternate steps.  At the end
+// of each run of units of one virtual block (a segment) the CTA folds its
+// per-virtual-thread maxima into the global scratch with atomicMax and adds
+// the segment's step count to the block's counter; the CTA that completes a
+// virtual block sums its 512 maxima into the statistics block and clears the
+// scratch, and the last CTA to finish folds the virtual-block sums (max over
+// blocks for push, sum for pull).  All vertex arithmetic is 32-bit (vertex
+// ids are below 2^31), and units that lie wholly below n take a path without
+// per-vertex bounds checks.
 template <typename G, typename F>
-__global__ void __launch_bounds__(INSPECT_THREADS, GSW_INSPECT_MINBLOCKS) k_inspect_vc(active_set_t as, G g, F f, unsigned long long *info,
-                                                               const int *skip_if = nullptr) {
+__global__ void __launch_bounds__(INSPECT_THREADS, GSW_INSPECT_MINBLOCKS)
+    k_inspect_vc(active_set_t as, G g, F f, unsigned long long *info, const int *skip_if = nullptr) {
   // captured loops: a level whose expand found an empty input ends the loop
   // before this inspection (the host loop stops there too)
   if (skip_if && *(volatile const int *)skip_if) return;
   __shared__ unsigned long long s_red[32];
   __shared__ unsigned s_mp[INSPECT_OWNERS][INSPECT_SPAN], s_ml[INSPECT_OWNERS][INSPECT_SPAN];
+  __shared__ int s_fold;
   __shared__ bool s_last;
-  for (int i = threadIdx.x; i < INSPECT_OWNERS * INSPECT_SPAN; i += blockDim.x) {
-    (&s_mp[0][0])[i] = 0;
-    (&s_ml[0][0])[i] = 0;
-  }
-  __syncthreads();
-  constexpr long long S = INSPECT_VTHREADS;
-  const int half = threadIdx.x / INSPECT_OWNERS;
-  const int q_local = threadIdx.x % INSPECT_OWNERS;
-  const long long first = 4ll * (blockIdx.x * INSPECT_OWNERS + q_local);  // virtual threads first .. first+3
-  const int lane = lane_id();
-  const long long n = as.size;
+  unsigned *vmax = reinterpret_cast<unsigned *>(info + STAT_SLOTS);  // [2][INSPECT_VTHREADS]
+  unsigned *vdone = vmax + 2 * INSPECT_VTHREADS;                      // [INSPECT_NVB]
+  constexpr unsigned S = INSPECT_VTHREADS;
+  const unsigned n = (unsigned)as.size;
+  const unsigned K = inspect_steps(as.size);
+  const unsigned long long U = (unsigned long long)INSPECT_NVB * K;
+  const unsigned long long lo = U * blockIdx.x / gridDim.x, hi = U * (blockIdx.x + 1) / gridDim.x;
+  const unsigned part = threadIdx.x / INSPECT_OWNERS;
+  const unsigned q = threadIdx.x % INSPECT_OWNERS;
+  const unsigned lane = lane_id();
   unsigned active_num = 0, inactive_num = 0;
   unsigned long long push_wl = 0, pull_wl = 0;
-  unsigned mp[INSPECT_SPAN] = {0, 0, 0, 0}, ml[INSPECT_SPAN] = {0, 0, 0, 0};
-  const long long step = INSPECT_HALVES * S;
-  // the warp's first vertex is first - 4 * lane: a multiple of 128
-  for (long long base = first + half * S; base - 4ll * lane < n; base += INSPECT_UNROLL * step) {
-    int od[INSPECT_UNROLL][INSPECT_SPAN];
-    Status st[INSPECT_UNROLL][INSPECT_SPAN];
+
+  for (unsigned long long u = lo; u < hi;) {
+    const unsigned b = (unsigned)(u / K);
+    const unsigned k0 = (unsigned)(u % K);
+    const unsigned k1 = (unsigned)MIN((unsigned long long)K, k0 + (hi - u));  // segment: steps [k0, k1) of b
+    const unsigned vq = b * INSPECT_VBLOCK + INSPECT_SPAN * q;  // this thread's first vertex of step 0
+    unsigned mp[INSPECT_SPAN] = {0, 0, 0, 0}, ml[INSPECT_SPAN] = {0, 0, 0, 0};
+
+    // UNROLL steps k, k + PARTS, ...; FULLU: all of them exist and lie below n
+    auto steps = [&](auto full_tag, unsigned k) {
+      constexpr bool FULLU = decltype(full_tag)::value;
+      int od[INSPECT_UNROLL][INSPECT_SPAN];
+      Status st[INSPECT_UNROLL][INSPECT_SPAN];
 #pragma unroll
-    for (int u = 0; u < INSPECT_UNROLL; ++u) {
-      const long long v = base + u * step;  // a multiple of 4: 16-byte aligned
-      if (v + 3 < n) {
-        const int4 d4 = __ldg(reinterpret_cast<const int4 *>(g.dg_odegree + v));
-        od[u][0] = d4.x, od[u][1] = d4.y, od[u][2] = d4.z, od[u][3] = d4.w;
-      } else {
+      for (int j = 0; j < INSPECT_UNROLL; ++j) {
+        const unsigned kj = k + j * INSPECT_PARTS;
+        const unsigned v = vq + kj * S;  // a multiple of 4: 16-byte aligned
+        if (FULLU || (kj < k1 && v + 3 < n)) {
+          const int4 d4 = __ldg(reinterpret_cast<const int4 *>(g.dg_odegree + v));
+          od[j][0] = d4.x, od[j][1] = d4.y, od[j][2] = d4.z, od[j][3] = d4.w;
+        } else {
 #pragma unroll
-        for (int i = 0; i < INSPECT_SPAN; ++i) od[u][i] = v + i < n ? __ldg(g.dg_odegree + v + i) : 0;
+          for (int i = 0; i < INSPECT_SPAN; ++i) od[j][i] = (kj < k1 && v + i < n) ? __ldg(g.dg_odegree + v + i) : 0;
+        }
       }
+#pragma unroll
+      for (int j = 0; j < INSPECT_UNROLL; ++j) {
+        const unsigned kj = k + j * INSPECT_PARTS;
+        const unsigned v = vq + kj * S;
+#pragma unroll
+        for (int i = 0; i < INSPECT_SPAN; ++i)
+          st[j][i] = (FULLU || (kj < k1 && v + i < n)) ? f.filter((int)(v + i), g) : Inactive;
+      }
+#pragma unroll
+      for (int j = 0; j < INSPECT_UNROLL; ++j) {
+        const unsigned kj = k + j * INSPECT_PARTS;
+        const unsigned v0 = vq + kj * S;
+        if (!FULLU && (kj >= k1 || v0 - INSPECT_SPAN * lane >= n)) break;  // warp-uniform
+        unsigned na = 0, ni = 0, oa[INSPECT_SPAN], oi[INSPECT_SPAN];
+#pragma unroll
+        for (int i = 0; i < INSPECT_SPAN; ++i) {
+          const bool tag_active = st[j][i] == Active;
+          const bool tag_inactive = st[j][i] != Inactive;  // 0 only for Inactive
+          na |= (unsigned)tag_active << i;
+          ni |= (unsigned)tag_inactive << i;
+          oa[i] = tag_active ? (unsigned)od[j][i] : 0u;
+          oi[i] = tag_inactive ? 0u : (unsigned)od[j][i];
+          mp[i] = max(mp[i], oa[i]);
+          ml[i] = max(ml[i], oi[i]);
+        }
+        // degrees are below 2^31, so a pair sums without overflow in 32 bits
+        push_wl += (unsigned long long)(oa[0] + oa[1]) + (oa[2] + oa[3]);
+        pull_wl += (unsigned long long)(oi[0] + oi[1]) + (oi[2] + oi[3]);
+        active_num += __popc(na);
+        // out-of-range vertices have status Inactive and degree 0, so only
+        // the count of valid vertices needs the bound
+        unsigned nvalid = INSPECT_SPAN;
+        if (!FULLU && v0 + INSPECT_SPAN > n) nvalid = v0 < n ? n - v0 : 0u;
+        inactive_num += nvalid - (unsigned)__popc(ni & ((1u << nvalid) - 1u));
+        // lanes 8j .. 8j+7 hold the 32 vertices of bitmap word j of the warp
+        unsigned wa = na << (4 * (lane & 7)), wi = ni << (4 * (lane & 7));
+#pragma unroll
+        for (int d = 1; d < 8; d <<= 1) {
+          wa |= __shfl_xor_sync(FULL, wa, d);
+          wi |= __shfl_xor_sync(FULL, wi, d);
+        }
+        if ((lane & 7) == 0 && (FULLU || v0 < n)) {
+          as.bitmap.active.dg_bits[v0 >> 5] = wa;
+          as.bitmap.inactive.dg_bits[v0 >> 5] = wi;
+        }
+      }
+    };
+    for (unsigned k = k0 + part; k < k1; k += INSPECT_PARTS * INSPECT_UNROLL) {
+      const unsigned klast = k + (INSPECT_UNROLL - 1) * INSPECT_PARTS;
+      // the last step's unit ends at or below n: every vertex is valid
+      if (klast < k1 && b * INSPECT_VBLOCK + klast * S + INSPECT_VBLOCK <= n)
+        steps(std::true_type{}, k);
+      else
+        steps(std::false_type{}, k);
     }
+
+    // fold the segment: group 1 hands its maxima to group 0, which publishes
+    if (part == 1)
 #pragma unroll
-    for (int u = 0; u < INSPECT_UNROLL; ++u)
-#pragma unroll
-      for (int i = 0; i < INSPECT_SPAN; ++i) {
-        const long long v = base + u * step + i;
-        st[u][i] = v < n ? f.filter((int)v, g) : Inactive;
-      }
-#pragma unroll
-    for (int u = 0; u < INSPECT_UNROLL; ++u) {
-      const long long v0 = base + u * step;
-      if (v0 - 4ll * lane >= n) break;  // warp-uniform
-      unsigned na = 0, ni = 0, nvalid = INSPECT_SPAN;
-      unsigned long long pw = 0, lw = 0;
-      // out-of-range vertices were given status Inactive and degree 0 above,
-      // so only the count of valid vertices needs the bound
-      if (v0 + INSPECT_SPAN > n) nvalid = v0 < n ? (unsigned)(n - v0) : 0u;
-#pragma unroll
-      for (int i = 0; i < INSPECT_SPAN; ++i) {
-        const bool tag_active = st[u][i] == Active;
-        const bool tag_inactive = st[u][i] != Inactive;  // 0 only for Inactive
-        na |= (unsigned)tag_active << i;
-        ni |= (unsigned)tag_inactive << i;
-        const unsigned oa = tag_active ? (unsigned)od[u][i] : 0u;
-        const unsigned oi = tag_inactive ? 0u : (unsigned)od[u][i];
-        pw += oa;
-        lw += oi;
-        mp[i] = max(mp[i], oa);
-        ml[i] = max(ml[i], oi);
-      }
-      push_wl += pw;
-      pull_wl += lw;
-      active_num += __popc(na);
-      inactive_num += nvalid - (unsigned)__popc(ni & ((1u << nvalid) - 1u));
-      // lanes 8j .. 8j+7 hold the 32 vertices of bitmap word j of the warp
-      unsigned wa = na << (4 * (lane & 7)), wi = ni << (4 * (lane & 7));
-#pragma unroll
-      for (int d = 1; d < 8; d <<= 1) {
-        wa |= __shfl_xor_sync(FULL, wa, d);
-        wi |= __shfl_xor_sync(FULL, wi, d);
-      }
-      if ((lane & 7) == 0 && v0 < n) {
-        as.bitmap.active.dg_bits[v0 >> 5] = wa;
-        as.bitmap.inactive.dg_bits[v0 >> 5] = wi;
-      }
-    }
-  }
-  // merge the halves of every virtual thread
-  for (int h = 1; h < INSPECT_HALVES; ++h) {
-    if (half == h)
-#pragma unroll
-      for (int i = 0; i < INSPECT_SPAN; ++i) {
-        s_mp[q_local][i] = MAX(s_mp[q_local][i], mp[i]);
-        s_ml[q_local][i] = MAX(s_ml[q_local][i], ml[i]);
-      }
+      for (int i = 0; i < INSPECT_SPAN; ++i) s_mp[q][i] = mp[i], s_ml[q][i] = ml[i];
     __syncthreads();
-  }
-  unsigned long long vmp = 0, vml = 0;  // sums over this thread's four virtual threads
-  if (half == 0)
+    if (part == 0) {
+      unsigned *vp = vmax + b * INSPECT_VBLOCK + INSPECT_SPAN * q;
 #pragma unroll
-    for (int i = 0; i < INSPECT_SPAN; ++i) {
-      vmp += MAX(mp[i], s_mp[q_local][i]);
-      vml += MAX(ml[i], s_ml[q_local][i]);
+      for (int i = 0; i < INSPECT_SPAN; ++i) {
+        const unsigned a = max(mp[i], s_mp[q][i]), c = max(ml[i], s_ml[q][i]);
+        if (a) atomicMax(vp + i, a);
+        if (c) atomicMax(vp + INSPECT_VTHREADS + i, c);
+      }
     }
+    __syncthreads();  // every maximum is issued before the count, and s_mp is free
+    if (threadIdx.x == 0) {
+      __threadfence();
+      s_fold = atomicAdd(vdone + b, k1 - k0) + (k1 - k0) == K;
+    }
+    __syncthreads();
+    if (s_fold) {  // this CTA completed virtual block b
+      __threadfence();
+      unsigned long long sp = 0, sl = 0;
+      for (int t = threadIdx.x; t < INSPECT_VBLOCK; t += blockDim.x) {
+        sp += atomicExch(vmax + b * INSPECT_VBLOCK + t, 0u);
+        sl += atomicExch(vmax + INSPECT_VTHREADS + b * INSPECT_VBLOCK + t, 0u);
+      }
+      sp = block_reduce(sp, s_red);
+      sl = block_reduce(sl, s_red);
+      if (threadIdx.x == 0) {
+        info[8 + b] = sp;
+        info[8 + INSPECT_NVB + b] = sl;
+        vdone[b] = 0;
+      }
+    }
+    u += k1 - k0;
+  }
+
   unsigned long long r;
   r = block_reduce((unsigned long long)active_num, s_red);
   if (threadIdx.x == 0 && r) atomicAdd(info + 0, r);
@@ -160,12 +220,6 @@ __global__ void __launch_bounds__(INSPECT_THREADS, GSW_INSPECT_MINBLOCKS) k_insp
   if (threadIdx.x == 0 && r) atomicAdd(info + 2, r);
   r = block_reduce(pull_wl, s_red);
   if (threadIdx.x == 0 && r) atomicAdd(info + 3, r);
-  const int vb = blockIdx.x;  // this CTA's virtual block
-  const int NVB = INSPECT_VTHREADS / INSPECT_VBLOCK;
-  r = block_reduce(vmp, s_red);
-  if (threadIdx.x == 0 && r) atomicAdd(info + 8 + vb, r);
-  r = block_reduce(vml, s_red);
-  if (threadIdx.x == 0 && r) atomicAdd(info + 8 + NVB + vb, r);
   if (threadIdx.x == 0) {
     __threadfence();
     s_last = atomicAdd(info + 6, 1ull) == (unsigned long long)gridDim.x - 1;
@@ -174,10 +228,10 @@ __global__ void __launch_bounds__(INSPECT_THREADS, GSW_INSPECT_MINBLOCKS) k_insp
   if (s_last) {  // last block: fold the virtual-block sums
     __threadfence();
     unsigned long long mpx = 0, sp = 0;
-    for (int i = threadIdx.x; i < NVB; i += blockDim.x) {
+    for (int i = threadIdx.x; i < INSPECT_NVB; i += blockDim.x) {
       const unsigned long long a = ((volatile unsigned long long *)info)[8 + i];
       mpx = MAX(mpx, a);
-      sp += ((volatile unsigned long long *)info)[8 + NVB + i];
+      sp += ((volatile unsigned long long *)info)[8 + INSPECT_NVB + i];
     }
     mpx = block_reduce<unsigned long long, true>(mpx, s_red);
     sp = block_reduce(sp, s_red);

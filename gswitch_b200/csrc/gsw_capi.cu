@@ -1478,7 +1478,7 @@ gsw_status gsw_bfs_inspect(gsw_ctx *ctx, gsw_graph *gr, const int32_t *levels, i
   stat_t &stats = ctx->stats;
   stats.build();
   stats.clean();
-  k_inspect_vc<<<INSPECT_CTAS, INSPECT_THREADS, 0, stream()>>>(*asp, g, f, stats.dg_runtime_info);
+  launch_inspect_vc(*asp, g, f, stats.dg_runtime_info);
   GSW_LAUNCHED();
   stats.collect(6);
   stats.clean();
