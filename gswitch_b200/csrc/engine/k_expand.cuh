@@ -34,6 +34,9 @@ namespace gsw {
 constexpr int EXPAND_THREADS = 256;
 constexpr int STRICT_TILE = 1024;   // slots per STRICT tile (4 per thread)
 constexpr int STRICT_ITEMS = 1024;  // frontier entries per STRICT scan block
+#ifndef GSW_PULL_TM_K
+#define GSW_PULL_TM_K 2
+#endif
 
 // ---- per-edge operations ---------------------------------------------------
 template <typename G, typename F>
@@ -184,15 +187,18 @@ __global__ void __launch_bounds__(EXPAND_THREADS) k_push_tm(active_set_t as, G g
   account(as, conf, cnt);
 }
 
-// Thread per candidate, four candidates per thread: the dependent chain of a
-// candidate (status bit -> offsets -> first in-neighbour -> its frontier bit)
-// is issued for all four before any of them is resolved, so a thread keeps
-// four memory requests in flight instead of one.  Most candidates of a large
-// pull level stop at the first neighbour.
+// Thread per candidate, GSW_PULL_TM_K (2) candidates per thread: the
+// dependent chain of a candidate (status bit -> offsets -> first in-neighbour
+// -> its frontier bit) is issued for both before either is resolved.  Most
+// candidates of a large pull level stop at the first neighbour; the rest walk
+// their lists one edge at a time, and a warp waits for its longest walk, so
+// more candidates per thread cost more in divergence than they gain in
+// overlap (RMAT s24 pull levels: 105 us at 1, 93 at 2, 103 at 4, 135 at 8;
+// fetching four neighbours per step of the walk was slower too).
 template <typename G, typename F>
 __global__ void __launch_bounds__(EXPAND_THREADS) k_pull_tm(active_set_t as, G g, F f, config_t conf) {
   using WA = typename F::wa_t;
-  constexpr int K = 4;
+  constexpr int K = GSW_PULL_TM_K;
   const int64_t n = as.get_size();
   GSW_HALT_IF_EMPTY(n);
   const Status want = conf.want();

@@ -28,7 +28,10 @@ constexpr int INSPECT_VBLOCK = 512;          // virtual threads per virtual bloc
 constexpr int INSPECT_NVB = INSPECT_VTHREADS / INSPECT_VBLOCK;
 constexpr int INSPECT_SPAN = 4;              // consecutive vertices a physical thread takes per step
 constexpr int INSPECT_OWNERS = INSPECT_VBLOCK / INSPECT_SPAN;  // 128 threads cover one virtual block
-constexpr int INSPECT_PARTS = 2;             // thread groups of a CTA taking alternate steps
+#ifndef GSW_INSPECT_PARTS
+#define GSW_INSPECT_PARTS 2
+#endif
+constexpr int INSPECT_PARTS = GSW_INSPECT_PARTS;  // thread groups of a CTA taking alternate steps
 constexpr int INSPECT_THREADS = INSPECT_OWNERS * INSPECT_PARTS;
 constexpr int INSPECT_SCRATCH_U32 = 2 * INSPECT_VTHREADS + INSPECT_NVB;
 constexpr int INSPECT_SCRATCH_U64 = (INSPECT_SCRATCH_U32 + 1) / 2;
@@ -173,16 +176,21 @@ __global__ void __launch_bounds__(INSPECT_THREADS, GSW_INSPECT_MINBLOCKS)
         steps(std::false_type{}, k);
     }
 
-    // fold the segment: group 1 hands its maxima to group 0, which publishes
-    if (part == 1)
+    // fold the segment: the other groups hand their maxima to group 0,
+    // which publishes
+    for (unsigned h = 1; h < INSPECT_PARTS; ++h) {
+      if (part == h)
 #pragma unroll
-      for (int i = 0; i < INSPECT_SPAN; ++i) s_mp[q][i] = mp[i], s_ml[q][i] = ml[i];
-    __syncthreads();
+        for (int i = 0; i < INSPECT_SPAN; ++i)
+          s_mp[q][i] = h == 1 ? mp[i] : max(s_mp[q][i], mp[i]), s_ml[q][i] = h == 1 ? ml[i] : max(s_ml[q][i], ml[i]);
+      __syncthreads();
+    }
     if (part == 0) {
       unsigned *vp = vmax + b * INSPECT_VBLOCK + INSPECT_SPAN * q;
 #pragma unroll
       for (int i = 0; i < INSPECT_SPAN; ++i) {
-        const unsigned a = max(mp[i], s_mp[q][i]), c = max(ml[i], s_ml[q][i]);
+        const unsigned a = INSPECT_PARTS > 1 ? max(mp[i], s_mp[q][i]) : mp[i];
+        const unsigned c = INSPECT_PARTS > 1 ? max(ml[i], s_ml[q][i]) : ml[i];
         if (a) atomicMax(vp + i, a);
         if (c) atomicMax(vp + INSPECT_VTHREADS + i, c);
       }
@@ -211,15 +219,24 @@ __global__ void __launch_bounds__(INSPECT_THREADS, GSW_INSPECT_MINBLOCKS)
     u += k1 - k0;
   }
 
-  unsigned long long r;
-  r = block_reduce((unsigned long long)active_num, s_red);
-  if (threadIdx.x == 0 && r) atomicAdd(info + 0, r);
-  r = block_reduce((unsigned long long)inactive_num, s_red);
-  if (threadIdx.x == 0 && r) atomicAdd(info + 1, r);
-  r = block_reduce(push_wl, s_red);
-  if (threadIdx.x == 0 && r) atomicAdd(info + 2, r);
-  r = block_reduce(pull_wl, s_red);
-  if (threadIdx.x == 0 && r) atomicAdd(info + 3, r);
+  // the four counters in one block reduction
+  {
+    unsigned long long c4[4] = {active_num, inactive_num, push_wl, pull_wl};
+    __shared__ unsigned long long s_c4[INSPECT_THREADS / 32][4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) c4[i] = warp_sum(c4[i]);
+    if (lane == 0)
+#pragma unroll
+      for (int i = 0; i < 4; ++i) s_c4[warp_id()][i] = c4[i];
+    __syncthreads();
+    if (threadIdx.x < 4) {
+      unsigned long long t = 0;
+      for (int w = 0; w < INSPECT_THREADS / 32; ++w) t += s_c4[w][threadIdx.x];
+      if (t) atomicAdd(info + threadIdx.x, t);
+      __threadfence();
+    }
+    __syncthreads();
+  }
   if (threadIdx.x == 0) {
     __threadfence();
     s_last = atomicAdd(info + 6, 1ull) == (unsigned long long)gridDim.x - 1;

@@ -1,6 +1,10 @@
 """Small fixed workloads for profiler captures (ncu -k ... python -m
 gswitch_b200.profile_cases <case>):
   bfs   three BFS runs on RMAT scale 22 (ef 16, seed 1), learned selector
+  bfs24 one BFS on RMAT scale 24 (ef 16, seed 1: the bench graph), learned
+        selector
+  sssp  SSSP on the 4096 x 4096 grid with 1% long-range edges (weights
+        U[1, 1000]), Push-Queue-WM-Fused levels one launch each
   pr    two PageRank iterations on RMAT scale 22, Pull-Bitmap-STRICT then 2D
   mbfs  batched 256-source BFS on RMAT scale 20
 """
@@ -24,6 +28,14 @@ def main(case: str) -> None:
         g = ctx.rmat(22, 16, seed=1)
         for r in g.roots(1000, 3):
             g.bfs(int(r), gs.RunOpts(selector="mlp"), out=False)
+    elif case == "bfs24":
+        g = ctx.rmat(24, 16, seed=1)
+        g.bfs(int(g.roots(1000, 1)[0]), gs.RunOpts(selector="mlp"), out=False)
+    elif case == "sssp":
+        g = ctx.grid(4096, 4096, 100, seed=1, wmax=1000, wseed=5)
+        o = gs.RunOpts.from_config("Push-Queue-WM-Fused")
+        o.persistent = False
+        g.sssp(int(g.roots(3, 1)[0]), o, out=False)
     elif case == "pr":
         g = ctx.rmat(22, 16, seed=1)
         g.pagerank(2, 0.85, 0.0, opts="Pull-Bitmap-STRICT", out=False)
@@ -32,7 +44,7 @@ def main(case: str) -> None:
         g = ctx.rmat(20, 16, seed=1)
         g.mbfs(g.roots(77, 256), batched=True, out=False)
     else:
-        raise SystemExit(f"unknown case {case!r} (bfs, pr, mbfs)")
+        raise SystemExit(f"unknown case {case!r} (bfs, bfs24, sssp, pr, mbfs)")
     print("ok", case)
     g.close()
     ctx.close()
