@@ -347,6 +347,46 @@ class host_graph_t<CSR, E> {
     attr.fill(odegrees, nvertexs);
   }
 
+  // Binary CSR cache (src/utils/fileIO.cuh:334-387): "<dir>/.csr_<file>"
+  // holds int nvertexs, int nedges, bool directed, bool with_weight, then
+  // odegrees[n], start_pos[n], adj_list[m] (+ edge_weights[m]) and, for
+  // directed graphs, the same four arrays of the reverse graph -- the
+  // reference's byte layout, so either side reads the other's cache.  An
+  // existing cache is left as it is; loading a missing one exits(1), both as
+  // the reference does.  A path without a directory resolves to ".".
+  static std::string binfile_path(const std::string &fname) {
+    const size_t k = fname.find_last_of('/');
+    const std::string dir = k == std::string::npos ? "." : fname.substr(0, k);
+    const std::string base = k == std::string::npos ? fname : fname.substr(k + 1);
+    return dir + "/.csr_" + base;
+  }
+  void store_to_binfile(std::string fname) {
+    const std::string fpath = binfile_path(fname);
+    if (FILE *chk = fopen(fpath.c_str(), "rb")) {
+      fclose(chk);
+      return;
+    }
+    std::ofstream fout(fpath, std::ios::binary);
+    fout.write((const char *)&nvertexs, sizeof(nvertexs));
+    fout.write((const char *)&nedges, sizeof(nvertexs));
+    fout.write((const char *)&directed, sizeof(directed));
+    fout.write((const char *)&with_weight, sizeof(with_weight));
+    write_side(fout, odegrees, start_pos, adj_list, edge_weights);
+    if (directed) write_side(fout, r_odegrees, r_start_pos, r_adj_list, r_edge_weights);
+  }
+  void load_from_binfile(std::string fname) {
+    const std::string fpath = binfile_path(fname);
+    std::ifstream fin(fpath, std::ios::binary);
+    if (!fin) exit(1);
+    fin.read((char *)&nvertexs, sizeof(nvertexs));
+    fin.read((char *)&nedges, sizeof(nvertexs));
+    fin.read((char *)&directed, sizeof(directed));
+    fin.read((char *)&with_weight, sizeof(with_weight));
+    read_side(fin, odegrees, start_pos, adj_list, edge_weights);
+    if (directed) read_side(fin, r_odegrees, r_start_pos, r_adj_list, r_edge_weights);
+    attr.fill(odegrees, nvertexs);
+  }
+
   // a random vertex with out-edges (C library random(), as the reference)
   int random_root() {
     while (true) {
@@ -356,6 +396,24 @@ class host_graph_t<CSR, E> {
   }
 
  private:
+  void write_side(std::ofstream &out, const int *deg, const int *sp, const int *adj, const E *w) const {
+    out.write((const char *)deg, sizeof(int) * nvertexs);
+    out.write((const char *)sp, sizeof(int) * nvertexs);
+    out.write((const char *)adj, sizeof(int) * nedges);
+    if (with_weight) out.write((const char *)w, sizeof(E) * nedges);
+  }
+  void read_side(std::ifstream &in, int *&deg, int *&sp, int *&adj, E *&w) {
+    free(deg), free(sp), free(adj), free(w);
+    deg = (int *)malloc(sizeof(int) * std::max(nvertexs, 1));
+    sp = (int *)malloc(sizeof(int) * (nvertexs + 1));
+    adj = (int *)malloc(sizeof(int) * std::max(nedges, 1));
+    w = with_weight ? (E *)malloc(sizeof(E) * std::max(nedges, 1)) : nullptr;
+    in.read((char *)deg, sizeof(int) * nvertexs);
+    in.read((char *)sp, sizeof(int) * nvertexs);
+    in.read((char *)adj, sizeof(int) * nedges);
+    if (with_weight) in.read((char *)w, sizeof(E) * nedges);
+    sp[nvertexs] = nedges;
+  }
   void prefix(int *sp, int *deg) {
     sp[0] = 0;
     for (int i = 1; i <= nvertexs; ++i) sp[i] = sp[i - 1] + deg[i - 1];
