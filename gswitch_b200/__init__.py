@@ -39,7 +39,7 @@ ABI_SYMBOLS = (
     "gsw_pagerank", "gsw_bc", "gsw_gc", "gsw_mbfs", "gsw_bfs_strict_noalloc",
     "gsw_graph_generate_powerlaw", "gsw_label_levels", "gsw_mlp_train", "gsw_mlp_grad", "gsw_mlp_infer",
     "gsw_mlp_load", "gsw_graph_generate_er_batch", "gsw_bfs_multi", "gsw_bfs_inspect", "gsw_tune_load",
-    "gsw_tune_save", "gsw_mlp_load_fusion",
+    "gsw_tune_save", "gsw_mlp_load_fusion", "gsw_pagerank_delta",
 )
 TUNE_ENTRIES = 64
 
@@ -112,6 +112,7 @@ def lib():
     L.gsw_sssp.argtypes = [vp, vp, i32, po, vp, ps]
     L.gsw_cc.argtypes = [vp, vp, po, vp, ps]
     L.gsw_pagerank.argtypes = [vp, vp, po, vp, ps]
+    L.gsw_pagerank_delta.argtypes = [vp, vp, po, vp, ps]
     L.gsw_bc.argtypes = [vp, vp, i32, po, vp, vp, ps]
     L.gsw_gc.argtypes = [vp, vp, po, vp, ps]
     L.gsw_mbfs.argtypes = [vp, vp, C.c_int, vp, C.c_int, po, vp, ps]
@@ -427,6 +428,15 @@ class Graph:
         opts.max_iters, opts.damping, opts.eps = iters, damping, eps
         pr = np.empty(self.n, dtype=np.float32) if out else None
         st = self._run(lib().gsw_pagerank, outs=[pr], opts=opts)
+        return pr, st
+
+    def pagerank_delta(self, eps=1e-4, damping=0.85, max_levels=0, opts=None, out=True):
+        """Delta-PageRank (gsw_pagerank_delta): the values pr (not pr/od)."""
+        if opts is None or isinstance(opts, str):
+            opts = RunOpts.from_config(opts) if isinstance(opts, str) else RunOpts()
+        opts.max_iters, opts.damping, opts.eps = max_levels, damping, eps
+        pr = np.empty(self.n, dtype=np.float32) if out else None
+        st = self._run(lib().gsw_pagerank_delta, outs=[pr], opts=opts)
         return pr, st
 
     def label(self, app, root=0, max_levels=64, pr_iters=3):

@@ -106,6 +106,42 @@ struct PR : Functor<VC, float, float, Empty> {
   }
 };
 
+// Delta-PageRank (the variant described at docs/index.md:178; the reference
+// ships no code for it): wa = change accumulated from in-neighbours since the
+// vertex last sent, ra = the message it sends to each out-neighbour, pr =
+// the PageRank value (the reference's unnormalised form, pr = (1-d) +
+// d * sum pr[u]/od[u]).  A vertex whose accumulated change exceeds eps times
+// its value adds the change to its value and becomes active; an active
+// vertex sends d * change / od to every out-neighbour, which accumulate it.
+// Every change is positive, so pr rises monotonically to within
+// eps / (1 - d) (normalised L1) of the fixed point.  Activation depends on a
+// whole level's accumulated change, which only the inspection's filter pass
+// sees, so this functor runs standalone levels only.
+struct PRDelta : Functor<VC, float, float, Empty> {
+  float damp = 0.85f;
+  float eps = 0.01f;
+  float *pr = nullptr;
+  __device__ __forceinline__ Status filter(int v, GE g) {
+    float *acc = wa_of(v);
+    const float a = *acc;
+    if (!(a > eps * pr[v])) return Inactive;
+    *acc = 0;
+    pr[v] += a;
+    const int od = g.get_out_degree(v);
+    *ra_of(v) = od ? damp * a / od : 0.0f;
+    return Active;
+  }
+  __device__ __forceinline__ float emit(int v, Empty *, GE) { return *ra_of(v); }
+  __device__ __forceinline__ bool comp(float *v, float nv, GE) {
+    *v += nv;
+    return true;
+  }
+  __device__ __forceinline__ bool compAtomic(float *v, float nv, GE) {
+    atomicAdd(v, nv);
+    return true;
+  }
+};
+
 // application/bc.cu:175-243 - forward: (level, path count); backward:
 // (path count, dependency) with the forward level as read-only data.
 struct fwdata_t {

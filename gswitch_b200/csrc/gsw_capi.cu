@@ -1735,6 +1735,102 @@ gsw_status gsw_pagerank(gsw_ctx *ctx, gsw_graph *gr, const gsw_run_opts *o, floa
 }
 
 // ---------------------------------------------------------------------------
+// Delta-PageRank (docs/index.md:178 of the reference describes it; its code
+// has none): the PageRank level loop above with the PRDelta functor.  Level 0
+// has every vertex send (1-d) worth of value; afterwards only vertices whose
+// accumulated change passed the threshold send.  The loop ends when no
+// vertex is active (or after max_iters levels when that is positive).
+// edges = out-edges of the vertices that sent, summed over levels.
+// ---------------------------------------------------------------------------
+__global__ void k_prd_init(const int *odeg, int64_t n, float damp, float *pr, float *ra, float *wa) {
+  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
+    pr[v] = 1 - damp;
+    ra[v] = odeg[v] ? damp * (1 - damp) / odeg[v] : 0.0f;
+    wa[v] = 0.0f;
+  }
+}
+
+gsw_status gsw_pagerank_delta(gsw_ctx *ctx, gsw_graph *gr, const gsw_run_opts *o, float *pr, gsw_run_stats *st) {
+  entry_guard eg(ctx);
+  if (!ctx || !gr) return fail(GSW_ERR_INVALID_ARG, "gsw_pagerank_delta: bad arguments");
+  if (o && o->captured) return fail(GSW_ERR_UNSUPPORTED, "gsw_pagerank_delta: no captured level loop");
+  begin_stats(st);
+  gsw_run_opts def;
+  gsw_run_opts_default(&def);
+  const gsw_run_opts *op = o ? o : &def;
+  if (op->eps <= 0 || op->damping <= 0 || op->damping >= 1)
+    return fail(GSW_ERR_INVALID_ARG, "gsw_pagerank_delta: need eps > 0 and 0 < damping < 1");
+  auto g = gr->view<Empty>();
+  app::PRDelta f;
+  f.damp = op->damping;
+  f.eps = op->eps;
+  f.data.size = gr->n;
+  f.data.dg_wa = (float *)ctx->buf("wa", sizeof(float) * (gr->n + 1));
+  f.data.dg_ra = (float *)ctx->buf("ra", sizeof(float) * (gr->n + 1));
+  f.pr = (float *)ctx->buf("prd", sizeof(float) * (gr->n + 1));
+  if (!f.data.dg_wa || !f.data.dg_ra || !f.pr) return eg.finish();
+  k_prd_init<<<grid_for(gr->n), 256, 0, stream()>>>(gr->odeg, gr->n, f.damp, f.pr, f.data.dg_ra, f.data.dg_wa);
+  f.data.zero = 0.0f;
+  feature_t fets;
+  config_t conf;
+  stat_t &stats = ctx->stats;
+  stats.clean();
+  inspector_t inspector;
+  selector_t selector;
+  executor_t &executor = ctx->executor;
+  executor.insp = &inspector;
+  executor.twod = twod_layout();
+  const int64_t plv0 = executor.persistent_levels, pln0 = executor.persistent_launches;
+  fets.centric = VC;
+  fets.pattern = ASSO;
+  fets.fromall = false;
+  fets.toall = true;
+  apply_opts(op, conf);
+  // Standalone levels only: a fused level enqueues the targets whose update
+  // reports success, but here a vertex becomes active only once everything a
+  // level sent it has been summed, which the inspection's filter pass sees
+  if (conf.force.has_fusion && conf.force.fusion == Fused)
+    return fail(GSW_ERR_UNSUPPORTED, "gsw_pagerank_delta: standalone levels only");
+  conf.force.has_fusion = true;
+  conf.force.fusion = Standalone;
+  set_graph_features(fets, gr);
+  init_conf_impl(stats, fets, conf, g, f, 0.0, gr->attr[0], false);
+  active_set_t *asp = ctx->aset(gr->n, conf.conf_qmode);
+  if (!asp) return eg.finish();
+  active_set_t &as = *asp;
+  as.reset();
+  as.init(ALL_ACTIVE);
+  loop_trace tr{st, MAX_LEVELS};
+  const int cap = op->max_iters > 0 ? op->max_iters : MAX_LEVELS;
+  int64_t work = 0;
+  timer tm(ctx);
+  for (int level = 0; ok(); level++) {
+    const bool inspected = level > 0 && !conf.conf_fuse_inspect;
+    inspector.inspect(as, g, f, stats, fets, conf);
+    if (level == cap) break;
+    if (finish(as, g, f, conf)) break;
+    work += level == 0 ? gr->m : (inspected ? stats.push_workload() : 0);
+    select_level(ctx, op, selector, stats, fets, conf);
+    executor.filter(as, g, f, stats, fets, conf);
+    g.update_level();
+    tr.level(conf, hints().frontier);
+    executor.expand(as, g, f, stats, fets, conf);
+    tr.done(stats);
+  }
+  const double ms = tm.stop();
+  tr.resolve();
+  end_checks(&as, st);
+  add_persistent_levels(st, executor, plv0, pln0);
+  if (st) {
+    st->ms = ms;
+    st->edges = work;
+  }
+  if (pr && ok()) GSW_CUDA(cudaMemcpyAsync(pr, f.pr, sizeof(float) * gr->n, cudaMemcpyDeviceToHost, stream()));
+  GSW_CUDA(cudaStreamSynchronize(stream()));
+  return eg.finish();
+}
+
+// ---------------------------------------------------------------------------
 // BC: application/bc.cu:246-309 (both phases) and :391-431 (set-up).  The
 // cached queue that replays the forward levels backwards is kept for every
 // start (the reference drops to a Normal queue when its fusion tree picks the

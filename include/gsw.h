@@ -185,6 +185,14 @@ gsw_status gsw_sssp(gsw_ctx *ctx, gsw_graph *g, int32_t root, const gsw_run_opts
                     gsw_run_stats *st);
 gsw_status gsw_cc(gsw_ctx *ctx, gsw_graph *g, const gsw_run_opts *o, int32_t *labels, gsw_run_stats *st);
 gsw_status gsw_pagerank(gsw_ctx *ctx, gsw_graph *g, const gsw_run_opts *o, float *pr_over_od, gsw_run_stats *st);
+/* Delta-PageRank: no reference function corresponds (the reference's
+ * docs/index.md:178 describes the algorithm; its code has none).  Same
+ * fixed point as gsw_pagerank in the unnormalised form pr = (1-d) +
+ * d * sum pr[u]/od[u]; a vertex sends only the change it accumulated, once
+ * that change exceeds o->eps times its value (o->damping = d; o->max_iters
+ * > 0 caps the levels).  pr receives the values themselves (not pr/od);
+ * st->edges counts the out-edges of the vertices that sent. */
+gsw_status gsw_pagerank_delta(gsw_ctx *ctx, gsw_graph *g, const gsw_run_opts *o, float *pr, gsw_run_stats *st);
 gsw_status gsw_bc(gsw_ctx *ctx, gsw_graph *g, int32_t root, const gsw_run_opts *o, int32_t *nsp, float *dep,
                   gsw_run_stats *st);
 gsw_status gsw_gc(gsw_ctx *ctx, gsw_graph *g, const gsw_run_opts *o, int32_t *colors, gsw_run_stats *st);
