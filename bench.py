@@ -128,9 +128,15 @@ def level_bytes(kind, n, A, U, D, E):
 
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per vertex of
 # one inspection launch, from the ncu capture summarised in
-# profiles/bfs_rmat22_inspect_pulltm.md (33.60 MB over 4,194,304 vertices);
-# the inspection streams every vertex once, so a launch's traffic scales with n
-INSPECT_TRAFFIC_PER_VERTEX = 33.60e6 / 4194304
+# profiles/bfs_rmat24_inspect_pulltm.md (135.47 MB + 5.62 MB over 16,777,216
+# vertices); the inspection streams every vertex once, so a launch's traffic
+# scales with n
+INSPECT_TRAFFIC_PER_VERTEX = (135.47e6 + 5.62e6) / 16777216
+# DRAM bytes per launch of the thread-mapped pull expand on the bench graph
+# (RMAT scale 24 ef 16 seed 1): the mean of the two launches of one BFS in the
+# same capture (600.38 MB and 329.71 MB); per-launch traffic depends on the
+# level, so this figure stands for the bench graph only
+PULL_TM_TRAFFIC_RMAT24 = (600.38e6 + 329.71e6) / 2
 
 
 def roofline_from(runs, n, peak_gbs, peak_kind):
@@ -156,18 +162,32 @@ def roofline_from(runs, n, peak_gbs, peak_kind):
                 rec[0] += timed.level_inspect_ms[i]
                 rec[1] += 8.0 * n + n / 4.0  # level + degree read, two bitmap words written
                 rec[2] += 1
-    dom = max(per.items(), key=lambda kv: kv[1][0])
-    name, (ms, byt, launches) = dom
-    achieved = byt / (ms * 1e-3) / 1e9 if ms > 0 else 0.0
     shares = {k: round(v[0] / sum(x[0] for x in per.values()), 4) for k, v in per.items()}
-    return {"bound": "hbm", "kernel": name, "achieved": round(achieved, 1), "peak": peak_gbs,
-            "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak_gbs, 4),
-            "bytes_per_launch": round(byt / max(launches, 1)), "launches": launches,
-            "avg_launch_ms": round(ms / max(launches, 1), 5),
-            "traffic": round(INSPECT_TRAFFIC_PER_VERTEX * n) if name == "inspect" else None,
-            "traffic_note": ("ncu DRAM bytes of one inspection at scale 22 scaled by vertices"
-                             if name == "inspect" else "no per-launch ncu figure for this kernel's level mix"),
-            "time_shares": shares}
+
+    def line(name):
+        ms, byt, launches = per[name]
+        achieved = byt / (ms * 1e-3) / 1e9 if ms > 0 else 0.0
+        if name == "inspect":
+            traffic = round(INSPECT_TRAFFIC_PER_VERTEX * n)
+            note = "ncu DRAM bytes of one inspection on the bench graph, per vertex, times n"
+        elif name == "expand Pull-Bitmap-TM-Standalone" and n == 1 << 24:
+            traffic = round(PULL_TM_TRAFFIC_RMAT24)
+            note = ("ncu DRAM bytes per launch on the bench graph (mean of one BFS's two pull levels); above the "
+                    "algorithmic bytes because each candidate's first in-neighbour costs a 32-byte sector")
+        else:
+            traffic, note = None, "no per-launch ncu figure for this kernel's level mix"
+        return {"bound": "hbm", "kernel": name, "achieved": round(achieved, 1), "peak": peak_gbs,
+                "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak_gbs, 4),
+                "bytes_per_launch": round(byt / max(launches, 1)), "launches": launches,
+                "avg_launch_ms": round(ms / max(launches, 1), 5), "traffic": traffic, "traffic_note": note}
+
+    dom = max(per.items(), key=lambda kv: kv[1][0])[0]
+    out = line(dom)
+    out["time_shares"] = shares
+    # the other kernels above a tenth of the time, same arithmetic
+    out["others"] = [line(k) for k, v in sorted(per.items(), key=lambda kv: -kv[1][0])
+                     if k != dom and shares[k] >= 0.1]
+    return out
 
 
 def run_opts(gs, selector, **kw):
