@@ -9,6 +9,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <map>
+#include <unordered_map>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -82,6 +83,56 @@ struct gsw_ctx {
   mlp_model mlp{};                // learned selector (valid = 0: none loaded)
   mlp_model mlp_fusion{};         // learned fusion decision of Mono-pattern runs
   mlp_model *dmlp = nullptr;      // its device copy (captured loops)
+
+  // Device blocks of destroyed graphs, kept for the next graph of a fitting
+  // size: a graph uploaded per call otherwise pays a fresh cudaMalloc and
+  // cudaFree's device-wide synchronisation every time (about 10 ms for a
+  // 2.2 GB CSR).  Blocks go back to the pool on graph destroy (stream order
+  // on the context's one stream keeps a reused block from being overwritten
+  // while a kernel still reads it); the pool keeps at most GRAPH_POOL_CAP
+  // bytes, gives back all of it when an allocation fails, and is freed with
+  // the context.
+  static constexpr size_t GRAPH_POOL_CAP = (size_t)48 << 30;
+  std::multimap<size_t, void *> graph_pool;     // free blocks by size
+  std::unordered_map<void *, size_t> graph_blocks;  // every pool-managed block
+  size_t graph_pool_bytes = 0;
+  void graph_pool_trim() {
+    for (auto &kv : graph_pool) {
+      graph_blocks.erase(kv.second);
+      cudaFree(kv.second);
+    }
+    graph_pool.clear();
+    graph_pool_bytes = 0;
+  }
+  void *graph_alloc(size_t bytes) {
+    bytes = bytes ? bytes : 1;
+    auto it = graph_pool.lower_bound(bytes);
+    if (it != graph_pool.end() && it->first <= bytes + bytes / 4) {  // at most a quarter unused
+      void *p = it->second;
+      graph_pool_bytes -= it->first;
+      graph_pool.erase(it);
+      return p;
+    }
+    void *p = nullptr;
+    if (cudaMalloc(&p, bytes) != cudaSuccess) {
+      cudaGetLastError();
+      graph_pool_trim();
+      if (GSW_CUDA(cudaMalloc(&p, bytes))) return nullptr;
+    }
+    graph_blocks[p] = bytes;
+    return p;
+  }
+  void graph_free(void *p) {
+    if (!p) return;
+    auto it = graph_blocks.find(p);
+    if (it == graph_blocks.end() || graph_pool_bytes + it->second > GRAPH_POOL_CAP) {
+      if (it != graph_blocks.end()) graph_blocks.erase(it);
+      cudaFree(p);
+      return;
+    }
+    graph_pool.emplace(it->second, p);
+    graph_pool_bytes += it->second;
+  }
 
   void *buf(const std::string &name, size_t bytes) {
     auto it = bufs.find(name);
@@ -237,7 +288,7 @@ __global__ void k_sum_weights(const int *w, int64_t m, unsigned long long *out) 
 void finalize_graph(gsw_graph *g) {
   int64_t *off = g->off;
   if (!g->odeg) {
-    if (GSW_CUDA(cudaMalloc((void **)&g->odeg, sizeof(int) * (g->n + 1)))) return;
+    if (!(g->odeg = (int *)g->ctx->graph_alloc(sizeof(int) * (g->n + 1)))) return;
     k_deg_to_i32<<<grid_for(g->n), 256, 0, stream()>>>(off, g->n, g->odeg);
     GSW_LAUNCHED();
   }
@@ -284,8 +335,8 @@ int csr_from_keys(gsw_graph *g, uint64_t *keys, int64_t nkeys) {
   cudaFree(flag);
   cudaFree(pos);
   g->m = m;
-  if (GSW_CUDA(cudaMalloc((void **)&g->col, sizeof(int) * ((size_t)m + 1)))) return err().code;
-  if (GSW_CUDA(cudaMalloc((void **)&g->off, sizeof(int64_t) * (g->n + 1)))) return err().code;
+  if (!(g->col = (int *)g->ctx->graph_alloc(sizeof(int) * ((size_t)m + 1)))) return err().code;
+  if (!(g->off = (int64_t *)g->ctx->graph_alloc(sizeof(int64_t) * (g->n + 1)))) return err().code;
   unsigned long long *deg = (unsigned long long *)g->off;  // count into off[1..n]
   GSW_CUDA(cudaMemsetAsync(g->off, 0, sizeof(int64_t) * (g->n + 1), stream()));
   k_split_keys<<<grid_for(m), 256, 0, stream()>>>(keys, m, g->col, deg + 1);
@@ -316,14 +367,9 @@ gsw_graph *new_graph(gsw_ctx *ctx, int64_t n) {
 
 void free_graph(gsw_graph *g) {
   if (!g) return;
-  cudaFree(g->off);
-  cudaFree(g->col);
-  cudaFree(g->odeg);
-  cudaFree(g->w);
-  cudaFree(g->roff);
-  cudaFree(g->rcol);
-  cudaFree(g->rdeg);
-  cudaFree(g->rw);
+  for (void *p : {(void *)g->off, (void *)g->col, (void *)g->odeg, (void *)g->w, (void *)g->roff, (void *)g->rcol,
+                  (void *)g->rdeg, (void *)g->rw})
+    g->ctx->graph_free(p);
   cudaFree(g->coo);
   if (g->twod) {
     cudaFree(g->twod->edge);
@@ -343,7 +389,7 @@ void free_graph(gsw_graph *g) {
 
 int add_weights(gsw_graph *g, int wmax, uint64_t wseed) {
   if (wmax <= 0) return GSW_OK;
-  if (GSW_CUDA(cudaMalloc((void **)&g->w, sizeof(int) * ((size_t)g->m + 1)))) return err().code;
+  if (!(g->w = (int *)g->ctx->graph_alloc(sizeof(int) * ((size_t)g->m + 1)))) return err().code;
   k_weights<<<grid_for(g->n), 256, 0, stream()>>>(g->off, g->col, g->n, stream_key(wseed, ST_W), wmax, g->w);
   g->weighted = true;
   return GSW_LAUNCHED();
@@ -1082,6 +1128,7 @@ gsw_status gsw_destroy(gsw_ctx *ctx) {
   cudaStreamSynchronize(ctx->stream);
   for (auto &kv : ctx->as_cache) kv.second.destroy();
   for (auto &kv : ctx->bufs) cudaFree(kv.second.first);
+  ctx->graph_pool_trim();
   for (auto &kv : ctx->dl) kv.second.destroy();
   cudaFree(ctx->dtrees);
   cudaFree(ctx->dmlp);
@@ -1107,7 +1154,7 @@ gsw_status gsw_graph_upload(gsw_ctx *ctx, int64_t n, int64_t m, const int64_t *r
   g->directed = directed != 0;
   g->weighted = weights != nullptr;
   auto up = [&](void **dst, const void *src, size_t bytes) {
-    if (GSW_CUDA(cudaMalloc(dst, bytes ? bytes : 1))) return false;
+    if (!(*dst = ctx->graph_alloc(bytes))) return false;
     if (bytes && GSW_CUDA(cudaMemcpyAsync(*dst, src, bytes, cudaMemcpyHostToDevice, stream()))) return false;
     return true;
   };
@@ -1130,7 +1177,7 @@ gsw_status gsw_graph_upload(gsw_ctx *ctx, int64_t n, int64_t m, const int64_t *r
           up((void **)&g->rcol, rcol.data(), sizeof(int) * m);
     if (okk && weights) okk = up((void **)&g->rw, rw.data(), sizeof(int) * m);
     if (okk) {
-      okk = GSW_CUDA(cudaMalloc((void **)&g->rdeg, sizeof(int) * (n + 1))) == GSW_OK;
+      okk = (g->rdeg = (int *)ctx->graph_alloc(sizeof(int) * (n + 1))) != nullptr;
       if (okk) k_deg_to_i32<<<grid_for(n), 256, 0, stream()>>>(g->roff, n, g->rdeg);
     }
     GSW_CUDA(cudaStreamSynchronize(stream()));

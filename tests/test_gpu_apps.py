@@ -311,3 +311,25 @@ def test_inspection_counters_on_multi_step_sizes(ctx):
         for level in (0, 1, 2, 3, 5):
             assert np.array_equal(g.bfs_inspect(lv, level), oracle.inspect_bfs(h, lv, level)), (h.n, level)
         g.close()
+
+
+def test_graph_blocks_reused_across_uploads(ctx, big):
+    """Destroyed graphs hand their device blocks to the next upload of a
+    fitting size; stale contents of a reused block must not leak into the
+    next graph's results."""
+    h, hw, root = big["rmat14"]
+    ref = oracle.bfs(h, root)
+    for _ in range(3):
+        g = ctx.upload(h.off, h.col)
+        lv, _ = g.bfs(root)
+        assert np.array_equal(lv, ref)
+        g.close()
+    # a slightly smaller graph reuses the larger one's blocks (within a quarter)
+    sub = oracle.er(h.n - 100, int(h.m // 2 * 0.9), seed=11)
+    r2 = int(oracle.roots(sub, 4, 1)[0])
+    g = ctx.upload(sub.off, sub.col)
+    lv, _ = g.bfs(r2)
+    assert np.array_equal(lv, oracle.bfs(sub, r2))
+    d, _ = ctx.upload(hw.off, hw.col, hw.w).sssp(root)
+    assert np.array_equal(d, oracle.sssp_dijkstra(hw, root))
+    g.close()
