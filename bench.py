@@ -261,15 +261,16 @@ def run_ours(args):
     clocks = sampler.stop()
     ms = e0.elapsed_time(e1)
     barrier()
-    ms_max, tot_edges = ms, edges
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_max = float(t.item())
-        t = torch.tensor([edges], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.SUM)
-        tot_edges = int(t.item())
+    ms_max, tot_edges = combine_ranks(dist, ms, edges, "cuda")
     value = tot_edges / (ms_max * 1e6)
+    # end to end through the C ABI on every rank (replicas), combined the same way
+    e2e_out = None
+    if not args.no_e2e:
+        e2e_ms, e2e_edges, e2e_steps, h2d, d2h = e2e(ctx, g, roots[W:W + min(K, 20)], gs, torch, selector)
+        e2e_ms, e2e_edges = combine_ranks(dist, e2e_ms, e2e_edges, "cuda")
+        e2e_out = {"value": round(e2e_edges / (e2e_ms * 1e6), 3), "unit": "GTEPS",
+                   "ms_per_step": round(e2e_ms / e2e_steps, 3), "h2d_bytes_per_step": h2d,
+                   "d2h_bytes_per_step": d2h}
 
     out = None
     if rank == 0:
@@ -301,8 +302,8 @@ def run_ours(args):
         }
         if world == 1 and not args.no_apps:
             out["apps"] = app_table(ctx, g, gs, args, roots[W:W + 3], selector)
-        if not args.no_e2e:
-            out["e2e"] = e2e(ctx, g, roots[W:W + min(K, 20)], gs, torch, selector)
+        if e2e_out:
+            out["e2e"] = e2e_out
         if world == 1 and not args.no_cpu:
             out["cpu_baseline"] = cpu_baseline(g, roots, args.cpu_seconds)
     g.close()
@@ -493,9 +494,25 @@ def er_batch_entry(ctx, gs, selector):
     return res
 
 
+def combine_ranks(dist, ms, edges, device):
+    """The job's time and work over replicas: the max of the ranks' device
+    times and the sum of their traversed edges.  Every rank calls it, in the
+    same order; without a process group it returns its arguments."""
+    if not dist:
+        return ms, edges
+    import torch
+
+    t = torch.tensor([float(ms)], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e = torch.tensor([float(edges)], device=device, dtype=torch.float64)
+    dist.all_reduce(e, op=dist.ReduceOp.SUM)
+    return float(t.item()), int(e.item())
+
+
 def e2e(ctx, g, roots, gs, torch, selector="rules"):
     """BFS through the C ABI with host buffers: upload (pinned CSR) + BFS +
-    levels back to host, per step."""
+    levels back to host, per step.  Returns (device ms, traversed edges,
+    steps, host-to-device bytes per step, device-to-host bytes per step)."""
     off, col, _ = g.download()
     poff = torch.from_numpy(off).pin_memory().numpy()
     pcol = torch.from_numpy(col).pin_memory().numpy()
@@ -513,8 +530,7 @@ def e2e(ctx, g, roots, gs, torch, selector="rules"):
     e1.record(stream)
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
-    return {"value": round(edges / (ms * 1e6), 3), "unit": "GTEPS", "ms_per_step": round(ms / len(roots), 3),
-            "h2d_bytes_per_step": int(poff.nbytes + pcol.nbytes), "d2h_bytes_per_step": int(plev.nbytes)}
+    return ms, edges, len(roots), int(poff.nbytes + pcol.nbytes), int(plev.nbytes)
 
 
 def cpu_baseline(g, roots, budget_s):
