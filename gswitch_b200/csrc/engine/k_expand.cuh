@@ -506,17 +506,31 @@ __global__ void __launch_bounds__(256) k_strict_scan(active_set_t as, G g, Statu
   __syncthreads();
   int64_t off = bsum[blockIdx.x] + s[warp_id()] + incl - loc;
   int64_t *eoff = as.workset.dg_eoff;
+  auto own = [&](int64_t t, int item) {
+    if (t < tile_cap)
+      tile_lo[t] = item;
+    else
+      as.raise(DEV_ERR_SCRATCH_OVERFLOW);
+  };
+  const int lane = lane_id();
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
     const int64_t idx = base + k;
-    if (idx < n) {
-      eoff[idx] = off;
-      for (int64_t t = (off + STRICT_TILE - 1) / STRICT_TILE; t * STRICT_TILE < off + d[k]; ++t) {
-        if (t < tile_cap)
-          tile_lo[t] = (int)idx;
-        else
-          as.raise(DEV_ERR_SCRATCH_OVERFLOW);
-      }
+    const bool valid = idx < n;
+    if (valid) eoff[idx] = off;
+    // tiles whose first slot falls in [off, off + d): ta <= t < tb
+    const int64_t ta = (off + STRICT_TILE - 1) / STRICT_TILE;
+    const int64_t tb = valid ? (off + d[k] + STRICT_TILE - 1) / STRICT_TILE : ta;
+    // a hub owns many tiles, and a sorted frontier puts the hubs side by
+    // side: long runs are written by the whole warp, 32 tiles a step
+    const bool many = tb - ta > 2;
+    if (!many)
+      for (int64_t t = ta; t < tb; ++t) own(t, (int)idx);
+    for (unsigned pend = __ballot_sync(FULL, many); pend; pend &= pend - 1) {
+      const int src = __ffs(pend) - 1;
+      const int64_t a = __shfl_sync(FULL, ta, src), b = __shfl_sync(FULL, tb, src);
+      const int item = __shfl_sync(FULL, (int)idx, src);
+      for (int64_t t = a + lane; t < b; t += 32) own(t, item);
     }
     off += d[k];
   }
