@@ -314,6 +314,12 @@ struct config_t {
 struct stat_t {
   unsigned long long *dg_runtime_info = nullptr;
   unsigned long long *h_runtime_info = nullptr;
+  // Zero-copy report of a VC inspection (mapped pinned, 8 words): the
+  // kernel's last CTA writes the six counters to [0..5], clears the device
+  // counters for the next launch and then writes the launch's sequence
+  // number to [7]; the host polls [7] instead of copying and synchronising.
+  unsigned long long *h_sig = nullptr, *d_sig = nullptr;
+  unsigned long long sig_seq = 0;
   int size = 0;
   double last_time = 0, avg_time = 0;
   double last_filter_time = 0, last_expand_time = 0;
@@ -331,12 +337,39 @@ struct stat_t {
     GSW_CUDA(cudaMemsetAsync(dg_runtime_info, 0, bytes, gsw::stream()));
     GSW_CUDA(cudaMallocHost((void **)&h_runtime_info, size * sizeof(unsigned long long)));
     memset(h_runtime_info, 0, size * sizeof(unsigned long long));
+    if (GSW_CUDA(cudaHostAlloc((void **)&h_sig, 8 * sizeof(unsigned long long), cudaHostAllocMapped)) == 0) {
+      memset(h_sig, 0, 8 * sizeof(unsigned long long));
+      if (GSW_CUDA(cudaHostGetDevicePointer((void **)&d_sig, h_sig, 0))) d_sig = nullptr;
+    }
   }
   void destroy() {
     cudaFree(dg_runtime_info);
     cudaFreeHost(h_runtime_info);
+    if (h_sig) cudaFreeHost(h_sig);
     dg_runtime_info = nullptr;
     h_runtime_info = nullptr;
+    h_sig = d_sig = nullptr;
+  }
+  // sequence number for the next signalled inspection (0: no report block)
+  unsigned long long arm() { return d_sig ? ++sig_seq : 0; }
+  // Waits for the report of inspection `seq` and takes its counters.  Every
+  // 256 polls the stream is queried, so the wait ends when the stream runs
+  // dry; false then (or on an error), and the caller reads the device block.
+  bool await(unsigned long long seq) {
+    volatile unsigned long long *h = h_sig;
+    for (unsigned spin = 1;; ++spin) {
+      if (h[7] == seq) break;
+      if ((spin & 255) == 0) {
+        const cudaError_t q = cudaStreamQuery(gsw::stream());
+        if (q != cudaErrorNotReady) {
+          if (h[7] == seq) break;
+          if (q != cudaSuccess) GSW_CUDA(q);
+          return false;
+        }
+      }
+    }
+    for (int i = 0; i < 6; ++i) h_runtime_info[i] = h[i];
+    return true;
   }
   void reset() {}
   void collect(int num) {

@@ -56,9 +56,10 @@ inline int clamp_grid(int64_t want, int cap) {
 // the VC inspection on one wave of resident CTAs (no more CTAs than units)
 template <typename G, typename F>
 inline void launch_inspect_vc(const active_set_t &as, const G &g, const F &f, unsigned long long *info,
-                              const int *skip_if = nullptr) {
+                              const int *skip_if = nullptr, unsigned long long *sig = nullptr,
+                              unsigned long long seq = 0) {
   const int grid = clamp_grid(inspect_units(as.size), resident_grid(k_inspect_vc<G, F>, INSPECT_THREADS));
-  k_inspect_vc<G, F><<<grid, INSPECT_THREADS, 0, stream()>>>(as, g, f, info, skip_if);
+  k_inspect_vc<G, F><<<grid, INSPECT_THREADS, 0, stream()>>>(as, g, f, info, skip_if, sig, seq);
 }
 
 inline double now_ms() {
@@ -240,10 +241,11 @@ struct inspector_t {
     marks().insp0 = marks().insp1 = -1;
     if (need_inspect) {
       if (opts().timing) marks().insp0 = timing_pool().record();
-      launch_inspect_vc(as, g, f, stat.dg_runtime_info);
+      const unsigned long long seq = stat.arm();
+      launch_inspect_vc(as, g, f, stat.dg_runtime_info, nullptr, seq ? stat.d_sig : nullptr, seq);
       GSW_LAUNCHED();
       if (opts().timing) marks().insp1 = timing_pool().record();
-      set_fets(as, stat, fets, conf, g.nvertexs, g.nedges);
+      set_fets(as, stat, fets, conf, g.nvertexs, g.nedges, seq);
     }
     fets.flatten();
   }
@@ -276,10 +278,14 @@ struct inspector_t {
     keep(fets_first(fets, nvertexs, nedges));
   }
 
+  // seq != 0: the inspection reports through the mapped block (and left the
+  // device counters zeroed); otherwise copy them back and clear them
   void set_fets(active_set_t &as, stat_t &stat, feature_t &fets, const config_t &conf, int64_t nvertexs,
-                int64_t nedges) {
-    stat.collect(6);  // the one synchronisation of a standalone level
-    stat.clean();
+                int64_t nedges, unsigned long long seq = 0) {
+    if (!(seq && stat.await(seq))) {
+      stat.collect(6);  // the one synchronisation of a standalone level
+      stat.clean();
+    }
     const level_counts c = {stat.active_num(),    stat.unactive_num(),   stat.push_workload(),
                             stat.pull_workload(), stat.max_deg_active(), stat.max_deg_unactive()};
     keep(c);

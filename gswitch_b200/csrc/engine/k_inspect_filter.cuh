@@ -75,7 +75,8 @@ __host__ __device__ __forceinline__ int64_t inspect_units(int64_t n) { return (i
 // per-vertex bounds checks.
 template <typename G, typename F>
 __global__ void __launch_bounds__(INSPECT_THREADS, GSW_INSPECT_MINBLOCKS)
-    k_inspect_vc(active_set_t as, G g, F f, unsigned long long *info, const int *skip_if = nullptr) {
+    k_inspect_vc(active_set_t as, G g, F f, unsigned long long *info, const int *skip_if = nullptr,
+                 unsigned long long *sig = nullptr, unsigned long long seq = 0) {
   // captured loops: a level whose expand found an empty input ends the loop
   // before this inspection (the host loop stops there too)
   if (skip_if && *(volatile const int *)skip_if) return;
@@ -255,6 +256,17 @@ __global__ void __launch_bounds__(INSPECT_THREADS, GSW_INSPECT_MINBLOCKS)
     if (threadIdx.x == 0) {
       info[4] = mpx;
       info[5] = sp;
+      if (sig) {  // report to the mapped host block, leave zeroed counters behind
+        volatile unsigned long long *vi = info;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) sig[i] = vi[i];
+        sig[4] = mpx;
+        sig[5] = sp;
+#pragma unroll
+        for (int i = 0; i < 7; ++i) vi[i] = 0;
+        __threadfence_system();
+        *(volatile unsigned long long *)(sig + 7) = seq;
+      }
     }
   }
 }
