@@ -164,11 +164,16 @@ struct queue_t {
     return mode == Normal ? subqueue[cursor ^ 1].dg_qsize : subqueue[1].dg_queue + cursor + 1;
   }
   void reset(bool _traceback = false) {
-    traceback = _traceback;
     if (mode == Normal) {
       clean_size(0);
       clean_size(1);
     }
+    reset_host(_traceback);
+  }
+  // reset() without clearing the Normal-mode sizes (active_set_t::reset
+  // clears them in its own kernel)
+  void reset_host(bool _traceback) {
+    traceback = _traceback;
     if (!traceback) {
       cursor = 0;
       offset_in = offset_out = 0;
@@ -332,12 +337,39 @@ inline void active_set_t::destroy() {
   *this = active_set_t();
 }
 
+// the device part of active_set_t::reset in one launch: the three bitmaps,
+// the halt flag and (Normal mode) both queue sizes
+static __global__ void k_as_reset(uint32_t *visited, uint32_t *active, uint32_t *inactive, int64_t words,
+                                  as_counters_t *c, bool clear_sizes) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < words; i += (int64_t)gridDim.x * blockDim.x) {
+    visited[i] = 0;
+    active[i] = 0;
+    inactive[i] = 0;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    c->halt = 0;
+    if (clear_sizes) c->qsize[0] = c->qsize[1] = 0;
+  }
+}
+
+// bitmap_t::init in one launch (see active_set_t::init)
+static __global__ void k_as_init(uint32_t *active, uint32_t *inactive, int64_t words, int64_t root) {
+  const uint32_t fill = root == ALL_ACTIVE ? 0xffffffffu : 0u;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < words; i += (int64_t)gridDim.x * blockDim.x) {
+    const uint32_t v = (root >= 0 && i == (root >> 5)) ? 1u << (root & 31) : fill;
+    active[i] = v;
+    inactive[i] = v;
+  }
+}
+
+inline int bitmap_grid(int64_t words) { return (int)MAX((int64_t)1, MIN((words + 255) / 256, (int64_t)2048)); }
+
 inline void active_set_t::reset(bool traceback) {
-  queue.reset(traceback);
-  fill_u32(bitmap.visited.dg_bits, 0, bitmap.visited.n_words);
-  fill_u32(bitmap.active.dg_bits, 0, bitmap.active.n_words);
-  fill_u32(bitmap.inactive.dg_bits, 0, bitmap.inactive.n_words);
-  GSW_CUDA(cudaMemsetAsync(&dg_cnt->halt, 0, sizeof(int), stream()));
+  queue.reset_host(traceback);
+  const int64_t w = bitmap.visited.n_words;
+  k_as_reset<<<bitmap_grid(w), 256, 0, stream()>>>(bitmap.visited.dg_bits, bitmap.active.dg_bits,
+                                                   bitmap.inactive.dg_bits, w, dg_cnt, queue.mode == Normal);
+  GSW_LAUNCHED();
   nt.reset();
 }
 
@@ -346,18 +378,7 @@ inline void active_set_t::reset(bool traceback) {
 // Inactive.  The queue is built from the bitmaps by the first filter.
 inline void active_set_t::init(int64_t root) {
   const int64_t w = bitmap.active.n_words;
-  if (root == ALL_ACTIVE) {
-    fill_u32(bitmap.active.dg_bits, 0xffffffffu, w);
-    fill_u32(bitmap.inactive.dg_bits, 0xffffffffu, w);
-  } else if (root >= 0) {
-    fill_u32(bitmap.active.dg_bits, 0, w);
-    fill_u32(bitmap.inactive.dg_bits, 0, w);
-    k_set_u32<<<1, 1, 0, stream()>>>(bitmap.active.dg_bits, root >> 5, 1u << (root & 31));
-    k_set_u32<<<1, 1, 0, stream()>>>(bitmap.inactive.dg_bits, root >> 5, 1u << (root & 31));
-  } else {
-    fill_u32(bitmap.active.dg_bits, 0, w);
-    fill_u32(bitmap.inactive.dg_bits, 0, w);
-  }
+  k_as_init<<<bitmap_grid(w), 256, 0, stream()>>>(bitmap.active.dg_bits, bitmap.inactive.dg_bits, w, root);
   GSW_LAUNCHED();
 }
 

@@ -68,9 +68,9 @@ __host__ __device__ __forceinline__ int64_t inspect_units(int64_t n) { return (i
 // of each run of units of one virtual block (a segment) the CTA folds its
 // per-virtual-thread maxima into the global scratch with atomicMax and adds
 // the segment's step count to the block's counter; the CTA that completes a
-// virtual block sums its 512 maxima into the statistics block and clears the
-// scratch, and the last CTA to finish folds the virtual-block sums (max over
-// blocks for push, sum for pull).  All vertex arithmetic is 32-bit (vertex
+// virtual block sums its 512 maxima, clears the scratch and folds the sum
+// into the push (max over blocks) and pull (sum over blocks) counters; the
+// last CTA to finish only reports.  All vertex arithmetic is 32-bit (vertex
 // ids are below 2^31), and units that lie wholly below n take a path without
 // per-vertex bounds checks.
 template <typename G, typename F>
@@ -214,6 +214,10 @@ __global__ void __launch_bounds__(INSPECT_THREADS, GSW_INSPECT_MINBLOCKS)
       if (threadIdx.x == 0) {
         info[8 + b] = sp;
         info[8 + INSPECT_NVB + b] = sl;
+        // fold into the two counters now (max over blocks for push, sum for
+        // pull: order-free on integers), so the last CTA has nothing left
+        if (sp) atomicMax(info + 4, sp);
+        if (sl) atomicAdd(info + 5, sl);
         vdone[b] = 0;
       }
     }
@@ -243,30 +247,16 @@ __global__ void __launch_bounds__(INSPECT_THREADS, GSW_INSPECT_MINBLOCKS)
     s_last = atomicAdd(info + 6, 1ull) == (unsigned long long)gridDim.x - 1;
   }
   __syncthreads();
-  if (s_last) {  // last block: fold the virtual-block sums
+  if (s_last && threadIdx.x == 0) {  // last block: every counter is final
     __threadfence();
-    unsigned long long mpx = 0, sp = 0;
-    for (int i = threadIdx.x; i < INSPECT_NVB; i += blockDim.x) {
-      const unsigned long long a = ((volatile unsigned long long *)info)[8 + i];
-      mpx = MAX(mpx, a);
-      sp += ((volatile unsigned long long *)info)[8 + INSPECT_NVB + i];
-    }
-    mpx = block_reduce<unsigned long long, true>(mpx, s_red);
-    sp = block_reduce(sp, s_red);
-    if (threadIdx.x == 0) {
-      info[4] = mpx;
-      info[5] = sp;
-      if (sig) {  // report to the mapped host block, leave zeroed counters behind
-        volatile unsigned long long *vi = info;
+    if (sig) {  // report to the mapped host block, leave zeroed counters behind
+      volatile unsigned long long *vi = info;
 #pragma unroll
-        for (int i = 0; i < 4; ++i) sig[i] = vi[i];
-        sig[4] = mpx;
-        sig[5] = sp;
+      for (int i = 0; i < 6; ++i) sig[i] = vi[i];
 #pragma unroll
-        for (int i = 0; i < 7; ++i) vi[i] = 0;
-        __threadfence_system();
-        *(volatile unsigned long long *)(sig + 7) = seq;
-      }
+      for (int i = 0; i < 7; ++i) vi[i] = 0;
+      __threadfence_system();
+      *(volatile unsigned long long *)(sig + 7) = seq;
     }
   }
 }
