@@ -29,8 +29,6 @@ static __global__ void k_fill_u32(uint32_t *p, uint32_t v, int64_t n) {
        i += (int64_t)gridDim.x * blockDim.x)
     p[i] = v;
 }
-static __global__ void k_set_u32(uint32_t *p, int64_t i, uint32_t v) { p[i] = v; }
-static __global__ void k_set_i32(int *p, int64_t i, int v) { p[i] = v; }
 
 inline int fill_u32(uint32_t *p, uint32_t v, int64_t n) {
   if (n <= 0) return GSW_OK;
