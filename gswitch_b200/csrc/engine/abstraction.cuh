@@ -315,9 +315,10 @@ struct stat_t {
   unsigned long long *dg_runtime_info = nullptr;
   unsigned long long *h_runtime_info = nullptr;
   // Zero-copy report of a VC inspection (mapped pinned, 8 words): the
-  // kernel's last CTA writes the six counters to [0..5], clears the device
-  // counters for the next launch and then writes the launch's sequence
-  // number to [7]; the host polls [7] instead of copying and synchronising.
+  // kernel's last CTA writes the six counters to [0..5], each word holding
+  // the value in its low 40 bits and the launch's tag (1 .. 2^24-1) in the
+  // top 24, and clears the device counters for the next launch; the host
+  // polls the tags instead of copying and synchronising.
   unsigned long long *h_sig = nullptr, *d_sig = nullptr;
   unsigned long long sig_seq = 0;
   int size = 0;
@@ -350,25 +351,30 @@ struct stat_t {
     h_runtime_info = nullptr;
     h_sig = d_sig = nullptr;
   }
-  // sequence number for the next signalled inspection (0: no report block)
-  unsigned long long arm() { return d_sig ? ++sig_seq : 0; }
-  // Waits for the report of inspection `seq` and takes its counters.  Every
-  // 256 polls the stream is queried, so the wait ends when the stream runs
-  // dry; false then (or on an error), and the caller reads the device block.
-  bool await(unsigned long long seq) {
+  // tag for the next signalled inspection (0: no report block)
+  unsigned long long arm() { return d_sig ? (++sig_seq % 0xffffffull) + 1 : 0; }
+  // Waits for the report tagged `tag` and takes its counters.  Every 256
+  // polls the stream is queried, so the wait ends when the stream runs dry;
+  // false then (or on an error), and the caller reads the device block.
+  bool await(unsigned long long tag) {
     volatile unsigned long long *h = h_sig;
+    auto arrived = [&] {
+      for (int i = 0; i < 6; ++i)
+        if ((h[i] >> 40) != tag) return false;
+      return true;
+    };
     for (unsigned spin = 1;; ++spin) {
-      if (h[7] == seq) break;
+      if (arrived()) break;
       if ((spin & 255) == 0) {
         const cudaError_t q = cudaStreamQuery(gsw::stream());
         if (q != cudaErrorNotReady) {
-          if (h[7] == seq) break;
+          if (arrived()) break;
           if (q != cudaSuccess) GSW_CUDA(q);
           return false;
         }
       }
     }
-    for (int i = 0; i < 6; ++i) h_runtime_info[i] = h[i];
+    for (int i = 0; i < 6; ++i) h_runtime_info[i] = h[i] & ((1ull << 40) - 1);
     return true;
   }
   void reset() {}

@@ -44,6 +44,8 @@ constexpr int INSPECT_SCRATCH_U64 = (INSPECT_SCRATCH_U32 + 1) / 2;
 constexpr int INSPECT_UNROLL = GSW_INSPECT_UNROLL;
 static_assert(STAT_SLOTS == 8 + 2 * INSPECT_NVB, "statistics block layout");
 static_assert(STAT_SCRATCH == INSPECT_SCRATCH_U64, "inspection scratch layout");
+constexpr int INSPECT_REPORT_BITS = 40;  // value bits of a zero-copy report word
+constexpr unsigned long long INSPECT_REPORT_MASK = (1ull << INSPECT_REPORT_BITS) - 1;
 constexpr int EC_INSPECT_CTAS = 256;
 constexpr int EC_INSPECT_THREADS = 512;
 
@@ -249,14 +251,20 @@ __global__ void __launch_bounds__(INSPECT_THREADS, GSW_INSPECT_MINBLOCKS)
   __syncthreads();
   if (s_last && threadIdx.x == 0) {  // last block: every counter is final
     __threadfence();
-    if (sig) {  // report to the mapped host block, leave zeroed counters behind
+    if (sig) {
+      // Report to the mapped host block and leave zeroed counters behind.
+      // Every counter is below 2^40 (each is bounded by the arc count), so
+      // each report word carries the launch's tag in its top 24 bits and the
+      // host takes the report once all six carry it: no write ordering, so
+      // no system-scope fence.
       volatile unsigned long long *vi = info;
+      unsigned long long w[6];
 #pragma unroll
-      for (int i = 0; i < 6; ++i) sig[i] = vi[i];
+      for (int i = 0; i < 6; ++i) w[i] = (vi[i] & INSPECT_REPORT_MASK) | (seq << INSPECT_REPORT_BITS);
 #pragma unroll
       for (int i = 0; i < 7; ++i) vi[i] = 0;
-      __threadfence_system();
-      *(volatile unsigned long long *)(sig + 7) = seq;
+#pragma unroll
+      for (int i = 0; i < 6; ++i) ((volatile unsigned long long *)sig)[i] = w[i];
     }
   }
 }
