@@ -128,10 +128,10 @@ def level_bytes(kind, n, A, U, D, E):
 
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per vertex of
 # one inspection launch, from the ncu capture summarised in
-# profiles/bfs_rmat24_inspect_pulltm.md (135.43 MB + 4.90 MB over 16,777,216
+# profiles/bfs_rmat24_inspect_pulltm.md (135.47 MB + 4.42 MB over 16,777,216
 # vertices); the inspection streams every vertex once, so a launch's traffic
 # scales with n
-INSPECT_TRAFFIC_PER_VERTEX = (135.43e6 + 4.90e6) / 16777216
+INSPECT_TRAFFIC_PER_VERTEX = (135.47e6 + 4.42e6) / 16777216
 # DRAM bytes per launch of the thread-mapped pull expand on the bench graph
 # (RMAT scale 24 ef 16 seed 1): the mean of the two launches of one BFS in the
 # same capture (600.38 MB and 329.71 MB); per-launch traffic depends on the
