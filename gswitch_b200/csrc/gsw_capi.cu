@@ -90,9 +90,9 @@ struct gsw_ctx {
   // 2.2 GB CSR).  Blocks go back to the pool on graph destroy (stream order
   // on the context's one stream keeps a reused block from being overwritten
   // while a kernel still reads it); the pool keeps at most GRAPH_POOL_CAP
-  // bytes, gives back all of it when an allocation fails, and is freed with
-  // the context.
-  static constexpr size_t GRAPH_POOL_CAP = (size_t)48 << 30;
+  // bytes, gives back all of it when any of the context's allocations fails,
+  // and is freed with the context.
+  static constexpr size_t GRAPH_POOL_CAP = (size_t)8 << 30;
   std::multimap<size_t, void *> graph_pool;     // free blocks by size
   std::unordered_map<void *, size_t> graph_blocks;  // every pool-managed block
   size_t graph_pool_bytes = 0;
@@ -142,7 +142,11 @@ struct gsw_ctx {
       bufs.erase(it);
     }
     void *p = nullptr;
-    if (GSW_CUDA(cudaMalloc(&p, bytes ? bytes : 1))) return nullptr;
+    if (cudaMalloc(&p, bytes ? bytes : 1) != cudaSuccess) {
+      cudaGetLastError();
+      graph_pool_trim();
+      if (GSW_CUDA(cudaMalloc(&p, bytes ? bytes : 1))) return nullptr;
+    }
     bufs[name] = {p, bytes};
     return p;
   }
@@ -153,7 +157,15 @@ struct gsw_ctx {
     active_set_t as;
     if (as.build(size, qm)) {
       as.destroy();
-      return nullptr;
+      if (graph_pool_bytes == 0) return nullptr;
+      // give the cached graph blocks back and try once more
+      clear_error();
+      graph_pool_trim();
+      as = active_set_t();
+      if (as.build(size, qm)) {
+        as.destroy();
+        return nullptr;
+      }
     }
     return &(as_cache[key] = as);
   }
