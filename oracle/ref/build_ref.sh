@@ -15,7 +15,7 @@ for app in BFS SSSP CC BC PR GC; do
   nvcc -std=c++14 -O2 --expt-extended-lambda -w \
     -gencode arch=compute_100a,code=sm_100a \
     -I "$REF" -I "$REF/src" -I "$REF/deps/moderngpu/src" \
-    -Dmain=gsw_ref_app_main -DGSW_REF_$app \
+    -Dmain=gsw_ref_app_main -DGSW_REF_$app -Xcompiler -pthread \
     "$HERE/ref_driver.cu" -o "$dst" &
 done
 wait

@@ -10,9 +10,11 @@
 // int64 off[n+1], int32 col[m], int32 w[m] if has_w.  The arcs are fed to the
 // reference's edgelist_t/host_graph_t as a directed list in CSR order with
 // quiet=true, so its host CSR is exactly the file's CSR (no rinse/renumber).
+#include <atomic>
 #include <chrono>
 #include <cstdint>
 #include <string>
+#include <thread>
 #include <cstdio>
 #include <cstdlib>
 #include <vector>
@@ -114,6 +116,39 @@ int main(int argc, char **argv) {
     int r;
     while (rf && fread(&r, 4, 1, rf) == 1) roots.push_back(r);
     if (rf) fclose(rf);
+    const int threads = argc > 5 ? atoi(argv[5]) : 1;
+    const size_t warm = argc > 6 ? (size_t)atoi(argv[6]) : 0;
+    if (threads > 1) {
+      // throughput mode: `threads` workers share the read-only CSR and each
+      // runs the reference's bfs_cpu on the next unclaimed root (bfs_cpu
+      // allocates its own state per call); the first `warm` roots run
+      // untimed, then one line: timed roots, wall milliseconds, edges
+      auto run_set = [&](size_t b, size_t e) {
+        std::atomic<size_t> next(b);
+        std::atomic<long long> edges(0);
+        std::vector<std::thread> ts;
+        for (int t = 0; t < threads; ++t)
+          ts.emplace_back([&] {
+            for (size_t i; (i = next++) < e;) {
+              int *lv = bfs_cpu(hg, roots[i]);
+              long long te = 0;
+              for (int64_t v = 0; v < fg.n; ++v)
+                if (lv[v] >= 0) te += fg.off[v + 1] - fg.off[v];
+              edges += te / 2;
+              free(lv);
+            }
+          });
+        for (auto &t : ts) t.join();
+        return edges.load();
+      };
+      run_set(0, std::min(warm, roots.size()));
+      auto t0 = std::chrono::steady_clock::now();
+      const long long te = run_set(std::min(warm, roots.size()), roots.size());
+      auto t1 = std::chrono::steady_clock::now();
+      printf("timed %zu %.6f %lld\n", roots.size() - std::min(warm, roots.size()),
+             std::chrono::duration<double, std::milli>(t1 - t0).count(), te);
+      return 0;
+    }
     for (int root : roots) {
       auto t0 = std::chrono::steady_clock::now();
       int *lv = bfs_cpu(hg, root);
