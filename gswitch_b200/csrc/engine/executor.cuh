@@ -80,8 +80,10 @@ inline engine_opts_t &opts() {
 
 // sizes the host knows without a device round trip
 struct hints_t {
-  int64_t frontier = -1;  // entries in the expand's work list
-  int64_t edges = -1;     // edges they touch
+  int64_t frontier = -1;     // entries in the expand's work list
+  int64_t edges = -1;        // edges they touch
+  bool persistent = false;   // the last expand ran as a persistent launch
+  int persistent_lb = -1;    // the load balance that launch's kernel reported
 };
 inline hints_t &hints() {
   static thread_local hints_t h;
@@ -698,9 +700,25 @@ struct executor_t {
   // selector can pick direction and format again.
   template <typename E, typename F>
   void launch_persistent(active_set_t &as, device_graph_t<CSR, E> &g, F &f, config_t &conf) {
+    switch (conf.conf_lb) {
+      case TM: return launch_persistent_lb<TM>(as, g, f, conf);
+      case CM: return launch_persistent_lb<CM>(as, g, f, conf);
+      case STRICT: return launch_persistent_lb<STRICT>(as, g, f, conf);
+      case TWC: return launch_persistent_lb<TWC>(as, g, f, conf);
+      default: return launch_persistent_lb<WM>(as, g, f, conf);
+    }
+  }
+
+  template <int LB, typename E, typename F>
+  void launch_persistent_lb(active_set_t &as, device_graph_t<CSR, E> &g, F &f, config_t &conf) {
     using G = device_graph_t<CSR, E>;
-    auto kern = k_fused_persistent<G, F>;
+    auto kern = k_fused_persistent<LB, G, F>;
     const int grid = resident_grid(kern, EXPAND_THREADS);
+    if (LB == STRICT) {
+      ensure_tiles(g.nedges + as.size + 1);
+      if (!ok()) return;
+      if (grid > as.workset.bsum_cap) return (void)set_error(GSW_ERR_OVERFLOW, "persistent strict: %s", "block sums");
+    }
     as_counters_t *c = as.dg_cnt;
     const int cur = as.queue.cursor;
     k_persist_prep<<<1, 1, 0, stream()>>>(c, cur);
@@ -717,16 +735,27 @@ struct executor_t {
     ps.leave_block = opts().barrier_leave_test ? 0 : -1;
     ps.levels_done = &c->plevels;
     ps.exit_reason = &c->preason;
+    ps.lb_out = &c->plb;
+    ps.eoff = as.workset.dg_eoff;
+    ps.eoff_cap = as.size + 2;
+    ps.bsum = as.workset.dg_bsum;
+    ps.tile_lo = dg_tile;
+    ps.tile_cap = tile_cap;
     void *args[] = {(void *)&as, (void *)&g, (void *)&f, (void *)&conf, (void *)&ps};
     if (GSW_CUDA(cudaLaunchCooperativeKernel((const void *)kern, grid, EXPAND_THREADS, args, 0, stream()))) return;
     GSW_LAUNCHED();
-    int res[2] = {0, -1};
+    int res[3] = {0, -1, -1};
     GSW_CUDA(cudaMemcpyAsync(res, &c->plevels, sizeof(res), cudaMemcpyDeviceToHost, stream()));
     GSW_CUDA(cudaStreamSynchronize(stream()));
     const int L = res[0], reason = res[1];
+    hints().persistent_lb = res[2];
     persistent_levels += L;
     persistent_launches++;
     last_persistent = true;
+    if (reason == 4) {
+      set_error(GSW_ERR_OVERFLOW, "%s", "persistent STRICT levels: frontier exceeds the scan buffer");
+      return;
+    }
     if (reason == 3 || reason < 0) {
       set_error(GSW_ERR_TIMEOUT, "%s", "persistent fused levels: grid barrier timed out");
       return;
@@ -798,6 +827,7 @@ struct executor_t {
     last_persistent = false;
     pattern = fets.pattern;
     dispatch(as, g, f, conf);
+    hints().persistent = last_persistent;
     marks().exp1 = opts().timing ? timing_pool().record() : -1;
     double e = s;
     if (sync_needed) {

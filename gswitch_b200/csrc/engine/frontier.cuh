@@ -51,6 +51,8 @@ struct as_counters_t {
   int pq[3];                       // persistent fused levels: rotating sizes
   int plevels;                     // persistent fused levels: levels done
   int preason;                     // persistent fused levels: exit reason
+  int plb;                         // persistent fused levels: the load
+                                   // balance the launched kernel ran
 };
 
 struct bits_t {

@@ -134,6 +134,29 @@ __device__ __forceinline__ void account(const active_set_t &as, const config_t &
   if (conf.conf_count_edges && c) atomicAdd(&as.dg_cnt->scanned, c);
 }
 
+// Where a push body reads its work list.  Per-launch kernels read the active
+// set (queue or bitmap, read-only path).  Levels inside a persistent launch
+// read the queue array the previous level wrote, with plain loads (the
+// read-only path may hold lines of an array written during the same launch),
+// and apply the deferred filter update of each vertex they fetch (what the
+// compensation launch does between per-launch fused levels).
+struct as_src_t {
+  const active_set_t *as;
+  Status want;
+  __device__ __forceinline__ int operator()(int64_t i) const { return as->fetch(i, want); }
+  template <typename G, typename F>
+  __device__ __forceinline__ void visit(int, const G &, F &) const {}
+};
+struct level_src_t {
+  const int *q;
+  bool compensate;
+  __device__ __forceinline__ int operator()(int64_t i) const { return q[i]; }
+  template <typename G, typename F>
+  __device__ __forceinline__ void visit(int v, const G &g, F &f) const {
+    if (compensate && v >= 0) f.filter(v, g);
+  }
+};
+
 #define GSW_HALT_IF_EMPTY(n)                                     \
   if ((n) == 0) {                                                \
     if (blockIdx.x == 0 && threadIdx.x == 0) as.halt_device();   \
@@ -143,6 +166,35 @@ __device__ __forceinline__ void account(const active_set_t &as, const config_t &
 // ===========================================================================
 // TM
 // ===========================================================================
+// fused TM level over src[0..n): warp-uniform trip counts, so the warp
+// stages its appends together
+template <typename G, typename F, typename Src>
+__device__ __forceinline__ void push_tm_fused_body(active_set_t &as, const G &g, F &f, const config_t &conf,
+                                                   const Src &src, int64_t n, warp_stage_t &stage) {
+  const int64_t STRIDE = (int64_t)blockDim.x * gridDim.x;
+  unsigned long long cnt = 0;
+  for (int64_t w0 = (threadIdx.x & ~31u) + (int64_t)blockIdx.x * blockDim.x; w0 < n; w0 += STRIDE) {
+    const int64_t idx = w0 + lane_id();
+    const int v = idx < n ? src(idx) : -1;
+    src.visit(v, g, f);
+    int64_t st;
+    int deg;
+    vertex_range(g, false, v, st, deg);
+    cnt += deg;
+    const int rounds = (int)__reduce_max_sync(FULL, (unsigned)deg);
+    for (int k = 0; k < rounds; ++k) {
+      bool tp = false;
+      int u = -1;
+      if (k < deg) {
+        u = __ldg(g.dg_adj_list + st + k);
+        tp = push_edge_fused(as, g, f, conf, v, u, st + k);
+      }
+      stage.push(tp, u);
+    }
+  }
+  account(as, conf, cnt);
+}
+
 template <bool FUSED, typename G, typename F>
 __global__ void __launch_bounds__(EXPAND_THREADS) k_push_tm(active_set_t as, G g, F f, config_t conf) {
   const int64_t n = as.get_size();
@@ -151,27 +203,9 @@ __global__ void __launch_bounds__(EXPAND_THREADS) k_push_tm(active_set_t as, G g
   const int64_t STRIDE = (int64_t)blockDim.x * gridDim.x;
   unsigned long long cnt = 0;
   if constexpr (FUSED) {
-    // warp-uniform trip counts, so the warp stages its appends together
     __shared__ int s_stage[EXPAND_THREADS / 32][STAGE_SLOTS];
     warp_stage_t stage(s_stage[warp_id()], as);
-    for (int64_t w0 = (threadIdx.x & ~31u) + (int64_t)blockIdx.x * blockDim.x; w0 < n; w0 += STRIDE) {
-      const int64_t idx = w0 + lane_id();
-      const int v = idx < n ? as.fetch(idx, want) : -1;
-      int64_t st;
-      int deg;
-      vertex_range(g, false, v, st, deg);
-      cnt += deg;
-      const int rounds = (int)__reduce_max_sync(FULL, (unsigned)deg);
-      for (int k = 0; k < rounds; ++k) {
-        bool tp = false;
-        int u = -1;
-        if (k < deg) {
-          u = __ldg(g.dg_adj_list + st + k);
-          tp = push_edge_fused(as, g, f, conf, v, u, st + k);
-        }
-        stage.push(tp, u);
-      }
-    }
+    push_tm_fused_body(as, g, f, conf, as_src_t{&as, want}, n, stage);
     stage.flush();
   } else {
     for (int64_t idx = threadIdx.x + (int64_t)blockIdx.x * blockDim.x; idx < n; idx += STRIDE) {
@@ -257,22 +291,19 @@ __global__ void __launch_bounds__(EXPAND_THREADS) k_pull_tm(active_set_t as, G g
 // ===========================================================================
 // WM: warp per 32 frontier vertices
 // ===========================================================================
-template <bool FUSED, typename G, typename F>
-__global__ void __launch_bounds__(EXPAND_THREADS) k_push_wm(active_set_t as, G g, F f, config_t conf) {
+template <bool FUSED, typename G, typename F, typename Src>
+__device__ __forceinline__ void push_wm_body(active_set_t &as, const G &g, F &f, const config_t &conf, const Src &src,
+                                             int64_t n, warp_stage_t &stage) {
   constexpr int W = EXPAND_THREADS / 32;
   __shared__ int s_scan[W][32];
   __shared__ int s_v[W][32];
   __shared__ int64_t s_st[W][32];
-  __shared__ int s_stage[FUSED ? W : 1][FUSED ? STAGE_SLOTS : 1];
-  const int64_t n = as.get_size();
-  GSW_HALT_IF_EMPTY(n);
-  const Status want = conf.want();
   const int lane = lane_id(), w = warp_id();
-  warp_stage_t stage(s_stage[FUSED ? w : 0], as);
   const int64_t nwarps = (int64_t)gridDim.x * W;
   for (int64_t tile = (int64_t)blockIdx.x * W + w; tile * 32 < n; tile += nwarps) {
     const int64_t idx = tile * 32 + lane;
-    const int v = idx < n ? as.fetch(idx, want) : -1;
+    const int v = idx < n ? src(idx) : -1;
+    src.visit(v, g, f);
     int64_t st;
     int deg;
     vertex_range(g, false, v, st, deg);
@@ -300,6 +331,15 @@ __global__ void __launch_bounds__(EXPAND_THREADS) k_push_wm(active_set_t as, G g
     }
     __syncwarp();
   }
+}
+
+template <bool FUSED, typename G, typename F>
+__global__ void __launch_bounds__(EXPAND_THREADS) k_push_wm(active_set_t as, G g, F f, config_t conf) {
+  __shared__ int s_stage[FUSED ? EXPAND_THREADS / 32 : 1][FUSED ? STAGE_SLOTS : 1];
+  const int64_t n = as.get_size();
+  GSW_HALT_IF_EMPTY(n);
+  warp_stage_t stage(s_stage[FUSED ? warp_id() : 0], as);
+  push_wm_body<FUSED>(as, g, f, conf, as_src_t{&as, conf.want()}, n, stage);
   if (FUSED) stage.flush();
 }
 
@@ -371,21 +411,18 @@ __global__ void __launch_bounds__(EXPAND_THREADS) k_pull_wm(active_set_t as, G g
 // ===========================================================================
 // CM: CTA per 256 frontier vertices
 // ===========================================================================
-template <bool FUSED, typename G, typename F>
-__global__ void __launch_bounds__(EXPAND_THREADS) k_push_cm(active_set_t as, G g, F f, config_t conf) {
+template <bool FUSED, typename G, typename F, typename Src>
+__device__ __forceinline__ void push_cm_body(active_set_t &as, const G &g, F &f, const config_t &conf, const Src &src,
+                                             int64_t n, warp_stage_t &stage) {
   constexpr int B = EXPAND_THREADS;
   __shared__ int s_scan[B];
   __shared__ int s_v[B];
   __shared__ int64_t s_st[B];
   __shared__ int s_tmp[33];
-  __shared__ int s_stage[FUSED ? B / 32 : 1][FUSED ? STAGE_SLOTS : 1];
-  const int64_t n = as.get_size();
-  GSW_HALT_IF_EMPTY(n);
-  const Status want = conf.want();
-  warp_stage_t stage(s_stage[FUSED ? warp_id() : 0], as);
   for (int64_t tile = blockIdx.x; tile * B < n; tile += gridDim.x) {
     const int64_t idx = tile * B + threadIdx.x;
-    const int v = idx < n ? as.fetch(idx, want) : -1;
+    const int v = idx < n ? src(idx) : -1;
+    src.visit(v, g, f);
     int64_t st;
     int deg;
     vertex_range(g, false, v, st, deg);
@@ -413,6 +450,15 @@ __global__ void __launch_bounds__(EXPAND_THREADS) k_push_cm(active_set_t as, G g
     }
     __syncthreads();
   }
+}
+
+template <bool FUSED, typename G, typename F>
+__global__ void __launch_bounds__(EXPAND_THREADS) k_push_cm(active_set_t as, G g, F f, config_t conf) {
+  __shared__ int s_stage[FUSED ? EXPAND_THREADS / 32 : 1][FUSED ? STAGE_SLOTS : 1];
+  const int64_t n = as.get_size();
+  GSW_HALT_IF_EMPTY(n);
+  warp_stage_t stage(s_stage[FUSED ? warp_id() : 0], as);
+  push_cm_body<FUSED>(as, g, f, conf, as_src_t{&as, conf.want()}, n, stage);
   if (FUSED) stage.flush();
 }
 
@@ -459,11 +505,51 @@ __global__ void __launch_bounds__(EXPAND_THREADS) k_pull_cm(active_set_t as, G g
 // STRICT: exact edge balance
 // ===========================================================================
 template <bool PULL, typename G>
-__device__ __forceinline__ int64_t strict_slots(const active_set_t &as, const G &g, int64_t idx, Status want) {
-  const int v = as.fetch(idx, want);
+__device__ __forceinline__ int64_t strict_slots_of(const G &g, int v) {
   if (v < 0) return 1;
   const int64_t *off = PULL ? g.dgr_row_off : g.dg_row_off;
   return __ldg(off + v + 1) - __ldg(off + v) + 1;
+}
+template <bool PULL, typename G>
+__device__ __forceinline__ int64_t strict_slots(const active_set_t &as, const G &g, int64_t idx, Status want) {
+  return strict_slots_of<PULL>(g, as.fetch(idx, want));
+}
+
+// Epilogue of the STRICT scan for 4 consecutive frontier entries base..base+3
+// (d[k] slots each, the first starting at slot `off`): eoff[idx] gets the
+// entry's first slot, tile_lo[t] the entry owning slot t*STRICT_TILE.  Every
+// lane of the warp calls it.
+__device__ __forceinline__ void strict_scan_epilogue(const active_set_t &as, int64_t base, int64_t n,
+                                                     const int64_t (&d)[4], int64_t off, int64_t *eoff, int *tile_lo,
+                                                     int64_t tile_cap) {
+  auto own = [&](int64_t t, int item) {
+    if (t < tile_cap)
+      tile_lo[t] = item;
+    else
+      as.raise(DEV_ERR_SCRATCH_OVERFLOW);
+  };
+  const int lane = lane_id();
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const int64_t idx = base + k;
+    const bool valid = idx < n;
+    if (valid) eoff[idx] = off;
+    // tiles whose first slot falls in [off, off + d): ta <= t < tb
+    const int64_t ta = (off + STRICT_TILE - 1) / STRICT_TILE;
+    const int64_t tb = valid ? (off + d[k] + STRICT_TILE - 1) / STRICT_TILE : ta;
+    // a hub owns many tiles, and a sorted frontier puts the hubs side by
+    // side: long runs are written by the whole warp, 32 tiles a step
+    const bool many = tb - ta > 2;
+    if (!many)
+      for (int64_t t = ta; t < tb; ++t) own(t, (int)idx);
+    for (unsigned pend = __ballot_sync(FULL, many); pend; pend &= pend - 1) {
+      const int src = __ffs(pend) - 1;
+      const int64_t a = __shfl_sync(FULL, ta, src), b = __shfl_sync(FULL, tb, src);
+      const int item = __shfl_sync(FULL, (int)idx, src);
+      for (int64_t t = a + lane; t < b; t += 32) own(t, item);
+    }
+    off += d[k];
+  }
 }
 
 template <bool PULL, typename G>
@@ -504,55 +590,25 @@ __global__ void __launch_bounds__(256) k_strict_scan(active_set_t as, G g, Statu
     if (lane_id() < (int)(blockDim.x >> 5)) s[lane_id()] = yi - y;
   }
   __syncthreads();
-  int64_t off = bsum[blockIdx.x] + s[warp_id()] + incl - loc;
+  const int64_t off = bsum[blockIdx.x] + s[warp_id()] + incl - loc;
   int64_t *eoff = as.workset.dg_eoff;
-  auto own = [&](int64_t t, int item) {
-    if (t < tile_cap)
-      tile_lo[t] = item;
-    else
-      as.raise(DEV_ERR_SCRATCH_OVERFLOW);
-  };
-  const int lane = lane_id();
-#pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    const int64_t idx = base + k;
-    const bool valid = idx < n;
-    if (valid) eoff[idx] = off;
-    // tiles whose first slot falls in [off, off + d): ta <= t < tb
-    const int64_t ta = (off + STRICT_TILE - 1) / STRICT_TILE;
-    const int64_t tb = valid ? (off + d[k] + STRICT_TILE - 1) / STRICT_TILE : ta;
-    // a hub owns many tiles, and a sorted frontier puts the hubs side by
-    // side: long runs are written by the whole warp, 32 tiles a step
-    const bool many = tb - ta > 2;
-    if (!many)
-      for (int64_t t = ta; t < tb; ++t) own(t, (int)idx);
-    for (unsigned pend = __ballot_sync(FULL, many); pend; pend &= pend - 1) {
-      const int src = __ffs(pend) - 1;
-      const int64_t a = __shfl_sync(FULL, ta, src), b = __shfl_sync(FULL, tb, src);
-      const int item = __shfl_sync(FULL, (int)idx, src);
-      for (int64_t t = a + lane; t < b; t += 32) own(t, item);
-    }
-    off += d[k];
-  }
+  strict_scan_epilogue(as, base, n, d, off, eoff, tile_lo, tile_cap);
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     eoff[n] = bsum[nblocks];
     as.dg_cnt->total_edges = (unsigned long long)bsum[nblocks];
   }
 }
 
-template <bool FUSED, typename G, typename F>
-__global__ void __launch_bounds__(EXPAND_THREADS) k_push_strict(active_set_t as, G g, F f, config_t conf,
-                                                                const int *tile_lo) {
+// STRICT push over the tiles of a scanned frontier src[0..n) (eoff: the
+// (degree+1) scan, tile_lo: tile owners)
+template <bool FUSED, typename G, typename F, typename Src>
+__device__ __forceinline__ void push_strict_body(active_set_t &as, const G &g, F &f, const config_t &conf,
+                                                 const Src &src, int64_t n, const int64_t *eoff, const int *tile_lo,
+                                                 warp_stage_t &stage) {
   constexpr int T = STRICT_TILE;
   __shared__ int s_v[T + 2];
   __shared__ int64_t s_sc[T + 2];
   __shared__ int64_t s_st[T + 2];
-  __shared__ int s_stage[FUSED ? EXPAND_THREADS / 32 : 1][FUSED ? STAGE_SLOTS : 1];
-  const int64_t n = as.get_size();
-  GSW_HALT_IF_EMPTY(n);
-  const Status want = conf.want();
-  warp_stage_t stage(s_stage[FUSED ? warp_id() : 0], as);
-  const int64_t *eoff = as.workset.dg_eoff;
   const int64_t total = eoff[n];
   const int64_t ntiles = (total + T - 1) / T;
   if (blockIdx.x == 0 && threadIdx.x == 0) account(as, conf, (unsigned long long)(total - n));
@@ -561,7 +617,7 @@ __global__ void __launch_bounds__(EXPAND_THREADS) k_push_strict(active_set_t as,
     const int64_t hi = (t + 1 < ntiles) ? tile_lo[t + 1] : n - 1;
     const int cnt = (int)(hi - lo + 1);
     for (int j = threadIdx.x; j < cnt; j += blockDim.x) {
-      const int v = as.fetch(lo + j, want);
+      const int v = src(lo + j);
       s_v[j] = v;
       s_sc[j] = eoff[lo + j];
       s_st[j] = v >= 0 ? __ldg(g.dg_row_off + v) : 0;
@@ -591,6 +647,16 @@ __global__ void __launch_bounds__(EXPAND_THREADS) k_push_strict(active_set_t as,
     }
     __syncthreads();
   }
+}
+
+template <bool FUSED, typename G, typename F>
+__global__ void __launch_bounds__(EXPAND_THREADS) k_push_strict(active_set_t as, G g, F f, config_t conf,
+                                                                const int *tile_lo) {
+  __shared__ int s_stage[FUSED ? EXPAND_THREADS / 32 : 1][FUSED ? STAGE_SLOTS : 1];
+  const int64_t n = as.get_size();
+  GSW_HALT_IF_EMPTY(n);
+  warp_stage_t stage(s_stage[FUSED ? warp_id() : 0], as);
+  push_strict_body<FUSED>(as, g, f, conf, as_src_t{&as, conf.want()}, n, as.workset.dg_eoff, tile_lo, stage);
   if (FUSED) stage.flush();
 }
 
@@ -779,8 +845,9 @@ __global__ void __launch_bounds__(EXPAND_THREADS) k_pull_strict_all(active_set_t
 // ===========================================================================
 // TWC: thread / warp / CTA tiers by degree
 // ===========================================================================
-template <bool FUSED, typename G, typename F>
-__global__ void __launch_bounds__(EXPAND_THREADS) k_push_twc(active_set_t as, G g, F f, config_t conf) {
+template <bool FUSED, typename G, typename F, typename Src>
+__device__ __forceinline__ void push_twc_body(active_set_t &as, const G &g, F &f, const config_t &conf, const Src &src,
+                                              int64_t n, warp_stage_t &stage) {
   constexpr int B = EXPAND_THREADS;
   __shared__ int s_owner;
   __shared__ int s_cv;
@@ -790,17 +857,13 @@ __global__ void __launch_bounds__(EXPAND_THREADS) k_push_twc(active_set_t as, G 
   __shared__ int s_v[B];
   __shared__ int64_t s_st[B];
   __shared__ int s_tmp[33];
-  __shared__ int s_stage[FUSED ? B / 32 : 1][FUSED ? STAGE_SLOTS : 1];
-  const int64_t n = as.get_size();
-  GSW_HALT_IF_EMPTY(n);
-  const Status want = conf.want();
   const int lane = lane_id();
-  warp_stage_t stage(s_stage[FUSED ? warp_id() : 0], as);
   if (threadIdx.x == 0) s_owner = -1;
   __syncthreads();
   for (int64_t tile = blockIdx.x; tile * B < n; tile += gridDim.x) {
     const int64_t idx = tile * B + threadIdx.x;
-    const int v = idx < n ? as.fetch(idx, want) : -1;
+    const int v = idx < n ? src(idx) : -1;
+    src.visit(v, g, f);
     int64_t st;
     int deg;
     vertex_range(g, false, v, st, deg);
@@ -888,6 +951,15 @@ __global__ void __launch_bounds__(EXPAND_THREADS) k_push_twc(active_set_t as, G 
     }
     __syncthreads();
   }
+}
+
+template <bool FUSED, typename G, typename F>
+__global__ void __launch_bounds__(EXPAND_THREADS) k_push_twc(active_set_t as, G g, F f, config_t conf) {
+  __shared__ int s_stage[FUSED ? EXPAND_THREADS / 32 : 1][FUSED ? STAGE_SLOTS : 1];
+  const int64_t n = as.get_size();
+  GSW_HALT_IF_EMPTY(n);
+  warp_stage_t stage(s_stage[FUSED ? warp_id() : 0], as);
+  push_twc_body<FUSED>(as, g, f, conf, as_src_t{&as, conf.want()}, n, stage);
   if (FUSED) stage.flush();
 }
 

@@ -231,13 +231,26 @@ def test_fused_levels_persistent_and_per_launch(ctx, big, persistent):
     for name in ["grid64", "rmat14", "er20k"]:
         h, hw, root = big[name]
         g = ctx.upload(h.off, h.col)
+        gw = ctx.upload(hw.off, hw.col, hw.w)
         for lb in ["WM", "TM", "CM", "STRICT", "TWC"]:
             lv, st = g.bfs(root, gs.RunOpts.from_config(f"Push-Queue-{lb}-Fused", persistent=persistent))
             assert np.array_equal(lv, oracle.bfs(h, root)), (name, lb, persistent)
             assert st.levels == int(lv.max()) + 1 or st.levels == int(lv.max()) + 2
-        gw = ctx.upload(hw.off, hw.col, hw.w)
-        dist, _ = gw.sssp(root, gs.RunOpts.from_config("Push-Queue-WM-Fused", persistent=persistent))
-        assert np.array_equal(dist, oracle.sssp_dijkstra(hw, root)), (name, persistent)
+            check_fused_kernels(st, lb, persistent)
+            dist, st = gw.sssp(root, gs.RunOpts.from_config(f"Push-Queue-{lb}-Fused", persistent=persistent))
+            assert np.array_equal(dist, oracle.sssp_dijkstra(hw, root)), (name, lb, persistent)
+            check_fused_kernels(st, lb, persistent)
+
+
+def check_fused_kernels(st, lb, persistent):
+    """Every fused level ran the forced load balance; in persistent mode the
+    LB is the one the launched kernel reported back, so a kernel that ran
+    another LB's body shows up here."""
+    fused = [(t, p) for t, p in zip(st.trace, st.level_persistent) if t[3] == "Fused"]
+    assert fused
+    for t, p in fused:
+        assert t[2] == lb, (t, lb)
+        assert p == persistent, (t, p, persistent)
 
 
 def test_path_graph_many_levels_persistent(ctx):
