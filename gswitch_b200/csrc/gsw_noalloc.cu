@@ -282,6 +282,10 @@ static gsw_status na_run(int64_t n, int64_t m, const int64_t *d_row_off, const i
   unsigned e = 0;
   if (GSW_CUDA(cudaMemcpyAsync(&e, &S->err, sizeof(unsigned), cudaMemcpyDeviceToHost, st))) return gsw::err().code;
   if (GSW_CUDA(cudaStreamSynchronize(st))) return gsw::err().code;
+  // a column index outside [0, n) is the caller's CSR at fault, not a
+  // capacity problem: the kernel skipped that arc and flagged it
+  if (e & gsw::DEV_ERR_BAD_VERTEX)
+    return gsw::set_error(GSW_ERR_INVALID_ARG, "%s", "gsw_bfs_strict_noalloc: column index out of range");
   if (e) return gsw::set_error(GSW_ERR_OVERFLOW, "%s", "gsw_bfs_strict_noalloc: scratch bound exceeded");
   return GSW_OK;
 }

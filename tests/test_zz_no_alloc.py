@@ -16,17 +16,23 @@ import oracle
 pytestmark = pytest.mark.gpu
 
 
-def _noalloc_levels(torch, h, root):
+def _noalloc_call(torch, off, col, root):
     dev = torch.device("cuda", 0)
-    d_off = torch.from_numpy(h.off).to(dev)
-    d_col = torch.from_numpy(h.col).to(dev)
-    d_lv = torch.full((h.n,), 7, dtype=torch.int32, device=dev)
+    d_off = torch.from_numpy(off).to(dev)
+    d_col = torch.from_numpy(col).to(dev)
+    n = len(off) - 1
+    d_lv = torch.full((n,), 7, dtype=torch.int32, device=dev)
     stream = torch.cuda.current_stream(dev).cuda_stream
-    rc = gs.lib().gsw_bfs_strict_noalloc(h.n, h.m, d_off.data_ptr(), d_col.data_ptr(), root, d_lv.data_ptr(),
+    rc = gs.lib().gsw_bfs_strict_noalloc(n, len(col), d_off.data_ptr(), d_col.data_ptr(), root, d_lv.data_ptr(),
                                          ctypes.c_void_p(stream))
-    assert rc == 0, gs.lib().gsw_last_error_string()
     torch.cuda.synchronize(dev)
-    return d_lv.cpu().numpy()
+    return rc, d_lv.cpu().numpy()
+
+
+def _noalloc_levels(torch, h, root):
+    rc, lv = _noalloc_call(torch, h.off, h.col, root)
+    assert rc == 0, gs.lib().gsw_last_error_string()
+    return lv
 
 
 def test_noalloc_matches_regular_entry_point_twice():
@@ -54,3 +60,18 @@ def test_noalloc_rejects_sizes_beyond_its_fixed_memory():
     rc = gs.lib().gsw_bfs_strict_noalloc(100, (1 << 28) + 1, ctypes.c_void_p(16), ctypes.c_void_p(16), 0,
                                          ctypes.c_void_p(16), None)
     assert rc == 6
+
+
+def test_noalloc_reports_out_of_range_column_as_invalid_argument():
+    """A column index >= n in the caller's CSR is an argument error, not a
+    capacity problem; the kernel skips that arc (it checks every index before
+    touching the levels) and the call still works afterwards."""
+    import torch
+
+    h = oracle.rmat(10, 8, seed=3)
+    col = h.col.copy()
+    col[h.off[0]] = h.n + 5  # the root's first arc, so the search reaches it
+    rc, _ = _noalloc_call(torch, h.off, col, 0)
+    assert rc == 1
+    assert b"column index out of range" in gs.lib().gsw_last_error_string()
+    assert np.array_equal(_noalloc_levels(torch, h, 0), oracle.bfs(h, 0))
