@@ -64,7 +64,10 @@ def lib():
     L.or_bfs.argtypes = [i64, I64P, I32P, i32, I32P]
     L.or_sssp_spfa.argtypes = [i64, I64P, I32P, I32P, i32, I32P]
     L.or_sssp_dijkstra.argtypes = [i64, I64P, I32P, I32P, i32, I32P]
+    L.or_sssp_dial.restype = C.c_int
+    L.or_sssp_dial.argtypes = [i64, I64P, I32P, I32P, i32, i32, I32P]
     L.or_cc.argtypes = [i64, I64P, I32P, I32P]
+    L.or_cc_linear.argtypes = [i64, I64P, I32P, I32P]
     L.or_bc_f32.argtypes = [i64, I64P, I32P, i32, I32P, F32P]
     L.or_bc_f64.argtypes = [i64, I64P, I32P, i32, F64P, F64P, I32P]
     L.or_pagerank.argtypes = [i64, I64P, I32P, C.c_int, dbl, F64P]
@@ -189,6 +192,21 @@ def sssp_spfa(g: Csr, root: int):
 def sssp_dijkstra(g: Csr, root: int):
     out = np.empty(g.n, dtype=np.int32)
     lib().or_sssp_dijkstra(g.n, g.off, g.col, g.w, root, out)
+    return out
+
+
+def sssp_dial(g: Csr, root: int, wmax: int):
+    """Exact distances for integer weights in [1, wmax] (bucket queue)."""
+    out = np.empty(g.n, dtype=np.int32)
+    if lib().or_sssp_dial(g.n, g.off, g.col, g.w, root, wmax, out) != 0:
+        raise ValueError("a weight lies outside [1, wmax]")
+    return out
+
+
+def cc_linear(g: Csr):
+    """cc()'s labels in linear time, for graphs with large hubs."""
+    out = np.empty(g.n, dtype=np.int32)
+    lib().or_cc_linear(g.n, g.off, g.col, out)
     return out
 
 

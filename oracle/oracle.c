@@ -414,6 +414,67 @@ void or_sssp_dijkstra(int64_t n, const int64_t *off, const int32_t *col,
   free(h);
 }
 
+/* Dial's bucket-queue shortest paths (R. B. Dial, CACM 12(11), 1969) for
+ * integer weights in [1, wmax]: wmax+1 circular buckets of vertex lists, a
+ * vertex settled when its bucket comes round with its label unchanged.  Same
+ * distances as spfa / Dijkstra (unique for positive weights) at O(m + n + D)
+ * cost, for the large graphs the heap version takes minutes on.  Returns -1
+ * when a weight lies outside [1, wmax] (nothing computed), else 0. */
+int or_sssp_dial(int64_t n, const int64_t *off, const int32_t *col,
+                 const int32_t *w, int32_t root, int32_t wmax, int32_t *dis) {
+  const int64_t m = off[n];
+  for (int64_t j = 0; j < m; ++j)
+    if (w[j] < 1 || w[j] > wmax) return -1;
+  const int64_t nb = (int64_t)wmax + 1;
+  /* bucket lists as singly linked entries (vertex, next) in a pool that grows
+   * by one entry per successful relaxation */
+  int64_t cap = n + 16, used = 0;
+  int32_t *ev = (int32_t *)malloc(sizeof(int32_t) * (size_t)cap);
+  int64_t *en = (int64_t *)malloc(sizeof(int64_t) * (size_t)cap);
+  int64_t *head = (int64_t *)malloc(sizeof(int64_t) * (size_t)nb);
+  for (int64_t b = 0; b < nb; ++b) head[b] = -1;
+  for (int64_t i = 0; i < n; ++i) dis[i] = INT_MAX;
+  dis[root] = 0;
+  ev[0] = root;
+  en[0] = -1;
+  head[0] = 0;
+  used = 1;
+  int64_t pending = 1;
+  for (int64_t d = 0; pending > 0; ++d) {
+    const int64_t b = d % nb;
+    int64_t e = head[b];
+    head[b] = -1;
+    while (e >= 0) {
+      const int32_t v = ev[e];
+      const int64_t next = en[e];
+      --pending;
+      if (dis[v] == d) {
+        for (int64_t j = off[v]; j < off[v + 1]; ++j) {
+          const int32_t u = col[j];
+          const int64_t nd = d + w[j];
+          if (nd < dis[u]) {
+            dis[u] = (int32_t)nd;
+            if (used == cap) {
+              cap *= 2;
+              ev = (int32_t *)realloc(ev, sizeof(int32_t) * (size_t)cap);
+              en = (int64_t *)realloc(en, sizeof(int64_t) * (size_t)cap);
+            }
+            ev[used] = u;
+            en[used] = head[nd % nb];
+            head[nd % nb] = used++;
+            ++pending;
+          }
+        }
+      }
+      e = next;
+    }
+  }
+  free(ev);
+  free(en);
+  free(head);
+  return 0;
+}
+
 /* CC_CPU: application/cc.cu:34-66 - components seeded in increasing id
  * order, so every label is the minimum vertex id of its component. */
 void or_cc(int64_t n, const int64_t *off, const int32_t *col, int32_t *id) {
@@ -436,6 +497,37 @@ void or_cc(int64_t n, const int64_t *off, const int32_t *col, int32_t *id) {
     }
   }
   free(q);
+}
+
+/* The labels of CC_CPU in linear time.  CC_CPU tests "id[u] == u" for
+ * "not yet labelled", which also holds for the component's seed, so the seed
+ * re-enters the queue once per neighbour and a hub of degree d costs d^2
+ * edge visits (hours at RMAT scale 24).  Here the seed is marked when its
+ * component starts; every other step is CC_CPU's, so the labels (the
+ * smallest vertex id of each component) are the same. */
+void or_cc_linear(int64_t n, const int64_t *off, const int32_t *col, int32_t *id) {
+  int32_t *q = (int32_t *)malloc(sizeof(int32_t) * (size_t)(n + 1));
+  char *seen = (char *)calloc((size_t)n, 1);
+  for (int64_t i = 0; i < n; ++i) id[i] = (int32_t)i;
+  for (int64_t i = 0; i < n; ++i) {
+    if (seen[i]) continue;
+    seen[i] = 1;
+    int64_t head = 0, tail = 0;
+    q[tail++] = (int32_t)i;
+    while (head < tail) {
+      int32_t v = q[head++];
+      for (int64_t j = off[v]; j < off[v + 1]; ++j) {
+        int32_t u = col[j];
+        if (!seen[u]) {
+          seen[u] = 1;
+          id[u] = (int32_t)i;
+          q[tail++] = u;
+        }
+      }
+    }
+  }
+  free(q);
+  free(seen);
 }
 
 /* bc_cpu: application/bc.cu:162-214, single source, int32 path counts and
@@ -504,20 +596,37 @@ void or_bc_f64(int64_t n, const int64_t *off, const int32_t *col, int32_t root,
 /* PageRank in the reference's unnormalised form (application/pagerank.cu:
  * 19-32,120-125): pr_0 = 1-d; pr_{k+1}(v) = (1-d) + d * sum_{u in N(v)}
  * pr_k(u)/od(u).  FP64 Jacobi for exactly iters steps; returns pr_iters. */
+typedef struct {
+  const int64_t *off;
+  const int32_t *col;
+  double damp;
+  double *pr, *contrib;
+} pr_job;
+static void pr_contrib_range(int64_t lo, int64_t hi, void *p) {
+  const pr_job *j = (const pr_job *)p;
+  for (int64_t v = lo; v < hi; ++v) {
+    int64_t od = j->off[v + 1] - j->off[v];
+    j->contrib[v] = od ? j->pr[v] / (double)od : j->pr[v];
+  }
+}
+static void pr_gather_range(int64_t lo, int64_t hi, void *p) {
+  const pr_job *j = (const pr_job *)p;
+  for (int64_t v = lo; v < hi; ++v) {
+    double s = 0;
+    for (int64_t e = j->off[v]; e < j->off[v + 1]; ++e) s += j->contrib[j->col[e]];
+    j->pr[v] = (1.0 - j->damp) + j->damp * s;
+  }
+}
+/* Each vertex's sum runs over its own list in list order whichever thread
+ * takes it, so the result does not depend on the thread count. */
 void or_pagerank(int64_t n, const int64_t *off, const int32_t *col, int iters,
                  double damp, double *pr) {
   double *contrib = (double *)malloc(sizeof(double) * (size_t)n);
   for (int64_t v = 0; v < n; ++v) pr[v] = 1.0 - damp;
+  pr_job j = {off, col, damp, pr, contrib};
   for (int it = 0; it < iters; ++it) {
-    for (int64_t v = 0; v < n; ++v) {
-      int64_t od = off[v + 1] - off[v];
-      contrib[v] = od ? pr[v] / (double)od : pr[v];
-    }
-    for (int64_t v = 0; v < n; ++v) {
-      double s = 0;
-      for (int64_t j = off[v]; j < off[v + 1]; ++j) s += contrib[col[j]];
-      pr[v] = (1.0 - damp) + damp * s;
-    }
+    parallel_for(n, 1 << 14, pr_contrib_range, &j);
+    parallel_for(n, 1 << 12, pr_gather_range, &j);
   }
   free(contrib);
 }

@@ -70,7 +70,14 @@ void or_sssp_spfa(int64_t n, const int64_t *off, const int32_t *col,
                   const int32_t *w, int32_t root, int32_t *dist);
 void or_sssp_dijkstra(int64_t n, const int64_t *off, const int32_t *col,
                       const int32_t *w, int32_t root, int32_t *dist);
+/* Dial's bucket queue for integer weights in [1, wmax]; -1 if a weight is
+ * outside that range. */
+int or_sssp_dial(int64_t n, const int64_t *off, const int32_t *col,
+                 const int32_t *w, int32_t root, int32_t wmax, int32_t *dis);
 void or_cc(int64_t n, const int64_t *off, const int32_t *col, int32_t *label);
+/* CC_CPU's labels in linear time (the seed is marked when its component
+ * starts instead of re-entering the queue from each neighbour). */
+void or_cc_linear(int64_t n, const int64_t *off, const int32_t *col, int32_t *id);
 void or_bc_f32(int64_t n, const int64_t *off, const int32_t *col, int32_t root,
                int32_t *nsp, float *dep);
 void or_bc_f64(int64_t n, const int64_t *off, const int32_t *col, int32_t root,
