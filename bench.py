@@ -305,7 +305,9 @@ def run_ours(args):
         if e2e_out:
             out["e2e"] = e2e_out
         if world == 1 and not args.no_cpu:
-            out["cpu_baseline"] = cpu_baseline(g, roots, args.cpu_seconds)
+            # the first two timed roots again, levels copied back, for the check
+            check = {int(r): g.bfs(int(r), run_opts(gs, selector))[0] for r in roots[W:W + 2]}
+            out["cpu_baseline"], out["parity"] = cpu_baseline(g, roots[W:], args.cpu_seconds, check)
     g.close()
     ctx.close()
     if dist:
@@ -533,23 +535,36 @@ def e2e(ctx, g, roots, gs, torch, selector="rules"):
     return ms, edges, len(roots), int(poff.nbytes + pcol.nbytes), int(plev.nbytes)
 
 
-def cpu_baseline(g, roots, budget_s):
+def cpu_baseline(g, roots, budget_s, gpu_levels=None):
+    """The oracle BFS (restated bfs_cpu) on the bench graph, one core, timed
+    over about budget_s of runs from the given roots.  As the checker it also
+    compares its levels with the GPU's for the roots in gpu_levels (the
+    bench's first timed roots, run again through the same switched form with
+    the levels copied back): returns (cpu_baseline entry, parity entry)."""
     import oracle
 
     off, col, _ = g.download()
     h = oracle.Csr(off, col)
+    gpu_levels = gpu_levels or {}
     t_total, e_total, runs = 0.0, 0, 0
+    checked, mismatches = [], 0
     for r in roots:
         t = time.perf_counter()
         lv = oracle.bfs(h, int(r))
         t_total += time.perf_counter() - t
         e_total += oracle.traversed_edges(h, lv)
         runs += 1
-        if t_total >= budget_s:
+        if int(r) in gpu_levels:
+            mismatches += int(np.count_nonzero(gpu_levels[int(r)] != lv))
+            checked.append(int(r))
+        if t_total >= budget_s and len(checked) == len(gpu_levels):
             break
-    return {"value": round(e_total / (t_total * 1e9), 5), "unit": "GTEPS", "cores": 1, "kind": "port",
+    base = {"value": round(e_total / (t_total * 1e9), 5), "unit": "GTEPS", "cores": 1, "kind": "port",
             "sample": f"{runs} full BFS runs on the same graph (oracle restatement of application/bfs.cu:38-62), "
                       f"{t_total:.1f} s", "cpu": cpu_model(), "nproc": os.cpu_count()}
+    parity = {"bfs_roots_checked": checked, "bfs_mismatches": mismatches, "vertices_per_root": int(h.n),
+              "against": "oracle bfs (restated application/bfs.cu:38-62) on the downloaded bench graph"}
+    return base, parity
 
 
 def cpu_model():
@@ -620,6 +635,52 @@ def run_reference(args):
     }))
 
 
+PROFILE_CASES = {
+    "bfs": "three BFS runs on RMAT scale 22 (ef 16, seed 1), learned selector",
+    "bfs24": "one BFS on RMAT scale 24 (ef 16, seed 1: the bench graph), learned selector",
+    "sssp": "SSSP on the 4096 x 4096 grid with 1% long-range edges (weights U[1, 1000]), "
+            "Push-Queue-WM-Fused levels one launch each",
+    "pr": "two PageRank iterations on RMAT scale 22, Pull-Bitmap-STRICT then 2D",
+    "mbfs": "batched 256-source BFS on RMAT scale 20",
+}
+
+
+def run_case(case: str) -> None:
+    """Small fixed workloads for profiler captures (ncu -k <kernel> python
+    bench.py --case <case>); they print no bench line."""
+    import gswitch_b200 as gs
+    from gswitch_b200.selector_train import load_model
+
+    if case not in PROFILE_CASES:
+        raise SystemExit(f"unknown case {case!r} ({', '.join(PROFILE_CASES)})")
+    ctx = gs.Context(0)
+    model, conf = load_model()
+    if model is not None:
+        ctx.mlp_load(model, conf)
+    if case == "bfs":
+        g = ctx.rmat(22, 16, seed=1)
+        for r in g.roots(1000, 3):
+            g.bfs(int(r), gs.RunOpts(selector="mlp"), out=False)
+    elif case == "bfs24":
+        g = ctx.rmat(24, 16, seed=1)
+        g.bfs(int(g.roots(1000, 1)[0]), gs.RunOpts(selector="mlp"), out=False)
+    elif case == "sssp":
+        g = ctx.grid(4096, 4096, 100, seed=1, wmax=1000, wseed=5)
+        o = gs.RunOpts.from_config("Push-Queue-WM-Fused")
+        o.persistent = False
+        g.sssp(int(g.roots(3, 1)[0]), o, out=False)
+    elif case == "pr":
+        g = ctx.rmat(22, 16, seed=1)
+        g.pagerank(2, 0.85, 0.0, opts="Pull-Bitmap-STRICT", out=False)
+        g.pagerank(2, 0.85, 0.0, opts="x-x-TWOD", out=False)
+    elif case == "mbfs":
+        g = ctx.rmat(20, 16, seed=1)
+        g.mbfs(g.roots(77, 256), batched=True, out=False)
+    print("ok", case)
+    g.close()
+    ctx.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -634,7 +695,11 @@ def main():
     ap.add_argument("--selector", default="mlp", choices=["mlp", "rules"])
     ap.add_argument("--no-apps", action="store_true")
     ap.add_argument("--c3", action="store_true", help="print config C3's switched-vs-fixed table instead")
+    ap.add_argument("--case", choices=sorted(PROFILE_CASES),
+                    help="run one small fixed workload for a profiler capture instead of the bench")
     args = ap.parse_args()
+    if args.case:
+        return run_case(args.case)
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
     if args.impl == "reference":

@@ -8,7 +8,9 @@ import tempfile
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-REF_APPS = "/root/reference/application"
+from gswitch_b200.compat import reference_tree
+
+REF_APPS = os.path.join(reference_tree(), "application")
 
 
 @pytest.mark.skipif(not os.path.isdir(REF_APPS), reason="reference tree not mounted")

@@ -13,7 +13,9 @@ import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 TABLES = os.path.join(ROOT, "gswitch_b200", "csrc", "engine", "selector_trees.h")
-REF_MODEL = "/root/reference/src/model"
+from gswitch_b200.compat import reference_tree
+
+REF_MODEL = os.path.join(reference_tree(), "src", "model")
 TREES = ["select_dir_idem", "select_dir_asso", "select_dir_asso_backup", "select_fmt", "select_fusion",
          "select_lb_idem", "select_lb_asso_forward", "select_lb_asso_forward_backup", "select_lb_asso_backward",
          "select_lb_asso_backward_backup", "select_stepping"]
