@@ -112,17 +112,25 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def level_bytes(kind, n, A, U, D, E):
+def level_bytes(kind, n, A, U, D, E, counted=-1):
     """Algorithmic bytes of one expand (int32 levels, bitmap state probes):
     push: work list + 16 B of row offsets per frontier vertex + 4 B column and
     2 bitmap probes per edge + 4 B level write per discovered vertex;
     pull: work list + 16 B offsets per candidate + 4 B column and one
-    frontier-bit probe per scanned edge + 4 B write per discovered vertex."""
+    frontier-bit probe per scanned edge + 4 B write per discovered vertex.
+    A kernel whose reads depend on the data counts the CSR side and the state
+    writes itself (counted > 0: the thread-mapped pull, 4 B first in-neighbour
+    per candidate, offsets and further columns only for the candidates that
+    walk on); the work list and the bitmap probes are added here."""
     direction, fmt = kind[0], kind[1]
     if direction == "Push":
         work = n / 8 if fmt == "Bitmap" else 4 * A
+        if counted > 0:
+            return work + counted + 0.25 * E
         return work + 16 * A + 4.25 * E + 4 * D
     work = n / 8 if fmt == "Bitmap" else 4 * U
+    if counted > 0:
+        return work + counted + 0.125 * E
     return work + 16 * U + 4.125 * E + 4 * D
 
 
@@ -151,8 +159,10 @@ def roofline_from(runs, n, peak_gbs, peak_kind):
             D = int(cnt[i + 1]) if i + 1 < len(cnt) else 0
             U = int(cnt[i + 1:].sum()) + unreached
             E = acc.level_edges[i] if i < len(acc.level_edges) else 0
+            counted = getattr(acc, "level_bytes", [])
+            counted = counted[i] if i < len(counted) else -1
             key = "expand " + "-".join(kind)
-            b = level_bytes(kind, n, A, U, D, max(E, 0))
+            b = level_bytes(kind, n, A, U, D, max(E, 0), counted)
             rec = per.setdefault(key, [0.0, 0.0, 0])
             rec[0] += timed.level_ms[i]
             rec[1] += b
@@ -321,6 +331,43 @@ FIXED = ["-".join((d, f, lb, "Standalone")) for d in ("Push", "Pull") for f in (
                                                           ("TM", "WM", "CM", "STRICT", "TWC")]
 
 
+def switch_headroom(g, app, root, pr_iters=2, ctx=None, model=None):
+    """How much per-level switching can gain over one fixed variant: every
+    standalone variant timed at each labelled level from the same state
+    (gsw_label_levels: all levels up to 24, then every 8th; PageRank's
+    iterations are alike, so two stand for all).  best_fixed = the smallest
+    column total over the variants that ran at every level; per_level_best =
+    the sum of each level's fastest; headroom = best_fixed / per_level_best
+    bounds the speed-up any per-level choice among these variants can reach.
+    With a model, the selectors' regret on the same levels: time of the
+    chosen variants over the per-level best, minus one (the rules' class and
+    the learned network's)."""
+    X, T, R = g.label(app, root, max_levels=4096, pr_iters=pr_iters)
+    if len(T) == 0:
+        return None
+    T = np.where(T > 0, T.astype(np.float64), np.inf)
+    full = np.isfinite(T).all(axis=0)
+    if not full.any():
+        return None
+    col_tot = T[:, full].sum(axis=0)
+    best_fixed = float(col_tot.min())
+    tbest = T.min(axis=1)
+    per_level = float(tbest.sum())
+    out = {"levels_labelled": int(len(T)), "best_fixed_ms": round(best_fixed, 4),
+           "per_level_best_ms": round(per_level, 4), "headroom": round(best_fixed / per_level, 3)}
+
+    def regret(choice):
+        t = T[np.arange(len(T)), np.clip(choice, 0, T.shape[1] - 1)]
+        ok = (choice >= 0) & np.isfinite(t)
+        return round(float(t[ok].sum() / tbest[ok].sum() - 1.0), 4) if ok.any() else None
+
+    out["regret_rules"] = regret(np.asarray(R))
+    if ctx is not None and model is not None:
+        cls, _ = ctx.mlp_infer(model, X)
+        out["regret_mlp"] = regret(np.asarray(cls))
+    return out
+
+
 def app_table(ctx, g, gs, args, roots, selector):
     """BFS, SSSP, CC and PageRank on the same RMAT
     graph (SSSP on an int32-weighted copy, weights U[1, 64]): the switched
@@ -331,6 +378,9 @@ def app_table(ctx, g, gs, args, roots, selector):
     sources) against 256 sequential switched BFS runs."""
     gw = ctx.rmat(args.scale, args.ef, 0.57, 0.19, 0.19, seed=1, wmax=64, wseed=2)
     root = int(roots[0])
+    from gswitch_b200.selector_train import load_model
+
+    model, _ = load_model()
     pr_iters = 5
 
     def once(app, o):
@@ -366,10 +416,24 @@ def app_table(ctx, g, gs, args, roots, selector):
                     continue
                 fixed[cfg] = round(measure(app, gs.RunOpts.from_config(cfg), 1)[0], 3)
         best = max(fixed.items(), key=lambda kv: kv[1])
+        if app != "cc":
+            lab = {"bfs": gs.APP_BFS, "sssp": gs.APP_SSSP, "pr": gs.APP_PR}[app]
+            row["switch_headroom_standalone"] = switch_headroom(gw if app == "sssp" else g, lab, root, ctx=ctx,
+                                                                 model=model)
         sw = row.get("switched_mlp" if selector == "mlp" and app != "cc" else "switched_rules")
         row.update({"fixed": fixed, "best_fixed": {"variant": best[0], "gteps": best[1]},
                     "switched_vs_best_fixed": round(sw / best[1], 3) if best[1] > 0 else None})
         table[app] = row
+    # hub sweeps of the tiered push (its CTA tier: lists of 256+ columns) with
+    # 4-byte loads, int4 loads, or shared-memory chunks filled by TMA bulk
+    # copies; GTEPS of the forced tiered variants on this graph
+    hubs = {}
+    for app in ("bfs", "sssp"):
+        for cfg in ("Push-Queue-TWC-Standalone", "Push-Queue-TWC-Fused"):
+            for name, hp in (("scalar", gs.HUB_SCALAR), ("vector", gs.HUB_VECTOR), ("staged_tma", gs.HUB_STAGED)):
+                o = gs.RunOpts.from_config(cfg, hub_path=hp)
+                hubs.setdefault(app, {}).setdefault(cfg, {})[name] = round(measure(app, o, 3)[0], 3)
+    table["hub_paths"] = hubs
     table["definitions"] = {"bfs": "sum deg(reached)/2 / t", "sssp": "sum deg(reached)/2 / t", "cc": "m/2 / t",
                             "pr": f"m x {pr_iters} iterations / t", "unit": "GTEPS", "graph": "same RMAT as the headline"}
     gw.close()

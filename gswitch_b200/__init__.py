@@ -35,8 +35,8 @@ ABI_SYMBOLS = (
     "gsw_init", "gsw_destroy", "gsw_last_error_string", "gsw_version",
     "gsw_graph_upload", "gsw_graph_generate_rmat", "gsw_graph_generate_grid",
     "gsw_graph_generate_er", "gsw_graph_info", "gsw_graph_attr", "gsw_graph_download",
-    "gsw_graph_destroy", "gsw_graph_roots", "gsw_ctx_stream", "gsw_run_opts_default", "gsw_bfs", "gsw_sssp", "gsw_cc",
-    "gsw_pagerank", "gsw_bc", "gsw_gc", "gsw_mbfs", "gsw_bfs_strict_noalloc",
+    "gsw_graph_destroy", "gsw_graph_roots", "gsw_ctx_stream", "gsw_ctx_record_features", "gsw_run_opts_default", "gsw_bfs", "gsw_sssp", "gsw_cc",
+    "gsw_pagerank", "gsw_bc", "gsw_bc_batch", "gsw_gc", "gsw_mbfs", "gsw_bfs_strict_noalloc",
     "gsw_graph_generate_powerlaw", "gsw_label_levels", "gsw_mlp_train", "gsw_mlp_grad", "gsw_mlp_infer",
     "gsw_mlp_load", "gsw_graph_generate_er_batch", "gsw_bfs_multi", "gsw_bfs_inspect", "gsw_tune_load",
     "gsw_tune_save", "gsw_mlp_load_fusion", "gsw_pagerank_delta",
@@ -67,7 +67,8 @@ class _Opts(C.Structure):
                 ("sorted_queue", C.c_int), ("max_iters", C.c_int), ("damping", C.c_float),
                 ("eps", C.c_float), ("selector", C.c_int), ("verbose", C.c_int), ("timing", C.c_int),
                 ("expand_grid", C.c_int), ("account", C.c_int), ("persistent", C.c_int), ("barrier_test", C.c_int),
-                ("captured", C.c_int), ("reserved", C.c_int * 4)]
+                ("captured", C.c_int), ("hub_path", C.c_int),
+                ("reserved", C.c_int * 3)]
 
 
 class _Stats(C.Structure):
@@ -75,7 +76,7 @@ class _Stats(C.Structure):
                 ("device_error", C.c_uint), ("launches", C.c_int64), ("ntrace", C.c_int),
                 ("level_cfg", C.c_int32 * MAX_TRACE), ("level_frontier", C.c_int64 * MAX_TRACE),
                 ("level_ms", C.c_float * MAX_TRACE), ("level_inspect_ms", C.c_float * MAX_TRACE),
-                ("level_edges", C.c_int64 * MAX_TRACE)]
+                ("level_edges", C.c_int64 * MAX_TRACE), ("level_bytes", C.c_int64 * MAX_TRACE)]
 
 
 _LIB = None
@@ -105,6 +106,7 @@ def lib():
     L.gsw_graph_destroy.argtypes = [vp]
     L.gsw_graph_roots.argtypes = [vp, u64, C.c_int, vp]
     L.gsw_ctx_stream.argtypes = [vp, pvp]
+    L.gsw_ctx_record_features.argtypes = [vp, C.c_char_p]
     L.gsw_run_opts_default.argtypes = [C.POINTER(_Opts)]
     L.gsw_run_opts_default.restype = None
     po, ps = C.POINTER(_Opts), C.POINTER(_Stats)
@@ -116,6 +118,7 @@ def lib():
     L.gsw_bc.argtypes = [vp, vp, i32, po, vp, vp, ps]
     L.gsw_gc.argtypes = [vp, vp, po, vp, ps]
     L.gsw_mbfs.argtypes = [vp, vp, C.c_int, vp, C.c_int, po, vp, ps]
+    L.gsw_bc_batch.argtypes = [vp, vp, C.c_int, vp, po, vp, vp, ps]
     L.gsw_bfs_strict_noalloc.argtypes = [i64, i64, vp, vp, i32, vp, vp]
     L.gsw_graph_generate_powerlaw.argtypes = [vp, i64, C.c_double, u64, C.c_int, u64, pvp]
     L.gsw_label_levels.argtypes = [vp, vp, C.c_int, i32, C.c_int, C.c_int, vp, vp, vp, C.POINTER(C.c_int)]
@@ -143,12 +146,17 @@ def _ptr(a):
     return None if a is None else a.ctypes.data_as(C.c_void_p)
 
 
+# how a CTA sweeps one hub's adjacency list (gsw_run_opts.hub_path)
+HUB_SCALAR, HUB_VECTOR, HUB_STAGED = 0, 1, 2
+
+
 class RunOpts:
     """Forced choices and knobs of one run (None = selector decides)."""
 
     def __init__(self, direction=None, asfmt=None, lb=None, fusion=None, sorted_queue=True,
                  max_iters=0, damping=0.85, eps=0.01, verbose=False, timing=False, expand_grid=0,
-                 account=False, persistent=None, barrier_test=False, captured=False, selector="rules"):
+                 account=False, persistent=None, barrier_test=False, captured=False, selector="rules",
+                 hub_path=None):
         self.direction, self.asfmt, self.lb, self.fusion = direction, asfmt, lb, fusion
         self.sorted_queue, self.max_iters, self.damping, self.eps = sorted_queue, max_iters, damping, eps
         self.verbose, self.timing, self.expand_grid = verbose, timing, expand_grid
@@ -157,6 +165,7 @@ class RunOpts:
         self.barrier_test = barrier_test
         self.captured = captured
         self.selector = selector  # "rules" (decision trees) or "mlp" (loaded network, rules as fallback)
+        self.hub_path = hub_path  # HUB_SCALAR / HUB_VECTOR / HUB_STAGED (None: by edge data)
 
     @classmethod
     def from_config(cls, cfg: str, **kw):
@@ -183,6 +192,7 @@ class RunOpts:
         o.barrier_test = int(self.barrier_test)
         o.captured = int(bool(self.captured))
         o.selector = SELECT_MLP if self.selector == "mlp" else SELECT_RULES
+        o.hub_path = AUTO if self.hub_path is None else int(self.hub_path)
         return o
 
 
@@ -195,9 +205,12 @@ class RunStats:
         self.launches = s.launches
         n = min(s.ntrace, MAX_TRACE)
         self.trace = [decode_cfg(s.level_cfg[i]) + (int(s.level_frontier[i]),) for i in range(n)]
+        # levels whose expand was a persistent (grid-barrier) launch
+        self.level_persistent = [bool(s.level_cfg[i] & 64) for i in range(n)]
         self.level_ms = [float(s.level_ms[i]) for i in range(n)]
         self.level_inspect_ms = [float(s.level_inspect_ms[i]) for i in range(n)]
         self.level_edges = [int(s.level_edges[i]) for i in range(n)]
+        self.level_bytes = [int(s.level_bytes[i]) for i in range(n)]
 
     @property
     def gteps(self) -> float:
@@ -238,6 +251,11 @@ class Context:
         s = C.c_void_p()
         _check(lib().gsw_ctx_stream(self._h, C.byref(s)))
         return s.value or 0
+
+    def record_features(self, path):
+        """Append the reference's training records (feature_t::record) of
+        every level of later runs to `path` (None: stop recording)."""
+        _check(lib().gsw_ctx_record_features(self._h, path.encode() if path else None))
 
     def __enter__(self):
         return self
@@ -462,6 +480,18 @@ class Graph:
         col = np.empty(self.n, dtype=np.int32) if out else None
         st = self._run(lib().gsw_gc, outs=[col], opts=opts)
         return col, st
+
+    def bc_batch(self, roots, opts=None, out=True):
+        """Path counts and dependencies from every root (rows of n, one per
+        root), the sources advancing together in batches of 32."""
+        roots = np.ascontiguousarray(roots, dtype=np.int32)
+        nsp = np.empty((len(roots), self.n), dtype=np.int32) if out else None
+        dep = np.empty((len(roots), self.n), dtype=np.float32) if out else None
+        st = _Stats()
+        o = self._opts(opts)
+        _check(lib().gsw_bc_batch(self.ctx._h, self._h, len(roots), _ptr(roots), C.byref(o), _ptr(nsp), _ptr(dep),
+                                  C.byref(st)))
+        return nsp, dep, RunStats(st)
 
     def mbfs(self, roots, batched=True, opts=None, out=True):
         roots = np.ascontiguousarray(roots, dtype=np.int32)

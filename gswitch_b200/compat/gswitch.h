@@ -93,7 +93,7 @@ inline void gsw_compat_help(const std::string &exec) {
             << "  -d, --directed         the graph is directed\n"
             << "  -c, --configs=Push-Queue-CM-Fused   force choices (x = selector)\n"
             << "  -D, --device=<int>     GPU\n"
-            << "  -j, --json=<string>    (accepted, unused)\n";
+            << "  -j, --json=<string>    append feature_t::record() blocks to this file\n";
 }
 
 inline void parse_cmd(int argc, char *argv[], std::string exec = "test") {
@@ -583,6 +583,9 @@ graph_t<gsw_graph_fmt<C, E>::value, E> build_graph(edgelist_t<E> el, feature_t &
   }
   g.dg = gsw_compat::upload(g.hg);
   gsw_compat::set_features(fets, g.el, g.hg);
+  // fets.record() appends to the -j file (features.cuh:96-104 reads
+  // cmd_opt.json the same way); no -j, no records
+  fets.record_path = cmd_opt.json.empty() ? nullptr : cmd_opt.json.c_str();
   return g;
 }
 

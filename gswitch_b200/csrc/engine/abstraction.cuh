@@ -11,6 +11,7 @@
 // a forced-variant override (the reference's `-c Dir-Fmt-LB-Fusion`) lives
 // in config_t so one process can run several forced configurations.
 #pragma once
+#include <sstream>
 #include <cmath>
 #include <cstdlib>
 #include <vector>
@@ -269,6 +270,12 @@ struct config_t {
   // engine extensions
   bool conf_sorted_queue = true;   // bitmap->queue in vertex order
   bool conf_persistent = false;    // run fused levels in one grid-wide launch
+  bool conf_pull_prefetch = false;  // thread-mapped pull: most candidates will
+                                   // walk on (start at the row offsets rather
+                                   // than the first-in-neighbour array)
+  int conf_hub_path = -1;          // how CTA-wide hub sweeps read columns
+                                   // (HUB_SCALAR / HUB_VECTOR / HUB_STAGED;
+                                   // -1: by the graph's edge data)
   bool conf_count_edges = false;   // accounting pass: expands count edges
   ins_t force;                     // forced choices (empty = selector decides)
 
@@ -327,6 +334,7 @@ struct stat_t {
   double avg_filter_time = 0, avg_expand_time = 0;
   int level = 0;
   int64_t last_scanned = 0;  // edges the last expand touched (accounting)
+  int64_t last_abytes = 0;   // algorithmic bytes it reported (0: none)
 
   void build(int _size = gsw::STAT_SLOTS) {
     if (dg_runtime_info) return;
@@ -430,7 +438,8 @@ struct feature_t {
   int thread_lim = 0, register_lim = 0, sm_num = 0;
 
   double fv[21] = {0};
-  const char *record_path = nullptr;  // JSON-lines sink for record()
+  const char *record_path = nullptr;  // sink of record() (nullptr: none)
+  int records = 0;                    // record() blocks written so far
 
   void reset() {}
 
@@ -497,14 +506,25 @@ struct feature_t {
     cur_max_deg_unactive = fv[18];
   }
 
+  // The training record of src/abstraction/features.cuh:86-104 with the
+  // writer of src/utils/json.cuh:34-48: the 21 flattened features and the
+  // last filter / expand times as keys "0".."22", values in the stream's
+  // default format (6 significant digits), one "{ ... }" block per call
+  // appended to record_path; a feature object writes at most 100 blocks.
   void record() {
     flatten();
     if (!record_path) return;
+    if (++records > 100) return;
+    std::ostringstream o;
+    o << "{\n";
+    for (int i = 0; i < 23; ++i) {
+      if (i > 0) o << ",\n";
+      o << "\"" << i << "\": " << (i < 21 ? fv[i] : i == 21 ? last_filter_time : last_expand_time);
+    }
+    o << "\n}\n";
     FILE *f = fopen(record_path, "a");
     if (!f) return;
-    fprintf(f, "{");
-    for (int i = 0; i < 21; ++i) fprintf(f, "\"%d\": %.17g, ", i, fv[i]);
-    fprintf(f, "\"21\": %.17g, \"22\": %.17g}\n", last_filter_time, last_expand_time);
+    fputs(o.str().c_str(), f);
     fclose(f);
   }
 

@@ -72,6 +72,7 @@ enum device_error_bits : unsigned {
   DEV_ERR_BARRIER_TIMEOUT = 2u,
   DEV_ERR_BAD_VERTEX = 4u,
   DEV_ERR_SCRATCH_OVERFLOW = 8u,
+  DEV_ERR_STAGE_TIMEOUT = 16u,  // a shared-memory staging copy did not complete
 };
 
 // Sticky host-side error (first error wins until cleared), one per thread.
@@ -258,6 +259,64 @@ __device__ __forceinline__ uint64_t globaltimer_ns() {
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
   return t;
 }
+
+// ---- 1-D TMA bulk copies global -> shared (cp.async.bulk, no multicast) ----
+// Used to stage runs of a hub's adjacency list in shared memory.  The source
+// is always this GPU's own memory (the graph's column array); source and
+// destination are 16-byte aligned and the size is a multiple of 16 bytes
+// (callers copy the aligned body of a run and read its ragged ends with
+// plain loads).  Completion is tracked by a CTA-local mbarrier: one thread
+// arms it with the byte count and issues the copy; every thread waits on the
+// barrier's phase parity.
+__device__ __forceinline__ unsigned smem_addr(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(unsigned long long *bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+// makes barrier initialisation visible to the async proxy (bulk copies)
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void mbar_inval(unsigned long long *bar) {
+  asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long *bar, unsigned bytes) {
+  unsigned long long state;
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 %0, [%1], %2;"
+               : "=l"(state)
+               : "r"(smem_addr(bar)), "r"(bytes)
+               : "memory");
+  asm volatile("" ::"l"(state));  // the arrival token is not needed
+}
+__device__ __forceinline__ void bulk_copy_g2s(void *dst, const void *src, unsigned bytes, unsigned long long *bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_addr(dst)),
+               "l"(src), "r"(bytes), "r"(smem_addr(bar))
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_test(unsigned long long *bar, unsigned parity) {
+  unsigned done;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(done)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+// Bounded wait for a phase: false (and DEV_ERR_STAGE_TIMEOUT in *err) after
+// about `budget_ns`; a copy from valid device memory completes long before.
+__device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned parity, unsigned *err,
+                                          uint64_t budget_ns = 200000000ull) {
+  if (mbar_test(bar, parity)) return true;
+  const uint64_t t0 = globaltimer_ns();
+  while (!mbar_test(bar, parity)) {
+    if (globaltimer_ns() - t0 > budget_ns) {
+      atomicOr(err, DEV_ERR_STAGE_TIMEOUT);
+      return false;
+    }
+  }
+  return true;
+}
+// orders this thread's earlier generic-proxy accesses of shared memory before
+// a following async-proxy (bulk copy) write to it
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
 }  // namespace gsw
 

@@ -685,7 +685,14 @@ struct executor_t {
           break;
         }
         case TM:
-        default: GSW_GO((k_pull_tm<G, F>), fr < 0 ? -1 : fr / B + 1, as, g, f, conf); break;
+        default: {
+          // a frontier that is a small share of the candidates settles few of
+          // them at their first in-neighbour: most walk on
+          config_t c = conf;
+          c.conf_pull_prefetch = insp && insp->raw_frontier * 20 < insp->raw_inactive;
+          GSW_GO((k_pull_tm<G, F>), fr < 0 ? -1 : fr / B + 1, as, g, f, c);
+          break;
+        }
       }
     }
 #undef GSW_GO
@@ -821,7 +828,10 @@ struct executor_t {
     const bool sync_needed = conf.conf_fuse_inspect || opts().verbose;
     if (sync_needed && !ev[0])
       for (auto &e : ev) cudaEventCreate(&e);
-    if (conf.conf_count_edges) GSW_CUDA(cudaMemsetAsync(&as.dg_cnt->scanned, 0, sizeof(unsigned long long), stream()));
+    if (conf.conf_count_edges) {
+      GSW_CUDA(cudaMemsetAsync(&as.dg_cnt->scanned, 0, sizeof(unsigned long long), stream()));
+      GSW_CUDA(cudaMemsetAsync(&as.dg_cnt->abytes, 0, sizeof(unsigned long long), stream()));
+    }
     if (sync_needed) cudaEventRecord(ev[0], stream());
     marks().exp0 = opts().timing ? timing_pool().record() : -1;
     last_persistent = false;
@@ -838,11 +848,14 @@ struct executor_t {
       e = s + ms;
     }
     stat.last_scanned = 0;
+    stat.last_abytes = 0;
     if (conf.conf_count_edges) {
-      unsigned long long c = 0;
+      unsigned long long c = 0, b = 0;
       GSW_CUDA(cudaMemcpyAsync(&c, &as.dg_cnt->scanned, sizeof(c), cudaMemcpyDeviceToHost, stream()));
+      GSW_CUDA(cudaMemcpyAsync(&b, &as.dg_cnt->abytes, sizeof(b), cudaMemcpyDeviceToHost, stream()));
       GSW_CUDA(cudaStreamSynchronize(stream()));
       stat.last_scanned = (int64_t)c;
+      stat.last_abytes = (int64_t)b;
     }
     stat.last_time = stat.last_filter_time + e - s;
     const int lv = g.level > 0 ? g.level : 1;

@@ -133,6 +133,12 @@ __device__ __forceinline__ void vertex_range(const G &g, bool pull, int v, int64
 __device__ __forceinline__ void account(const active_set_t &as, const config_t &conf, unsigned long long c) {
   if (conf.conf_count_edges && c) atomicAdd(&as.dg_cnt->scanned, c);
 }
+// accounting pass only: the bytes of the CSR side of the algorithm (offsets,
+// columns, first in-neighbours) and of the vertex-state writes that a kernel
+// whose reads depend on its data counts for itself
+__device__ __forceinline__ void account_bytes(const active_set_t &as, const config_t &conf, unsigned long long b) {
+  if (conf.conf_count_edges && b) atomicAdd(&as.dg_cnt->abytes, b);
+}
 
 // Where a push body reads its work list.  Per-launch kernels read the active
 // set (queue or bitmap, read-only path).  Levels inside a persistent launch
@@ -229,15 +235,26 @@ __global__ void __launch_bounds__(EXPAND_THREADS) k_push_tm(active_set_t as, G g
 // more candidates per thread cost more in divergence than they gain in
 // overlap (RMAT s24 pull levels: 105 us at 1, 93 at 2, 103 at 4, 135 at 8;
 // fetching four neighbours per step of the walk was slower too).
+//
+// With the first-in-neighbour array (graphs without edge data) the chain
+// starts at one coalesced 4-byte read: a candidate whose first in-neighbour
+// is in the frontier is settled without its row offsets or a 32-byte column
+// sector; only the others read their offsets and walk on.
 template <typename G, typename F>
 __global__ void __launch_bounds__(EXPAND_THREADS) k_pull_tm(active_set_t as, G g, F f, config_t conf) {
   using WA = typename F::wa_t;
   constexpr int K = GSW_PULL_TM_K;
+  constexpr bool NO_EDATA = std::is_same<typename G::edge_t, Empty>::value;
   const int64_t n = as.get_size();
   GSW_HALT_IF_EMPTY(n);
   const Status want = conf.want();
   const int64_t STRIDE = (int64_t)blockDim.x * gridDim.x;
-  unsigned long long cnt = 0;
+  // the side array pays off where most candidates settle at their first
+  // in-neighbour; where most walk on (conf_pull_prefetch: the frontier is a
+  // small share of the candidates) the walk starts at the row offsets, and
+  // the first column shares its sector with the rest of the walk
+  const bool first_path = NO_EDATA && g.dgr_first != nullptr && !conf.conf_pull_prefetch;
+  unsigned long long cnt = 0, abytes = 0;
   for (int64_t base = threadIdx.x + (int64_t)blockIdx.x * blockDim.x; base < n; base += K * STRIDE) {
     int v[K], deg[K], u0[K];
     int64_t st[K];
@@ -246,13 +263,39 @@ __global__ void __launch_bounds__(EXPAND_THREADS) k_pull_tm(active_set_t as, G g
     for (int k = 0; k < K; ++k) {
       const int64_t idx = base + k * STRIDE;
       v[k] = idx < n ? as.fetch(idx, want) : -1;
+      // a vertex without in-edges has nothing to pull; in the bitmap format
+      // its bit is read beside the status word, not after it
+      const int64_t probe = as.fmt == Bitmap ? idx : (int64_t)v[k];
+      if (probe >= 0 && probe < n && g.dgr_nonempty && !((__ldg(g.dgr_nonempty + (probe >> 5)) >> (probe & 31)) & 1u))
+        v[k] = -1;
     }
+    if (first_path) {
 #pragma unroll
-    for (int k = 0; k < K; ++k) vertex_range(g, true, v[k], st[k], deg[k]);
+      for (int k = 0; k < K; ++k) u0[k] = v[k] >= 0 ? __ldg(g.dgr_first + v[k]) : -1;
 #pragma unroll
-    for (int k = 0; k < K; ++k) u0[k] = deg[k] > 0 ? __ldg(g.dgr_adj_list + st[k]) : 0;
+      for (int k = 0; k < K; ++k) abytes += v[k] >= 0 ? 4 : 0;
 #pragma unroll
-    for (int k = 0; k < K; ++k) a0[k] = deg[k] > 0 && (conf.conf_fromall || as.bitmap.is_active(u0[k]));
+      for (int k = 0; k < K; ++k) a0[k] = u0[k] >= 0 && (conf.conf_fromall || as.bitmap.is_active(u0[k]));
+#pragma unroll
+      for (int k = 0; k < K; ++k) {
+        if (u0[k] >= 0 && !(a0[k] && conf.conf_pruning)) {
+          vertex_range(g, true, v[k], st[k], deg[k]);
+          abytes += 16;  // offsets
+        } else {
+          st[k] = 0;
+          deg[k] = u0[k] >= 0 ? 1 : 0;  // settled at the first in-neighbour, or no in-edges
+        }
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < K; ++k) vertex_range(g, true, v[k], st[k], deg[k]);
+#pragma unroll
+      for (int k = 0; k < K; ++k) abytes += v[k] >= 0 ? 16 : 0;
+#pragma unroll
+      for (int k = 0; k < K; ++k) u0[k] = deg[k] > 0 ? __ldg(g.dgr_adj_list + st[k]) : 0;
+#pragma unroll
+      for (int k = 0; k < K; ++k) a0[k] = deg[k] > 0 && (conf.conf_fromall || as.bitmap.is_active(u0[k]));
+    }
 #pragma unroll
     for (int k = 0; k < K; ++k) {
       if (v[k] < 0 || deg[k] == 0) continue;
@@ -282,10 +325,14 @@ __global__ void __launch_bounds__(EXPAND_THREADS) k_pull_tm(active_set_t as, G g
         }
       }
       cnt += e;
+      // column entries read (the first came from the side array on that
+      // path), and the state write
+      abytes += 4ull * (e - (first_path ? 1 : 0)) + (have ? sizeof(WA) : 0);
       if (have) f.comp(f.wa_of(v[k]), acc, g);
     }
   }
   account(as, conf, cnt);
+  account_bytes(as, conf, abytes);
 }
 
 // ===========================================================================
@@ -843,6 +890,103 @@ __global__ void __launch_bounds__(EXPAND_THREADS) k_pull_strict_all(active_set_t
 }
 
 // ===========================================================================
+// Hub runs: the edges [a, a + len) of one vertex swept by the whole CTA
+// ===========================================================================
+// How a CTA reads a hub's columns (config_t::conf_hub_path):
+//   HUB_SCALAR  4-byte read-only loads, one column per thread per round;
+//   HUB_VECTOR  the 16-byte-aligned body of the run with int4 loads, four
+//               consecutive columns per thread per round;
+//   HUB_STAGED  the aligned body moves to shared memory in HUB_CHUNK-column
+//               chunks by 1-D TMA bulk copies into two buffers (chunk c+2 is
+//               issued into a buffer as soon as chunk c has been consumed, so
+//               the next chunk is in flight while the CTA works on one).
+// The ragged head and tail of a run (fewer than 4 columns each) are read
+// with plain loads.  `edge(valid, u, ei)` runs for every thread in every
+// round (warp-uniform trip counts, so fused levels can stage their appends
+// per warp).  The staged form returns false, in every thread, if a copy did
+// not complete in time; the caller then leaves the kernel.
+enum { HUB_SCALAR = 0, HUB_VECTOR = 1, HUB_STAGED = 2 };
+constexpr int HUB_CHUNK = 2048;  // columns per staged chunk (8 KB)
+
+struct hub_stage_t {
+  int (*buf)[HUB_CHUNK];     // [2][HUB_CHUNK] in shared memory, 16-byte aligned
+  unsigned long long *bar;   // [2] mbarriers, initialised with count 1
+  unsigned ph[2] = {0, 0};   // phase parity each buffer waits for next
+};
+
+template <int B, typename EDGE>
+__device__ __forceinline__ bool hub_run(const int *col, int64_t a, int64_t len, int path, hub_stage_t &hs,
+                                        unsigned *err, EDGE &&edge) {
+  const int t = threadIdx.x;
+  const int64_t e = a + len;
+  const int64_t ba = (a + 3) & ~int64_t(3), bb = e & ~int64_t(3);
+  if (path == HUB_SCALAR || bb - ba < 4 * B) {
+    for (int64_t base = a; base < e; base += B) {
+      const int64_t k = base + t;
+      edge(k < e, k < e ? __ldg(col + k) : -1, k);
+    }
+    return true;
+  }
+  {  // ragged ends: head [a, ba) on threads 0.., tail [bb, e) after them
+    const int nh = (int)(ba - a), nt = (int)(e - bb);
+    const int64_t k = t < nh ? a + t : bb + (t - nh);
+    const bool valid = t < nh + nt;
+    edge(valid, valid ? __ldg(col + k) : -1, k);
+  }
+  if (path == HUB_VECTOR) {
+    const int4 *c4 = reinterpret_cast<const int4 *>(col + ba);
+    const int64_t n4 = (bb - ba) >> 2;
+    for (int64_t r = t; r - t < n4; r += B) {
+      const bool valid = r < n4;
+      int4 q = make_int4(-1, -1, -1, -1);
+      if (valid) q = __ldg(c4 + r);
+      const int64_t k = ba + 4 * r;
+      edge(valid, q.x, k);
+      edge(valid, q.y, k + 1);
+      edge(valid, q.z, k + 2);
+      edge(valid, q.w, k + 3);
+    }
+    return true;
+  }
+  // staged: chunks [ba + c*HUB_CHUNK, ...) of the body
+  const int64_t body = bb - ba;
+  const int nch = (int)((body + HUB_CHUNK - 1) / HUB_CHUNK);
+  auto issue = [&](int c) {
+    const int64_t c0 = ba + (int64_t)c * HUB_CHUNK;
+    const unsigned bytes = (unsigned)(4 * MIN((int64_t)HUB_CHUNK, bb - c0));
+    fence_proxy_async_smem();
+    mbar_expect_tx(&hs.bar[c & 1], bytes);
+    bulk_copy_g2s(hs.buf[c & 1], col + c0, bytes, &hs.bar[c & 1]);
+  };
+  __syncthreads();  // the buffers' previous contents are consumed
+  if (t == 0) {
+    issue(0);
+    if (nch > 1) issue(1);
+  }
+  bool okk = true;
+  for (int c = 0; c < nch; ++c) {
+    const int b = c & 1;
+    const bool arrived = mbar_wait(&hs.bar[b], hs.ph[b], err);
+    hs.ph[b] ^= 1u;
+    okk = __syncthreads_and(arrived) != 0;
+    if (!okk) {
+      // let a copy still in flight land before the CTA leaves
+      if (t == 0 && c + 1 < nch) mbar_wait(&hs.bar[b ^ 1], hs.ph[b ^ 1], err);
+      return false;
+    }
+    const int64_t c0 = ba + (int64_t)c * HUB_CHUNK;
+    const int cn = (int)MIN((int64_t)HUB_CHUNK, bb - c0);
+    for (int base = 0; base < cn; base += B) {
+      const int k = base + t;
+      edge(k < cn, k < cn ? hs.buf[b][k] : -1, c0 + k);
+    }
+    __syncthreads();  // chunk c consumed: its buffer takes chunk c+2
+    if (t == 0 && c + 2 < nch) issue(c + 2);
+  }
+  return true;
+}
+
+// ===========================================================================
 // TWC: thread / warp / CTA tiers by degree
 // ===========================================================================
 template <bool FUSED, typename G, typename F, typename Src>
@@ -857,8 +1001,24 @@ __device__ __forceinline__ void push_twc_body(active_set_t &as, const G &g, F &f
   __shared__ int s_v[B];
   __shared__ int64_t s_st[B];
   __shared__ int s_tmp[33];
+  __shared__ __align__(16) int s_hub[2][HUB_CHUNK];
+  __shared__ __align__(8) unsigned long long s_bar[2];
   const int lane = lane_id();
-  if (threadIdx.x == 0) s_owner = -1;
+  // measured on RMAT scale 24 (forced tiered push, whole runs): staging in
+  // shared memory is fastest without edge data (BFS 7.3 -> 11.5 GTEPS), int4
+  // loads with it (SSSP 6.1 -> 10.7); the edge data stays in global memory
+  const int hub_path = conf.conf_hub_path >= 0 ? conf.conf_hub_path
+                                               : (std::is_same<typename G::edge_t, Empty>::value ? HUB_STAGED
+                                                                                                 : HUB_VECTOR);
+  hub_stage_t hs{s_hub, s_bar};
+  if (threadIdx.x == 0) {
+    s_owner = -1;
+    if (hub_path == HUB_STAGED) {
+      mbar_init(&s_bar[0], 1);
+      mbar_init(&s_bar[1], 1);
+      fence_mbar_init();
+    }
+  }
   __syncthreads();
   for (int64_t tile = blockIdx.x; tile * B < n; tile += gridDim.x) {
     const int64_t idx = tile * B + threadIdx.x;
@@ -885,19 +1045,18 @@ __device__ __forceinline__ void push_twc_body(active_set_t &as, const G &g, F &f
       const int cv = s_cv, cdeg = s_cdeg;
       const int64_t cst = s_cst;
       if (threadIdx.x == 0) account(as, conf, (unsigned long long)cdeg);
-      for (int base = 0; base < cdeg; base += B) {
-        const int k = base + threadIdx.x;
-        bool tp = false;
-        int u = -1;
-        if (k < cdeg) {
-          u = __ldg(g.dg_adj_list + cst + k);
-          if (FUSED)
-            tp = push_edge_fused(as, g, f, conf, cv, u, cst + k);
-          else
-            push_edge_std(as, g, f, conf, cv, u, cst + k);
-        }
-        if (FUSED) stage.push(tp, u);
-      }
+      const bool okk = hub_run<B>(g.dg_adj_list, cst, cdeg, hub_path, hs, &as.dg_cnt->err,
+                                  [&](bool valid, int u, int64_t ei) {
+                                    bool tp = false;
+                                    if (valid) {
+                                      if (FUSED)
+                                        tp = push_edge_fused(as, g, f, conf, cv, u, ei);
+                                      else
+                                        push_edge_std(as, g, f, conf, cv, u, ei);
+                                    }
+                                    if (FUSED) stage.push(tp, u);
+                                  });
+      if (!okk) return;  // a staging copy timed out (recorded in the error word)
       __syncthreads();
     }
     // warp tier
@@ -950,6 +1109,12 @@ __device__ __forceinline__ void push_twc_body(active_set_t &as, const G &g, F &f
       if (FUSED) stage.push(tp, u);
     }
     __syncthreads();
+  }
+  // the barriers may be initialised again by the next call (persistent
+  // launches run this body once per level); every copy has landed
+  if (hub_path == HUB_STAGED && threadIdx.x == 0) {
+    mbar_inval(&s_bar[0]);
+    mbar_inval(&s_bar[1]);
   }
 }
 

@@ -51,29 +51,31 @@ __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned *p) {
   return v;
 }
 
-// Sense-free generation barrier over all blocks of a cooperative launch.
-// Returns false (in every thread) after a timeout or a recorded error.
-__device__ __forceinline__ bool grid_barrier(as_counters_t *c, unsigned &gen, unsigned long long budget_ns) {
+// Sense-free generation barrier over all blocks of a cooperative launch, on
+// an arrival counter, a generation word and an error word in global memory.
+// Returns false (in every thread) after a timeout or a recorded timeout.
+__device__ __forceinline__ bool grid_barrier(unsigned *count, unsigned *genw, unsigned *err, unsigned &gen,
+                                             unsigned long long budget_ns) {
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
     const unsigned target = gen + 1;
     __threadfence();
-    const unsigned arrived = atomicAdd(&c->bar_count, 1u) + 1;
+    const unsigned arrived = atomicAdd(count, 1u) + 1;
     bool okk = true;
     if (arrived == gridDim.x) {
-      atomicExch(&c->bar_count, 0u);
+      atomicExch(count, 0u);
       __threadfence();
-      atomicExch(&c->bar_gen, target);
+      atomicExch(genw, target);
     } else {
       const unsigned long long t0 = globaltimer_ns();
-      while (ld_acquire_u32(&c->bar_gen) != target) {
-        if (ld_acquire_u32(&c->err) & DEV_ERR_BARRIER_TIMEOUT) {
+      while (ld_acquire_u32(genw) != target) {
+        if (ld_acquire_u32(err) & DEV_ERR_BARRIER_TIMEOUT) {
           okk = false;
           break;
         }
         if (globaltimer_ns() - t0 > budget_ns) {
-          atomicOr(&c->err, DEV_ERR_BARRIER_TIMEOUT);
+          atomicOr(err, DEV_ERR_BARRIER_TIMEOUT);
           okk = false;
           break;
         }
@@ -89,6 +91,9 @@ __device__ __forceinline__ bool grid_barrier(as_counters_t *c, unsigned &gen, un
   // state written by other SMs in the previous level see the new values
   __threadfence();
   return s_ok != 0;
+}
+__device__ __forceinline__ bool grid_barrier(as_counters_t *c, unsigned &gen, unsigned long long budget_ns) {
+  return grid_barrier(&c->bar_count, &c->bar_gen, &c->err, gen, budget_ns);
 }
 
 // Grid-wide (degree+1) scan of a STRICT level's frontier src[0..n): block b

@@ -20,6 +20,7 @@
 #include "engine/devloop.cuh"
 #include "engine/mlp.cuh"
 #include "graphgen.cuh"
+#include "bc_batch.cuh"
 #include "mbfs.cuh"
 
 using namespace gsw;
@@ -35,6 +36,8 @@ struct gsw_graph {
   int *col = nullptr, *odeg = nullptr, *w = nullptr;
   int64_t *roff = nullptr;
   int *rcol = nullptr, *rdeg = nullptr, *rw = nullptr;
+  int *first = nullptr, *rfirst = nullptr;  // first (in-)neighbour per vertex, -1: none
+  uint32_t *nonempty = nullptr, *rnonempty = nullptr;  // bit per vertex: has (in-)edges
   packed_t *coo = nullptr;
   int64_t ncoo = -1;
   double attr[6] = {0, 0, 0, 0, 0, 0};
@@ -60,6 +63,8 @@ struct gsw_graph {
     g.dgr_adj_list = directed ? rcol : col;
     g.dgr_odegree = directed ? rdeg : odeg;
     g.dgr_edgedata = (E *)(directed ? rw : w);
+    g.dgr_first = directed ? rfirst : first;
+    g.dgr_nonempty = directed ? rnonempty : nonempty;
     g.nvertexs = (int)n;
     g.nedges = m;
     g.level = 0;
@@ -83,6 +88,7 @@ struct gsw_ctx {
   mlp_model mlp{};                // learned selector (valid = 0: none loaded)
   mlp_model mlp_fusion{};         // learned fusion decision of Mono-pattern runs
   mlp_model *dmlp = nullptr;      // its device copy (captured loops)
+  std::string record_path;        // per-level feature records (empty: off)
 
   // Device blocks of destroyed graphs, kept for the next graph of a fitting
   // size: a graph uploaded per call otherwise pays a fresh cudaMalloc and
@@ -179,12 +185,21 @@ thread_local std::string g_last_error;
 
 namespace {
 
+// where the level loops of the current call write feature records (nullptr:
+// nowhere); set from the context on every entry
+inline const char *&record_sink() {
+  static thread_local const char *p = nullptr;
+  return p;
+}
+
 struct entry_guard {  // binds the context's device and stream for one call
   explicit entry_guard(gsw_ctx *ctx) {
     clear_error();
+    record_sink() = nullptr;
     if (ctx) {
       cudaSetDevice(ctx->device);
       stream() = ctx->stream;
+      if (!ctx->record_path.empty()) record_sink() = ctx->record_path.c_str();
     }
   }
   gsw_status finish() {
@@ -297,11 +312,51 @@ __global__ void k_sum_weights(const int *w, int64_t m, unsigned long long *out) 
   if (lane_id() == 0 && s) atomicAdd(out, s);
 }
 
+__global__ void k_first_nbr(const int64_t *off, const int *col, int64_t n, int *first) {
+  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t a = off[v];
+    first[v] = off[v + 1] > a ? col[a] : -1;
+  }
+}
+
+__global__ void k_nonempty_bits(const int64_t *off, int64_t n, uint32_t *bits) {
+  const int64_t nw = (n + 31) >> 5;
+  for (int64_t w = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; w < nw; w += (int64_t)gridDim.x * blockDim.x) {
+    uint32_t b = 0;
+    for (int i = 0; i < 32; ++i) {
+      const int64_t v = w * 32 + i;
+      if (v < n && off[v + 1] > off[v]) b |= 1u << i;
+    }
+    bits[w] = b;
+  }
+}
+
 void finalize_graph(gsw_graph *g) {
   int64_t *off = g->off;
   if (!g->odeg) {
     if (!(g->odeg = (int *)g->ctx->graph_alloc(sizeof(int) * (g->n + 1)))) return;
     k_deg_to_i32<<<grid_for(g->n), 256, 0, stream()>>>(off, g->n, g->odeg);
+    GSW_LAUNCHED();
+  }
+  if (!g->first) {
+    if (!(g->first = (int *)g->ctx->graph_alloc(sizeof(int) * (g->n + 1)))) return;
+    k_first_nbr<<<grid_for(g->n), 256, 0, stream()>>>(off, g->col, g->n, g->first);
+    GSW_LAUNCHED();
+  }
+  if (g->directed && g->roff && g->rcol && !g->rfirst) {
+    if (!(g->rfirst = (int *)g->ctx->graph_alloc(sizeof(int) * (g->n + 1)))) return;
+    k_first_nbr<<<grid_for(g->n), 256, 0, stream()>>>(g->roff, g->rcol, g->n, g->rfirst);
+    GSW_LAUNCHED();
+  }
+  const int64_t nwords = (g->n + 31) / 32 + 1;
+  if (!g->nonempty) {
+    if (!(g->nonempty = (uint32_t *)g->ctx->graph_alloc(sizeof(uint32_t) * nwords))) return;
+    k_nonempty_bits<<<grid_for(nwords), 256, 0, stream()>>>(off, g->n, g->nonempty);
+    GSW_LAUNCHED();
+  }
+  if (g->directed && g->roff && !g->rnonempty) {
+    if (!(g->rnonempty = (uint32_t *)g->ctx->graph_alloc(sizeof(uint32_t) * nwords))) return;
+    k_nonempty_bits<<<grid_for(nwords), 256, 0, stream()>>>(g->roff, g->n, g->rnonempty);
     GSW_LAUNCHED();
   }
   if (g->weighted) {
@@ -380,7 +435,8 @@ gsw_graph *new_graph(gsw_ctx *ctx, int64_t n) {
 void free_graph(gsw_graph *g) {
   if (!g) return;
   for (void *p : {(void *)g->off, (void *)g->col, (void *)g->odeg, (void *)g->w, (void *)g->roff, (void *)g->rcol,
-                  (void *)g->rdeg, (void *)g->rw})
+                  (void *)g->rdeg, (void *)g->rw, (void *)g->first, (void *)g->rfirst, (void *)g->nonempty,
+                  (void *)g->rnonempty})
     g->ctx->graph_free(p);
   cudaFree(g->coo);
   if (g->twod) {
@@ -681,6 +737,7 @@ void apply_opts(const gsw_run_opts *o, config_t &conf) {
   conf.conf_sorted_queue = o->sorted_queue != 0;
   conf.conf_count_edges = o->account != 0;
   conf.conf_persistent = o->persistent != 0;
+  conf.conf_hub_path = (o->hub_path >= 0 && o->hub_path <= 2) ? o->hub_path : -1;
   opts().barrier_leave_test = o->barrier_test != 0;
   opts().verbose = o->verbose != 0;
   opts().timing = o->timing != 0;
@@ -716,14 +773,25 @@ struct loop_trace {
       st->level_frontier[last] = frontier;
       st->level_ms[last] = 0;
       st->level_edges[last] = -1;
+      st->level_bytes[last] = -1;
       st->ntrace++;
     }
     st->levels++;
   }
-  // after the expand: edge count now, kernel times once the run is over
-  void done(const stat_t &stats) {
+  // after the expand: the feature record where the reference's applications
+  // keep their (commented-out) training hook (application/bfs.cu:95), the
+  // edge count now, kernel times once the run is over
+  void done(const stat_t &stats, feature_t &fets) {
+    if (record_sink()) {
+      fets.record_path = record_sink();
+      fets.record();
+    }
     if (!st || last < 0) return;
+    // a persistent launch reports the load balance its kernel ran
+    if (hints().persistent)
+      st->level_cfg[last] = (st->level_cfg[last] & ~(7 << 2)) | ((hints().persistent_lb & 7) << 2) | (1 << 6);
     st->level_edges[last] = stats.last_scanned;
+    st->level_bytes[last] = stats.last_abytes > 0 ? stats.last_abytes : -1;
     st->level_inspect_ms[last] = 0;
     if (opts().timing) {
       if ((int)pending.size() <= last) pending.resize(last + 1);
@@ -786,6 +854,7 @@ unsigned end_checks(active_set_t *as, gsw_run_stats *st) {
   if (e & DEV_ERR_QUEUE_OVERFLOW) set_error(GSW_ERR_OVERFLOW, "%s", "frontier queue overflow");
   if (e & DEV_ERR_SCRATCH_OVERFLOW) set_error(GSW_ERR_OVERFLOW, "%s", "STRICT tile table overflow");
   if (e & DEV_ERR_BARRIER_TIMEOUT) set_error(GSW_ERR_TIMEOUT, "%s", "grid barrier timed out");
+  if (e & DEV_ERR_STAGE_TIMEOUT) set_error(GSW_ERR_TIMEOUT, "%s", "shared-memory staging copy did not complete");
   if (e & DEV_ERR_BAD_VERTEX) set_error(GSW_ERR_CUDA, "%s", "pointer chain longer than n");
   GSW_CUDA(cudaMemsetAsync(&as->dg_cnt->err, 0, sizeof(unsigned), stream()));
   return e;
@@ -956,6 +1025,7 @@ void dl_collect(dl_run &R, gsw_run_stats *st) {
       st->level_cfg[i] = cfg[i];
       st->level_frontier[i] = fr[i];
       st->level_edges[i] = ed[i];
+      st->level_bytes[i] = -1;
       st->level_ms[i] = 0;
       st->level_inspect_ms[i] = 0;
     }
@@ -1115,6 +1185,7 @@ void gsw_run_opts_default(gsw_run_opts *o) {
   o->eps = 0.01f;
   o->selector = GSW_SELECT_RULES;
   o->persistent = GSW_AUTO;
+  o->hub_path = GSW_AUTO;
 }
 
 gsw_status gsw_init(int device, gsw_ctx **out) {
@@ -1414,6 +1485,12 @@ gsw_status gsw_graph_roots(const gsw_graph *g, uint64_t seed, int count, int32_t
   return eg.finish();
 }
 
+gsw_status gsw_ctx_record_features(gsw_ctx *ctx, const char *path) {
+  if (!ctx) return fail(GSW_ERR_INVALID_ARG, "gsw_ctx_record_features: bad arguments");
+  ctx->record_path = path ? path : "";
+  return GSW_OK;
+}
+
 gsw_status gsw_ctx_stream(gsw_ctx *ctx, void **s) {
   if (!ctx || !s) return fail(GSW_ERR_INVALID_ARG, "gsw_ctx_stream: bad arguments");
   *s = (void *)ctx->stream;
@@ -1497,7 +1574,7 @@ gsw_status bfs_run(gsw_ctx *ctx, gsw_graph *gr, const int32_t *roots, int nroots
     g.update_level();
     tr.level(conf, hints().frontier);
     executor.expand(as, g, f, stats, fets, conf);
-    tr.done(stats);
+    tr.done(stats, fets);
     if (finish(as, g, f, conf)) break;
   }
   const double ms = tm.stop();
@@ -1607,7 +1684,7 @@ gsw_status gsw_sssp(gsw_ctx *ctx, gsw_graph *gr, int32_t root, const gsw_run_opt
     g.update_level();
     tr.level(conf, hints().frontier);
     executor.expand(as, g, f, stats, fets, conf);
-    tr.done(stats);
+    tr.done(stats, fets);
     if (finish(as, g, f, conf)) break;
   }
   const double ms = tm.stop();
@@ -1678,7 +1755,7 @@ gsw_status gsw_cc(gsw_ctx *ctx, gsw_graph *gr, const gsw_run_opts *o, int32_t *l
     g.update_level();
     tr.level(conf, hints().frontier);
     executor.expand(as, g, f, stats, fets, conf);
-    tr.done(stats);
+    tr.done(stats, fets);
     p_jump(f, gr->n, as);
     if (finish(as, g, f, conf)) break;
   }
@@ -1770,7 +1847,7 @@ gsw_status gsw_pagerank(gsw_ctx *ctx, gsw_graph *gr, const gsw_run_opts *o, floa
     g.update_level();
     tr.level(conf, hints().frontier);
     executor.expand(as, g, f, stats, fets, conf);
-    tr.done(stats);
+    tr.done(stats, fets);
     steps++;
     if (finish(as, g, f, conf)) break;
   }
@@ -1874,7 +1951,7 @@ gsw_status gsw_pagerank_delta(gsw_ctx *ctx, gsw_graph *gr, const gsw_run_opts *o
     g.update_level();
     tr.level(conf, hints().frontier);
     executor.expand(as, g, f, stats, fets, conf);
-    tr.done(stats);
+    tr.done(stats, fets);
   }
   const double ms = tm.stop();
   tr.resolve();
@@ -1988,7 +2065,7 @@ gsw_status gsw_bc(gsw_ctx *ctx, gsw_graph *gr, int32_t root, const gsw_run_opts 
     g.update_level();
     tr.level(conf, hints().frontier);
     executor.expand(as, g, f, stats, fets, conf);
-    tr.done(stats);
+    tr.done(stats, fets);
     if (finish(as, g, f, conf)) break;
   }
   const int64_t fwd_edges = st ? reached_edges(ctx, gr, (const int *)f.data.dg_wa, 2, -100) : 0;
@@ -2010,7 +2087,7 @@ gsw_status gsw_bc(gsw_ctx *ctx, gsw_graph *gr, int32_t root, const gsw_run_opts 
     g.update_level(-1);
     tr.level(conf, hints().frontier);
     executor.expand(as, g, h, stats, fets, conf);
-    tr.done(stats);
+    tr.done(stats, fets);
     if (finish(as, g, h, conf)) break;
   }
   const double ms = tm.stop();
@@ -2088,7 +2165,7 @@ gsw_status gsw_gc(gsw_ctx *ctx, gsw_graph *gr, const gsw_run_opts *o, int32_t *c
     g.update_level();
     tr.level(conf, hints().frontier);
     executor.expand(as, g, f, stats, fets, conf);
-    tr.done(stats);
+    tr.done(stats, fets);
     if (finish(as, g, f, conf)) break;
   }
   const double ms = tm.stop();
@@ -2137,12 +2214,50 @@ gsw_status gsw_mbfs(gsw_ctx *ctx, gsw_graph *gr, int nsrc, const int32_t *roots,
     return GSW_OK;
   }
   begin_stats(st);
+  // every level in one cooperative launch unless the options turn persistent
+  // launches off
+  const bool persistent = !o || o->persistent != 0;
   mbfs_result r = run_mbfs_batched(
-      gr->view<Empty>(), nsrc, roots, [&](const char *name, size_t bytes) { return ctx->buf(name, bytes); }, levels);
+      gr->view<Empty>(), nsrc, roots, [&](const char *name, size_t bytes) { return ctx->buf(name, bytes); }, levels,
+      persistent);
   if (st && ok()) {
     st->ms = r.ms;
     st->levels = r.levels;
     st->edges = r.edges;
+  }
+  return eg.finish();
+}
+
+// ---------------------------------------------------------------------------
+// batched BC (bc_batch.cuh): the sources in batches of BCB_SOURCES
+// ---------------------------------------------------------------------------
+gsw_status gsw_bc_batch(gsw_ctx *ctx, gsw_graph *gr, int nsrc, const int32_t *roots, const gsw_run_opts *o,
+                        int32_t *nsp, float *dep, gsw_run_stats *st) {
+  entry_guard eg(ctx);
+  if (!ctx || !gr || nsrc <= 0 || !roots) return fail(GSW_ERR_INVALID_ARG, "gsw_bc_batch: bad arguments");
+  if (o && o->captured) return fail(GSW_ERR_UNSUPPORTED, "gsw_bc_batch: no captured level loop");
+  if (gr->directed) return fail(GSW_ERR_UNSUPPORTED, "gsw_bc_batch: undirected graphs only");
+  for (int s = 0; s < nsrc; ++s)
+    if (roots[s] < 0 || roots[s] >= gr->n) return fail(GSW_ERR_INVALID_ARG, "gsw_bc_batch: root out of range");
+  begin_stats(st);
+  double ms = 0;
+  int64_t edges = 0;
+  int levels = 0;
+  auto buf = [&](const char *name, size_t bytes) { return ctx->buf(name, bytes); };
+  for (int s0 = 0; s0 < nsrc && ok(); s0 += BCB_SOURCES) {
+    const int k = std::min(BCB_SOURCES, nsrc - s0);
+    const size_t row = (size_t)gr->n;
+    bcb_result r = bc_batch_run(gr->view<Empty>(), k, roots + s0, buf, nsp ? nsp + row * s0 : nullptr,
+                                dep ? dep + row * s0 : nullptr, !o || o->persistent != 0);
+    ms += r.ms;
+    edges += r.edges;
+    levels = std::max(levels, r.levels);
+  }
+  if (st && ok()) {
+    st->ms = ms;
+    st->edges = edges;
+    st->levels = levels;
+    st->launches = launch_count();
   }
   return eg.finish();
 }

@@ -59,13 +59,23 @@ __global__ void k_mbfs_chunk_fill(const int64_t *off, int64_t n, const int64_t *
     }
 }
 
+// Frontier words are rewritten every level; inside a persistent launch they
+// must be read with plain loads (RO = false), per-level launches may use the
+// read-only path.
+template <bool RO>
+__device__ __forceinline__ uint64_t mbfs_ld(const uint64_t *p) {
+  if constexpr (RO)
+    return __ldg(p);
+  else
+    return *(volatile const uint64_t *)p;
+}
+
 // push, warp per chunk: the chunk's vertex's frontier bits go to every
 // neighbour that has not seen them
-template <int W>
-__global__ void __launch_bounds__(256) k_mbfs_push_chunks(device_graph_t<CSR, Empty> g, const int *cv,
-                                                           const int64_t *cbeg, int64_t nchunks,
-                                                           const uint64_t *frontier, const uint64_t *seen,
-                                                           uint64_t *next) {
+template <int W, bool RO>
+__device__ __forceinline__ void mbfs_push_body(const device_graph_t<CSR, Empty> &g, const int *cv, const int64_t *cbeg,
+                                               int64_t nchunks, const uint64_t *frontier, const uint64_t *seen,
+                                               uint64_t *next) {
   const int lane = lane_id();
   const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
   for (int64_t c = (int64_t)blockIdx.x * (blockDim.x >> 5) + warp_id(); c < nchunks; c += nwarps) {
@@ -74,7 +84,7 @@ __global__ void __launch_bounds__(256) k_mbfs_push_chunks(device_graph_t<CSR, Em
     bool any = false;
 #pragma unroll
     for (int k = 0; k < W; ++k) {
-      f[k] = __ldg(frontier + (int64_t)v * W + k);
+      f[k] = mbfs_ld<RO>(frontier + (int64_t)v * W + k);
       any |= f[k] != 0;
     }
     if (!any) continue;
@@ -89,15 +99,21 @@ __global__ void __launch_bounds__(256) k_mbfs_push_chunks(device_graph_t<CSR, Em
     }
   }
 }
+template <int W>
+__global__ void __launch_bounds__(256) k_mbfs_push_chunks(device_graph_t<CSR, Empty> g, const int *cv,
+                                                           const int64_t *cbeg, int64_t nchunks,
+                                                           const uint64_t *frontier, const uint64_t *seen,
+                                                           uint64_t *next) {
+  mbfs_push_body<W, true>(g, cv, cbeg, nchunks, frontier, seen, next);
+}
 
 // pull, warp per chunk: OR of the in-neighbours' frontier words over the
 // chunk, cut short once every bit the vertex still needs is covered; a vertex
 // with several chunks combines them with atomicOr
-template <int W>
-__global__ void __launch_bounds__(256) k_mbfs_pull_chunks(device_graph_t<CSR, Empty> g, const int *cv,
-                                                           const int64_t *cbeg, int64_t nchunks,
-                                                           const uint64_t *frontier, const uint64_t *seen,
-                                                           uint64_t *next, const uint64_t *valid) {
+template <int W, bool RO>
+__device__ __forceinline__ void mbfs_pull_body(const device_graph_t<CSR, Empty> &g, const int *cv, const int64_t *cbeg,
+                                               int64_t nchunks, const uint64_t *frontier, const uint64_t *seen,
+                                               uint64_t *next, const uint64_t *valid) {
   const int lane = lane_id();
   const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
   for (int64_t c = (int64_t)blockIdx.x * (blockDim.x >> 5) + warp_id(); c < nchunks; c += nwarps) {
@@ -118,7 +134,7 @@ __global__ void __launch_bounds__(256) k_mbfs_pull_chunks(device_graph_t<CSR, Em
       if (i < e) {
         const int u = __ldg(g.dgr_adj_list + i);
 #pragma unroll
-        for (int k = 0; k < W; ++k) acc[k] |= __ldg(frontier + (int64_t)u * W + k);
+        for (int k = 0; k < W; ++k) acc[k] |= mbfs_ld<RO>(frontier + (int64_t)u * W + k);
       }
       // every 32 edges: stop when the warp's bits cover what v needs
       bool covered = true;
@@ -149,11 +165,18 @@ __global__ void __launch_bounds__(256) k_mbfs_pull_chunks(device_graph_t<CSR, Em
     }
   }
 }
+template <int W>
+__global__ void __launch_bounds__(256) k_mbfs_pull_chunks(device_graph_t<CSR, Empty> g, const int *cv,
+                                                           const int64_t *cbeg, int64_t nchunks,
+                                                           const uint64_t *frontier, const uint64_t *seen,
+                                                           uint64_t *next, const uint64_t *valid) {
+  mbfs_pull_body<W, true>(g, cv, cbeg, nchunks, frontier, seen, next, valid);
+}
 
 template <int W>
-__global__ void __launch_bounds__(256) k_mbfs_update(device_graph_t<CSR, Empty> g, uint64_t *frontier, uint64_t *seen,
-                                                      uint64_t *next, int *levels, int nsrc, int level,
-                                                      const uint64_t *valid, mbfs_counters *cnt) {
+__device__ __forceinline__ void mbfs_update_body(const device_graph_t<CSR, Empty> &g, uint64_t *frontier,
+                                                 uint64_t *seen, uint64_t *next, int *levels, int nsrc, int level,
+                                                 const uint64_t *valid, mbfs_counters *cnt) {
   __shared__ unsigned long long s_red[32];
   const int64_t n = g.nvertexs;
   const int64_t STRIDE = (int64_t)blockDim.x * gridDim.x;
@@ -192,6 +215,167 @@ __global__ void __launch_bounds__(256) k_mbfs_update(device_graph_t<CSR, Empty> 
   if (threadIdx.x == 0 && r) atomicAdd(&cnt->active_e, r);
   r = block_reduce(ue, s_red);
   if (threadIdx.x == 0 && r) atomicAdd(&cnt->unseen_e, r);
+}
+template <int W>
+__global__ void __launch_bounds__(256) k_mbfs_update(device_graph_t<CSR, Empty> g, uint64_t *frontier, uint64_t *seen,
+                                                      uint64_t *next, int *levels, int nsrc, int level,
+                                                      const uint64_t *valid, mbfs_counters *cnt) {
+  mbfs_update_body<W>(g, frontier, seen, next, levels, nsrc, level, valid, cnt);
+}
+
+// ---- batched BC passes over the vertex-major levels of a <= 32-source batch
+// (bc_batch.cuh drives them; lane s of a warp is source s) ----------------
+constexpr int BCB_SOURCES = 32;  // sources per batch: one per lane
+
+// forward pass of level L (L >= 1): nsp[v] = sum of nsp[u] over the
+// in-neighbours one level closer, per source (undirected graphs: the chunk
+// list covers the adjacency lists, which are the in-lists as well)
+__device__ __forceinline__ void bcb_forward_body(const device_graph_t<CSR, Empty> &g, const int *cv, const int64_t *cbeg,
+                                                 int64_t nchunks, const int *lvl, int nsrc, int L, int *nsp) {
+  const int lane = lane_id();
+  const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t c = (int64_t)blockIdx.x * (blockDim.x >> 5) + warp_id(); c < nchunks; c += nwarps) {
+    const int v = cv[c];
+    const bool mine = lane < nsrc && lvl[(int64_t)v * nsrc + lane] == L;
+    if (!__any_sync(FULL, mine)) continue;
+    const int64_t st = __ldg(g.dg_row_off + v), en = __ldg(g.dg_row_off + v + 1);
+    const int64_t b = cbeg[c], e = MIN(b + MBFS_CHUNK, en);
+    int acc = 0;
+    for (int64_t base = b; base < e; base += 32) {
+      const int cnt = (int)MIN((int64_t)32, e - base);
+      const int u_l = lane < cnt ? __ldg(g.dg_adj_list + base + lane) : 0;
+      for (int j = 0; j < cnt; ++j) {
+        const int u = __shfl_sync(FULL, u_l, j);
+        const bool parent = mine && lvl[(int64_t)u * nsrc + lane] == L - 1;
+        if (parent) acc += nsp[(int64_t)u * nsrc + lane];  // int32, wraps like the reference
+      }
+    }
+    if (mine) {
+      int *dst = nsp + (int64_t)v * nsrc + lane;
+      if (e - b == en - st)
+        *dst = acc;  // the vertex's only chunk
+      else
+        atomicAdd(dst, acc);
+    }
+  }
+}
+
+// backward pass of level L: sum[v] = sum over children w of (1 + dep[w]) /
+// nsp[w], with dep[w] = nsp[w] * sum[w] from the pass of level L+1
+__device__ __forceinline__ void bcb_backward_body(const device_graph_t<CSR, Empty> &g, const int *cv,
+                                                  const int64_t *cbeg, int64_t nchunks, const int *lvl, int nsrc, int L,
+                                                  const int *nsp, float *sum) {
+  const int lane = lane_id();
+  const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t c = (int64_t)blockIdx.x * (blockDim.x >> 5) + warp_id(); c < nchunks; c += nwarps) {
+    const int v = cv[c];
+    const bool mine = lane < nsrc && lvl[(int64_t)v * nsrc + lane] == L;
+    if (!__any_sync(FULL, mine)) continue;
+    const int64_t st = __ldg(g.dg_row_off + v), en = __ldg(g.dg_row_off + v + 1);
+    const int64_t b = cbeg[c], e = MIN(b + MBFS_CHUNK, en);
+    float acc = 0.0f;
+    for (int64_t base = b; base < e; base += 32) {
+      const int cnt = (int)MIN((int64_t)32, e - base);
+      const int w_l = lane < cnt ? __ldg(g.dg_adj_list + base + lane) : 0;
+      for (int j = 0; j < cnt; ++j) {
+        const int w = __shfl_sync(FULL, w_l, j);
+        const int64_t r = (int64_t)w * nsrc + lane;
+        if (mine && lvl[r] == L + 1) {
+          const float nw = (float)nsp[r];
+          acc += (1.0f + nw * sum[r]) / nw;
+        }
+      }
+    }
+    if (mine) {
+      float *dst = sum + (int64_t)v * nsrc + lane;
+      if (e - b == en - st)
+        *dst = acc;
+      else
+        atomicAdd(dst, acc);
+    }
+  }
+}
+
+// dep = nsp * sum, in place over the sums
+__device__ __forceinline__ void bcb_finish_body(const int *nsp, float *sum, int64_t cells) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < cells; i += (int64_t)gridDim.x * blockDim.x)
+    sum[i] = (float)nsp[i] * sum[i];
+}
+
+__global__ void __launch_bounds__(256) k_bcb_forward(device_graph_t<CSR, Empty> g, const int *cv, const int64_t *cbeg,
+                                                     int64_t nchunks, const int *lvl, int nsrc, int L, int *nsp) {
+  bcb_forward_body(g, cv, cbeg, nchunks, lvl, nsrc, L, nsp);
+}
+__global__ void __launch_bounds__(256) k_bcb_backward(device_graph_t<CSR, Empty> g, const int *cv, const int64_t *cbeg,
+                                                      int64_t nchunks, const int *lvl, int nsrc, int L, const int *nsp,
+                                                      float *sum) {
+  bcb_backward_body(g, cv, cbeg, nchunks, lvl, nsrc, L, nsp, sum);
+}
+__global__ void k_bcb_finish(const int *nsp, float *sum, int64_t cells) { bcb_finish_body(nsp, sum, cells); }
+// roots: nsp = 1 for their own source
+__global__ void k_bcb_seed(const int *roots, int nsrc, int *nsp) {
+  const int s = threadIdx.x;
+  if (s < nsrc) nsp[(int64_t)roots[s] * nsrc + s] = 1;
+}
+
+// ---- every level in one cooperative launch ----------------------------------
+// The per-level loop above needs the host after every level (the counters
+// decide the next direction).  The persistent form keeps the whole grid
+// resident: push or pull, a grid barrier, the update (counters into the
+// level's slot of two), a grid barrier, and every block reads the same
+// counters to stop or to pick the next direction (Beamer's test, alpha = 14).
+// With BC, the same launch continues with the forward passes (levels 1 ..
+// depth-1) and the backward passes (depth-2 .. 0), a barrier after each, and
+// the final dep = nsp * sum.  Barrier waits are bounded (budget_ns each);
+// after a timeout every block leaves and status says so.
+struct mbfs_persist_t {
+  unsigned *bar;             // [0] arrivals, [1] generation, [2] error word
+  mbfs_counters *cnt;        // [2], by level parity, zero at launch
+  int *out;                  // [0] levels (the one that found nothing), [1] status (0 ok, 1 barrier timeout)
+  unsigned long long budget_ns;
+  int max_levels;
+};
+
+template <int W, bool BC>
+__global__ void __launch_bounds__(256) k_mbfs_persistent(device_graph_t<CSR, Empty> g, const int *cv,
+                                                          const int64_t *cbeg, int64_t nchunks, uint64_t *frontier,
+                                                          uint64_t *seen, uint64_t *next, int *levels, int nsrc,
+                                                          const uint64_t *valid, mbfs_persist_t P, int *nsp,
+                                                          float *sum) {
+  unsigned gen = 0;
+  auto barrier = [&]() { return grid_barrier(P.bar, P.bar + 1, P.bar + 2, gen, P.budget_ns); };
+  bool push = true, okk = true;
+  int level = 1;
+  for (; level <= P.max_levels; ++level) {
+    if (push)
+      mbfs_push_body<W, false>(g, cv, cbeg, nchunks, frontier, seen, next);
+    else
+      mbfs_pull_body<W, false>(g, cv, cbeg, nchunks, frontier, seen, next, valid);
+    if (!(okk = barrier())) break;
+    // the slot of the next level was last read before the barrier above
+    if (blockIdx.x == 0 && threadIdx.x == 0) P.cnt[(level + 1) & 1] = mbfs_counters{0, 0, 0, 0};
+    mbfs_update_body<W>(g, frontier, seen, next, levels, nsrc, level, valid, &P.cnt[level & 1]);
+    if (!(okk = barrier())) break;
+    const volatile mbfs_counters *c = &P.cnt[level & 1];
+    if (c->active_v == 0) break;
+    push = c->active_e * 14 < c->unseen_e;
+  }
+  if constexpr (BC) {
+    const int depth = level;
+    for (int L = 1; okk && L < depth; ++L) {
+      bcb_forward_body(g, cv, cbeg, nchunks, levels, nsrc, L, nsp);
+      okk = barrier();
+    }
+    for (int L = depth - 2; okk && L >= 0; --L) {
+      bcb_backward_body(g, cv, cbeg, nchunks, levels, nsrc, L, nsp, sum);
+      okk = barrier();
+    }
+    if (okk) bcb_finish_body(nsp, sum, (int64_t)g.nvertexs * nsrc);
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    P.out[0] = level;
+    P.out[1] = okk ? 0 : 1;
+  }
 }
 
 template <int W>
@@ -248,8 +432,14 @@ __global__ void k_mbfs_fill(T *p, T v, int64_t n) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) p[i] = v;
 }
 
+// transpose = false leaves the levels vertex-major in the "mb_levels_vm"
+// buffer (row v holds nsrc levels) for a caller that keeps working on them.
+// persistent = true runs every level in one cooperative launch; with
+// bc_nsp / bc_sum (W = 1, at most BCB_SOURCES sources) that launch also runs
+// the batched BC passes into them.
 template <int W, typename Buf>
-mbfs_result mbfs_impl(device_graph_t<CSR, Empty> g, int nsrc, const int32_t *roots_host, Buf buf, int32_t *levels_host) {
+mbfs_result mbfs_impl(device_graph_t<CSR, Empty> g, int nsrc, const int32_t *roots_host, Buf buf, int32_t *levels_host,
+                      bool transpose = true, bool persistent = false, int *bc_nsp = nullptr, float *bc_sum = nullptr) {
   mbfs_result res;
   const int64_t n = g.nvertexs;
   const int grid = sm_count() * 8;
@@ -299,11 +489,40 @@ mbfs_result mbfs_impl(device_graph_t<CSR, Empty> g, int nsrc, const int32_t *roo
   GSW_CUDA(cudaMemsetAsync(seen, 0, sizeof(uint64_t) * n * W, s));
   GSW_CUDA(cudaMemsetAsync(next, 0, sizeof(uint64_t) * n * W, s));
   k_mbfs_fill<int><<<grid, 256, 0, s>>>(levels, -1, n * (int64_t)nsrc);
+  const bool bc = bc_nsp && bc_sum;
+  if (bc) {
+    GSW_CUDA(cudaMemsetAsync(bc_nsp, 0, sizeof(int) * (size_t)n * nsrc, s));
+    GSW_CUDA(cudaMemsetAsync(bc_sum, 0, sizeof(float) * (size_t)n * nsrc, s));
+  }
   cudaEventRecord(e0, s);
   k_mbfs_seed<W><<<1, 256, 0, s>>>(frontier, seen, roots, nsrc, levels, n);
+  if (bc) k_bcb_seed<<<1, BCB_SOURCES, 0, s>>>(roots, nsrc, bc_nsp);
+  if (persistent) {
+    unsigned *bar = (unsigned *)buf("mb_bar", sizeof(unsigned) * 4);
+    mbfs_counters *pc = (mbfs_counters *)buf("mb_pcnt", sizeof(mbfs_counters) * 2);
+    int *pout = (int *)buf("mb_pout", sizeof(int) * 2);
+    if (bar && pc && pout) {
+      GSW_CUDA(cudaMemsetAsync(bar, 0, sizeof(unsigned) * 4, s));
+      GSW_CUDA(cudaMemsetAsync(pc, 0, sizeof(mbfs_counters) * 2, s));
+      mbfs_persist_t P{bar, pc, pout, 2000000000ull, (int)MIN(n + 1, (int64_t)INT32_MAX - 1)};
+      auto kern = bc ? k_mbfs_persistent<W, true> : k_mbfs_persistent<W, false>;
+      const int pgrid = resident_grid(kern, 256);
+      void *args[] = {(void *)&g,    (void *)&cv,     (void *)&cbeg,   (void *)&nchunks, (void *)&frontier,
+                      (void *)&seen, (void *)&next,   (void *)&levels, (void *)&nsrc,    (void *)&valid,
+                      (void *)&P,    (void *)&bc_nsp, (void *)&bc_sum};
+      if (!GSW_CUDA(cudaLaunchCooperativeKernel((const void *)kern, pgrid, 256, args, 0, s))) {
+        GSW_LAUNCHED();
+        int out[2] = {0, 1};
+        GSW_CUDA(cudaMemcpyAsync(out, pout, sizeof(out), cudaMemcpyDeviceToHost, s));
+        GSW_CUDA(cudaStreamSynchronize(s));
+        res.levels = out[0];
+        if (out[1] != 0) set_error(GSW_ERR_TIMEOUT, "%s", "batched BFS: grid barrier timed out");
+      }
+    }
+  }
   // the first level pushes from the sources
   bool push = true;
-  for (int level = 1; level <= n + 1 && ok(); ++level) {
+  for (int level = 1; !persistent && level <= n + 1 && ok(); ++level) {
     if (push)
       k_mbfs_push_chunks<W><<<grid, 256, 0, s>>>(g, cv, cbeg, nchunks, frontier, seen, next);
     else
@@ -317,7 +536,7 @@ mbfs_result mbfs_impl(device_graph_t<CSR, Empty> g, int nsrc, const int32_t *roo
     // Beamer's direction test with alpha = 14
     push = hcnt->active_e * 14 < hcnt->unseen_e;
   }
-  k_mbfs_transpose<<<sm_count() * 8, dim3(32, 8), 0, s>>>(levels, n, nsrc, levels_sm);
+  if (transpose) k_mbfs_transpose<<<sm_count() * 8, dim3(32, 8), 0, s>>>(levels, n, nsrc, levels_sm);
   cudaEventRecord(e1, s);
   cudaEventSynchronize(e1);
   float ms = 0;
@@ -328,7 +547,7 @@ mbfs_result mbfs_impl(device_graph_t<CSR, Empty> g, int nsrc, const int32_t *roo
   GSW_CUDA(cudaMemcpyAsync(hcnt, cnt, sizeof(mbfs_counters), cudaMemcpyDeviceToHost, s));
   GSW_CUDA(cudaStreamSynchronize(s));
   res.edges = (int64_t)(hcnt->reached_e / 2);
-  if (levels_host && ok())
+  if (levels_host && transpose && ok())
     GSW_CUDA(cudaMemcpyAsync(levels_host, levels_sm, sizeof(int) * (size_t)n * nsrc, cudaMemcpyDeviceToHost, s));
   GSW_CUDA(cudaStreamSynchronize(s));
   cudaFreeHost(hcnt);
@@ -339,12 +558,12 @@ mbfs_result mbfs_impl(device_graph_t<CSR, Empty> g, int nsrc, const int32_t *roo
 
 template <typename Buf>
 mbfs_result run_mbfs_batched(device_graph_t<CSR, Empty> g, int nsrc, const int32_t *roots, Buf buf,
-                             int32_t *levels_host) {
+                             int32_t *levels_host, bool persistent) {
   const int w = (nsrc + 63) / 64;
-  if (w <= 1) return mbfs_impl<1>(g, nsrc, roots, buf, levels_host);
-  if (w <= 2) return mbfs_impl<2>(g, nsrc, roots, buf, levels_host);
-  if (w <= 4) return mbfs_impl<4>(g, nsrc, roots, buf, levels_host);
-  if (w <= 8) return mbfs_impl<8>(g, nsrc, roots, buf, levels_host);
+  if (w <= 1) return mbfs_impl<1>(g, nsrc, roots, buf, levels_host, true, persistent);
+  if (w <= 2) return mbfs_impl<2>(g, nsrc, roots, buf, levels_host, true, persistent);
+  if (w <= 4) return mbfs_impl<4>(g, nsrc, roots, buf, levels_host, true, persistent);
+  if (w <= 8) return mbfs_impl<8>(g, nsrc, roots, buf, levels_host, true, persistent);
   set_error(GSW_ERR_UNSUPPORTED, "%s", "mbfs: at most 512 sources per batch");
   return mbfs_result();
 }

@@ -101,6 +101,16 @@ gsw_status gsw_graph_roots(const gsw_graph *g, uint64_t seed, int count, int32_t
  * work around the library's launches. */
 gsw_status gsw_ctx_stream(gsw_ctx *ctx, void **stream);
 
+/* Training records: replaces feature_t::record with cmd_opt.json
+ * (src/abstraction/features.cuh:86-104, src/utils/json.cuh:34-48, the -j
+ * option of src/utils/cmdline.cuh:208).  After this call every application
+ * run on the context appends, after each expand (where the reference's
+ * applications keep their training hook, application/bfs.cu:95), one block
+ * {"0": fv[0], ..., "20": fv[20], "21": last filter ms, "22": last expand
+ * ms} in the reference's layout to `path`, at most 100 blocks per run.
+ * NULL or "" turns recording off. */
+gsw_status gsw_ctx_record_features(gsw_ctx *ctx, const char *path);
+
 /* ---- level-loop configuration --------------------------------------------
  * Replaces the -c Dir-Fmt-LB-Fusion override of src/utils/cmdline.cuh:51-94
  * (any field may be left to the selector with -1). */
@@ -137,7 +147,12 @@ typedef struct gsw_run_opts {
   int captured;      /* 1: run the whole level loop as one CUDA graph with
                         device-side selection and termination (BFS, PR;
                         GSW_ERR_UNSUPPORTED elsewhere); 0: host-driven loop */
-  int reserved[4];
+  int hub_path;      /* how a CTA sweeps one hub's adjacency list (the
+                        thread/warp/CTA-tiered push's CTA tier): 0 four-byte
+                        loads, 1 int4 loads of the 16-byte-aligned body,
+                        2 shared-memory staging by 1-D TMA bulk copies;
+                        GSW_AUTO: 2 without edge data, 1 with it */
+  int reserved[3];
 } gsw_run_opts;
 
 void gsw_run_opts_default(gsw_run_opts *o);
@@ -150,12 +165,20 @@ typedef struct gsw_run_stats {
   unsigned device_error;   /* DEV_ERR bits seen by kernels (0 = clean) */
   int64_t launches;        /* kernels launched by the run */
   int ntrace;              /* entries in the per-level trace below */
-  /* per level: dir | fmt<<1 | lb<<2 | fused<<5 | persistent<<6 */
+  /* per level: dir | fmt<<1 | lb<<2 | fused<<5 | persistent<<6; on a level
+   * that ran inside a persistent launch, lb is the load balance the launched
+   * kernel reported back */
   int32_t level_cfg[GSW_MAX_TRACE];
   int64_t level_frontier[GSW_MAX_TRACE];
   float level_ms[GSW_MAX_TRACE];         /* expand time, with opts.timing */
   float level_inspect_ms[GSW_MAX_TRACE]; /* inspection time, with opts.timing */
   int64_t level_edges[GSW_MAX_TRACE];    /* edges touched, with opts.account */
+  int64_t level_bytes[GSW_MAX_TRACE];    /* with opts.account: algorithmic bytes
+                                            of the CSR side and the state writes
+                                            that the expand counted itself (the
+                                            thread-mapped pull, whose reads
+                                            depend on where each candidate
+                                            settles); -1: not counted */
 } gsw_run_stats;
 
 /* ---- applications ----------------------------------------------------------
@@ -199,6 +222,20 @@ gsw_status gsw_gc(gsw_ctx *ctx, gsw_graph *g, const gsw_run_opts *o, int32_t *co
 /* Multi-source BFS.  batched = 0 runs the single-source loop per source
  * (as application/mbfs.cu does); batched = 1 runs all sources together with
  * bit-sliced frontiers (64 sources per word) in one launch sequence. */
+/* Betweenness centrality from many sources: no reference function
+ * corresponds (application/bc.cu:246-309 runs one source); per source the
+ * results are those of gsw_bc / bc_cpu (application/bc.cu:162-214): int32
+ * path counts (wrapping like the reference's) and FP32 dependencies, rows of
+ * n per source (nsrc x n, source-major).  Sources advance together in
+ * batches of 32 (bit-sliced levels, then one forward and one backward pass
+ * per level over all of a batch's sources), each batch in one cooperative
+ * launch (o->persistent = 0: one launch per pass).  Undirected graphs only.
+ * st->edges counts the forward traversals (Graph500 edges summed over the
+ * sources). */
+gsw_status gsw_bc_batch(gsw_ctx *ctx, gsw_graph *g, int nsrc, const int32_t *roots, const gsw_run_opts *o,
+                        int32_t *nsp, float *dep, gsw_run_stats *st);
+/* (gsw_mbfs with batched = 1 runs every level of a batch in one cooperative
+ * launch; o->persistent = 0 launches per level.) */
 gsw_status gsw_mbfs(gsw_ctx *ctx, gsw_graph *g, int nsrc, const int32_t *roots, int batched, const gsw_run_opts *o,
                     int32_t *levels, gsw_run_stats *st);
 

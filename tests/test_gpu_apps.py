@@ -346,3 +346,78 @@ def test_graph_blocks_reused_across_uploads(ctx, big):
     d, _ = ctx.upload(hw.off, hw.col, hw.w).sssp(root)
     assert np.array_equal(d, oracle.sssp_dijkstra(hw, root))
     g.close()
+
+
+@pytest.mark.parametrize("hub_path", [gs.HUB_SCALAR, gs.HUB_VECTOR, gs.HUB_STAGED])
+def test_hub_paths_of_the_tiered_push(ctx, big, hub_path):
+    """The CTA tier of the tiered push reads a hub's columns with 4-byte
+    loads, int4 loads of the aligned body, or shared-memory chunks filled by
+    TMA bulk copies (ragged ends with plain loads): BFS and SSSP stay exact,
+    standalone, per-launch fused and persistent fused, on graphs whose hubs
+    span many chunks (RMAT 2^14 ef 16 and a denser G(n, m) with lists of
+    every alignment)."""
+    graphs = [big["rmat14"], (oracle.er(3000, 3000 * 400, seed=6), None, 7)]
+    for h, hw, root in graphs:
+        hw = hw if hw is not None else oracle.add_weights(h, 5, 64)
+        g = ctx.upload(h.off, h.col)
+        gw = ctx.upload(hw.off, hw.col, hw.w)
+        ref, dref = oracle.bfs(h, root), oracle.sssp_dijkstra(hw, root)
+        for cfg, persistent in (("Push-Queue-TWC-Standalone", None), ("Push-Queue-TWC-Fused", False),
+                                ("Push-Queue-TWC-Fused", True), ("Push-Bitmap-TWC-Standalone", None)):
+            o = gs.RunOpts.from_config(cfg, persistent=persistent, hub_path=hub_path)
+            lv, st = g.bfs(root, o)
+            assert np.array_equal(lv, ref), (cfg, persistent, hub_path)
+            assert st.device_error == 0
+            d, st = gw.sssp(root, o)
+            assert np.array_equal(d, dref), (cfg, persistent, hub_path)
+            assert st.device_error == 0
+        g.close()
+        gw.close()
+
+
+@pytest.mark.parametrize("name,nsrc", [("rmat14", 1), ("rmat14", 32), ("rmat14", 45), ("grid64", 40), ("er20k", 33)])
+def test_bc_batch_every_source(ctx, big, name, nsrc):
+    """Batched BC (bit-sliced levels, then per-level forward / backward passes
+    over a batch of up to 32 sources): per source, path counts equal the
+    reference's int32 counts bit for bit and dependencies are within 1e-5 of
+    the FP64 oracle, for one source, a full batch, and batches with a
+    partial tail; hubs of RMAT spread over many adjacency chunks."""
+    h, _, _ = big[name]
+    g = ctx.upload(h.off, h.col)
+    roots = oracle.roots(h, 23, nsrc)
+    nsp, dep, st = g.bc_batch(roots)
+    assert nsp.shape == (nsrc, h.n) and dep.shape == (nsrc, h.n)
+    edges = 0
+    for i, r in enumerate(roots):
+        _bc_check(nsp[i], dep[i], h, int(r))
+        edges += oracle.traversed_edges(h, oracle.bfs(h, int(r)))
+    assert st.edges == edges
+    g.close()
+
+
+def test_bc_batch_matches_single_source_runs(ctx, big):
+    h, _, _ = big["rmat14"]
+    g = ctx.upload(h.off, h.col)
+    roots = oracle.roots(h, 29, 8)
+    nsp, dep, _ = g.bc_batch(roots)
+    for i, r in enumerate(roots):
+        n1, d1, _ = g.bc(int(r))
+        assert np.array_equal(nsp[i], n1)
+        assert np.allclose(dep[i], d1, rtol=1e-5, atol=1e-5)
+    g.close()
+
+
+@pytest.mark.parametrize("persistent", [True, False])
+def test_batched_sources_persistent_and_per_level(ctx, big, persistent):
+    """Batched MBFS and batched BC give the same answers whether all levels
+    run in one cooperative launch (grid barriers, direction chosen on the
+    device) or one launch per level / pass."""
+    h, _, _ = big["rmat14"]
+    g = ctx.upload(h.off, h.col)
+    roots = oracle.roots(h, 31, 70)
+    lv, _ = g.mbfs(roots, batched=True, opts=gs.RunOpts(persistent=persistent))
+    assert np.array_equal(lv, oracle.mbfs(h, roots))
+    nsp, dep, _ = g.bc_batch(roots[:40], opts=gs.RunOpts(persistent=persistent))
+    for i, r in enumerate(roots[:40]):
+        _bc_check(nsp[i], dep[i], h, int(r))
+    g.close()

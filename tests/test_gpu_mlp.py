@@ -182,6 +182,9 @@ def test_committed_model_beats_rules_on_held_out_graphs(ctx):
     both = (T[rows, cls] > 0) & (T[rows, np.clip(R, 0, gs.MLP_CLASSES - 1)] > 0) & (R >= 0)
     r_mlp, r_rules = regret(T[both], cls[both]), regret(T[both], R[both])
     assert r_mlp["chosen_ms"] < r_rules["chosen_ms"], (r_mlp, r_rules)
+    # the selector's target: within 10% of the exhaustively timed best variant,
+    # time-weighted over the held-out levels
+    assert regret(T, cls)["time_weighted"] <= 0.10, regret(T, cls)
 
 
 def test_committed_model_speeds_up_pagerank(ctx):
@@ -231,10 +234,10 @@ def test_sssp_exact_under_both_fusion_decisions(ctx):
 
 
 def test_committed_fusion_model_not_slower_than_the_tree_on_fresh_graphs(ctx):
-    """SSSP on graphs the fusion corpus never saw: total device time with the
-    learned fused/standalone decision is not above the reference tree's (5%
-    timing slack: where both pick the same form the times only differ by
-    noise; the held-out gain is in the model file's report)."""
+    """SSSP on graphs the fusion corpus never saw: on a graph where the
+    learned fused/standalone decision and the reference tree pick different
+    forms, the network's pick is faster; where they pick the same form the
+    times differ only by noise (5% slack)."""
     from gswitch_b200.selector_train import load_fusion_model
 
     fm, fc = load_fusion_model()
@@ -245,18 +248,22 @@ def test_committed_fusion_model_not_slower_than_the_tree_on_fresh_graphs(ctx):
     graphs = [ctx.er(1 << 19, 4 << 19, seed=91001, wmax=64, wseed=3),
               ctx.grid(2900, 2900, 100, seed=91002, wmax=1000, wseed=3),
               ctx.rmat(19, 16, 0.55, 0.2, 0.2, seed=91003, wmax=64, wseed=3)]
-    t_mlp = t_tree = 0.0
+    out = []
     for g in graphs:
         root = int(g.roots(8, 1)[0])
+        t, form = {}, {}
         for sel in ("mlp", "rules"):
             o = gs.RunOpts(selector=sel)
             g.sssp(root, o, out=False)
-            ms = min(g.sssp(root, o, out=False)[1].ms for _ in range(2))
-            if sel == "mlp":
-                t_mlp += ms
-            else:
-                t_tree += ms
+            runs = [g.sssp(root, o, out=False)[1] for _ in range(2)]
+            t[sel] = min(st.ms for st in runs)
+            form[sel] = runs[0].trace[0][3] if runs[0].trace else None  # fused or standalone from the start
+        out.append((form["mlp"] == form["rules"], t["mlp"], t["rules"], form))
         g.close()
     ctx.mlp_load_fusion(None)
     ctx.mlp_load(None)
-    assert t_mlp <= 1.05 * t_tree, (t_mlp, t_tree)
+    for same, t_mlp, t_tree, form in out:
+        if same:
+            assert t_mlp <= 1.05 * t_tree, (t_mlp, t_tree, form)
+        else:
+            assert t_mlp < t_tree, (t_mlp, t_tree, form)
