@@ -112,25 +112,18 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def level_bytes(kind, n, A, U, D, E, counted=-1):
-    """Algorithmic bytes of one expand (int32 levels, bitmap state probes):
+def level_bytes(kind, n, A, U, D, E):
+    """Algorithmic bytes of one expand (int32 levels, bitmap state probes), the
+    per-unit figures of the path's roofline definition:
     push: work list + 16 B of row offsets per frontier vertex + 4 B column and
     2 bitmap probes per edge + 4 B level write per discovered vertex;
     pull: work list + 16 B offsets per candidate + 4 B column and one
-    frontier-bit probe per scanned edge + 4 B write per discovered vertex.
-    A kernel whose reads depend on the data counts the CSR side and the state
-    writes itself (counted > 0: the thread-mapped pull, 4 B first in-neighbour
-    per candidate, offsets and further columns only for the candidates that
-    walk on); the work list and the bitmap probes are added here."""
+    frontier-bit probe per scanned edge + 4 B write per discovered vertex."""
     direction, fmt = kind[0], kind[1]
     if direction == "Push":
         work = n / 8 if fmt == "Bitmap" else 4 * A
-        if counted > 0:
-            return work + counted + 0.25 * E
         return work + 16 * A + 4.25 * E + 4 * D
     work = n / 8 if fmt == "Bitmap" else 4 * U
-    if counted > 0:
-        return work + counted + 0.125 * E
     return work + 16 * U + 4.125 * E + 4 * D
 
 
@@ -159,10 +152,8 @@ def roofline_from(runs, n, peak_gbs, peak_kind):
             D = int(cnt[i + 1]) if i + 1 < len(cnt) else 0
             U = int(cnt[i + 1:].sum()) + unreached
             E = acc.level_edges[i] if i < len(acc.level_edges) else 0
-            counted = getattr(acc, "level_bytes", [])
-            counted = counted[i] if i < len(counted) else -1
             key = "expand " + "-".join(kind)
-            b = level_bytes(kind, n, A, U, D, max(E, 0), counted)
+            b = level_bytes(kind, n, A, U, D, max(E, 0))
             rec = per.setdefault(key, [0.0, 0.0, 0])
             rec[0] += timed.level_ms[i]
             rec[1] += b
@@ -226,9 +217,9 @@ def run_ours(args):
             dist.barrier()
 
     ctx = gs.Context(local)
-    from gswitch_b200.autotune import load_table
+    from gswitch_b200.autotune import load_into
 
-    ctx.tune_load(load_table())  # autotuned expand grids (defaults when absent)
+    load_into(ctx, args.tune)  # autotuned expand grids and shapes (defaults when absent)
     selector = args.selector
     if selector == "mlp":
         from gswitch_b200.selector_train import load_fusion_model
@@ -455,11 +446,11 @@ def app_table(ctx, g, gs, args, roots, selector):
 
 def run_c3(args):
     import gswitch_b200 as gs
-    from gswitch_b200.autotune import load_table
+    from gswitch_b200.autotune import load_into
     from gswitch_b200.selector_train import load_model
 
     ctx = gs.Context(0)
-    ctx.tune_load(load_table())
+    load_into(ctx, args.tune)
     selector = "rules"
     model, min_conf = load_model()
     if args.selector == "mlp" and model is not None:
@@ -478,6 +469,9 @@ def c3_table(ctx, gs, selector):
     """Config C3 (separate run, `--c3`): the 4096 x 4096 grid with 1%
     long-range edges (weights U[1, 1000]) for BFS, SSSP and BC, and RMAT
     scale 26 for BFS: the switched form against the fixed variants."""
+    from gswitch_b200.selector_train import load_model
+
+    model, _ = load_model()
     out = {}
     grid = ctx.grid(4096, 4096, 100, seed=1, wmax=1000, wseed=5)
     r26 = ctx.rmat(26, 16, 0.57, 0.19, 0.19, seed=1)
@@ -508,6 +502,9 @@ def c3_table(ctx, gs, selector):
             row.update({"fixed": {k: v["gteps"] for k, v in fixed.items()},
                         "best_fixed": {"variant": best[0], **best[1]},
                         "switched_vs_best_fixed": round(row["switched_mlp"]["gteps"] / best[1]["gteps"], 3)})
+            if app in ("bfs", "sssp"):
+                row["switch_headroom_standalone"] = switch_headroom(
+                    g, gs.APP_BFS if app == "bfs" else gs.APP_SSSP, root, ctx=ctx, model=model)
             out[f"{app}_{gname}"] = row
     out["definitions"] = {"bfs/sssp/bc": "sum deg(reached)/2 / t (BC: both phases timed)", "unit": "GTEPS"}
     grid.close()
@@ -706,6 +703,10 @@ PROFILE_CASES = {
             "Push-Queue-WM-Fused levels one launch each",
     "pr": "two PageRank iterations on RMAT scale 22, Pull-Bitmap-STRICT then 2D",
     "mbfs": "batched 256-source BFS on RMAT scale 20",
+    "twc24": "one BFS on RMAT scale 24 with the tiered push forced at every level (hubs staged in shared "
+             "memory by TMA bulk copies)",
+    "strict24": "one BFS on RMAT scale 24 with the edge-balanced (STRICT) push forced at every level",
+    "bc20": "batched BC from 32 sources on RMAT scale 20 (one cooperative launch)",
 }
 
 
@@ -740,6 +741,13 @@ def run_case(case: str) -> None:
     elif case == "mbfs":
         g = ctx.rmat(20, 16, seed=1)
         g.mbfs(g.roots(77, 256), batched=True, out=False)
+    elif case in ("twc24", "strict24"):
+        g = ctx.rmat(24, 16, seed=1)
+        cfg = "Push-Queue-TWC-Standalone" if case == "twc24" else "Push-Queue-STRICT-Standalone"
+        g.bfs(int(g.roots(1000, 1)[0]), gs.RunOpts.from_config(cfg), out=False)
+    elif case == "bc20":
+        g = ctx.rmat(20, 16, seed=1)
+        g.bc_batch(g.roots(99, 32), out=False)
     print("ok", case)
     g.close()
     ctx.close()
@@ -759,6 +767,7 @@ def main():
     ap.add_argument("--selector", default="mlp", choices=["mlp", "rules"])
     ap.add_argument("--no-apps", action="store_true")
     ap.add_argument("--c3", action="store_true", help="print config C3's switched-vs-fixed table instead")
+    ap.add_argument("--tune", default=None, help="tuning table to load (default: the committed one)")
     ap.add_argument("--case", choices=sorted(PROFILE_CASES),
                     help="run one small fixed workload for a profiler capture instead of the bench")
     args = ap.parse_args()

@@ -39,7 +39,7 @@ ABI_SYMBOLS = (
     "gsw_pagerank", "gsw_bc", "gsw_bc_batch", "gsw_gc", "gsw_mbfs", "gsw_bfs_strict_noalloc",
     "gsw_graph_generate_powerlaw", "gsw_label_levels", "gsw_mlp_train", "gsw_mlp_grad", "gsw_mlp_infer",
     "gsw_mlp_load", "gsw_graph_generate_er_batch", "gsw_bfs_multi", "gsw_bfs_inspect", "gsw_tune_load",
-    "gsw_tune_save", "gsw_mlp_load_fusion", "gsw_pagerank_delta",
+    "gsw_tune_save", "gsw_tune_load_shapes", "gsw_tune_save_shapes", "gsw_mlp_load_fusion", "gsw_pagerank_delta",
 )
 TUNE_ENTRIES = 64
 
@@ -76,7 +76,7 @@ class _Stats(C.Structure):
                 ("device_error", C.c_uint), ("launches", C.c_int64), ("ntrace", C.c_int),
                 ("level_cfg", C.c_int32 * MAX_TRACE), ("level_frontier", C.c_int64 * MAX_TRACE),
                 ("level_ms", C.c_float * MAX_TRACE), ("level_inspect_ms", C.c_float * MAX_TRACE),
-                ("level_edges", C.c_int64 * MAX_TRACE), ("level_bytes", C.c_int64 * MAX_TRACE)]
+                ("level_edges", C.c_int64 * MAX_TRACE)]
 
 
 _LIB = None
@@ -131,6 +131,8 @@ def lib():
     L.gsw_bfs_multi.argtypes = [vp, vp, C.c_int, vp, po, vp, ps]
     L.gsw_bfs_inspect.argtypes = [vp, vp, vp, i32, vp]
     L.gsw_tune_load.argtypes = [vp, vp]
+    L.gsw_tune_load_shapes.argtypes = [vp, vp]
+    L.gsw_tune_save_shapes.argtypes = [vp, vp]
     L.gsw_mlp_load_fusion.argtypes = [vp, vp, C.c_float]
     L.gsw_tune_save.argtypes = [vp, vp]
     _LIB = L
@@ -210,7 +212,6 @@ class RunStats:
         self.level_ms = [float(s.level_ms[i]) for i in range(n)]
         self.level_inspect_ms = [float(s.level_inspect_ms[i]) for i in range(n)]
         self.level_edges = [int(s.level_edges[i]) for i in range(n)]
-        self.level_bytes = [int(s.level_bytes[i]) for i in range(n)]
 
     @property
     def gteps(self) -> float:
@@ -346,6 +347,18 @@ class Context:
         q = np.zeros(TUNE_ENTRIES, dtype=np.int32)
         _check(lib().gsw_tune_save(self._h, _ptr(q)))
         return q
+
+    def tune_load_shapes(self, shapes=None):
+        """Tuned tile / candidates-per-thread shapes per variant (None: defaults)."""
+        t = None if shapes is None else np.ascontiguousarray(shapes, dtype=np.int32)
+        if t is not None and t.shape != (TUNE_ENTRIES,):
+            raise ValueError(f"shape table has {TUNE_ENTRIES} entries")
+        _check(lib().gsw_tune_load_shapes(self._h, _ptr(t)))
+
+    def tune_save_shapes(self):
+        t = np.zeros(TUNE_ENTRIES, dtype=np.int32)
+        _check(lib().gsw_tune_save_shapes(self._h, _ptr(t)))
+        return t
 
     def mlp_load_fusion(self, model=None, min_conf=0.0):
         m = None if model is None else np.ascontiguousarray(model, dtype=np.float32)

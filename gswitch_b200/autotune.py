@@ -1,8 +1,11 @@
-"""Autotuner of the expand grids: for every variant (direction x format x
+"""Autotuner of the expand launches: for every variant (direction x format x
 load balance, and the fused push forms) times the variant's expands under
-grid caps of 1/4 .. 16x the kernel's resident grid on seeded synthetic graphs
-and keeps the fastest cap (CUDA-event expand times summed over levels; BFS
-from three roots per graph).  The table loads with Context.tune_load().
+grid caps of 1/4 .. 16x the kernel's resident grid and, where the variant has
+them, under each of its shapes (STRICT: tiles of 512 / 1,024 / 2,048 slots;
+thread-mapped pull: candidates per thread) on seeded synthetic graphs, and
+keeps the fastest
+(CUDA-event expand times summed over levels; BFS from three roots per graph).
+The tables load with Context.tune_load() and Context.tune_load_shapes().
 
     python -m gswitch_b200.autotune --out gswitch_b200/models/tune.json
 """
@@ -20,6 +23,16 @@ if __package__ in (None, ""):
 import gswitch_b200 as gs  # noqa: E402
 
 QUARTERS = (1, 2, 4, 8, 16, 32, 64)  # grid cap = resident grid x q / 4
+STRICT_SHAPES = 3   # tile 1024 (default), 512, 2048
+PULL_TM_SHAPES = 3  # candidates per thread: 2 (default), 1, 4
+
+
+def shapes_of(direction, lb):
+    if lb == "STRICT":
+        return STRICT_SHAPES
+    if direction == "Pull" and lb == "TM":
+        return PULL_TM_SHAPES
+    return 1
 VARIANTS = [(d, f, lb, False) for d in ("Push", "Pull") for f in ("Queue", "Bitmap")
             for lb in ("TM", "WM", "CM", "STRICT", "TWC")] + [("Push", "Queue", lb, True)
                                                               for lb in ("TM", "WM", "CM", "STRICT", "TWC")]
@@ -36,29 +49,37 @@ def expand_ms(g, roots, cfg):
 
 def tune(ctx, graphs, reps=2, log=None):
     table = np.zeros(gs.TUNE_ENTRIES, dtype=np.int32)
+    shapes = np.zeros(gs.TUNE_ENTRIES, dtype=np.int32)
     report = {}
     for d, f, lb, fused in VARIANTS:
         cfg = f"{d}-{f}-{lb}-{'Fused' if fused else 'Standalone'}"
         idx = gs.Context.tune_index(d, f, lb, fused)
         times = {}
-        for q in QUARTERS:
-            t = np.zeros(gs.TUNE_ENTRIES, dtype=np.int32)
-            t[idx] = q
-            ctx.tune_load(t)
-            tot = 0.0
-            for g, roots in graphs:
-                expand_ms(g, roots, cfg)  # warm-up
-                tot += min(expand_ms(g, roots, cfg) for _ in range(reps))
-            times[q] = tot
+        for sh in range(shapes_of(d, lb)):
+            s = np.zeros(gs.TUNE_ENTRIES, dtype=np.int32)
+            s[idx] = sh
+            ctx.tune_load_shapes(s)
+            for q in QUARTERS:
+                t = np.zeros(gs.TUNE_ENTRIES, dtype=np.int32)
+                t[idx] = q
+                ctx.tune_load(t)
+                tot = 0.0
+                for g, roots in graphs:
+                    expand_ms(g, roots, cfg)  # warm-up
+                    tot += min(expand_ms(g, roots, cfg) for _ in range(reps))
+                times[(sh, q)] = tot
         best = min(times, key=times.get)
-        # keep the default unless another cap is clearly faster
-        if times[best] < 0.97 * times[4]:
-            table[idx] = best
-        report[cfg] = {"quarters": int(table[idx]) or 4, "ms": {str(k): round(v, 4) for k, v in times.items()}}
+        # keep the default (shape 0, the resident grid) unless another choice
+        # is clearly faster
+        if times[best] < 0.97 * times[(0, 4)]:
+            shapes[idx], table[idx] = best[0], (0 if best[1] == 4 else best[1])
+        report[cfg] = {"shape": int(shapes[idx]), "quarters": int(table[idx]) or 4,
+                       "ms": {f"{k[0]}/{k[1]}": round(v, 4) for k, v in times.items()}}
         if log:
-            log(f"{cfg}: {report[cfg]}")
+            log(f"{cfg}: shape {report[cfg]['shape']} quarters {report[cfg]['quarters']}")
     ctx.tune_load(None)
-    return table, report
+    ctx.tune_load_shapes(None)
+    return table, shapes, report
 
 
 def load_table(path=None):
@@ -66,6 +87,21 @@ def load_table(path=None):
     if not os.path.exists(path):
         return None
     return np.asarray(json.load(open(path))["quarters"], dtype=np.int32)
+
+
+def load_shapes(path=None):
+    """The tuned shapes (None when the table has none)."""
+    path = path or DEFAULT_PATH
+    if not os.path.exists(path):
+        return None
+    d = json.load(open(path))
+    return np.asarray(d["shapes"], dtype=np.int32) if "shapes" in d else None
+
+
+def load_into(ctx, path=None):
+    """Loads both tables into a context (defaults where absent)."""
+    ctx.tune_load(load_table(path))
+    ctx.tune_load_shapes(load_shapes(path))
 
 
 def main(argv=None):
@@ -78,14 +114,16 @@ def main(argv=None):
     for g in (ctx.rmat(args.scale, 16, seed=11), ctx.grid(1024, 1024, 100, seed=12),
               ctx.er(1 << args.scale, 8 << args.scale, seed=13)):
         graphs.append((g, g.roots(5, 3)))
-    table, report = tune(ctx, graphs, log=lambda m: print(m, file=sys.stderr, flush=True))
+    table, shapes, report = tune(ctx, graphs, log=lambda m: print(m, file=sys.stderr, flush=True))
     os.makedirs(os.path.dirname(args.out), exist_ok=True)
     with open(args.out, "w") as f:
-        json.dump({"format": "gswitch_b200 expand grid caps, quarters of the resident grid, "
+        json.dump({"format": "gswitch_b200 expand grid caps, quarters of the resident grid, and shapes (STRICT "
+                             "tile, thread-mapped pull candidates per thread), "
                              "index ((pull*2+bitmap)*8+lb)*2+fused", "quarters": [int(x) for x in table],
+                   "shapes": [int(x) for x in shapes],
                    "graphs": [f"rmat{args.scale}", "grid1024x1024_lr100", f"er2^{args.scale}"], "report": report}, f,
                   indent=0)
-    print(json.dumps({k: v["quarters"] for k, v in report.items()}))
+    print(json.dumps({k: [v["shape"], v["quarters"]] for k, v in report.items()}))
     ctx.close()
 
 

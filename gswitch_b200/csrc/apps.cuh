@@ -39,7 +39,7 @@ struct SSSP : Functor<VC, int, int, int> {
     int *nd = wa_of(v);
     int *od = ra_of(v);
     if (*nd == *od) return Inactive;
-    if (data.window.in((float)*nd)) {
+    if (data.win().in((float)*nd)) {
       *od = *nd;
       return Active;
     }
@@ -49,13 +49,13 @@ struct SSSP : Functor<VC, int, int, int> {
   __device__ __forceinline__ bool comp(int *d, int nv, GW) {
     if (*d > nv) {
       *d = nv;
-      return data.window.in((float)nv);
+      return data.win().in((float)nv);
     }
     return false;
   }
   __device__ __forceinline__ bool compAtomic(int *v, int nv, GW) {
     const int old = atomicMin(v, nv);
-    return old > nv ? data.window.in((float)nv) : false;
+    return old > nv ? data.win().in((float)nv) : false;
   }
   __device__ __forceinline__ bool cond(int v, int msg, GW) { return *wa_of(v) > msg; }
   __device__ __forceinline__ bool exit(int v, GW) { return *wa_of(v) != *ra_of(v); }

@@ -71,14 +71,19 @@ struct window_t {
   int win_top = 33679;
   bool enable = false;
 
-  bool too_large(double size) const { return size > 5 * 33679; }
-  bool ok(int size) const { return size <= win_top && size > win_bot; }
+  __host__ __device__ bool too_large(double size) const { return size > 5 * 33679; }
+  __host__ __device__ bool ok(int size) const { return size <= win_top && size > win_bot; }
   void set_lim(int bot, int top) {
     win_bot = bot;
     win_top = top;
   }
   template <typename FT, typename CT>
   void adjust(const FT &fets, const CT &conf) {
+    adjust_with(fets, conf, gsw::select_stepping_tree);
+  }
+  // the same step on the device, with a device copy of the stepping tree
+  template <typename FT, typename CT>
+  __host__ __device__ void adjust_with(const FT &fets, const CT &conf, const gsw::tree_node *stepping) {
     if (conf.conf_fusion) {
       wsz = wsz_lim;
       return;
@@ -86,7 +91,7 @@ struct window_t {
     double v1[2];
     v1[0] = fets.active_vertex;
     v1[1] = v1[0] * fets.cur_avg_deg_active;
-    int l = gsw::eval_tree(gsw::select_stepping_tree, v1);
+    int l = gsw::eval_tree(stepping, v1);
     if (enable) {
       if (l == 1) {
         shrink();
@@ -101,8 +106,8 @@ struct window_t {
     wsz_lim = lim;
     wsz = lim;
   }
-  void shrink() { wsz = wsz * shrink_rate; }
-  void inflat() {
+  __host__ __device__ void shrink() { wsz = wsz * shrink_rate; }
+  __host__ __device__ void inflat() {
     wsz = wsz / inflat_rate;
     if (wsz > wsz_lim) wsz = wsz_lim;
   }
@@ -112,7 +117,7 @@ struct window_t {
   }
   __host__ __device__ __forceinline__ bool less(float x) const { return x < th; }
   __host__ __device__ __forceinline__ bool greater(float x) const { return x >= th + wsz; }
-  void reset() {
+  __host__ __device__ void reset() {
     th = th + wsz;
     wsz = wsz_lim * reset_rate;
   }
@@ -133,6 +138,15 @@ struct vdata_t {
   WA *sb = nullptr;  // 2D-partition partial-contribution buffer
   int64_t sb_size = 0;
   window_t window;
+  // captured level loops keep the window in device memory (the loop moves
+  // it between levels); null: the by-value member above
+  const window_t *dwin = nullptr;
+  __host__ __device__ __forceinline__ const window_t &win() const {
+#ifdef __CUDA_ARCH__
+    if (dwin) return *dwin;
+#endif
+    return window;
+  }
 
   void build(int64_t n) {
     size = n;
@@ -270,9 +284,6 @@ struct config_t {
   // engine extensions
   bool conf_sorted_queue = true;   // bitmap->queue in vertex order
   bool conf_persistent = false;    // run fused levels in one grid-wide launch
-  bool conf_pull_prefetch = false;  // thread-mapped pull: most candidates will
-                                   // walk on (start at the row offsets rather
-                                   // than the first-in-neighbour array)
   int conf_hub_path = -1;          // how CTA-wide hub sweeps read columns
                                    // (HUB_SCALAR / HUB_VECTOR / HUB_STAGED;
                                    // -1: by the graph's edge data)
@@ -334,7 +345,6 @@ struct stat_t {
   double avg_filter_time = 0, avg_expand_time = 0;
   int level = 0;
   int64_t last_scanned = 0;  // edges the last expand touched (accounting)
-  int64_t last_abytes = 0;   // algorithmic bytes it reported (0: none)
 
   void build(int _size = gsw::STAT_SLOTS) {
     if (dg_runtime_info) return;

@@ -84,6 +84,17 @@ struct dloop_t {
   int inspect_kernels;
   int n_expand_bodies;
   cudaGraphConditionalHandle h_loop, h_filter, h_expand, h_inspect;
+  // stepping window of Mono patterns (SSSP): the kernels read `win` through
+  // vdata_t::dwin; when a level finds no input the probe body (the deferred
+  // filter of fused runs, then k_exit into probe_flag) looks for values the
+  // window kept out, and the next decision resets the window or stops
+  window_t win;
+  const tree_node *stepping;   // the stepping tree (device copy)
+  int probe_flag;              // k_exit's flag: some value lies outside the window
+  int window_on;               // the window is in use
+  int probe_armed;             // the probe ran this iteration
+  int probe_kernels;
+  cudaGraphConditionalHandle h_probe;
 };
 
 __device__ inline void dl_stop(dloop_t &d, int status) {
@@ -94,18 +105,56 @@ __device__ inline void dl_stop(dloop_t &d, int status) {
   cudaGraphSetConditional(d.h_inspect, 0);
 }
 
+// an iteration without filter or expand: only the inspection (after a window
+// reset) or nothing but the probe (a level that inspected no active vertex)
+__device__ inline void dl_skip_level(dloop_t &d, bool inspect) {
+  cudaGraphSetConditional(d.h_filter, DL_FILTER_BODIES);
+  cudaGraphSetConditional(d.h_expand, 2 * DL_VARIANTS);
+  cudaGraphSetConditional(d.h_inspect, inspect ? 1 : 0);
+  d.inspected = inspect ? 1 : 0;
+  d.launches += 1 + (inspect ? d.inspect_kernels : 0);
+}
+
+// after the expand and the inspection: arm the window's exit probe when the
+// level found no input (one thread)
+__global__ void k_dl_gate(dloop_t *d) {
+  const bool probe = d->status == DL_RUNNING && d->window_on && d->halt;
+  cudaGraphSetConditional(d->h_probe, probe ? 1 : 0);
+  d->probe_armed = probe ? 1 : 0;
+  d->launches += 1 + (probe ? d->probe_kernels : 0);
+}
+
+// DL_GO: the level runs; DL_INSPECT_ONLY / DL_PROBE_ONLY: see dl_skip_level
+enum { DL_STOPPED = 0, DL_GO = 1, DL_INSPECT_ONLY = 2, DL_PROBE_ONLY = 3 };
+
 // One level's decisions: the host loop's inspect-finish-select sequence
 // (gsw_capi.cu runners) on device state, by one thread.  Returns false when
 // the loop stops here.
-__device__ inline bool dl_decide(dloop_t &d, const level_counts &c, unsigned long long scanned) {
+__device__ inline int dl_decide(dloop_t &d, const level_counts &c, unsigned long long scanned) {
   auto stop = [&](int status) {
     dl_stop(d, status);
-    return false;
+    return (int)DL_STOPPED;
   };
   if (d.ntrace > 0 && d.ntrace <= d.trace_cap) d.trace_edges[d.ntrace - 1] = (long long)scanned;
-  if (d.halt) return stop(DL_DONE);  // the last expand found an empty input
   feature_t &fets = d.fets;
   config_t &conf = d.conf;
+  if (d.halt) {  // the last expand found an empty input (or the inspection no active vertex)
+    if (!(d.window_on && d.probe_armed)) return stop(DL_DONE);
+    // the host loop's window_exit (executor.cuh): a vertex whose value the
+    // window kept out restarts the loop on the next window
+    d.probe_armed = 0;
+    if (!d.probe_flag) return stop(DL_DONE);
+    d.probe_flag = 0;
+    d.win.reset();
+    d.halt = 0;
+    if (conf.conf_fusion) {
+      conf.conf_fuse_inspect = false;
+      conf.conf_switch_to_fusion = true;
+    }
+    if (d.iter >= d.iter_cap) return stop(DL_LEVEL_CAP);
+    d.iter++;
+    return DL_INSPECT_ONLY;
+  }
   fets_level_init(fets, d.level, d.nvertexs, d.nedges);
   bool need = !conf.conf_fuse_inspect;
   bool done = false;
@@ -120,12 +169,16 @@ __device__ inline bool dl_decide(dloop_t &d, const level_counts &c, unsigned lon
   }
   fets.flatten();
   if (d.max_iters > 0 && d.iter == d.max_iters) return stop(DL_DONE);
+  if (done && d.window_on) {  // nothing active in this window: probe before stopping
+    d.halt = 1;
+    return DL_PROBE_ONLY;
+  }
   if (done) return stop(DL_DONE);
   if (d.iter >= d.iter_cap) return stop(DL_LEVEL_CAP);
   selector_t sel;
   sel.trees = &d.trees;
   sel.decide(fets, conf);
-  return true;
+  return DL_GO;
 }
 
 // the filter-update-trace part of the level, after the selector (and the
@@ -175,6 +228,9 @@ __device__ inline void dl_commit(dloop_t &d) {
   cudaGraphSetConditional(d.h_filter, fbody);
   cudaGraphSetConditional(d.h_expand, ebody);
   cudaGraphSetConditional(d.h_inspect, d.inspected ? 1 : 0);
+  // the window the next inspection and expand read (the host loop adjusts it
+  // at the start of its next inspection, from the same features)
+  if (d.window_on) d.win.adjust_with(fets, conf, d.stepping);
 }
 
 // The decision thread works on a shared-memory copy of the loop state and of
@@ -220,8 +276,13 @@ __global__ void __launch_bounds__(256) k_dl_select(dloop_t *d) {
                         sh + (dev.fusion - base),          sh + (dev.lb_idem - base),
                         sh + (dev.lb_asso_forward - base), sh + (dev.lb_asso_backward - base),
                         sh + (dev.lb_asso_backward_backup - base)};
-    s_go = dl_decide(sd, s_c, s_scanned);
+    const tree_node *dev_step = sd.stepping;
+    if (dev_step) sd.stepping = sh + (dev_step - base);
+    const int code = dl_decide(sd, s_c, s_scanned);
+    if (code == DL_INSPECT_ONLY || code == DL_PROBE_ONLY) dl_skip_level(sd, code == DL_INSPECT_ONLY);
+    s_go = code == DL_GO;
     sd.trees = dev;
+    sd.stepping = dev_step;
     s_mlp = s_go && sd.mlp && mlp_applicable(*sd.mlp, sd.fets, sd.conf);
     if (s_mlp) mlp_features(sd.fets, s_x);
   }
@@ -304,6 +365,7 @@ bool dl_build(dloop_graph &L, executor_t &ex, dloop_t *d, active_set_t as, devic
   using G = device_graph_t<CSR, E>;
   L.destroy();
   g.dlevel = &d->level;
+  f.data.dwin = &d->win;
   as.nt.dg_tag = &d->halt;
   as.nt.already = false;
   as.queue.traceback = false;
@@ -351,8 +413,9 @@ bool dl_build(dloop_graph &L, executor_t &ex, dloop_t *d, active_set_t as, devic
   cudaGraph_t top = nullptr;
   good = good && !GSW_CUDA(cudaGraphCreate(&top, 0));
   L.graph = top;
-  cudaGraphConditionalHandle hl = 0, hf = 0, he = 0, hi = 0;
-  std::vector<cudaGraph_t> wbody, fbodies, ebodies, ibody;
+  cudaGraphConditionalHandle hl = 0, hf = 0, he = 0, hi = 0, hp = 0;
+  std::vector<cudaGraph_t> wbody, fbodies, ebodies, ibody, pbody;
+  const bool window = conf.conf_window;
   if (good) good = !GSW_CUDA(cudaGraphConditionalHandleCreate(&hl, top, 1, cudaGraphCondAssignDefault));
   if (good) {
     cudaGraphNodeParams p = {};
@@ -369,15 +432,20 @@ bool dl_build(dloop_graph &L, executor_t &ex, dloop_t *d, active_set_t as, devic
     cudaGraph_t B = wbody[0];
     good = !GSW_CUDA(cudaGraphConditionalHandleCreate(&hf, B, DL_FILTER_BODIES, 0)) &&
            !GSW_CUDA(cudaGraphConditionalHandleCreate(&he, B, 2 * DL_VARIANTS, 0)) &&
-           !GSW_CUDA(cudaGraphConditionalHandleCreate(&hi, B, 0, 0));
+           !GSW_CUDA(cudaGraphConditionalHandleCreate(&hi, B, 0, 0)) &&
+           (!window || !GSW_CUDA(cudaGraphConditionalHandleCreate(&hp, B, 0, 0)));
     if (good)
       good = dl_capture(B, [&] {
         k_dl_select<<<1, 256, 0, stream()>>>(d);
         if (dl_add_conditional(stream(), hf, cudaGraphCondTypeSwitch, DL_FILTER_BODIES, fbodies) &&
-            dl_add_conditional(stream(), he, cudaGraphCondTypeSwitch, nexp, ebodies))
-          dl_add_conditional(stream(), hi, cudaGraphCondTypeIf, 1, ibody);
+            dl_add_conditional(stream(), he, cudaGraphCondTypeSwitch, nexp, ebodies) &&
+            dl_add_conditional(stream(), hi, cudaGraphCondTypeIf, 1, ibody) && window) {
+          k_dl_gate<<<1, 1, 0, stream()>>>(d);
+          dl_add_conditional(stream(), hp, cudaGraphCondTypeIf, 1, pbody);
+        }
       });
-    good = good && fbodies.size() == DL_FILTER_BODIES && ebodies.size() == nexp && ibody.size() == 1;
+    good = good && fbodies.size() == DL_FILTER_BODIES && ebodies.size() == nexp && ibody.size() == 1 &&
+           (!window || pbody.size() == 1);
   }
   // filter bodies
   for (int sorted = 0; good && sorted < 2; ++sorted)
@@ -423,11 +491,21 @@ bool dl_build(dloop_graph &L, executor_t &ex, dloop_t *d, active_set_t as, devic
     });
     im.inspect_kernels = 1;
   }
+  // window exit probe: the deferred filter of fused runs, then the probe
+  // (window_delay_update and window_exit of the host loop)
+  if (good && window) {
+    good = dl_capture(pbody[0], [&] {
+      if (conf.conf_fusion) window_delay_update(as, g, f);
+      k_exit<<<resident_grid(k_exit<G, F>, 512), 512, 0, stream()>>>(g, f, &d->probe_flag);
+    });
+    im.probe_kernels = dl_count_nodes(pbody[0]);
+  }
   if (good) good = !GSW_CUDA(cudaGraphInstantiate(&L.exec, top, 0));
   im.h_loop = hl;
   im.h_filter = hf;
   im.h_expand = he;
   im.h_inspect = hi;
+  im.h_probe = hp;
   opts().timing = saved_timing;
   launch_count() = launches0;
   hints() = saved_hints;

@@ -483,6 +483,21 @@ struct selector_t {
 };
 
 // ===========================================================================
+// tuned shapes
+// ===========================================================================
+constexpr int STRICT_TILE_MIN = 512;
+constexpr int STRICT_SHAPES = 3;   // tile 1024 (default), 512, 2048
+constexpr int PULL_TM_SHAPES = 3;  // candidates per thread: 2 (default), 1, 4
+inline int strict_tile_of(int shape) { return shape == 1 ? 512 : (shape == 2 ? 2048 : STRICT_TILE); }
+inline int pull_tm_k_of(int shape) { return shape == 1 ? 1 : (shape == 2 ? 4 : 2); }
+// shapes a variant may take (1: none but the default)
+inline int shape_count(bool pull, int lb) {
+  if (lb == STRICT) return STRICT_SHAPES;
+  if (pull && lb == TM) return PULL_TM_SHAPES;
+  return 1;
+}
+
+// ===========================================================================
 // executor_t
 // ===========================================================================
 struct executor_t {
@@ -491,6 +506,10 @@ struct executor_t {
   // cap in quarters of the kernel's resident grid (0: the resident grid).
   struct tune_t {
     int quarters[2][2][8][2] = {};
+    // tuned shape per variant (0: the default): STRICT variants pick the tile
+    // (strict_tile_of), the thread-mapped pull its candidates per thread
+    // (pull_tm_k_of); other variants have no shape
+    int shapes[2][2][8][2] = {};
   } tune;
   twod_layout twod;                 // 2D-partition layout of the current graph
   int64_t persistent_levels = 0;    // levels run inside persistent launches
@@ -587,8 +606,9 @@ struct executor_t {
   template <typename E, typename F>
   void compensation(active_set_t &, device_graph_t<COO, E> &, F &) {}
 
+  // the table is sized for the smallest tile any shape uses
   void ensure_tiles(int64_t slots_cap) {
-    const int64_t need = slots_cap / STRICT_TILE + 2;
+    const int64_t need = slots_cap / STRICT_TILE_MIN + 2;
     if (need <= tile_cap) return;
     cudaFree(dg_tile);
     dg_tile = nullptr;
@@ -596,7 +616,7 @@ struct executor_t {
     tile_cap = need;
   }
 
-  template <bool PULL, typename G>
+  template <bool PULL, int T, typename G>
   void strict_prepare(active_set_t &as, G &g, Status want) {
     const int64_t items = hints().frontier >= 0 ? hints().frontier : (as.fmt == Queue ? as.size + 1 : as.size);
     const int64_t nb = items / STRICT_ITEMS + 1;
@@ -605,7 +625,7 @@ struct executor_t {
     if (nb + 1 > as.workset.bsum_cap) return (void)set_error(GSW_ERR_OVERFLOW, "strict: %s", "block sums");
     k_strict_count<PULL><<<(unsigned)nb, 256, 0, stream()>>>(as, g, want, as.workset.dg_bsum);
     k_scan_single_block<<<1, 1024, 0, stream()>>>(as.workset.dg_bsum, nb);
-    k_strict_scan<PULL><<<(unsigned)nb, 256, 0, stream()>>>(as, g, want, as.workset.dg_bsum, nb, dg_tile, tile_cap);
+    k_strict_scan<PULL, T><<<(unsigned)nb, 256, 0, stream()>>>(as, g, want, as.workset.dg_bsum, nb, dg_tile, tile_cap);
     GSW_LAUNCHED();
   }
 
@@ -619,6 +639,7 @@ struct executor_t {
     const int fg = opts().force_grid;
     // autotuned grid of this variant: quarters of the resident grid
     const int tq = tune.quarters[conf.conf_dir == Pull][as.fmt == Bitmap][(int)conf.conf_lb & 7][fused ? 1 : 0];
+    const int shape = tune.shapes[conf.conf_dir == Pull][as.fmt == Bitmap][(int)conf.conf_lb & 7][fused ? 1 : 0];
     auto grid_for = [&](auto kern, int64_t want) {
       const int res = resident_grid(kern, B);
       if (fg > 0) return fg;
@@ -653,11 +674,20 @@ struct executor_t {
           else GSW_GO((k_push_twc<false, G, F>), fr < 0 ? -1 : fr / B + 1, as, g, f, conf);
           break;
         case STRICT: {
-          strict_prepare<false>(as, g, conf.want());
+          auto go = [&](auto tile) {
+            constexpr int T = decltype(tile)::value;
+            strict_prepare<false, T>(as, g, conf.want());
+            if (!ok()) return;
+            const int64_t want = (ed < 0 || fr < 0) ? -1 : (ed + fr) / T + 1;
+            if (fused) GSW_GO((k_push_strict<true, T, G, F>), want, as, g, f, conf, dg_tile);
+            else GSW_GO((k_push_strict<false, T, G, F>), want, as, g, f, conf, dg_tile);
+          };
+          switch (strict_tile_of(shape)) {
+            case 512: go(std::integral_constant<int, 512>{}); break;
+            case 2048: go(std::integral_constant<int, 2048>{}); break;
+            default: go(std::integral_constant<int, STRICT_TILE>{}); break;
+          }
           if (!ok()) return;
-          const int64_t want = (ed < 0 || fr < 0) ? -1 : (ed + fr) / STRICT_TILE + 1;
-          if (fused) GSW_GO((k_push_strict<true, G, F>), want, as, g, f, conf, dg_tile);
-          else GSW_GO((k_push_strict<false, G, F>), want, as, g, f, conf, dg_tile);
           break;
         }
         case WM:
@@ -672,25 +702,41 @@ struct executor_t {
         case CM: GSW_GO((k_pull_cm<G, F>), fr < 0 ? -1 : fr / B + 1, as, g, f, conf); break;
         case TWC: GSW_GO((k_pull_twc<G, F>), fr < 0 ? -1 : fr / B + 1, as, g, f, conf); break;
         case STRICT: {
-          strict_prepare<true>(as, g, conf.want());
-          if (!ok()) return;
-          const int64_t want = (ed < 0 || fr < 0) ? -1 : (ed + fr) / STRICT_TILE + 1;
-          if constexpr (sizeof(typename F::wa_t) <= 4) {
-            if (conf.conf_fromall) {
-              GSW_GO((k_pull_strict_all<G, F>), want, as, g, f, conf, dg_tile);
-              break;
+          // from-all pulls stage a per-vertex sum too: their tiles stop at
+          // 1,024 slots (48 KB of static shared memory)
+          const bool all = sizeof(typename F::wa_t) <= 4 && conf.conf_fromall;
+          auto go = [&](auto tile) {
+            constexpr int T = decltype(tile)::value;
+            strict_prepare<true, T>(as, g, conf.want());
+            if (!ok()) return;
+            const int64_t want = (ed < 0 || fr < 0) ? -1 : (ed + fr) / T + 1;
+            if constexpr (sizeof(typename F::wa_t) <= 4 && T <= 1024) {
+              if (all) {
+                GSW_GO((k_pull_strict_all<T, G, F>), want, as, g, f, conf, dg_tile);
+                return;
+              }
             }
-          }
-          GSW_GO((k_pull_strict<G, F>), want, as, g, f, conf, dg_tile);
+            GSW_GO((k_pull_strict<T, G, F>), want, as, g, f, conf, dg_tile);
+          };
+          const int t = strict_tile_of(shape);
+          if (t == 512)
+            go(std::integral_constant<int, 512>{});
+          else if (t == 2048 && !all)
+            go(std::integral_constant<int, 2048>{});
+          else
+            go(std::integral_constant<int, STRICT_TILE>{});
+          if (!ok()) return;
           break;
         }
         case TM:
         default: {
-          // a frontier that is a small share of the candidates settles few of
-          // them at their first in-neighbour: most walk on
-          config_t c = conf;
-          c.conf_pull_prefetch = insp && insp->raw_frontier * 20 < insp->raw_inactive;
-          GSW_GO((k_pull_tm<G, F>), fr < 0 ? -1 : fr / B + 1, as, g, f, c);
+          const int k = pull_tm_k_of(shape);
+          if (k == 1)
+            GSW_GO((k_pull_tm<1, G, F>), fr < 0 ? -1 : fr / B + 1, as, g, f, conf);
+          else if (k == 4)
+            GSW_GO((k_pull_tm<4, G, F>), fr < 0 ? -1 : fr / B + 1, as, g, f, conf);
+          else
+            GSW_GO((k_pull_tm<2, G, F>), fr < 0 ? -1 : fr / B + 1, as, g, f, conf);
           break;
         }
       }
@@ -828,10 +874,7 @@ struct executor_t {
     const bool sync_needed = conf.conf_fuse_inspect || opts().verbose;
     if (sync_needed && !ev[0])
       for (auto &e : ev) cudaEventCreate(&e);
-    if (conf.conf_count_edges) {
-      GSW_CUDA(cudaMemsetAsync(&as.dg_cnt->scanned, 0, sizeof(unsigned long long), stream()));
-      GSW_CUDA(cudaMemsetAsync(&as.dg_cnt->abytes, 0, sizeof(unsigned long long), stream()));
-    }
+    if (conf.conf_count_edges) GSW_CUDA(cudaMemsetAsync(&as.dg_cnt->scanned, 0, sizeof(unsigned long long), stream()));
     if (sync_needed) cudaEventRecord(ev[0], stream());
     marks().exp0 = opts().timing ? timing_pool().record() : -1;
     last_persistent = false;
@@ -848,14 +891,11 @@ struct executor_t {
       e = s + ms;
     }
     stat.last_scanned = 0;
-    stat.last_abytes = 0;
     if (conf.conf_count_edges) {
-      unsigned long long c = 0, b = 0;
+      unsigned long long c = 0;
       GSW_CUDA(cudaMemcpyAsync(&c, &as.dg_cnt->scanned, sizeof(c), cudaMemcpyDeviceToHost, stream()));
-      GSW_CUDA(cudaMemcpyAsync(&b, &as.dg_cnt->abytes, sizeof(b), cudaMemcpyDeviceToHost, stream()));
       GSW_CUDA(cudaStreamSynchronize(stream()));
       stat.last_scanned = (int64_t)c;
-      stat.last_abytes = (int64_t)b;
     }
     stat.last_time = stat.last_filter_time + e - s;
     const int lv = g.level > 0 ? g.level : 1;

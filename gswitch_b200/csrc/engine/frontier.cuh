@@ -53,8 +53,6 @@ struct as_counters_t {
   int preason;                     // persistent fused levels: exit reason
   int plb;                         // persistent fused levels: the load
                                    // balance the launched kernel ran
-  unsigned long long abytes;       // accounting: algorithmic bytes an expand
-                                   // reported (kernels that count their own)
 };
 
 struct bits_t {

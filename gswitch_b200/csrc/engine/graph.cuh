@@ -25,15 +25,6 @@ struct device_graph_t<CSR, E> {
   const int *dgr_adj_list;
   const int *dgr_odegree;
   E *dgr_edgedata;
-  // first in-neighbour of every vertex (dgr_adj_list[dgr_row_off[v]], -1
-  // without in-edges): one coalesced 4-byte read settles a pull candidate
-  // whose first in-neighbour is in the frontier, with no row offsets and no
-  // 32-byte column sector fetched for 4 useful bytes (null: not built)
-  const int *dgr_first = nullptr;
-  // bit v set when v has in-edges: a pull skips the vertices without any
-  // (43% of an RMAT graph's ids) at the bitmap test, before touching their
-  // per-vertex arrays (null: not built)
-  const uint32_t *dgr_nonempty = nullptr;
 
   int nvertexs;
   int64_t nedges;

@@ -32,11 +32,9 @@
 namespace gsw {
 
 constexpr int EXPAND_THREADS = 256;
-constexpr int STRICT_TILE = 1024;   // slots per STRICT tile (4 per thread)
+constexpr int STRICT_TILE = 1024;   // default slots per STRICT tile (4 per thread); the
+                                    // autotuner may pick 512 or 2048 per variant
 constexpr int STRICT_ITEMS = 1024;  // frontier entries per STRICT scan block
-#ifndef GSW_PULL_TM_K
-#define GSW_PULL_TM_K 2
-#endif
 
 // ---- per-edge operations ---------------------------------------------------
 template <typename G, typename F>
@@ -133,12 +131,6 @@ __device__ __forceinline__ void vertex_range(const G &g, bool pull, int v, int64
 __device__ __forceinline__ void account(const active_set_t &as, const config_t &conf, unsigned long long c) {
   if (conf.conf_count_edges && c) atomicAdd(&as.dg_cnt->scanned, c);
 }
-// accounting pass only: the bytes of the CSR side of the algorithm (offsets,
-// columns, first in-neighbours) and of the vertex-state writes that a kernel
-// whose reads depend on its data counts for itself
-__device__ __forceinline__ void account_bytes(const active_set_t &as, const config_t &conf, unsigned long long b) {
-  if (conf.conf_count_edges && b) atomicAdd(&as.dg_cnt->abytes, b);
-}
 
 // Where a push body reads its work list.  Per-launch kernels read the active
 // set (queue or bitmap, read-only path).  Levels inside a persistent launch
@@ -227,34 +219,27 @@ __global__ void __launch_bounds__(EXPAND_THREADS) k_push_tm(active_set_t as, G g
   account(as, conf, cnt);
 }
 
-// Thread per candidate, GSW_PULL_TM_K (2) candidates per thread: the
-// dependent chain of a candidate (status bit -> offsets -> first in-neighbour
-// -> its frontier bit) is issued for both before either is resolved.  Most
-// candidates of a large pull level stop at the first neighbour; the rest walk
-// their lists one edge at a time, and a warp waits for its longest walk, so
-// more candidates per thread cost more in divergence than they gain in
-// overlap (RMAT s24 pull levels: 105 us at 1, 93 at 2, 103 at 4, 135 at 8;
-// fetching four neighbours per step of the walk was slower too).
-//
-// With the first-in-neighbour array (graphs without edge data) the chain
-// starts at one coalesced 4-byte read: a candidate whose first in-neighbour
-// is in the frontier is settled without its row offsets or a 32-byte column
-// sector; only the others read their offsets and walk on.
-template <typename G, typename F>
+// Thread per candidate, K candidates per thread (2 by default; the autotuner
+// may pick 1 or 4): the dependent chain of a candidate (status bit -> offsets
+// -> first in-neighbour -> its frontier bit) is issued for all K before any
+// is resolved.  Most candidates of a large pull level stop at the first
+// neighbour; the rest walk their lists one edge at a time, and a warp waits
+// for its longest walk, so more candidates per thread cost more in
+// divergence than they gain in overlap (RMAT s24 pull levels: 105 us at 1,
+// 93 at 2, 103 at 4, 135 at 8).  Measured and not kept (section 3 of the
+// design notes has the numbers): fetching four neighbours per walk step, a
+// warp-cooperative walk of the unresolved candidates, a first-in-neighbour
+// side array (less DRAM traffic, no faster), skipping vertices without
+// in-edges by a bitmap, and capping thread walks at 8 edges with 8-lane
+// groups finishing the rest (40 registers, 75% occupancy, slower).
+template <int K, typename G, typename F>
 __global__ void __launch_bounds__(EXPAND_THREADS) k_pull_tm(active_set_t as, G g, F f, config_t conf) {
   using WA = typename F::wa_t;
-  constexpr int K = GSW_PULL_TM_K;
-  constexpr bool NO_EDATA = std::is_same<typename G::edge_t, Empty>::value;
   const int64_t n = as.get_size();
   GSW_HALT_IF_EMPTY(n);
   const Status want = conf.want();
   const int64_t STRIDE = (int64_t)blockDim.x * gridDim.x;
-  // the side array pays off where most candidates settle at their first
-  // in-neighbour; where most walk on (conf_pull_prefetch: the frontier is a
-  // small share of the candidates) the walk starts at the row offsets, and
-  // the first column shares its sector with the rest of the walk
-  const bool first_path = NO_EDATA && g.dgr_first != nullptr && !conf.conf_pull_prefetch;
-  unsigned long long cnt = 0, abytes = 0;
+  unsigned long long cnt = 0;
   for (int64_t base = threadIdx.x + (int64_t)blockIdx.x * blockDim.x; base < n; base += K * STRIDE) {
     int v[K], deg[K], u0[K];
     int64_t st[K];
@@ -263,39 +248,13 @@ __global__ void __launch_bounds__(EXPAND_THREADS) k_pull_tm(active_set_t as, G g
     for (int k = 0; k < K; ++k) {
       const int64_t idx = base + k * STRIDE;
       v[k] = idx < n ? as.fetch(idx, want) : -1;
-      // a vertex without in-edges has nothing to pull; in the bitmap format
-      // its bit is read beside the status word, not after it
-      const int64_t probe = as.fmt == Bitmap ? idx : (int64_t)v[k];
-      if (probe >= 0 && probe < n && g.dgr_nonempty && !((__ldg(g.dgr_nonempty + (probe >> 5)) >> (probe & 31)) & 1u))
-        v[k] = -1;
     }
-    if (first_path) {
 #pragma unroll
-      for (int k = 0; k < K; ++k) u0[k] = v[k] >= 0 ? __ldg(g.dgr_first + v[k]) : -1;
+    for (int k = 0; k < K; ++k) vertex_range(g, true, v[k], st[k], deg[k]);
 #pragma unroll
-      for (int k = 0; k < K; ++k) abytes += v[k] >= 0 ? 4 : 0;
+    for (int k = 0; k < K; ++k) u0[k] = deg[k] > 0 ? __ldg(g.dgr_adj_list + st[k]) : 0;
 #pragma unroll
-      for (int k = 0; k < K; ++k) a0[k] = u0[k] >= 0 && (conf.conf_fromall || as.bitmap.is_active(u0[k]));
-#pragma unroll
-      for (int k = 0; k < K; ++k) {
-        if (u0[k] >= 0 && !(a0[k] && conf.conf_pruning)) {
-          vertex_range(g, true, v[k], st[k], deg[k]);
-          abytes += 16;  // offsets
-        } else {
-          st[k] = 0;
-          deg[k] = u0[k] >= 0 ? 1 : 0;  // settled at the first in-neighbour, or no in-edges
-        }
-      }
-    } else {
-#pragma unroll
-      for (int k = 0; k < K; ++k) vertex_range(g, true, v[k], st[k], deg[k]);
-#pragma unroll
-      for (int k = 0; k < K; ++k) abytes += v[k] >= 0 ? 16 : 0;
-#pragma unroll
-      for (int k = 0; k < K; ++k) u0[k] = deg[k] > 0 ? __ldg(g.dgr_adj_list + st[k]) : 0;
-#pragma unroll
-      for (int k = 0; k < K; ++k) a0[k] = deg[k] > 0 && (conf.conf_fromall || as.bitmap.is_active(u0[k]));
-    }
+    for (int k = 0; k < K; ++k) a0[k] = deg[k] > 0 && (conf.conf_fromall || as.bitmap.is_active(u0[k]));
 #pragma unroll
     for (int k = 0; k < K; ++k) {
       if (v[k] < 0 || deg[k] == 0) continue;
@@ -325,14 +284,10 @@ __global__ void __launch_bounds__(EXPAND_THREADS) k_pull_tm(active_set_t as, G g
         }
       }
       cnt += e;
-      // column entries read (the first came from the side array on that
-      // path), and the state write
-      abytes += 4ull * (e - (first_path ? 1 : 0)) + (have ? sizeof(WA) : 0);
       if (have) f.comp(f.wa_of(v[k]), acc, g);
     }
   }
   account(as, conf, cnt);
-  account_bytes(as, conf, abytes);
 }
 
 // ===========================================================================
@@ -566,6 +521,7 @@ __device__ __forceinline__ int64_t strict_slots(const active_set_t &as, const G 
 // (d[k] slots each, the first starting at slot `off`): eoff[idx] gets the
 // entry's first slot, tile_lo[t] the entry owning slot t*STRICT_TILE.  Every
 // lane of the warp calls it.
+template <int T = STRICT_TILE>
 __device__ __forceinline__ void strict_scan_epilogue(const active_set_t &as, int64_t base, int64_t n,
                                                      const int64_t (&d)[4], int64_t off, int64_t *eoff, int *tile_lo,
                                                      int64_t tile_cap) {
@@ -582,8 +538,8 @@ __device__ __forceinline__ void strict_scan_epilogue(const active_set_t &as, int
     const bool valid = idx < n;
     if (valid) eoff[idx] = off;
     // tiles whose first slot falls in [off, off + d): ta <= t < tb
-    const int64_t ta = (off + STRICT_TILE - 1) / STRICT_TILE;
-    const int64_t tb = valid ? (off + d[k] + STRICT_TILE - 1) / STRICT_TILE : ta;
+    const int64_t ta = (off + T - 1) / T;
+    const int64_t tb = valid ? (off + d[k] + T - 1) / T : ta;
     // a hub owns many tiles, and a sorted frontier puts the hubs side by
     // side: long runs are written by the whole warp, 32 tiles a step
     const bool many = tb - ta > 2;
@@ -615,7 +571,7 @@ __global__ void __launch_bounds__(256) k_strict_count(active_set_t as, G g, Stat
 
 // eoff[idx] = exclusive scan of (degree+1); tile_lo[t] = frontier index that
 // owns slot t*STRICT_TILE.  Each thread scans 4 consecutive entries.
-template <bool PULL, typename G>
+template <bool PULL, int T, typename G>
 __global__ void __launch_bounds__(256) k_strict_scan(active_set_t as, G g, Status want, const int64_t *bsum,
                                                      int64_t nblocks, int *tile_lo, int64_t tile_cap) {
   __shared__ int64_t s[33];
@@ -639,7 +595,7 @@ __global__ void __launch_bounds__(256) k_strict_scan(active_set_t as, G g, Statu
   __syncthreads();
   const int64_t off = bsum[blockIdx.x] + s[warp_id()] + incl - loc;
   int64_t *eoff = as.workset.dg_eoff;
-  strict_scan_epilogue(as, base, n, d, off, eoff, tile_lo, tile_cap);
+  strict_scan_epilogue<T>(as, base, n, d, off, eoff, tile_lo, tile_cap);
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     eoff[n] = bsum[nblocks];
     as.dg_cnt->total_edges = (unsigned long long)bsum[nblocks];
@@ -648,11 +604,10 @@ __global__ void __launch_bounds__(256) k_strict_scan(active_set_t as, G g, Statu
 
 // STRICT push over the tiles of a scanned frontier src[0..n) (eoff: the
 // (degree+1) scan, tile_lo: tile owners)
-template <bool FUSED, typename G, typename F, typename Src>
+template <bool FUSED, int T, typename G, typename F, typename Src>
 __device__ __forceinline__ void push_strict_body(active_set_t &as, const G &g, F &f, const config_t &conf,
                                                  const Src &src, int64_t n, const int64_t *eoff, const int *tile_lo,
                                                  warp_stage_t &stage) {
-  constexpr int T = STRICT_TILE;
   __shared__ int s_v[T + 2];
   __shared__ int64_t s_sc[T + 2];
   __shared__ int64_t s_st[T + 2];
@@ -696,14 +651,14 @@ __device__ __forceinline__ void push_strict_body(active_set_t &as, const G &g, F
   }
 }
 
-template <bool FUSED, typename G, typename F>
+template <bool FUSED, int T, typename G, typename F>
 __global__ void __launch_bounds__(EXPAND_THREADS) k_push_strict(active_set_t as, G g, F f, config_t conf,
                                                                 const int *tile_lo) {
   __shared__ int s_stage[FUSED ? EXPAND_THREADS / 32 : 1][FUSED ? STAGE_SLOTS : 1];
   const int64_t n = as.get_size();
   GSW_HALT_IF_EMPTY(n);
   warp_stage_t stage(s_stage[FUSED ? warp_id() : 0], as);
-  push_strict_body<FUSED>(as, g, f, conf, as_src_t{&as, conf.want()}, n, as.workset.dg_eoff, tile_lo, stage);
+  push_strict_body<FUSED, T>(as, g, f, conf, as_src_t{&as, conf.want()}, n, as.workset.dg_eoff, tile_lo, stage);
   if (FUSED) stage.flush();
 }
 
@@ -717,11 +672,10 @@ __global__ void __launch_bounds__(EXPAND_THREADS) k_push_strict(active_set_t as,
 // comp() when the run holds every in-edge of its vertex, with compAtomic()
 // when the vertex's edges continue in another pass or tile.  A hub therefore
 // costs one atomic per 32 edges instead of one per thread.
-template <typename G, typename F>
+template <int T, typename G, typename F>
 __global__ void __launch_bounds__(EXPAND_THREADS) k_pull_strict(active_set_t as, G g, F f, config_t conf,
                                                                 const int *tile_lo) {
   using WA = typename F::wa_t;
-  constexpr int T = STRICT_TILE;
   constexpr int B = EXPAND_THREADS;
   constexpr int PER = T / B;
   __shared__ int s_v[T + 2];
@@ -808,11 +762,10 @@ __global__ void __launch_bounds__(EXPAND_THREADS) k_pull_strict(active_set_t as,
 // tails meet in shared memory, and every vertex
 // of the tile is written once: comp() when all its slots lie in the tile,
 // compAtomic() otherwise.
-template <typename G, typename F>
+template <int T, typename G, typename F>
 __global__ void __launch_bounds__(EXPAND_THREADS) k_pull_strict_all(active_set_t as, G g, F f, config_t conf,
                                                                     const int *tile_lo) {
   using WA = typename F::wa_t;
-  constexpr int T = STRICT_TILE;
   constexpr int WSLOTS = T / (EXPAND_THREADS / 32);  // slots per warp
   __shared__ int s_v[T + 2];
   __shared__ int64_t s_sc[T + 2];

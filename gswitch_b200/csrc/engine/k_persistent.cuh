@@ -147,7 +147,8 @@ __device__ bool persist_strict_scan(active_set_t &as, const G &g, F &f, const le
       if (lane_id() == 31) s_w[32] = yi;
     }
     __syncthreads();
-    strict_scan_epilogue(as, base, c1, d, pre + s_w[warp_id()] + incl - loc, ps.eoff, ps.tile_lo, ps.tile_cap);
+    strict_scan_epilogue<STRICT_TILE>(as, base, c1, d, pre + s_w[warp_id()] + incl - loc, ps.eoff, ps.tile_lo,
+                                      ps.tile_cap);
     pre += s_w[32];
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) ps.eoff[n] = tot;
@@ -193,7 +194,8 @@ __global__ void __launch_bounds__(EXPAND_THREADS) k_fused_persistent(active_set_
         reason = 3;
         break;
       }
-      push_strict_body<true>(as, g, f, conf, level_src_t{ps.q[L & 1], false}, n, ps.eoff, ps.tile_lo, stage);
+      push_strict_body<true, STRICT_TILE>(as, g, f, conf, level_src_t{ps.q[L & 1], false}, n, ps.eoff, ps.tile_lo,
+                                          stage);
     } else {
       push_wm_body<true>(as, g, f, conf, src, n, stage);
     }

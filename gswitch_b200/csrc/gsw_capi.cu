@@ -36,8 +36,6 @@ struct gsw_graph {
   int *col = nullptr, *odeg = nullptr, *w = nullptr;
   int64_t *roff = nullptr;
   int *rcol = nullptr, *rdeg = nullptr, *rw = nullptr;
-  int *first = nullptr, *rfirst = nullptr;  // first (in-)neighbour per vertex, -1: none
-  uint32_t *nonempty = nullptr, *rnonempty = nullptr;  // bit per vertex: has (in-)edges
   packed_t *coo = nullptr;
   int64_t ncoo = -1;
   double attr[6] = {0, 0, 0, 0, 0, 0};
@@ -63,8 +61,6 @@ struct gsw_graph {
     g.dgr_adj_list = directed ? rcol : col;
     g.dgr_odegree = directed ? rdeg : odeg;
     g.dgr_edgedata = (E *)(directed ? rw : w);
-    g.dgr_first = directed ? rfirst : first;
-    g.dgr_nonempty = directed ? rnonempty : nonempty;
     g.nvertexs = (int)n;
     g.nedges = m;
     g.level = 0;
@@ -84,6 +80,7 @@ struct gsw_ctx {
   tree_node *dtrees = nullptr;  // the selector's trees in device memory
   int ntree_nodes = 0;
   tree_set dts{};
+  const tree_node *dstepping = nullptr;  // the window's stepping tree, in dtrees
   std::map<int, dloop_graph> dl;  // captured level loops, one per application
   mlp_model mlp{};                // learned selector (valid = 0: none loaded)
   mlp_model mlp_fusion{};         // learned fusion decision of Mono-pattern runs
@@ -312,51 +309,11 @@ __global__ void k_sum_weights(const int *w, int64_t m, unsigned long long *out) 
   if (lane_id() == 0 && s) atomicAdd(out, s);
 }
 
-__global__ void k_first_nbr(const int64_t *off, const int *col, int64_t n, int *first) {
-  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t a = off[v];
-    first[v] = off[v + 1] > a ? col[a] : -1;
-  }
-}
-
-__global__ void k_nonempty_bits(const int64_t *off, int64_t n, uint32_t *bits) {
-  const int64_t nw = (n + 31) >> 5;
-  for (int64_t w = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; w < nw; w += (int64_t)gridDim.x * blockDim.x) {
-    uint32_t b = 0;
-    for (int i = 0; i < 32; ++i) {
-      const int64_t v = w * 32 + i;
-      if (v < n && off[v + 1] > off[v]) b |= 1u << i;
-    }
-    bits[w] = b;
-  }
-}
-
 void finalize_graph(gsw_graph *g) {
   int64_t *off = g->off;
   if (!g->odeg) {
     if (!(g->odeg = (int *)g->ctx->graph_alloc(sizeof(int) * (g->n + 1)))) return;
     k_deg_to_i32<<<grid_for(g->n), 256, 0, stream()>>>(off, g->n, g->odeg);
-    GSW_LAUNCHED();
-  }
-  if (!g->first) {
-    if (!(g->first = (int *)g->ctx->graph_alloc(sizeof(int) * (g->n + 1)))) return;
-    k_first_nbr<<<grid_for(g->n), 256, 0, stream()>>>(off, g->col, g->n, g->first);
-    GSW_LAUNCHED();
-  }
-  if (g->directed && g->roff && g->rcol && !g->rfirst) {
-    if (!(g->rfirst = (int *)g->ctx->graph_alloc(sizeof(int) * (g->n + 1)))) return;
-    k_first_nbr<<<grid_for(g->n), 256, 0, stream()>>>(g->roff, g->rcol, g->n, g->rfirst);
-    GSW_LAUNCHED();
-  }
-  const int64_t nwords = (g->n + 31) / 32 + 1;
-  if (!g->nonempty) {
-    if (!(g->nonempty = (uint32_t *)g->ctx->graph_alloc(sizeof(uint32_t) * nwords))) return;
-    k_nonempty_bits<<<grid_for(nwords), 256, 0, stream()>>>(off, g->n, g->nonempty);
-    GSW_LAUNCHED();
-  }
-  if (g->directed && g->roff && !g->rnonempty) {
-    if (!(g->rnonempty = (uint32_t *)g->ctx->graph_alloc(sizeof(uint32_t) * nwords))) return;
-    k_nonempty_bits<<<grid_for(nwords), 256, 0, stream()>>>(g->roff, g->n, g->rnonempty);
     GSW_LAUNCHED();
   }
   if (g->weighted) {
@@ -435,8 +392,7 @@ gsw_graph *new_graph(gsw_ctx *ctx, int64_t n) {
 void free_graph(gsw_graph *g) {
   if (!g) return;
   for (void *p : {(void *)g->off, (void *)g->col, (void *)g->odeg, (void *)g->w, (void *)g->roff, (void *)g->rcol,
-                  (void *)g->rdeg, (void *)g->rw, (void *)g->first, (void *)g->rfirst, (void *)g->nonempty,
-                  (void *)g->rnonempty})
+                  (void *)g->rdeg, (void *)g->rw})
     g->ctx->graph_free(p);
   cudaFree(g->coo);
   if (g->twod) {
@@ -773,7 +729,6 @@ struct loop_trace {
       st->level_frontier[last] = frontier;
       st->level_ms[last] = 0;
       st->level_edges[last] = -1;
-      st->level_bytes[last] = -1;
       st->ntrace++;
     }
     st->levels++;
@@ -791,7 +746,6 @@ struct loop_trace {
     if (hints().persistent)
       st->level_cfg[last] = (st->level_cfg[last] & ~(7 << 2)) | ((hints().persistent_lb & 7) << 2) | (1 << 6);
     st->level_edges[last] = stats.last_scanned;
-    st->level_bytes[last] = stats.last_abytes > 0 ? stats.last_abytes : -1;
     st->level_inspect_ms[last] = 0;
     if (opts().timing) {
       if ((int)pending.size() <= last) pending.resize(last + 1);
@@ -868,24 +822,26 @@ inline int level_cap(int64_t n) { return (int)std::min<int64_t>(std::max<int64_t
 // ---------------------------------------------------------------------------
 // captured level loop (engine/devloop.cuh)
 // ---------------------------------------------------------------------------
-enum { DL_APP_BFS = 0, DL_APP_PR = 1 };
+enum { DL_APP_BFS = 0, DL_APP_PR = 1, DL_APP_CC = 2, DL_APP_SSSP = 3 };
 
 const tree_set *device_trees(gsw_ctx *ctx) {
   if (ctx->dtrees) return &ctx->dts;
-  const tree_node *h[9] = {select_dir_idem_tree,        select_dir_asso_tree,         select_dir_asso_backup_tree,
-                           select_fmt_tree,             select_fusion_tree,           select_lb_idem_tree,
-                           select_lb_asso_forward_tree, select_lb_asso_backward_tree, select_lb_asso_backward_backup_tree};
-  const int sz[9] = {select_dir_idem_tree_size,        select_dir_asso_tree_size,
-                     select_dir_asso_backup_tree_size, select_fmt_tree_size,
-                     select_fusion_tree_size,          select_lb_idem_tree_size,
-                     select_lb_asso_forward_tree_size, select_lb_asso_backward_tree_size,
-                     select_lb_asso_backward_backup_tree_size};
+  // the selector's nine trees, then the stepping tree of the window
+  const tree_node *h[10] = {select_dir_idem_tree,        select_dir_asso_tree,         select_dir_asso_backup_tree,
+                            select_fmt_tree,             select_fusion_tree,           select_lb_idem_tree,
+                            select_lb_asso_forward_tree, select_lb_asso_backward_tree, select_lb_asso_backward_backup_tree,
+                            select_stepping_tree};
+  const int sz[10] = {select_dir_idem_tree_size,        select_dir_asso_tree_size,
+                      select_dir_asso_backup_tree_size, select_fmt_tree_size,
+                      select_fusion_tree_size,          select_lb_idem_tree_size,
+                      select_lb_asso_forward_tree_size, select_lb_asso_backward_tree_size,
+                      select_lb_asso_backward_backup_tree_size, select_stepping_tree_size};
   int total = 0;
   for (int x : sz) total += x;
   if (total > DL_MAX_TREE_NODES) return fail(GSW_ERR_UNSUPPORTED, "selector trees exceed the in-stream copy"), nullptr;
   std::vector<tree_node> all;
   all.reserve(total);
-  for (int i = 0; i < 9; ++i) all.insert(all.end(), h[i], h[i] + sz[i]);
+  for (int i = 0; i < 10; ++i) all.insert(all.end(), h[i], h[i] + sz[i]);
   if (GSW_CUDA(cudaMalloc((void **)&ctx->dtrees, sizeof(tree_node) * total))) return nullptr;
   if (GSW_CUDA(cudaMemcpy(ctx->dtrees, all.data(), sizeof(tree_node) * total, cudaMemcpyHostToDevice))) return nullptr;
   ctx->ntree_nodes = total;
@@ -896,6 +852,7 @@ const tree_set *device_trees(gsw_ctx *ctx) {
     off += sz[i];
   }
   ctx->dts = tree_set{p[0], p[1], p[2], p[3], p[4], p[5], p[6], p[7], p[8]};
+  ctx->dstepping = ctx->dtrees + off;
   return &ctx->dts;
 }
 
@@ -927,9 +884,8 @@ struct dl_run {
 template <typename E, typename F>
 bool dl_prepare(dl_run &R, gsw_ctx *ctx, int app, dl_key key, active_set_t &as, device_graph_t<CSR, E> g, F &f,
                 const config_t &conf, const feature_t &fets, int max_iters, int iter_cap, int selector) {
-  if (conf.conf_qmode != Normal || conf.conf_window || conf.conf_compensation || fets.centric != VC)
-    return fail(GSW_ERR_UNSUPPORTED, "captured level loop: needs a Normal queue without window or compensation"),
-           false;
+  if (conf.conf_qmode != Normal || conf.conf_compensation || fets.centric != VC)
+    return fail(GSW_ERR_UNSUPPORTED, "captured level loop: needs a Normal queue without compensation"), false;
   const tree_set *trees = device_trees(ctx);
   R.ctx = ctx;
   R.d = (dloop_t *)ctx->buf("dl_state", sizeof(dloop_t));
@@ -947,11 +903,14 @@ bool dl_prepare(dl_run &R, gsw_ctx *ctx, int app, dl_key key, active_set_t &as, 
       << as.dg_cnt << as.workset.dg_eoff << as.workset.dg_bsum << as.workset.bsum_cap;
   key << conf.conf_pruning << conf.conf_count_edges << conf.conf_sorted_queue << fets.fromall << fets.toall
       << ex.dg_tile << ex.tile_cap << ex.twod.edge << opts().force_grid << ctx->stats.dg_runtime_info;
+  key << conf.conf_window << conf.conf_fusion << f.data.dg_ra;
   for (int q : ex.tune.quarters[0][0][0]) key << q;  // first row: cheap change detector
   {
     const int *flat = &ex.tune.quarters[0][0][0][0];
-    unsigned long long h = 1469598103934665603ull;  // FNV-1a over the whole table
+    const int *shp = &ex.tune.shapes[0][0][0][0];
+    unsigned long long h = 1469598103934665603ull;  // FNV-1a over both tables
     for (size_t i = 0; i < sizeof(ex.tune.quarters) / sizeof(int); ++i) h = (h ^ (unsigned)flat[i]) * 1099511628211ull;
+    for (size_t i = 0; i < sizeof(ex.tune.shapes) / sizeof(int); ++i) h = (h ^ (unsigned)shp[i]) * 1099511628211ull;
     key << h;
   }
   dloop_graph &L = ctx->dl[app];
@@ -990,6 +949,11 @@ bool dl_prepare(dl_run &R, gsw_ctx *ctx, int app, dl_key key, active_set_t &as, 
   im.nedges = g.nedges;
   im.as_size = as.size;
   im.launches = 0;
+  im.win = f.data.window;
+  im.window_on = conf.conf_window ? 1 : 0;
+  im.stepping = ctx->dstepping;
+  im.probe_flag = 0;
+  im.probe_armed = 0;
   return ok();
 }
 
@@ -1025,7 +989,6 @@ void dl_collect(dl_run &R, gsw_run_stats *st) {
       st->level_cfg[i] = cfg[i];
       st->level_frontier[i] = fr[i];
       st->level_edges[i] = ed[i];
-      st->level_bytes[i] = -1;
       st->level_ms[i] = 0;
       st->level_inspect_ms[i] = 0;
     }
@@ -1638,7 +1601,6 @@ gsw_status gsw_sssp(gsw_ctx *ctx, gsw_graph *gr, int32_t root, const gsw_run_opt
                     gsw_run_stats *st) {
   entry_guard eg(ctx);
   if (!ctx || !gr || root < 0 || root >= gr->n) return fail(GSW_ERR_INVALID_ARG, "gsw_sssp: bad arguments");
-  if (o && o->captured) return fail(GSW_ERR_UNSUPPORTED, "gsw_sssp: no captured level loop");
   if (!gr->weighted) return fail(GSW_ERR_INVALID_ARG, "gsw_sssp: graph has no weights");
   begin_stats(st);
   auto g = gr->view<int>();
@@ -1675,8 +1637,14 @@ gsw_status gsw_sssp(gsw_ctx *ctx, gsw_graph *gr, int32_t root, const gsw_run_opt
   as.reset();
   as.init(root);
   loop_trace tr{st, MAX_LEVELS};
+  const bool captured = o && o->captured;
+  dl_run R;
+  if (captured && !dl_prepare(R, ctx, DL_APP_SSSP, dl_key() << f.data.dg_wa, as, g, f, conf, fets, 0, MAX_LEVELS,
+                              o->selector))
+    return eg.finish();
   timer tm(ctx);
-  for (int level = 0; ok(); level++) {
+  if (captured) dl_launch(R);
+  for (int level = 0; !captured && ok(); level++) {
     inspector.inspect(as, g, f, stats, fets, conf);
     select_level(ctx, o, selector, stats, fets, conf);
     if (g_label) label_level(ctx, as, g, f, stats, fets, conf);
@@ -1688,6 +1656,7 @@ gsw_status gsw_sssp(gsw_ctx *ctx, gsw_graph *gr, int32_t root, const gsw_run_opt
     if (finish(as, g, f, conf)) break;
   }
   const double ms = tm.stop();
+  if (captured) dl_collect(R, st);
   tr.resolve();
   end_checks(&as, st);
   add_persistent_levels(st, executor, plv0, pln0);
@@ -1708,10 +1677,181 @@ __global__ void k_iota(int *p, int64_t n) {
     p[i] = (int)i;
 }
 
+// Captured CC: the edge-centric loop of application/cc.cu:82-108 as one CUDA
+// graph.  WHILE { inspection of the active edges (k_inspect_ec); one thread
+// reads the active count and stops, or picks the format the host loop picks
+// (queue below 80% active, else bitmap: selector.cuh:22-76 for EC);
+// SWITCH { queue: bitmap -> queue, hooking, pointer jumping | bitmap:
+// hooking, pointer jumping } }.  The first iteration's inspection finds every
+// edge active (labels start as vertex ids and no edge is a self-loop), which
+// is what the host loop assumes for its first level without inspecting; the
+// format rule is the host loop's (active edges over the vertex count, the
+// bitmap at the first level).
+struct cc_loop_t {
+  unsigned long long *info;  // the inspection's active-edge counter
+  long long nedges, nvertexs;
+  int iter, iter_cap, status;  // status: dl_status_t
+  int ntrace, trace_cap;
+  int *trace_cfg;
+  long long *trace_frontier;
+  long long launches, per_queue, per_bitmap, per_inspect;
+  cudaGraphConditionalHandle h_loop, h_body;
+};
+
+__global__ void k_cc_select(cc_loop_t *d) {
+  cc_loop_t &s = *d;
+  const unsigned long long a = *s.info;
+  *s.info = 0;  // the next inspection counts from zero
+  s.launches += s.per_inspect + 1;
+  if (a == 0 || s.iter >= s.iter_cap) {
+    s.status = a == 0 ? DL_DONE : DL_LEVEL_CAP;
+    cudaGraphSetConditional(s.h_loop, 0);
+    cudaGraphSetConditional(s.h_body, 2);  // no body
+    return;
+  }
+  // the host loop's rule: active edges over the vertex count (the reference's
+  // active_vertex_ratio of an edge-centric run), 1 at the first level
+  const double ratio = s.iter == 0 ? 1.0 : (double)a / (double)s.nvertexs;
+  const bool bitmap = ratio > 0.8;
+  cudaGraphSetConditional(s.h_body, bitmap ? 1 : 0);
+  s.launches += bitmap ? s.per_bitmap : s.per_queue;
+  if (s.ntrace < s.trace_cap) {
+    s.trace_cfg[s.ntrace] = (bitmap ? 1 : 0) << 1;
+    s.trace_frontier[s.ntrace] = (long long)a;
+  }
+  s.ntrace++;
+  s.iter++;
+}
+
+static bool cc_captured_run(gsw_ctx *ctx, device_graph_t<COO, Empty> g, app::CC f, active_set_t as, int iter_cap,
+                            gsw_run_stats *st, double *ms_out) {
+  executor_t &ex = ctx->executor;
+  cc_loop_t *d = (cc_loop_t *)ctx->buf("cc_loop", sizeof(cc_loop_t));
+  int *tcfg = (int *)ctx->buf("cc_trace_cfg", sizeof(int) * GSW_MAX_TRACE);
+  long long *tfr = (long long *)ctx->buf("cc_trace_fr", sizeof(long long) * GSW_MAX_TRACE);
+  unsigned long long *info = ctx->stats.dg_runtime_info;
+  if (!d || !tcfg || !tfr || !info) return false;
+  dl_key key;
+  key << DL_APP_CC << d << g.dg_coo << g.nedges << g.nvertexs << f.data.dg_wa << as.size << as.bitmap.active.dg_bits
+      << as.queue.subqueue[0].dg_queue << as.queue.subqueue[1].dg_queue << as.dg_cnt << as.workset.dg_bsum << info;
+  dloop_graph &L = ctx->dl[DL_APP_CC];
+  cc_loop_t im{};
+  if (L.key != key.v || !L.exec) {
+    L.destroy();
+    cudaGraph_t top = nullptr;
+    bool good = !GSW_CUDA(cudaGraphCreate(&top, 0));
+    L.graph = top;
+    cudaGraphConditionalHandle hl = 0, hb = 0;
+    std::vector<cudaGraph_t> wbody, bodies;
+    if (good) good = !GSW_CUDA(cudaGraphConditionalHandleCreate(&hl, top, 1, cudaGraphCondAssignDefault));
+    if (good) {
+      cudaGraphNodeParams p = {};
+      p.type = cudaGraphNodeTypeConditional;
+      p.conditional.handle = hl;
+      p.conditional.type = cudaGraphCondTypeWhile;
+      p.conditional.size = 1;
+      cudaGraphNode_t wn;
+      good = !GSW_CUDA(cudaGraphAddNode(&wn, top, nullptr, 0, &p));
+      if (good) wbody.assign(p.conditional.phGraph_out, p.conditional.phGraph_out + 1);
+    }
+    // queue form: the inspection's bitmap -> queue (into subqueue 1), then
+    // the expand reads subqueue 1; bitmap form: the expand reads the bitmap
+    active_set_t aq = as, ae = as, ab = as;
+    aq.fmt = Queue;
+    aq.queue.cursor = 0;
+    ae.fmt = Queue;
+    ae.queue.cursor = 1;
+    ab.fmt = Bitmap;
+    const long long launches0 = launch_count();
+    if (good) {
+      cudaGraph_t B = wbody[0];
+      good = !GSW_CUDA(cudaGraphConditionalHandleCreate(&hb, B, 2, 0));
+      if (good)
+        good = dl_capture(B, [&] {
+          k_inspect_ec<<<EC_INSPECT_CTAS, EC_INSPECT_THREADS, 0, stream()>>>(as, g, f, info);
+          k_cc_select<<<1, 1, 0, stream()>>>(d);
+          dl_add_conditional(stream(), hb, cudaGraphCondTypeSwitch, 2, bodies);
+        });
+      good = good && bodies.size() == 2;
+    }
+    if (good)
+      good = dl_capture(bodies[0], [&] {
+        ex.build_queue(aq, Active, true);
+        ex.launch_ec(ae, g, f);
+        p_jump(f, g.nvertexs, as);
+      });
+    if (good) {
+      im.per_queue = dl_count_nodes(bodies[0]);
+      good = dl_capture(bodies[1], [&] {
+        ex.launch_ec(ab, g, f);
+        p_jump(f, g.nvertexs, as);
+      });
+      im.per_bitmap = dl_count_nodes(bodies[1]);
+    }
+    launch_count() = launches0;
+    if (good) good = !GSW_CUDA(cudaGraphInstantiate(&L.exec, top, 0));
+    if (!good) {
+      L.destroy();
+      if (ok()) set_error(GSW_ERR_CUDA, "%s", "captured CC loop: graph construction failed");
+      return false;
+    }
+    im.h_loop = hl;
+    im.h_body = hb;
+    L.image.h_loop = hl;
+    L.image.h_expand = hb;
+    L.image.expand_kernels[0] = (int)im.per_queue;
+    L.image.expand_kernels[1] = (int)im.per_bitmap;
+    L.key = key.v;
+  } else {
+    im.h_loop = L.image.h_loop;
+    im.h_body = L.image.h_expand;
+    im.per_queue = L.image.expand_kernels[0];
+    im.per_bitmap = L.image.expand_kernels[1];
+  }
+  im.info = info;
+  im.nedges = g.nedges;
+  im.nvertexs = g.nvertexs;
+  im.iter_cap = iter_cap;
+  im.status = DL_RUNNING;
+  im.trace_cap = GSW_MAX_TRACE;
+  im.trace_cfg = tcfg;
+  im.trace_frontier = tfr;
+  im.per_inspect = 1;
+  GSW_CUDA(cudaMemsetAsync(info, 0, sizeof(unsigned long long), stream()));
+  timer tm(ctx);
+  GSW_CUDA(cudaMemcpyAsync(d, &im, sizeof(im), cudaMemcpyHostToDevice, stream()));
+  GSW_CUDA(cudaGraphLaunch(L.exec, stream()));
+  *ms_out = tm.stop();
+  cc_loop_t out;
+  if (GSW_CUDA(cudaMemcpyAsync(&out, d, sizeof(out), cudaMemcpyDeviceToHost, stream()))) return false;
+  if (GSW_CUDA(cudaStreamSynchronize(stream()))) return false;
+  launch_count() += out.launches;
+  if (out.status == DL_LEVEL_CAP) set_error(GSW_ERR_TIMEOUT, "%s", "level loop did not converge within the level cap");
+  else if (out.status != DL_DONE) set_error(GSW_ERR_CUDA, "%s", "captured CC loop did not finish");
+  if (st) {
+    st->levels = out.iter;
+    const int nt = std::min(out.ntrace, (int)GSW_MAX_TRACE);
+    st->ntrace = nt;
+    std::vector<int> cfg(nt);
+    std::vector<long long> fr(nt);
+    if (nt > 0) {
+      GSW_CUDA(cudaMemcpyAsync(cfg.data(), tcfg, sizeof(int) * nt, cudaMemcpyDeviceToHost, stream()));
+      GSW_CUDA(cudaMemcpyAsync(fr.data(), tfr, sizeof(long long) * nt, cudaMemcpyDeviceToHost, stream()));
+      GSW_CUDA(cudaStreamSynchronize(stream()));
+    }
+    for (int i = 0; i < nt; ++i) {
+      st->level_cfg[i] = cfg[i];
+      st->level_frontier[i] = fr[i];
+      st->level_ms[i] = st->level_inspect_ms[i] = 0;
+      st->level_edges[i] = -1;
+    }
+  }
+  return ok();
+}
+
 gsw_status gsw_cc(gsw_ctx *ctx, gsw_graph *gr, const gsw_run_opts *o, int32_t *labels, gsw_run_stats *st) {
   entry_guard eg(ctx);
   if (!ctx || !gr) return fail(GSW_ERR_INVALID_ARG, "gsw_cc: bad arguments");
-  if (o && o->captured) return fail(GSW_ERR_UNSUPPORTED, "gsw_cc: no captured level loop");
   begin_stats(st);
   if (ensure_coo(gr)) return eg.finish();
   device_graph_t<COO, Empty> g;
@@ -1745,6 +1885,19 @@ gsw_status gsw_cc(gsw_ctx *ctx, gsw_graph *gr, const gsw_run_opts *o, int32_t *l
   active_set_t &as = *asp;
   as.reset();
   as.init(ALL_ACTIVE);
+  if (o && o->captured) {
+    double ms = 0;
+    if (gr->ncoo > 0) cc_captured_run(ctx, g, f, as, MAX_LEVELS, st, &ms);
+    end_checks(&as, st);
+    if (st) {
+      st->ms = ms;
+      st->edges = gr->ncoo;
+    }
+    if (labels && ok())
+      GSW_CUDA(cudaMemcpyAsync(labels, f.data.dg_wa, sizeof(int) * gr->n, cudaMemcpyDeviceToHost, stream()));
+    GSW_CUDA(cudaStreamSynchronize(stream()));
+    return eg.finish();
+  }
   loop_trace tr{st, MAX_LEVELS};
   timer tm(ctx);
   for (int level = 0; ok() && gr->ncoo > 0; level++) {
@@ -2425,6 +2578,29 @@ gsw_status gsw_tune_load(gsw_ctx *ctx, const int32_t *quarters) {
     if (v < 0 || v > 64) return fail(GSW_ERR_INVALID_ARG, "gsw_tune_load: entries are 0..64 quarters");
     flat[i] = v;
   }
+  return GSW_OK;
+}
+
+gsw_status gsw_tune_load_shapes(gsw_ctx *ctx, const int32_t *shapes) {
+  entry_guard eg(ctx);
+  if (!ctx) return fail(GSW_ERR_INVALID_ARG, "gsw_tune_load_shapes: NULL context");
+  auto &t = ctx->executor.tune.shapes;
+  for (int pull = 0; pull < 2; ++pull)
+    for (int bm = 0; bm < 2; ++bm)
+      for (int lb = 0; lb < 8; ++lb)
+        for (int fu = 0; fu < 2; ++fu) {
+          const int i = ((pull * 2 + bm) * 8 + lb) * 2 + fu;
+          const int v = shapes ? shapes[i] : 0;
+          if (v < 0 || v >= shape_count(pull != 0, lb))
+            return fail(GSW_ERR_INVALID_ARG, "gsw_tune_load_shapes: shape out of range for its variant");
+        }
+  for (int i = 0; i < (int)(sizeof(t) / sizeof(int)); ++i) (&t[0][0][0][0])[i] = shapes ? shapes[i] : 0;
+  return GSW_OK;
+}
+
+gsw_status gsw_tune_save_shapes(gsw_ctx *ctx, int32_t *shapes) {
+  if (!ctx || !shapes) return fail(GSW_ERR_INVALID_ARG, "gsw_tune_save_shapes: bad arguments");
+  memcpy(shapes, &ctx->executor.tune.shapes[0][0][0][0], sizeof(ctx->executor.tune.shapes));
   return GSW_OK;
 }
 

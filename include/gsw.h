@@ -145,7 +145,7 @@ typedef struct gsw_run_opts {
                         others' wait (bounded to 20 ms) expires and the call
                         returns GSW_ERR_TIMEOUT */
   int captured;      /* 1: run the whole level loop as one CUDA graph with
-                        device-side selection and termination (BFS, PR;
+                        device-side selection and termination (BFS, SSSP, PR, CC;
                         GSW_ERR_UNSUPPORTED elsewhere); 0: host-driven loop */
   int hub_path;      /* how a CTA sweeps one hub's adjacency list (the
                         thread/warp/CTA-tiered push's CTA tier): 0 four-byte
@@ -173,12 +173,6 @@ typedef struct gsw_run_stats {
   float level_ms[GSW_MAX_TRACE];         /* expand time, with opts.timing */
   float level_inspect_ms[GSW_MAX_TRACE]; /* inspection time, with opts.timing */
   int64_t level_edges[GSW_MAX_TRACE];    /* edges touched, with opts.account */
-  int64_t level_bytes[GSW_MAX_TRACE];    /* with opts.account: algorithmic bytes
-                                            of the CSR side and the state writes
-                                            that the expand counted itself (the
-                                            thread-mapped pull, whose reads
-                                            depend on where each candidate
-                                            settles); -1: not counted */
 } gsw_run_stats;
 
 /* ---- applications ----------------------------------------------------------
@@ -293,6 +287,13 @@ gsw_status gsw_mlp_load_fusion(gsw_ctx *ctx, const float *model, float min_conf)
 #define GSW_TUNE_ENTRIES 64
 gsw_status gsw_tune_load(gsw_ctx *ctx, const int32_t *quarters); /* NULL: defaults */
 gsw_status gsw_tune_save(gsw_ctx *ctx, int32_t *quarters);
+/* Tuned shapes, same indexing (0 = default everywhere): the STRICT variants'
+ * tile (0: 1,024 slots, 1: 512, 2: 2,048; from-all pulls use at most 1,024)
+ * and the thread-mapped pull's candidates per thread (0: 2, 1: 1, 2: 4);
+ * every other variant takes 0 only.  The reference fixes these in THDNUM / SCRATH
+ * (src/utils/common.cuh:12-24); NULL restores the defaults. */
+gsw_status gsw_tune_load_shapes(gsw_ctx *ctx, const int32_t *shapes);
+gsw_status gsw_tune_save_shapes(gsw_ctx *ctx, int32_t *shapes);
 
 /* No counterpart in the reference.  BFS levels (-1 unreached) computed with
  * the edge-balanced push expand, for callers that cannot allocate device

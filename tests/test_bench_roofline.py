@@ -26,10 +26,6 @@ def test_level_bytes_push_and_pull():
     assert bench.level_bytes(("Push", "Queue", "TM", "Standalone"), n, A=10, U=0, D=7, E=100) == 40 + 160 + 425 + 28
     # pull, bitmap: n/8 B of status words + 16 B per candidate + 4.125 B per scanned edge + 4 B per discovery
     assert bench.level_bytes(("Pull", "Bitmap", "TM", "Standalone"), n, A=0, U=50, D=20, E=80) == 128 + 800 + 330 + 80
-    # a kernel that counted its CSR-side bytes and writes itself: status words
-    # and frontier-bit probes are added to its count
-    assert bench.level_bytes(("Pull", "Bitmap", "TM", "Standalone"), n, A=0, U=50, D=20, E=80,
-                             counted=500) == 128 + 500 + 10
 
 
 def test_roofline_dominant_kernel_traffic_and_others():

@@ -104,12 +104,74 @@ def test_captured_pagerank_fixpoint(ctx, graphs):
     assert st.levels > 1
 
 
+@pytest.mark.parametrize("name", golden_names())
+def test_captured_cc_goldens(ctx, name):
+    """Captured CC (edge-centric inspection, on-device stop and format
+    choice, hooking and pointer jumping in one graph): the reference's labels."""
+    d = load_golden(name)
+    g = ctx.upload(d["off"], d["col"])
+    lab, st = g.cc(cap())
+    assert np.array_equal(lab, d["cc"])
+    assert st.device_error == 0
+
+
+@pytest.mark.parametrize("name", ["rmat14", "grid64", "er20k"])
+def test_captured_cc_large(ctx, graphs, name):
+    h, _ = graphs[name]
+    g = ctx.upload(h.off, h.col)
+    ref = oracle.cc(h)
+    lab_h, st_h = g.cc()
+    # hooking races (atomicMin from many edges), so the number of rounds may
+    # differ from run to run; the labels may not
+    for _ in range(2):  # the second run reuses the cached graph
+        lab, st = g.cc(cap())
+        assert np.array_equal(lab, ref)
+        assert st.levels >= 1 and st.device_error == 0
+        assert st.trace[0][1] == "Bitmap"  # every edge active at the first level: the bitmap form
+    assert np.array_equal(lab_h, ref)
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_captured_sssp_goldens(ctx, name):
+    """Captured SSSP: the stepping window lives in device memory, the exit
+    probe runs inside the graph when a level finds no input, and the loop
+    restarts on the next window until no value lies outside it: the
+    reference's distances, standalone and fused levels."""
+    d = load_golden(name)
+    g = ctx.upload(d["off"], d["col"], d["w"])
+    for cfg in ["", "Push-Queue-WM-Standalone", "Push-Queue-WM-Fused", "Push-Queue-STRICT-Fused", "Pull-Bitmap-TM"]:
+        dist, st = g.sssp(int(d["root"]), cap(cfg))
+        assert np.array_equal(dist, d["dist"]), (name, cfg)
+        assert st.device_error == 0
+
+
+@pytest.mark.parametrize("name", ["rmat14", "grid64", "er20k"])
+def test_captured_sssp_large(ctx, graphs, name):
+    h, root = graphs[name]
+    hw = oracle.add_weights(h, 5, 1000 if name.startswith("grid") else 64)
+    g = ctx.upload(hw.off, hw.col, hw.w)
+    ref = oracle.sssp_dijkstra(hw, root)
+    from gswitch_b200.selector_train import load_fusion_model, load_model
+    model, conf = load_model()
+    ctx.mlp_load(model, conf)
+    fm, fc = load_fusion_model()
+    ctx.mlp_load_fusion(fm, fc)
+    try:
+        for o in (cap(), cap(selector="mlp"), cap("Push-Queue-TWC-Fused"), cap("Push-Bitmap-CM-Standalone")):
+            for _ in range(2):  # the second run reuses the cached graph
+                dist, st = g.sssp(root, o)
+                assert np.array_equal(dist, ref), (name, vars(o))
+                assert st.device_error == 0
+    finally:
+        ctx.mlp_load_fusion(None)
+        ctx.mlp_load(None)
+
+
 def test_captured_rejected_where_unsupported(ctx, graphs):
     h, root = graphs["er20k"]
-    hw = oracle.add_weights(h, 5, 64)
-    g = ctx.upload(hw.off, hw.col, hw.w)
+    g = ctx.upload(h.off, h.col)
     with pytest.raises(gs.GswError) as e:
-        g.sssp(root, cap())
+        g.bc(root, cap())
     assert gs.STATUS[e.value.code] == "UNSUPPORTED"
 
 

@@ -30,7 +30,7 @@ import pytest
 
 import gswitch_b200 as gs
 import oracle
-from gswitch_b200.autotune import load_table
+from gswitch_b200.autotune import load_into
 from gswitch_b200.selector_train import load_fusion_model, load_model
 from test_gpu_apps import ALL_VARIANTS
 
@@ -50,10 +50,10 @@ def report(**kw):
 
 @pytest.fixture(scope="module")
 def bctx():
-    """A context set up as the bench sets it up: tuned grids, the learned
+    """A context set up as the bench sets it up: tuned grids and shapes, the learned
     selector and the fusion network loaded."""
     c = gs.Context(0)
-    c.tune_load(load_table())
+    load_into(c)
     model, conf = load_model()
     if model is not None:
         c.mlp_load(model, conf)

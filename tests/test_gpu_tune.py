@@ -49,3 +49,53 @@ def test_committed_table_is_well_formed():
     t = load_table()
     assert t is not None and t.shape == (gs.TUNE_ENTRIES,)
     assert np.all((t >= 0) & (t <= 64))
+
+
+def test_shape_table_round_trip_and_validation(ctx):
+    """Shapes exist only for the STRICT variants (3 tiles) and the thread-mapped
+    pull (3 candidates-per-thread counts); anything else is rejected."""
+    s = np.zeros(gs.TUNE_ENTRIES, dtype=np.int32)
+    s[gs.Context.tune_index("Push", "Queue", "STRICT")] = 2
+    s[gs.Context.tune_index("Pull", "Bitmap", "TM")] = 2
+    ctx.tune_load_shapes(s)
+    assert np.array_equal(ctx.tune_save_shapes(), s)
+    for bad in ((gs.Context.tune_index("Push", "Queue", "WM"), 1), (gs.Context.tune_index("Pull", "Bitmap", "STRICT"), 3),
+                (gs.Context.tune_index("Pull", "Bitmap", "TM"), 3)):
+        b = s.copy()
+        b[bad[0]] = bad[1]
+        with pytest.raises(gs.GswError):
+            ctx.tune_load_shapes(b)
+    ctx.tune_load_shapes(None)
+    assert not ctx.tune_save_shapes().any()
+
+
+@pytest.mark.parametrize("shape", [1, 2])
+def test_results_exact_under_every_shape(ctx, shape):
+    """Every STRICT tile and every pull candidates-per-thread count gives the
+    oracle's BFS, SSSP and PageRank."""
+    h = oracle.rmat(14, 16, seed=7)
+    hw = oracle.add_weights(h, 3, 64)
+    root = int(oracle.roots(h, 4, 1)[0])
+    g = ctx.upload(hw.off, hw.col, hw.w)
+    gu = ctx.upload(h.off, h.col)
+    s = np.zeros(gs.TUNE_ENTRIES, dtype=np.int32)
+    for d in ("Push", "Pull"):
+        for f in ("Queue", "Bitmap"):
+            for fused in ((False, True) if d == "Push" else (False,)):
+                s[gs.Context.tune_index(d, f, "STRICT", fused)] = shape
+            s[gs.Context.tune_index("Pull", f, "TM")] = shape
+    ctx.tune_load_shapes(s)
+    try:
+        ref, dref = oracle.bfs(h, root), oracle.sssp_dijkstra(hw, root)
+        for cfg in ["Push-Queue-STRICT", "Pull-Bitmap-STRICT", "Push-Queue-STRICT-Fused", "Pull-Bitmap-TM",
+                    "Pull-Queue-TM", ""]:
+            lv, _ = gu.bfs(root, gs.RunOpts.from_config(cfg, persistent=False))
+            assert np.array_equal(lv, ref), (shape, cfg)
+            d, _ = g.sssp(root, gs.RunOpts.from_config(cfg, persistent=False))
+            assert np.array_equal(d, dref), (shape, cfg)
+        from test_gpu_apps import _pr_l1
+        for cfg in ["Pull-Bitmap-STRICT", "Pull-Bitmap-TM"]:
+            pr, _ = gu.pagerank(iters=20, eps=0.0, opts=cfg)
+            assert _pr_l1(pr, h)[0] <= 1e-6, (shape, cfg)
+    finally:
+        ctx.tune_load_shapes(None)
