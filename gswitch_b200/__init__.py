@@ -40,6 +40,7 @@ ABI_SYMBOLS = (
     "gsw_graph_generate_powerlaw", "gsw_label_levels", "gsw_mlp_train", "gsw_mlp_grad", "gsw_mlp_infer",
     "gsw_mlp_load", "gsw_graph_generate_er_batch", "gsw_bfs_multi", "gsw_bfs_inspect", "gsw_tune_load",
     "gsw_tune_save", "gsw_tune_load_shapes", "gsw_tune_save_shapes", "gsw_mlp_load_fusion", "gsw_pagerank_delta",
+    "gsw_mlp_save", "gsw_select",
 )
 TUNE_ENTRIES = 64
 
@@ -132,6 +133,8 @@ def lib():
     L.gsw_bfs_inspect.argtypes = [vp, vp, vp, i32, vp]
     L.gsw_tune_load.argtypes = [vp, vp]
     L.gsw_tune_load_shapes.argtypes = [vp, vp]
+    L.gsw_mlp_save.argtypes = [vp, vp, vp]
+    L.gsw_select.argtypes = [vp, vp, C.c_int, vp]
     L.gsw_tune_save_shapes.argtypes = [vp, vp]
     L.gsw_mlp_load_fusion.argtypes = [vp, vp, C.c_float]
     L.gsw_tune_save.argtypes = [vp, vp]
@@ -150,6 +153,19 @@ def _ptr(a):
 
 # how a CTA sweeps one hub's adjacency list (gsw_run_opts.hub_path)
 HUB_SCALAR, HUB_VECTOR, HUB_STAGED = 0, 1, 2
+
+
+class LevelStats(C.Structure):
+    """gsw_level_stats: one level's inspection counters and the graph's degree
+    statistics, the input of Context.select()."""
+    _fields_ = [("nvertexs", C.c_int64), ("nedges", C.c_int64), ("attr", C.c_double * 6), ("active", C.c_int64),
+                ("inactive", C.c_int64), ("push_workload", C.c_int64), ("pull_workload", C.c_int64),
+                ("max_push", C.c_int64), ("max_pull", C.c_int64), ("pattern", C.c_int), ("fromall", C.c_int),
+                ("toall", C.c_int), ("level", C.c_int), ("first_level", C.c_int), ("root_degree", C.c_int64)]
+
+
+class LevelChoice(C.Structure):
+    _fields_ = [("direction", C.c_int), ("asfmt", C.c_int), ("lb", C.c_int), ("done", C.c_int)]
 
 
 class RunOpts:
@@ -363,6 +379,22 @@ class Context:
     def mlp_load_fusion(self, model=None, min_conf=0.0):
         m = None if model is None else np.ascontiguousarray(model, dtype=np.float32)
         _check(lib().gsw_mlp_load_fusion(self._h, _ptr(m), min_conf))
+
+    def mlp_save(self):
+        """The loaded model and its min_conf."""
+        m = np.zeros(MLP_MODEL_FLOATS, dtype=np.float32)
+        c = C.c_float(0.0)
+        _check(lib().gsw_mlp_save(self._h, _ptr(m), C.byref(c)))
+        return m, c.value
+
+    def select(self, stats: "LevelStats", selector="rules"):
+        """One level's standalone variant ("Push"|"Pull", "Queue"|"Bitmap", LB
+        name) and whether the counters end the run (gsw_select)."""
+        out = LevelChoice()
+        _check(lib().gsw_select(self._h, C.byref(stats), SELECT_MLP if selector == "mlp" else SELECT_RULES,
+                                C.byref(out)))
+        return (("Pull" if out.direction == PULL else "Push"), ("Bitmap" if out.asfmt == BITMAP else "Queue"),
+                LB_NAMES.get(out.lb, "?")), bool(out.done)
 
     def mlp_load(self, model=None, min_conf=0.0):
         m = None if model is None else np.ascontiguousarray(model, dtype=np.float32)

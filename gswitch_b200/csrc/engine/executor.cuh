@@ -502,6 +502,8 @@ inline int shape_count(bool pull, int lb) {
 // ===========================================================================
 struct executor_t {
   int *dg_tile = nullptr;  // STRICT tile owners
+  hub_piece_t *dg_hubs = nullptr;  // tiered push: hub pieces of the level
+  int64_t hub_cap = 0;
   // Autotuned expand grids: for (pull, bitmap, load balance, fused) the grid
   // cap in quarters of the kernel's resident grid (0: the resident grid).
   struct tune_t {
@@ -524,6 +526,9 @@ struct executor_t {
     cudaFree(dg_tile);
     dg_tile = nullptr;
     tile_cap = 0;
+    cudaFree(dg_hubs);
+    dg_hubs = nullptr;
+    hub_cap = 0;
     for (auto &e : ev)
       if (e) {
         cudaEventDestroy(e);
@@ -606,6 +611,17 @@ struct executor_t {
   template <typename E, typename F>
   void compensation(active_set_t &, device_graph_t<COO, E> &, F &) {}
 
+  // room for every hub piece a level can list: at most one piece per
+  // EXPAND_THREADS arcs plus one per TWC_HUB_PIECE arcs
+  void ensure_hubs(int64_t arcs) {
+    const int64_t need = arcs / EXPAND_THREADS + arcs / TWC_HUB_PIECE + 2;
+    if (need <= hub_cap) return;
+    cudaFree(dg_hubs);
+    dg_hubs = nullptr;
+    if (GSW_CUDA(cudaMalloc((void **)&dg_hubs, sizeof(hub_piece_t) * need))) return;
+    hub_cap = need;
+  }
+
   // the table is sized for the smallest tile any shape uses
   void ensure_tiles(int64_t slots_cap) {
     const int64_t need = slots_cap / STRICT_TILE_MIN + 2;
@@ -623,9 +639,15 @@ struct executor_t {
     ensure_tiles(g.nedges + as.size + 1);
     if (!ok()) return;
     if (nb + 1 > as.workset.bsum_cap) return (void)set_error(GSW_ERR_OVERFLOW, "strict: %s", "block sums");
-    k_strict_count<PULL><<<(unsigned)nb, 256, 0, stream()>>>(as, g, want, as.workset.dg_bsum);
-    k_scan_single_block<<<1, 1024, 0, stream()>>>(as.workset.dg_bsum, nb);
-    k_strict_scan<PULL, T><<<(unsigned)nb, 256, 0, stream()>>>(as, g, want, as.workset.dg_bsum, nb, dg_tile, tile_cap);
+    if (nb == 1 && hints().frontier >= 0) {
+      // a frontier known to fit one scan block: one launch, no block sums
+      k_strict_scan<PULL, T><<<1, 256, 0, stream()>>>(as, g, want, nullptr, 1, dg_tile, tile_cap);
+    } else {
+      k_strict_count<PULL><<<(unsigned)nb, 256, 0, stream()>>>(as, g, want, as.workset.dg_bsum);
+      k_scan_single_block<<<1, 1024, 0, stream()>>>(as.workset.dg_bsum, nb);
+      k_strict_scan<PULL, T><<<(unsigned)nb, 256, 0, stream()>>>(as, g, want, as.workset.dg_bsum, nb, dg_tile,
+                                                                tile_cap);
+    }
     GSW_LAUNCHED();
   }
 
@@ -669,10 +691,20 @@ struct executor_t {
           if (fused) GSW_GO((k_push_cm<true, G, F>), fr < 0 ? -1 : fr / B + 1, as, g, f, conf);
           else GSW_GO((k_push_cm<false, G, F>), fr < 0 ? -1 : fr / B + 1, as, g, f, conf);
           break;
-        case TWC:
-          if (fused) GSW_GO((k_push_twc<true, G, F>), fr < 0 ? -1 : fr / B + 1, as, g, f, conf);
-          else GSW_GO((k_push_twc<false, G, F>), fr < 0 ? -1 : fr / B + 1, as, g, f, conf);
+        case TWC: {
+          // tiles, then the hub pieces they listed (one piece per CTA)
+          ensure_hubs(g.nedges);
+          if (!ok()) return;
+          const hub_list_t hl{dg_hubs, &as.dg_cnt->hub_pieces, &as.dg_cnt->hub_done, hub_cap};
+          if (fused) {
+            GSW_GO((k_push_twc<true, G, F>), fr < 0 ? -1 : fr / B + 1, as, g, f, conf, hl);
+            GSW_GO((k_push_twc_hubs<true, G, F>), -1, as, g, f, conf, hl);
+          } else {
+            GSW_GO((k_push_twc<false, G, F>), fr < 0 ? -1 : fr / B + 1, as, g, f, conf, hl);
+            GSW_GO((k_push_twc_hubs<false, G, F>), -1, as, g, f, conf, hl);
+          }
           break;
+        }
         case STRICT: {
           auto go = [&](auto tile) {
             constexpr int T = decltype(tile)::value;

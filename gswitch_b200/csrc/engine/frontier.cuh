@@ -53,6 +53,8 @@ struct as_counters_t {
   int preason;                     // persistent fused levels: exit reason
   int plb;                         // persistent fused levels: the load
                                    // balance the launched kernel ran
+  int hub_pieces;                  // tiered push: pieces in the hub list
+  unsigned hub_done;               // tiered push: hub-kernel CTAs that read it
 };
 
 struct bits_t {

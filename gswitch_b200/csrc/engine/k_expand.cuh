@@ -591,14 +591,17 @@ __global__ void __launch_bounds__(256) k_strict_scan(active_set_t as, G g, Statu
     int64_t y = lane_id() < (int)(blockDim.x >> 5) ? s[lane_id()] : 0;
     int64_t yi = warp_inclusive_sum(y);
     if (lane_id() < (int)(blockDim.x >> 5)) s[lane_id()] = yi - y;
+    if (lane_id() == 31) s[32] = yi;  // the block's total
   }
   __syncthreads();
-  const int64_t off = bsum[blockIdx.x] + s[warp_id()] + incl - loc;
+  // bsum == nullptr: the whole frontier is this one block (no block sums)
+  const int64_t off = (bsum ? bsum[blockIdx.x] : 0) + s[warp_id()] + incl - loc;
   int64_t *eoff = as.workset.dg_eoff;
   strict_scan_epilogue<T>(as, base, n, d, off, eoff, tile_lo, tile_cap);
   if (blockIdx.x == 0 && threadIdx.x == 0) {
-    eoff[n] = bsum[nblocks];
-    as.dg_cnt->total_edges = (unsigned long long)bsum[nblocks];
+    const int64_t total = bsum ? bsum[nblocks] : s[32];
+    eoff[n] = total;
+    as.dg_cnt->total_edges = (unsigned long long)total;
   }
 }
 
@@ -942,9 +945,30 @@ __device__ __forceinline__ bool hub_run(const int *col, int64_t a, int64_t len, 
 // ===========================================================================
 // TWC: thread / warp / CTA tiers by degree
 // ===========================================================================
+// Per-launch tiered pushes do not sweep their hubs in the tile that found
+// them: a level whose frontier is a few hubs would run on one CTA (its grid is
+// sized by frontier vertices).  Each hub is cut into pieces of at most
+// TWC_HUB_PIECE columns appended to a hub list, and a second kernel sweeps one
+// piece per CTA with the hub path's loads.  Persistent launches keep the
+// in-tile sweep (the list would need one more grid barrier per level), and so
+// does a hub that finds the list full (a fused queue may hold a vertex more
+// than once).  The hub kernel's last CTA to read the count sets it back to 0
+// for the next level, so no memset node sits in captured loops.
+constexpr int TWC_HUB_PIECE = 8192;
+struct hub_piece_t {
+  int v;
+  int len;
+  int64_t st;
+};
+struct hub_list_t {
+  hub_piece_t *piece = nullptr;  // null: sweep hubs in their tile
+  int *count = nullptr;
+  unsigned *done = nullptr;
+  int64_t cap = 0;
+};
 template <bool FUSED, typename G, typename F, typename Src>
 __device__ __forceinline__ void push_twc_body(active_set_t &as, const G &g, F &f, const config_t &conf, const Src &src,
-                                              int64_t n, warp_stage_t &stage) {
+                                              int64_t n, warp_stage_t &stage, hub_list_t hubs = hub_list_t()) {
   constexpr int B = EXPAND_THREADS;
   __shared__ int s_owner;
   __shared__ int s_cv;
@@ -980,6 +1004,21 @@ __device__ __forceinline__ void push_twc_body(active_set_t &as, const G &g, F &f
     int64_t st;
     int deg;
     vertex_range(g, false, v, st, deg);
+    if (hubs.piece && deg >= B) {
+      // hub: into the list, in pieces, for the hub kernel; if it does not fit
+      // whole, its slots below the cap get empty pieces and the tile sweeps it
+      const int np = (deg + TWC_HUB_PIECE - 1) / TWC_HUB_PIECE;
+      const int at = atomicAdd(hubs.count, np);
+      const bool fits = (int64_t)at + np <= hubs.cap;
+      for (int k = 0; k < np && (int64_t)at + k < hubs.cap; ++k)
+        hubs.piece[at + k] = fits ? hub_piece_t{v, MIN(TWC_HUB_PIECE, deg - k * TWC_HUB_PIECE),
+                                                st + (int64_t)k * TWC_HUB_PIECE}
+                                  : hub_piece_t{v, 0, 0};
+      if (fits) {
+        account(as, conf, (unsigned long long)deg);
+        deg = 0;
+      }
+    }
     // CTA tier
     for (;;) {
       if (deg >= B) s_owner = threadIdx.x;
@@ -1072,12 +1111,67 @@ __device__ __forceinline__ void push_twc_body(active_set_t &as, const G &g, F &f
 }
 
 template <bool FUSED, typename G, typename F>
-__global__ void __launch_bounds__(EXPAND_THREADS) k_push_twc(active_set_t as, G g, F f, config_t conf) {
+__global__ void __launch_bounds__(EXPAND_THREADS) k_push_twc(active_set_t as, G g, F f, config_t conf,
+                                                             hub_list_t hubs) {
   __shared__ int s_stage[FUSED ? EXPAND_THREADS / 32 : 1][FUSED ? STAGE_SLOTS : 1];
   const int64_t n = as.get_size();
   GSW_HALT_IF_EMPTY(n);
   warp_stage_t stage(s_stage[FUSED ? warp_id() : 0], as);
-  push_twc_body<FUSED>(as, g, f, conf, as_src_t{&as, conf.want()}, n, stage);
+  push_twc_body<FUSED>(as, g, f, conf, as_src_t{&as, conf.want()}, n, stage, hubs);
+  if (FUSED) stage.flush();
+}
+
+// the hub pieces the tiered push listed: one piece per CTA at a time
+template <bool FUSED, typename G, typename F>
+__global__ void __launch_bounds__(EXPAND_THREADS) k_push_twc_hubs(active_set_t as, G g, F f, config_t conf,
+                                                                  hub_list_t hubs) {
+  constexpr int B = EXPAND_THREADS;
+  __shared__ int s_stage[FUSED ? B / 32 : 1][FUSED ? STAGE_SLOTS : 1];
+  __shared__ __align__(16) int s_hub[2][HUB_CHUNK];
+  __shared__ __align__(8) unsigned long long s_bar[2];
+  __shared__ int s_np;
+  if (threadIdx.x == 0) {
+    s_np = (int)MIN((int64_t)*(volatile int *)hubs.count, hubs.cap);
+    __threadfence();
+    if (atomicAdd(hubs.done, 1u) == gridDim.x - 1) {  // every CTA has read the count
+      *hubs.count = 0;
+      *hubs.done = 0;
+    }
+  }
+  __syncthreads();
+  const int np = s_np;
+  if ((int)blockIdx.x >= np) return;  // no piece for this CTA (uniform)
+  const int hub_path = conf.conf_hub_path >= 0 ? conf.conf_hub_path
+                                               : (std::is_same<typename G::edge_t, Empty>::value ? HUB_STAGED
+                                                                                                 : HUB_VECTOR);
+  warp_stage_t stage(s_stage[FUSED ? warp_id() : 0], as);
+  hub_stage_t hs{s_hub, s_bar};
+  if (threadIdx.x == 0 && hub_path == HUB_STAGED) {
+    mbar_init(&s_bar[0], 1);
+    mbar_init(&s_bar[1], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  bool okk = true;
+  for (int p = blockIdx.x; okk && p < np; p += gridDim.x) {
+    const hub_piece_t pc = hubs.piece[p];
+    okk = hub_run<B>(g.dg_adj_list, pc.st, pc.len, hub_path, hs, &as.dg_cnt->err, [&](bool valid, int u, int64_t ei) {
+      bool tp = false;
+      if (valid) {
+        if (FUSED)
+          tp = push_edge_fused(as, g, f, conf, pc.v, u, ei);
+        else
+          push_edge_std(as, g, f, conf, pc.v, u, ei);
+      }
+      if (FUSED) stage.push(tp, u);
+    });
+    __syncthreads();
+  }
+  if (!okk) return;  // a staging copy timed out (recorded in the error word)
+  if (hub_path == HUB_STAGED && threadIdx.x == 0) {
+    mbar_inval(&s_bar[0]);
+    mbar_inval(&s_bar[1]);
+  }
   if (FUSED) stage.flush();
 }
 

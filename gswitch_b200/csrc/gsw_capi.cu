@@ -2621,6 +2621,66 @@ gsw_status gsw_mlp_load_fusion(gsw_ctx *ctx, const float *model, float min_conf)
   return GSW_OK;
 }
 
+gsw_status gsw_mlp_save(gsw_ctx *ctx, float *model, float *min_conf) {
+  entry_guard eg(ctx);
+  if (!ctx || !model) return fail(GSW_ERR_INVALID_ARG, "gsw_mlp_save: bad arguments");
+  if (!ctx->mlp.valid) return fail(GSW_ERR_INVALID_ARG, "gsw_mlp_save: no model loaded");
+  memcpy(model, &ctx->mlp, sizeof(float) * GSW_MLP_MODEL_FLOATS);
+  if (min_conf) *min_conf = ctx->mlp.min_conf;
+  return GSW_OK;
+}
+
+gsw_status gsw_select(gsw_ctx *ctx, const gsw_level_stats *in, int sel_kind, gsw_level_choice *out) {
+  entry_guard eg(ctx);
+  if (!ctx || !in || !out || in->nvertexs <= 0 || in->pattern < 0 || in->pattern > 2)
+    return fail(GSW_ERR_INVALID_ARG, "gsw_select: bad arguments");
+  feature_t fets;
+  config_t conf;
+  fets.centric = VC;
+  fets.pattern = in->pattern == 0 ? Idem : (in->pattern == 1 ? Mono : ASSO);
+  fets.fromall = in->fromall != 0;
+  fets.toall = in->toall != 0;
+  fets.nvertexs = in->nvertexs;
+  fets.nedges = in->nedges;
+  fets.avg_deg = in->attr[0];
+  fets.std_deg = in->attr[1];
+  fets.range = in->attr[2];
+  fets.max_deg = in->attr[3];
+  fets.GI = in->attr[4];
+  fets.Her = in->attr[5];
+  fets.architecture_features();
+  conf.conf_pruning = fets.pattern == Idem;
+  conf.conf_fromall = fets.fromall;
+  conf.conf_toall = fets.toall;
+  conf.conf_fusion = false;
+  conf.conf_fuse_inspect = false;
+  conf.force.has_fusion = true;  // fusion stays with the caller's loop
+  conf.force.fusion = Standalone;
+  fets_level_init(fets, in->level, in->nvertexs, in->nedges);
+  bool done = false;
+  if (in->first_level) {
+    fets.use_root = 0;
+    fets.first_active = (double)std::max<int64_t>(in->active, 1);
+    fets.first_workload = (double)in->root_degree;
+    fets_first(fets, in->nvertexs, in->nedges);
+  } else {
+    const level_counts c = {in->active, in->inactive, in->push_workload, in->pull_workload, in->max_push, in->max_pull};
+    done = fets_from_counts(fets, c, in->nvertexs, in->nedges);
+  }
+  fets.flatten();
+  out->done = done ? 1 : 0;
+  // the host loop's order: the trees, the network, then the filter step's
+  // grid bookkeeping (a tiny STRICT level goes to CM)
+  selector_t selector;
+  selector.decide(fets, conf);
+  if (sel_kind == GSW_SELECT_MLP && ctx->mlp.valid) mlp_override(ctx->mlp, fets, conf);
+  level_grid_bookkeeping(fets, conf);
+  out->direction = conf.conf_dir == Pull ? GSW_PULL : GSW_PUSH;
+  out->asfmt = conf.conf_asfmt == Bitmap ? GSW_BITMAP : GSW_QUEUE;
+  out->lb = (int)conf.conf_lb;
+  return eg.finish();
+}
+
 gsw_status gsw_mlp_load(gsw_ctx *ctx, const float *model, float min_conf) {
   entry_guard eg(ctx);
   if (!ctx) return fail(GSW_ERR_INVALID_ARG, "gsw_mlp_load: NULL context");

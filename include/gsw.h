@@ -272,6 +272,36 @@ gsw_status gsw_mlp_infer(gsw_ctx *ctx, const float *model, const float *features
  * opts.selector = GSW_SELECT_MLP; below min_conf top-class probability the
  * rules decide. */
 gsw_status gsw_mlp_load(gsw_ctx *ctx, const float *model, float min_conf);
+/* The loaded model (GSW_MLP_MODEL_FLOATS floats) and its min_conf;
+ * GSW_ERR_INVALID_ARG when none is loaded. */
+gsw_status gsw_mlp_save(gsw_ctx *ctx, float *model, float *min_conf);
+
+/* ---- one level's decision, for callers that drive their own level loop ----
+ * Replaces inspector_t::set_fets + selector_t::select of one level
+ * (src/abstraction/inspector.cuh:206-241, selector.cuh:22-303): from the
+ * graph's degree statistics (graph_attr_t::fill, src/utils/fileIO.cuh:35-67,
+ * as gsw_graph_attr returns them) and the inspection's six counters of the
+ * level, the features are built and flattened as the host loop builds them,
+ * the reference's trees pick the standalone variant, and with
+ * GSW_SELECT_MLP the loaded network may override them.  Fusion, the idle
+ * count and the wall-clock rule depend on the run's history and stay with
+ * the caller's loop (the choice is always standalone).  first_level = 1
+ * uses the first level's known counters (one root: its degree) instead. */
+typedef struct gsw_level_stats {
+  int64_t nvertexs, nedges;
+  double attr[6];              /* average degree, deviation, range, max degree, Gini, Hoover */
+  int64_t active, inactive;    /* the six counters of the level's inspection */
+  int64_t push_workload, pull_workload, max_push, max_pull;
+  int pattern;                 /* 0 idempotent (BFS), 1 monotone (SSSP), 2 associative (PR, BC) */
+  int fromall, toall;          /* the functor's from-all / to-all flags */
+  int level, first_level;      /* level number; 1: the run's first level (root_degree holds its workload) */
+  int64_t root_degree;
+} gsw_level_stats;
+typedef struct gsw_level_choice {
+  int direction, asfmt, lb;    /* GSW_PUSH / GSW_PULL, GSW_QUEUE / GSW_BITMAP, GSW_LB_* */
+  int done;                    /* 1: the counters end the run (no active vertex) */
+} gsw_level_choice;
+gsw_status gsw_select(gsw_ctx *ctx, const gsw_level_stats *in, int selector, gsw_level_choice *out);
 /* The second network: whether a Mono-pattern run (SSSP) runs fused or
  * standalone levels, from graph features (avg, std and range of degree, Gini,
  * entropy, log n, log m, pattern); class 0 standalone, 1 fused.  Used with

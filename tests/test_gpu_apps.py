@@ -375,6 +375,56 @@ def test_hub_paths_of_the_tiered_push(ctx, big, hub_path):
         gw.close()
 
 
+def hub_frontier_graph():
+    """Vertex 0 joined to six hubs whose lists hold 256 (the smallest hub),
+    8,191, 8,192, 8,193, 30,001 and 70,000 leaves (pieces of 8,192 columns
+    with ragged ends, lists at every alignment); the hubs share some leaves
+    and a chain hangs off the last leaf, so level 2 is the six hubs alone."""
+    degs = [256, 8191, 8192, 8193, 30001, 70000]
+    src, dst, nxt = [], [], 7
+    for i, d in enumerate(degs, start=1):
+        src.append(0)
+        dst.append(i)
+        leaves = np.arange(nxt, nxt + d)
+        src += [i] * d
+        dst += list(leaves)
+        nxt += d // 2  # half of each list is shared with the next hub
+    n = int(leaves[-1]) + 41
+    chain = np.arange(int(leaves[-1]), n - 1)
+    src += list(chain)
+    dst += list(chain + 1)
+    return oracle.csr_from_pairs(n, np.array(src), np.array(dst))
+
+
+@pytest.mark.parametrize("hub_path", [gs.HUB_SCALAR, gs.HUB_VECTOR, gs.HUB_STAGED])
+def test_tiered_push_hub_list_spreads_a_hub_frontier(ctx, hub_path):
+    """A per-launch tiered push lists the frontier's hubs in pieces of at most
+    8,192 columns and a second kernel sweeps one piece per CTA: on a level
+    that is six hubs, BFS and SSSP stay exact, every edge is counted once,
+    and the persistent form (hubs swept in their tile) agrees."""
+    h = hub_frontier_graph()
+    hw = oracle.add_weights(h, 3, 64)
+    ref, dref = oracle.bfs(h, 0), oracle.sssp_dijkstra(hw, 0)
+    per_level = [int(x) for x in np.bincount(ref[ref >= 0], weights=h.degrees()[ref >= 0])]
+    g, gw = ctx.upload(h.off, h.col), ctx.upload(hw.off, hw.col, hw.w)
+    for cfg, persistent in (("Push-Queue-TWC-Standalone", None), ("Push-Queue-TWC-Fused", False),
+                            ("Push-Queue-TWC-Fused", True), ("Push-Bitmap-TWC-Standalone", None)):
+        o = gs.RunOpts.from_config(cfg, persistent=persistent, hub_path=hub_path, account=True)
+        for _ in range(2):  # the list's count is back at 0 for the next run
+            lv, st = g.bfs(0, o)
+            assert np.array_equal(lv, ref), (cfg, persistent)
+            assert st.device_error == 0
+            if cfg == "Push-Queue-TWC-Standalone":  # the queue's size (fused levels do not count it)
+                assert st.trace[1][-1] == 6  # level 2: the hubs
+            if persistent is not True:  # the hubs' level and the next: every arc examined once
+                assert st.level_edges[1:3] == per_level[1:3], (cfg, persistent, st.level_edges[:3])
+        d, st = gw.sssp(0, o)
+        assert np.array_equal(d, dref), (cfg, persistent)
+        assert st.device_error == 0
+    g.close()
+    gw.close()
+
+
 @pytest.mark.parametrize("name,nsrc", [("rmat14", 1), ("rmat14", 32), ("rmat14", 45), ("grid64", 40), ("er20k", 33)])
 def test_bc_batch_every_source(ctx, big, name, nsrc):
     """Batched BC (bit-sliced levels, then per-level forward / backward passes
@@ -421,3 +471,43 @@ def test_batched_sources_persistent_and_per_level(ctx, big, persistent):
     for i, r in enumerate(roots[:40]):
         _bc_check(nsp[i], dep[i], h, int(r))
     g.close()
+
+
+@pytest.mark.parametrize("selector", ["rules", "mlp"])
+def test_select_entry_point_reproduces_the_loop_choices(ctx, big, selector):
+    """gsw_select, given one level's inspection counters and the graph's
+    degree statistics, picks the standalone variant the BFS loop itself
+    picked at that level (standalone levels forced, so no fusion history)."""
+    from gswitch_b200.selector_train import load_model
+
+    if selector == "mlp":
+        model, conf = load_model()
+        ctx.mlp_load(model, conf)
+        saved, c2 = ctx.mlp_save()
+        assert np.array_equal(saved, model) and c2 == pytest.approx(conf)
+    try:
+        for name in ("rmat14", "grid64", "er20k"):
+            h, _, root = big[name]
+            g = ctx.upload(h.off, h.col)
+            lv = oracle.bfs(h, root)
+            _, st = g.bfs(root, gs.RunOpts(fusion=gs.STANDALONE, selector=selector))
+            attr = g.attr()
+            for i, t in enumerate(st.trace):
+                s = gs.LevelStats()
+                s.nvertexs, s.nedges = h.n, h.m
+                for k in range(6):
+                    s.attr[k] = attr[k]
+                s.pattern, s.level = 0, i
+                if i == 0:
+                    s.first_level, s.active, s.root_degree = 1, 1, int(h.degrees()[root])
+                else:
+                    state = np.where((lv >= 0) & (lv <= i), lv, -1).astype(np.int32)
+                    c = g.bfs_inspect(state, i)
+                    (s.active, s.inactive, s.push_workload, s.pull_workload, s.max_push,
+                     s.max_pull) = (int(x) for x in c)
+                choice, done = ctx.select(s, selector)
+                assert not done
+                assert choice == tuple(t[:3]), (name, i, choice, t)
+            g.close()
+    finally:
+        ctx.mlp_load(None)
