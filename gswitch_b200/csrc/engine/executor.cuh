@@ -517,6 +517,10 @@ struct executor_t {
   int64_t persistent_levels = 0;    // levels run inside persistent launches
   int64_t persistent_launches = 0;  // persistent launches
   bool last_persistent = false;     // the last expand was a persistent launch
+  // zero-copy report of persistent launches (mapped pinned, 3 words; see
+  // persist_state::sig) and the tag of the last one
+  unsigned long long *h_psig = nullptr, *d_psig = nullptr;
+  unsigned long long psig_seq = 0;
   Computation pattern = Idem;       // pattern of the run being expanded
   int64_t tile_cap = 0;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -529,6 +533,8 @@ struct executor_t {
     cudaFree(dg_hubs);
     dg_hubs = nullptr;
     hub_cap = 0;
+    if (h_psig) cudaFreeHost(h_psig);
+    h_psig = d_psig = nullptr;
     for (auto &e : ev)
       if (e) {
         cudaEventDestroy(e);
@@ -821,6 +827,24 @@ struct executor_t {
     ps.levels_done = &c->plevels;
     ps.exit_reason = &c->preason;
     ps.lb_out = &c->plb;
+    ps.cur = cur;
+    if (!h_psig) {
+      // without the mapped block the launch reports through a copy-back
+      if (cudaHostAlloc((void **)&h_psig, 4 * sizeof(unsigned long long), cudaHostAllocMapped) == cudaSuccess) {
+        memset(h_psig, 0, 4 * sizeof(unsigned long long));
+        if (cudaHostGetDevicePointer((void **)&d_psig, h_psig, 0) != cudaSuccess) {
+          cudaGetLastError();
+          cudaFreeHost(h_psig);
+          h_psig = d_psig = nullptr;
+        }
+      } else {
+        cudaGetLastError();
+        h_psig = nullptr;
+      }
+    }
+    const unsigned long long seq = d_psig ? (++psig_seq % 0xffffffull) + 1 : 0;
+    ps.sig = seq ? d_psig : nullptr;
+    ps.seq = seq;
     ps.eoff = as.workset.dg_eoff;
     ps.eoff_cap = as.size + 2;
     ps.bsum = as.workset.dg_bsum;
@@ -830,8 +854,10 @@ struct executor_t {
     if (GSW_CUDA(cudaLaunchCooperativeKernel((const void *)kern, grid, EXPAND_THREADS, args, 0, stream()))) return;
     GSW_LAUNCHED();
     int res[3] = {0, -1, -1};
-    GSW_CUDA(cudaMemcpyAsync(res, &c->plevels, sizeof(res), cudaMemcpyDeviceToHost, stream()));
-    GSW_CUDA(cudaStreamSynchronize(stream()));
+    if (!(seq && await_persist(seq, res))) {
+      GSW_CUDA(cudaMemcpyAsync(res, &c->plevels, sizeof(res), cudaMemcpyDeviceToHost, stream()));
+      GSW_CUDA(cudaStreamSynchronize(stream()));
+    }
     const int L = res[0], reason = res[1];
     hints().persistent_lb = res[2];
     persistent_levels += L;
@@ -846,11 +872,8 @@ struct executor_t {
       return;
     }
     if (L > 0) g.level += L - 1;
-    // the next input is the last output: q[L & 1], size pq[L % 3]
-    const int out_idx = cur ^ (L & 1);
-    if (out_idx == cur) as.queue.cursor ^= 1;
-    k_persist_finish<<<1, 1, 0, stream()>>>(c, out_idx, as.queue.cursor, L % 3);
-    GSW_LAUNCHED();
+    // the kernel published its last output (q[L & 1]) in the output slot
+    as.queue.cursor = (cur ^ (L & 1)) ^ 1;
     if (reason == 0) as.halt_host();
     if (reason == 1) {
       // back to inspected levels: the queue is rebuilt from the bitmaps
@@ -858,6 +881,31 @@ struct executor_t {
       as.queue.clean_size(0);
       as.queue.clean_size(1);
     }
+  }
+
+  // Waits for the persistent launch tagged `seq` to report {levels, reason,
+  // LB} through the mapped block.  Every 256 polls the stream is queried, so
+  // a launch that ended without reporting (a block left early) ends the wait:
+  // false then, and the caller copies the device words back.
+  bool await_persist(unsigned long long seq, int res[3]) {
+    volatile unsigned long long *h = h_psig;
+    auto arrived = [&] { return (h[0] >> 40) == seq && (h[1] >> 40) == seq && (h[2] >> 40) == seq; };
+    for (unsigned spin = 1;; ++spin) {
+      if (arrived()) break;
+      if ((spin & 255) == 0) {
+        const cudaError_t q = cudaStreamQuery(stream());
+        if (q != cudaErrorNotReady) {
+          if (arrived()) break;
+          if (q != cudaSuccess) GSW_CUDA(q);
+          return false;
+        }
+      }
+    }
+    const unsigned long long m = (1ull << 40) - 1;
+    res[0] = (int)(h[0] & m);
+    res[1] = (int)(h[1] & m) - 1;
+    res[2] = (int)(h[2] & m);
+    return true;
   }
 
   // 2D-partition expand (k_twod.cuh): all sources to all destinations, so

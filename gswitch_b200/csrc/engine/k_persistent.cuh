@@ -34,6 +34,11 @@ struct persist_state {
   int *exit_reason;     // out: 0 empty, 1 growth, 2 level cap, 3 barrier
                         // timeout, 4 STRICT scan capacity exceeded
   int *lb_out;          // out: the kernel's load balance (LB value)
+  int cur;              // the Normal queue's input cursor at the launch
+  // zero-copy report (mapped pinned, 3 words: levels, reason + 1, LB), each
+  // word tagged with `seq` in its top 24 bits; null: the host copies back
+  unsigned long long *sig;
+  unsigned long long seq;
   int leave_block;      // test hook: this block leaves before the first
                         // barrier so the others' bounded wait expires (-1: none)
   // STRICT levels: (degree+1) scan of the frontier, per-block chunk sums and
@@ -226,6 +231,19 @@ __global__ void __launch_bounds__(EXPAND_THREADS) k_fused_persistent(active_set_
     *ps.levels_done = L;
     *ps.exit_reason = reason;
     *ps.lb_out = LB;
+    // the last output (q[L & 1], size pq[L % 3]) becomes the Normal queue's
+    // output slot, where the next level's swap expects it; the host sets
+    // its cursor to out ^ 1
+    const int out = ps.cur ^ (L & 1);
+    c->qsize[out] = ((volatile int *)c->pq)[L % 3];
+    c->qsize[out ^ 1] = 0;
+    if (ps.sig) {
+      volatile unsigned long long *h = ps.sig;
+      const unsigned long long t = ps.seq << 40;
+      h[0] = t | (unsigned)L;
+      h[1] = t | (unsigned)(reason + 1);
+      h[2] = t | (unsigned)LB;
+    }
   }
 }
 
@@ -239,12 +257,6 @@ __global__ void k_persist_prep(as_counters_t *c, int cursor) {
   c->plb = -1;
   c->bar_count = 0;
   c->bar_gen = 0;
-}
-
-// publishes the persistent launch's last output as the Normal queue's output
-__global__ void k_persist_finish(as_counters_t *c, int out_idx, int cursor, int slot) {
-  c->qsize[out_idx] = c->pq[slot];
-  c->qsize[cursor] = 0;
 }
 
 }  // namespace gsw
