@@ -734,6 +734,7 @@ PROFILE_CASES = {
     "twc24": "one BFS on RMAT scale 24 with the tiered push forced at every level (hub pieces swept one per "
              "CTA, staged in shared memory by TMA bulk copies)",
     "strict24": "one BFS on RMAT scale 24 with the edge-balanced (STRICT) push forced at every level",
+    "cm24": "one BFS on RMAT scale 24 with the CTA-mapped (CM) push forced at every level",
     "bc20": "batched BC from 32 sources on RMAT scale 20 (one cooperative launch)",
 }
 
@@ -769,9 +770,10 @@ def run_case(case: str) -> None:
     elif case == "mbfs":
         g = ctx.rmat(20, 16, seed=1)
         g.mbfs(g.roots(77, 256), batched=True, out=False)
-    elif case in ("twc24", "strict24"):
+    elif case in ("twc24", "strict24", "cm24"):
         g = ctx.rmat(24, 16, seed=1)
-        cfg = "Push-Queue-TWC-Standalone" if case == "twc24" else "Push-Queue-STRICT-Standalone"
+        cfg = {"twc24": "Push-Queue-TWC-Standalone", "strict24": "Push-Queue-STRICT-Standalone",
+               "cm24": "Push-Queue-CM-Standalone"}[case]
         g.bfs(int(g.roots(1000, 1)[0]), gs.RunOpts.from_config(cfg), out=False)
     elif case == "bc20":
         g = ctx.rmat(20, 16, seed=1)

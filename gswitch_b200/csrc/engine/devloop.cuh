@@ -78,6 +78,7 @@ struct dloop_t {
   int *qsize;                   // the Normal queue's two size words
   long long nvertexs, nedges, as_size;
   long long launches;           // kernels the loop ran
+  unsigned long long push_sum;  // push workload of the inspected levels that ran
   int variant_body[DL_VARIANTS];  // variant -> expand body (-1: none)
   int expand_kernels[2 * DL_VARIANTS];
   int filter_kernels[DL_FILTER_BODIES];
@@ -175,6 +176,7 @@ __device__ inline int dl_decide(dloop_t &d, const level_counts &c, unsigned long
   }
   if (done) return stop(DL_DONE);
   if (d.iter >= d.iter_cap) return stop(DL_LEVEL_CAP);
+  if (need) d.push_sum += (unsigned long long)c.push;
   selector_t sel;
   sel.trees = &d.trees;
   sel.decide(fets, conf);

@@ -822,7 +822,7 @@ inline int level_cap(int64_t n) { return (int)std::min<int64_t>(std::max<int64_t
 // ---------------------------------------------------------------------------
 // captured level loop (engine/devloop.cuh)
 // ---------------------------------------------------------------------------
-enum { DL_APP_BFS = 0, DL_APP_PR = 1, DL_APP_CC = 2, DL_APP_SSSP = 3 };
+enum { DL_APP_BFS = 0, DL_APP_PR = 1, DL_APP_CC = 2, DL_APP_SSSP = 3, DL_APP_GC = 4, DL_APP_PRD = 5 };
 
 const tree_set *device_trees(gsw_ctx *ctx) {
   if (ctx->dtrees) return &ctx->dts;
@@ -879,6 +879,7 @@ struct dl_run {
   int *trace_cfg = nullptr;
   long long *trace_frontier = nullptr, *trace_edges = nullptr;
   dloop_t image;
+  unsigned long long push_sum = 0;  // after dl_collect: the loop's push workload
 };
 
 template <typename E, typename F>
@@ -949,6 +950,7 @@ bool dl_prepare(dl_run &R, gsw_ctx *ctx, int app, dl_key key, active_set_t &as, 
   im.nedges = g.nedges;
   im.as_size = as.size;
   im.launches = 0;
+  im.push_sum = 0;
   im.win = f.data.window;
   im.window_on = conf.conf_window ? 1 : 0;
   im.stepping = ctx->dstepping;
@@ -970,6 +972,7 @@ void dl_collect(dl_run &R, gsw_run_stats *st) {
   if (GSW_CUDA(cudaMemcpyAsync(&out, R.d, sizeof(dloop_t), cudaMemcpyDeviceToHost, stream()))) return;
   if (GSW_CUDA(cudaStreamSynchronize(stream()))) return;
   launch_count() += out.launches;
+  R.push_sum = out.push_sum;
   if (out.status == DL_LEVEL_CAP) set_error(GSW_ERR_TIMEOUT, "%s", "level loop did not converge within the level cap");
   if (out.status == DL_NO_BODY) set_error(GSW_ERR_UNSUPPORTED, "%s", "captured level loop: variant has no body");
   if (out.status == DL_NOT_INSPECTED) set_error(GSW_ERR_CUDA, "%s", "captured level loop: inspection missing");
@@ -2042,7 +2045,6 @@ __global__ void k_prd_init(const int *odeg, int64_t n, float damp, float *pr, fl
 gsw_status gsw_pagerank_delta(gsw_ctx *ctx, gsw_graph *gr, const gsw_run_opts *o, float *pr, gsw_run_stats *st) {
   entry_guard eg(ctx);
   if (!ctx || !gr) return fail(GSW_ERR_INVALID_ARG, "gsw_pagerank_delta: bad arguments");
-  if (o && o->captured) return fail(GSW_ERR_UNSUPPORTED, "gsw_pagerank_delta: no captured level loop");
   begin_stats(st);
   gsw_run_opts def;
   gsw_run_opts_default(&def);
@@ -2092,8 +2094,16 @@ gsw_status gsw_pagerank_delta(gsw_ctx *ctx, gsw_graph *gr, const gsw_run_opts *o
   loop_trace tr{st, MAX_LEVELS};
   const int cap = op->max_iters > 0 ? op->max_iters : MAX_LEVELS;
   int64_t work = 0;
+  // captured: the loop stops at `cap` iterations after that iteration's
+  // inspection, as here, and sums the push workload of the levels it ran
+  const bool captured = op->captured != 0;
+  dl_run R;
+  if (captured && !dl_prepare(R, ctx, DL_APP_PRD, dl_key() << f.data.dg_wa << f.pr << f.damp << f.eps, as, g, f,
+                              conf, fets, cap, cap + 1, op->selector))
+    return eg.finish();
   timer tm(ctx);
-  for (int level = 0; ok(); level++) {
+  if (captured) dl_launch(R);
+  for (int level = 0; !captured && ok(); level++) {
     const bool inspected = level > 0 && !conf.conf_fuse_inspect;
     inspector.inspect(as, g, f, stats, fets, conf);
     if (level == cap) break;
@@ -2107,6 +2117,10 @@ gsw_status gsw_pagerank_delta(gsw_ctx *ctx, gsw_graph *gr, const gsw_run_opts *o
     tr.done(stats, fets);
   }
   const double ms = tm.stop();
+  if (captured) {
+    dl_collect(R, st);
+    work = gr->m + (int64_t)R.push_sum;  // the first level sends along every arc
+  }
   tr.resolve();
   end_checks(&as, st);
   add_persistent_levels(st, executor, plv0, pln0);
@@ -2270,7 +2284,6 @@ gsw_status gsw_bc(gsw_ctx *ctx, gsw_graph *gr, int32_t root, const gsw_run_opts 
 gsw_status gsw_gc(gsw_ctx *ctx, gsw_graph *gr, const gsw_run_opts *o, int32_t *colors, gsw_run_stats *st) {
   entry_guard eg(ctx);
   if (!ctx || !gr) return fail(GSW_ERR_INVALID_ARG, "gsw_gc: bad arguments");
-  if (o && o->captured) return fail(GSW_ERR_UNSUPPORTED, "gsw_gc: no captured level loop");
   begin_stats(st);
   auto g = gr->view<Empty>();
   app::GC f;
@@ -2309,8 +2322,15 @@ gsw_status gsw_gc(gsw_ctx *ctx, gsw_graph *gr, const gsw_run_opts *o, int32_t *c
   as.reset();
   as.init(ALL_ACTIVE);
   loop_trace tr{st, MAX_LEVELS};
+  // captured: the rule trees decide on the device, as selector.select does here
+  const bool captured = o && o->captured;
+  dl_run R;
+  if (captured && !dl_prepare(R, ctx, DL_APP_GC, dl_key() << f.data.dg_wa, as, g, f, conf, fets, 0, MAX_LEVELS,
+                              GSW_SELECT_RULES))
+    return eg.finish();
   timer tm(ctx);
-  for (int level = 0; ok(); level++) {
+  if (captured) dl_launch(R);
+  for (int level = 0; !captured && ok(); level++) {
     inspector.inspect(as, g, f, stats, fets, conf);
     if (finish(as, g, f, conf)) break;
     selector.select(stats, fets, conf);
@@ -2322,6 +2342,7 @@ gsw_status gsw_gc(gsw_ctx *ctx, gsw_graph *gr, const gsw_run_opts *o, int32_t *c
     if (finish(as, g, f, conf)) break;
   }
   const double ms = tm.stop();
+  if (captured) dl_collect(R, st);
   tr.resolve();
   end_checks(&as, st);
   add_persistent_levels(st, executor, plv0, pln0);

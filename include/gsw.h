@@ -145,8 +145,10 @@ typedef struct gsw_run_opts {
                         others' wait (bounded to 20 ms) expires and the call
                         returns GSW_ERR_TIMEOUT */
   int captured;      /* 1: run the whole level loop as one CUDA graph with
-                        device-side selection and termination (BFS, SSSP, PR, CC;
-                        GSW_ERR_UNSUPPORTED elsewhere); 0: host-driven loop */
+                        device-side selection and termination (BFS, SSSP, PR,
+                        delta-PR, CC, GC; GSW_ERR_UNSUPPORTED for BC, MBFS and
+                        batched BC, whose batched forms run every level in one
+                        cooperative launch); 0: host-driven loop */
   int hub_path;      /* how a CTA sweeps one hub's adjacency list (the
                         thread/warp/CTA-tiered push's CTA tier): 0 four-byte
                         loads, 1 int4 loads of the 16-byte-aligned body,

@@ -167,6 +167,58 @@ def test_captured_sssp_large(ctx, graphs, name):
         ctx.mlp_load(None)
 
 
+@pytest.mark.parametrize("name", golden_names())
+def test_captured_gc_goldens(ctx, name):
+    """Graph colouring through the captured loop (rule trees on the device):
+    the reference's level colouring bit for bit, the host loop's levels."""
+    d = load_golden(name)
+    h = oracle.Csr(d["off"], d["col"])
+    g = ctx.upload(d["off"], d["col"])
+    ref = oracle.gc_levels(h)
+    for cfg in ["", "Push-Queue-WM-Standalone", "Pull-Bitmap-TM-Standalone", "Push-Bitmap-STRICT-Standalone"]:
+        _, host = g.gc(gs.RunOpts.from_config(cfg))
+        for _ in range(2):  # the second run reuses the cached graph
+            col, st = g.gc(cap(cfg))
+            assert np.array_equal(col, ref), (name, cfg)
+            assert oracle.gc_check(h, col) < 0
+            assert st.levels == host.levels, (name, cfg)
+
+
+def test_captured_gc_large(ctx, graphs):
+    for name in ("rmat14", "grid64"):
+        h, _ = graphs[name]
+        g = ctx.upload(h.off, h.col)
+        col, st = g.gc(cap())
+        assert np.array_equal(col, oracle.gc_levels(h)), name
+        assert st.device_error == 0
+
+
+@pytest.mark.parametrize("name", ["rmat10", "grid24_lr", "er1500", "path10", "twocomp_isolated"])
+def test_captured_delta_pagerank(ctx, name):
+    """Delta-PageRank through the captured loop: the oracle's fixed point
+    within the delta tolerance, the host loop's values, level count and work
+    up to the order of FP32 atomic sums (which moves a vertex across its
+    activation threshold now and then); an iteration cap stops both loops at
+    the same level."""
+    d = load_golden(name)
+    h = oracle.Csr(d["off"], d["col"])
+    ref = oracle.pagerank(h, 400, 0.85)
+    g = ctx.upload(d["off"], d["col"])
+    for cfg in ["", "Push-Queue-WM-Standalone", "Pull-Bitmap-TM-Standalone"]:
+        hp, hst = g.pagerank_delta(eps=1e-5, max_levels=2000, opts=cfg)
+        for _ in range(2):
+            pr, st = g.pagerank_delta(eps=1e-5, max_levels=2000, opts=cap(cfg))
+            l1 = np.abs(pr / pr.sum() - ref / ref.sum()).sum()
+            assert l1 <= 1e-5 / 0.15 + 1e-5, (name, cfg, l1)
+            assert np.allclose(pr, hp, rtol=5e-4, atol=1e-6), (name, cfg)
+            assert abs(st.levels - hst.levels) <= 1, (name, cfg, st.levels, hst.levels)
+            assert st.edges > 0 and "Fused" not in {t[3] for t in st.trace}
+        _, c5 = g.pagerank_delta(eps=1e-5, max_levels=5, opts=cap(cfg))
+        _, h5 = g.pagerank_delta(eps=1e-5, max_levels=5, opts=cfg)
+        assert c5.levels == h5.levels == 5, (name, cfg, c5.levels, h5.levels)
+        assert abs(c5.edges - h5.edges) <= 0.01 * h5.edges, (name, cfg, c5.edges, h5.edges)
+
+
 def test_captured_rejected_where_unsupported(ctx, graphs):
     h, root = graphs["er20k"]
     g = ctx.upload(h.off, h.col)
