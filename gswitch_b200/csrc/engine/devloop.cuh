@@ -378,6 +378,7 @@ bool dl_build(dloop_graph &L, executor_t &ex, dloop_t *d, active_set_t as, devic
   const hints_t saved_hints = hints();
   hints().frontier = -1;
   hints().edges = -1;
+  hints().max_deg = -1;  // a captured body sweeps whatever hubs its level lists
   ex.ensure_tiles(g.nedges + as.size + 1);
   dloop_t &im = L.image;
   im = dloop_t();

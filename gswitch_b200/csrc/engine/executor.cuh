@@ -84,6 +84,7 @@ struct hints_t {
   int64_t edges = -1;        // edges they touch
   bool persistent = false;   // the last expand ran as a persistent launch
   int persistent_lb = -1;    // the load balance that launch's kernel reported
+  int64_t max_deg = -1;      // bound on the largest degree in the work list (-1: unknown)
 };
 inline hints_t &hints() {
   static thread_local hints_t h;
@@ -301,10 +302,13 @@ struct inspector_t {
     raw_inactive = c.inactive;
     raw_push = c.push;
     raw_pull = c.pull;
+    // the push max counter sums per-thread maxima, so it bounds the largest
+    // active degree from above; the first level has only its workload
+    raw_max_push = c.max_push > 0 ? c.max_push : c.push;
   }
 
   // raw counters of the last inspection (before cross() folding)
-  int64_t raw_frontier = 0, raw_inactive = 0, raw_push = 0, raw_pull = 0;
+  int64_t raw_frontier = 0, raw_inactive = 0, raw_push = 0, raw_pull = 0, raw_max_push = 0;
 };
 
 // ===========================================================================
@@ -604,6 +608,10 @@ struct executor_t {
     else
       h.edges = -1;
     if (h.frontier < 0 || h.frontier > as.size) h.frontier = -1;
+    h.max_deg = (!conf.conf_fuse_inspect && insp && conf.conf_dir == Push && conf.conf_target == Active &&
+                 as.fmt == Queue)
+                    ? insp->raw_max_push
+                    : -1;
   }
 
   // deferred filter updates of fused levels (kernel_fusion.cuh:54-109)
@@ -616,6 +624,17 @@ struct executor_t {
   }
   template <typename E, typename F>
   void compensation(active_set_t &, device_graph_t<COO, E> &, F &) {}
+
+  // The hub list of a per-launch push whose hubs start at min_deg columns,
+  // or none when the inspection bounds the frontier's degrees below that
+  template <typename E>
+  hub_list_t hub_list_for(active_set_t &as, const device_graph_t<CSR, E> &g, int min_deg) {
+    const int64_t md = hints().max_deg;
+    if (md >= 0 && md < min_deg) return hub_list_t();
+    ensure_hubs(g.nedges);
+    if (!ok() || !dg_hubs) return hub_list_t();
+    return hub_list_t{dg_hubs, &as.dg_cnt->hub_pieces, &as.dg_cnt->hub_done, hub_cap};
+  }
 
   // room for every hub piece a level can list: at most one piece per
   // EXPAND_THREADS arcs plus one per TWC_HUB_PIECE arcs
@@ -679,6 +698,14 @@ struct executor_t {
     auto _k = kern;                                               \
     _k<<<grid_for(_k, want), B, 0, stream()>>>(__VA_ARGS__);      \
   } while (0)
+// the hub pieces a per-launch push listed, one per CTA
+#define GSW_HUBS(hl)                                                          \
+  do {                                                                        \
+    if ((hl).piece) {                                                         \
+      if (fused) GSW_GO((k_push_twc_hubs<true, G, F>), -1, as, g, f, conf, hl);  \
+      else GSW_GO((k_push_twc_hubs<false, G, F>), -1, as, g, f, conf, hl);       \
+    }                                                                         \
+  } while (0)
     if (conf.conf_lb == TWOD) {
       launch_twod(g, f, conf);
       return;
@@ -694,21 +721,21 @@ struct executor_t {
           else GSW_GO((k_push_tm<false, G, F>), fr < 0 ? -1 : fr / B + 1, as, g, f, conf);
           break;
         case CM:
-          if (fused) GSW_GO((k_push_cm<true, G, F>), fr < 0 ? -1 : fr / B + 1, as, g, f, conf);
-          else GSW_GO((k_push_cm<false, G, F>), fr < 0 ? -1 : fr / B + 1, as, g, f, conf);
+          {
+            const hub_list_t hl = hub_list_for(as, g, CM_HUB_MIN);
+            if (!ok()) return;
+            if (fused) GSW_GO((k_push_cm<true, G, F>), fr < 0 ? -1 : fr / B + 1, as, g, f, conf, hl);
+            else GSW_GO((k_push_cm<false, G, F>), fr < 0 ? -1 : fr / B + 1, as, g, f, conf, hl);
+            GSW_HUBS(hl);
+          }
           break;
         case TWC: {
           // tiles, then the hub pieces they listed (one piece per CTA)
-          ensure_hubs(g.nedges);
+          const hub_list_t hl = hub_list_for(as, g, B);
           if (!ok()) return;
-          const hub_list_t hl{dg_hubs, &as.dg_cnt->hub_pieces, &as.dg_cnt->hub_done, hub_cap};
-          if (fused) {
-            GSW_GO((k_push_twc<true, G, F>), fr < 0 ? -1 : fr / B + 1, as, g, f, conf, hl);
-            GSW_GO((k_push_twc_hubs<true, G, F>), -1, as, g, f, conf, hl);
-          } else {
-            GSW_GO((k_push_twc<false, G, F>), fr < 0 ? -1 : fr / B + 1, as, g, f, conf, hl);
-            GSW_GO((k_push_twc_hubs<false, G, F>), -1, as, g, f, conf, hl);
-          }
+          if (fused) GSW_GO((k_push_twc<true, G, F>), fr < 0 ? -1 : fr / B + 1, as, g, f, conf, hl);
+          else GSW_GO((k_push_twc<false, G, F>), fr < 0 ? -1 : fr / B + 1, as, g, f, conf, hl);
+          GSW_HUBS(hl);
           break;
         }
         case STRICT: {
@@ -730,8 +757,13 @@ struct executor_t {
         }
         case WM:
         default:
-          if (fused) GSW_GO((k_push_wm<true, G, F>), fr < 0 ? -1 : fr / B + 1, as, g, f, conf);
-          else GSW_GO((k_push_wm<false, G, F>), fr < 0 ? -1 : fr / B + 1, as, g, f, conf);
+          {
+            const hub_list_t hl = hub_list_for(as, g, WM_HUB_MIN);
+            if (!ok()) return;
+            if (fused) GSW_GO((k_push_wm<true, G, F>), fr < 0 ? -1 : fr / B + 1, as, g, f, conf, hl);
+            else GSW_GO((k_push_wm<false, G, F>), fr < 0 ? -1 : fr / B + 1, as, g, f, conf, hl);
+            GSW_HUBS(hl);
+          }
           break;
       }
     } else {
@@ -779,6 +811,7 @@ struct executor_t {
         }
       }
     }
+#undef GSW_HUBS
 #undef GSW_GO
     GSW_LAUNCHED();
   }

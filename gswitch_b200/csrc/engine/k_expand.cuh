@@ -291,11 +291,57 @@ __global__ void __launch_bounds__(EXPAND_THREADS) k_pull_tm(active_set_t as, G g
 }
 
 // ===========================================================================
+// Hub lists of per-launch pushes
+// ===========================================================================
+// A push whose grid is sized by frontier vertices runs a level whose frontier
+// is a few hubs on a few CTAs, and a tile (warp or CTA) that holds a hub
+// sweeps all of its columns alone.  Per-launch tiered (TWC), warp-mapped (WM)
+// and CTA-mapped (CM) pushes therefore cut each vertex of at least their hub
+// degree into pieces of at most TWC_HUB_PIECE columns, append them to a hub
+// list, and a second kernel (k_push_twc_hubs) sweeps one piece per CTA over
+// the resident grid.  Persistent launches keep the in-tile sweep (the list
+// would need one more grid barrier per level), and so does a hub that finds
+// the list full (a fused queue may hold a vertex more than once).  The hub
+// kernel's last CTA to read the count sets it back to 0 for the next level,
+// so no memset node sits in captured loops.
+constexpr int TWC_HUB_PIECE = 8192;
+constexpr int WM_HUB_MIN = 1024;  // WM: a warp would take 32+ rounds alone
+constexpr int CM_HUB_MIN = 4096;  // CM: a CTA would take 16+ rounds alone
+struct hub_piece_t {
+  int v;
+  int len;
+  int64_t st;
+};
+struct hub_list_t {
+  hub_piece_t *piece = nullptr;  // null: sweep hubs in their tile
+  int *count = nullptr;
+  unsigned *done = nullptr;
+  int64_t cap = 0;
+};
+// Lists v's columns as hub pieces when a list is given and deg >= min_deg;
+// true when they were listed (the caller then drops them).  A hub that does
+// not fit whole writes empty pieces into its slots below the cap and stays
+// with its tile.
+__device__ __forceinline__ bool defer_hub(active_set_t &as, const config_t &conf, const hub_list_t &hubs, int v,
+                                          int64_t st, int deg, int min_deg) {
+  if (!hubs.piece || deg < min_deg) return false;
+  const int np = (deg + TWC_HUB_PIECE - 1) / TWC_HUB_PIECE;
+  const int at = atomicAdd(hubs.count, np);
+  const bool fits = (int64_t)at + np <= hubs.cap;
+  for (int k = 0; k < np && (int64_t)at + k < hubs.cap; ++k)
+    hubs.piece[at + k] = fits ? hub_piece_t{v, MIN(TWC_HUB_PIECE, deg - k * TWC_HUB_PIECE),
+                                            st + (int64_t)k * TWC_HUB_PIECE}
+                              : hub_piece_t{v, 0, 0};
+  if (fits) account(as, conf, (unsigned long long)deg);
+  return fits;
+}
+
+// ===========================================================================
 // WM: warp per 32 frontier vertices
 // ===========================================================================
 template <bool FUSED, typename G, typename F, typename Src>
 __device__ __forceinline__ void push_wm_body(active_set_t &as, const G &g, F &f, const config_t &conf, const Src &src,
-                                             int64_t n, warp_stage_t &stage) {
+                                             int64_t n, warp_stage_t &stage, hub_list_t hubs = hub_list_t()) {
   constexpr int W = EXPAND_THREADS / 32;
   __shared__ int s_scan[W][32];
   __shared__ int s_v[W][32];
@@ -309,6 +355,7 @@ __device__ __forceinline__ void push_wm_body(active_set_t &as, const G &g, F &f,
     int64_t st;
     int deg;
     vertex_range(g, false, v, st, deg);
+    if (defer_hub(as, conf, hubs, v, st, deg, WM_HUB_MIN)) deg = 0;
     const int incl = warp_inclusive_sum(deg);
     const int total = __shfl_sync(FULL, incl, 31);
     if (lane == 0) account(as, conf, (unsigned long long)total);
@@ -336,12 +383,13 @@ __device__ __forceinline__ void push_wm_body(active_set_t &as, const G &g, F &f,
 }
 
 template <bool FUSED, typename G, typename F>
-__global__ void __launch_bounds__(EXPAND_THREADS) k_push_wm(active_set_t as, G g, F f, config_t conf) {
+__global__ void __launch_bounds__(EXPAND_THREADS) k_push_wm(active_set_t as, G g, F f, config_t conf,
+                                                            hub_list_t hubs) {
   __shared__ int s_stage[FUSED ? EXPAND_THREADS / 32 : 1][FUSED ? STAGE_SLOTS : 1];
   const int64_t n = as.get_size();
   GSW_HALT_IF_EMPTY(n);
   warp_stage_t stage(s_stage[FUSED ? warp_id() : 0], as);
-  push_wm_body<FUSED>(as, g, f, conf, as_src_t{&as, conf.want()}, n, stage);
+  push_wm_body<FUSED>(as, g, f, conf, as_src_t{&as, conf.want()}, n, stage, hubs);
   if (FUSED) stage.flush();
 }
 
@@ -415,7 +463,7 @@ __global__ void __launch_bounds__(EXPAND_THREADS) k_pull_wm(active_set_t as, G g
 // ===========================================================================
 template <bool FUSED, typename G, typename F, typename Src>
 __device__ __forceinline__ void push_cm_body(active_set_t &as, const G &g, F &f, const config_t &conf, const Src &src,
-                                             int64_t n, warp_stage_t &stage) {
+                                             int64_t n, warp_stage_t &stage, hub_list_t hubs = hub_list_t()) {
   constexpr int B = EXPAND_THREADS;
   __shared__ int s_scan[B];
   __shared__ int s_v[B];
@@ -428,6 +476,7 @@ __device__ __forceinline__ void push_cm_body(active_set_t &as, const G &g, F &f,
     int64_t st;
     int deg;
     vertex_range(g, false, v, st, deg);
+    if (defer_hub(as, conf, hubs, v, st, deg, CM_HUB_MIN)) deg = 0;
     int total;
     const int ex = block_exclusive_scan(deg, s_tmp, &total);
     if (threadIdx.x == 0) account(as, conf, (unsigned long long)total);
@@ -455,12 +504,13 @@ __device__ __forceinline__ void push_cm_body(active_set_t &as, const G &g, F &f,
 }
 
 template <bool FUSED, typename G, typename F>
-__global__ void __launch_bounds__(EXPAND_THREADS) k_push_cm(active_set_t as, G g, F f, config_t conf) {
+__global__ void __launch_bounds__(EXPAND_THREADS) k_push_cm(active_set_t as, G g, F f, config_t conf,
+                                                            hub_list_t hubs) {
   __shared__ int s_stage[FUSED ? EXPAND_THREADS / 32 : 1][FUSED ? STAGE_SLOTS : 1];
   const int64_t n = as.get_size();
   GSW_HALT_IF_EMPTY(n);
   warp_stage_t stage(s_stage[FUSED ? warp_id() : 0], as);
-  push_cm_body<FUSED>(as, g, f, conf, as_src_t{&as, conf.want()}, n, stage);
+  push_cm_body<FUSED>(as, g, f, conf, as_src_t{&as, conf.want()}, n, stage, hubs);
   if (FUSED) stage.flush();
 }
 
@@ -945,27 +995,9 @@ __device__ __forceinline__ bool hub_run(const int *col, int64_t a, int64_t len, 
 // ===========================================================================
 // TWC: thread / warp / CTA tiers by degree
 // ===========================================================================
-// Per-launch tiered pushes do not sweep their hubs in the tile that found
-// them: a level whose frontier is a few hubs would run on one CTA (its grid is
-// sized by frontier vertices).  Each hub is cut into pieces of at most
-// TWC_HUB_PIECE columns appended to a hub list, and a second kernel sweeps one
-// piece per CTA with the hub path's loads.  Persistent launches keep the
-// in-tile sweep (the list would need one more grid barrier per level), and so
-// does a hub that finds the list full (a fused queue may hold a vertex more
-// than once).  The hub kernel's last CTA to read the count sets it back to 0
-// for the next level, so no memset node sits in captured loops.
-constexpr int TWC_HUB_PIECE = 8192;
-struct hub_piece_t {
-  int v;
-  int len;
-  int64_t st;
-};
-struct hub_list_t {
-  hub_piece_t *piece = nullptr;  // null: sweep hubs in their tile
-  int *count = nullptr;
-  unsigned *done = nullptr;
-  int64_t cap = 0;
-};
+// Per-launch tiered pushes list their hubs (deg >= EXPAND_THREADS) for the
+// hub kernel instead of sweeping them in the tile that found them (see
+// hub_list_t above).
 template <bool FUSED, typename G, typename F, typename Src>
 __device__ __forceinline__ void push_twc_body(active_set_t &as, const G &g, F &f, const config_t &conf, const Src &src,
                                               int64_t n, warp_stage_t &stage, hub_list_t hubs = hub_list_t()) {
@@ -1004,21 +1036,7 @@ __device__ __forceinline__ void push_twc_body(active_set_t &as, const G &g, F &f
     int64_t st;
     int deg;
     vertex_range(g, false, v, st, deg);
-    if (hubs.piece && deg >= B) {
-      // hub: into the list, in pieces, for the hub kernel; if it does not fit
-      // whole, its slots below the cap get empty pieces and the tile sweeps it
-      const int np = (deg + TWC_HUB_PIECE - 1) / TWC_HUB_PIECE;
-      const int at = atomicAdd(hubs.count, np);
-      const bool fits = (int64_t)at + np <= hubs.cap;
-      for (int k = 0; k < np && (int64_t)at + k < hubs.cap; ++k)
-        hubs.piece[at + k] = fits ? hub_piece_t{v, MIN(TWC_HUB_PIECE, deg - k * TWC_HUB_PIECE),
-                                                st + (int64_t)k * TWC_HUB_PIECE}
-                                  : hub_piece_t{v, 0, 0};
-      if (fits) {
-        account(as, conf, (unsigned long long)deg);
-        deg = 0;
-      }
-    }
+    if (defer_hub(as, conf, hubs, v, st, deg, B)) deg = 0;  // hub: swept by the hub kernel
     // CTA tier
     for (;;) {
       if (deg >= B) s_owner = threadIdx.x;
