@@ -128,10 +128,9 @@ def level_bytes(kind, n, A, U, D, E):
 
 
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per vertex of
-# one inspection launch, from the ncu capture summarised in
-# profiles/bfs_rmat24_inspect_pulltm.md (135.47 MB + 4.42 MB over 16,777,216
-# vertices); the inspection streams every vertex once, so a launch's traffic
-# scales with n
+# one inspection launch, from an ncu capture of the third inspection of one
+# BFS on the bench graph (135.47 MB + 4.42 MB over 16,777,216 vertices); the
+# inspection streams every vertex once, so a launch's traffic scales with n
 INSPECT_TRAFFIC_PER_VERTEX = (135.47e6 + 4.42e6) / 16777216
 # DRAM bytes per launch of the thread-mapped pull expand on the bench graph
 # (RMAT scale 24 ef 16 seed 1): the mean of the two launches of one BFS in the
