@@ -40,7 +40,8 @@ ABI_SYMBOLS = (
     "gsw_graph_generate_powerlaw", "gsw_label_levels", "gsw_mlp_train", "gsw_mlp_grad", "gsw_mlp_infer",
     "gsw_mlp_load", "gsw_graph_generate_er_batch", "gsw_bfs_multi", "gsw_bfs_inspect", "gsw_tune_load",
     "gsw_tune_save", "gsw_tune_load_shapes", "gsw_tune_save_shapes", "gsw_mlp_load_fusion", "gsw_pagerank_delta",
-    "gsw_mlp_save", "gsw_select",
+    "gsw_mlp_save", "gsw_select", "gsw_traversal_begin", "gsw_level_begin", "gsw_level_end",
+    "gsw_traversal_end",
 )
 TUNE_ENTRIES = 64
 
@@ -135,6 +136,10 @@ def lib():
     L.gsw_tune_load_shapes.argtypes = [vp, vp]
     L.gsw_mlp_save.argtypes = [vp, vp, vp]
     L.gsw_select.argtypes = [vp, vp, C.c_int, vp]
+    L.gsw_traversal_begin.argtypes = [vp, vp, C.c_int, i32, vp, pvp]
+    L.gsw_level_begin.argtypes = [vp, vp, C.POINTER(C.c_int)]
+    L.gsw_level_end.argtypes = [vp, vp]
+    L.gsw_traversal_end.argtypes = [vp, vp, vp]
     L.gsw_tune_save_shapes.argtypes = [vp, vp]
     L.gsw_mlp_load_fusion.argtypes = [vp, vp, C.c_float]
     L.gsw_tune_save.argtypes = [vp, vp]
@@ -166,6 +171,41 @@ class LevelStats(C.Structure):
 
 class LevelChoice(C.Structure):
     _fields_ = [("direction", C.c_int), ("asfmt", C.c_int), ("lb", C.c_int), ("done", C.c_int)]
+
+
+class Traversal:
+    """A BFS whose level loop the caller drives (gsw_traversal_* and
+    gsw_level_*): level_begin() inspects the level and returns its
+    LevelStats and whether the run is over; level_end(choice) runs that level
+    as the standalone variant `choice` -- a LevelChoice or a (direction,
+    format, LB) tuple of names as Context.select() returns; end() returns the
+    levels and the run statistics and frees the state."""
+
+    def __init__(self, graph, root, opts=None):
+        self.graph = graph
+        h = C.c_void_p()
+        o = graph._opts(opts)
+        _check(lib().gsw_traversal_begin(graph.ctx._h, graph._h, APP_BFS, C.c_int32(root), C.byref(o), C.byref(h)))
+        self._h = h
+
+    def level_begin(self):
+        st = LevelStats()
+        done = C.c_int(0)
+        _check(lib().gsw_level_begin(self._h, C.byref(st), C.byref(done)))
+        return st, bool(done.value)
+
+    def level_end(self, choice):
+        if not isinstance(choice, LevelChoice):
+            d, a, b = choice
+            choice = LevelChoice(PULL if d == "Pull" else PUSH, BITMAP if a == "Bitmap" else QUEUE, LB[b], 0)
+        _check(lib().gsw_level_end(self._h, C.byref(choice)))
+
+    def end(self, out=True):
+        lv = np.empty(self.graph.n, dtype=np.int32) if out else None
+        st = _Stats()
+        h, self._h = self._h, None
+        _check(lib().gsw_traversal_end(h, _ptr(lv), C.byref(st)))
+        return lv, RunStats(st)
 
 
 class RunOpts:
@@ -457,6 +497,11 @@ class Graph:
         lv = np.empty(self.n, dtype=np.int32) if out else None
         st = self._run(lib().gsw_bfs, C.c_int32(root), outs=[lv], opts=opts)
         return lv, st
+
+    def traversal(self, root, opts=None):
+        """A BFS level loop driven from Python (gsw_traversal_begin); see
+        Traversal.  Nothing else may run on the context until it ends."""
+        return Traversal(self, root, opts)
 
     def bfs_inspect(self, levels, level):
         """The inspector's six counters for a BFS state (gsw_bfs_inspect)."""

@@ -1598,6 +1598,179 @@ gsw_status gsw_bfs_multi(gsw_ctx *ctx, gsw_graph *gr, int nroots, const int32_t 
 }
 
 // ---------------------------------------------------------------------------
+// A BFS level loop that the caller drives (the reference's per-level calls
+// from application/bfs.cu:78-102: inspector.inspect, selector.select,
+// executor.filter, g.update_level, executor.expand, as.finish), one level per
+// gsw_level_begin / gsw_level_end pair.  The state lives in the context's
+// buffers, so nothing else may run on the context between begin and end.
+// ---------------------------------------------------------------------------
+}  // extern "C"
+struct gsw_traversal {
+  gsw_ctx *ctx = nullptr;
+  gsw_graph *gr = nullptr;
+  device_graph_t<CSR, Empty> g;
+  app::BFS f;
+  feature_t fets;
+  config_t conf;
+  inspector_t inspector;
+  active_set_t *as = nullptr;
+  gsw_run_stats st;
+  loop_trace tr{nullptr, 0};
+  int64_t root_degree = 0;
+  int64_t plv0 = 0, pln0 = 0;
+  double ms = 0;
+  int first = 1;      // the next level is the run's first (not inspected)
+  int done = 0;       // the loop is over
+  int inspected = 0;  // gsw_level_begin ran for the current level
+};
+extern "C" {
+
+gsw_status gsw_traversal_begin(gsw_ctx *ctx, gsw_graph *gr, int app, int32_t root, const gsw_run_opts *o,
+                               gsw_traversal **out) {
+  entry_guard eg(ctx);
+  if (!ctx || !gr || !out || app != GSW_APP_BFS || root < 0 || root >= gr->n)
+    return fail(GSW_ERR_INVALID_ARG, "gsw_traversal_begin: bad arguments (BFS from a vertex of the graph)");
+  if (o && o->captured) return fail(GSW_ERR_UNSUPPORTED, "gsw_traversal_begin: the caller drives the loop");
+  *out = nullptr;
+  auto *t = new gsw_traversal();
+  t->ctx = ctx;
+  t->gr = gr;
+  begin_stats(&t->st);
+  t->g = gr->view<Empty>();
+  t->f.data.size = gr->n;
+  t->f.data.dg_wa = (int *)ctx->buf("wa", sizeof(int) * (gr->n + 1));
+  if (!t->f.data.dg_wa) return delete t, eg.finish();
+  fill_root<int>(t->f.data.dg_wa, -1, 0, root, gr->n);
+  t->root_degree = root_deg(gr, root);
+  ctx->stats.clean();
+  executor_t &executor = ctx->executor;
+  executor.insp = &t->inspector;
+  executor.twod = twod_layout();
+  t->plv0 = executor.persistent_levels;
+  t->pln0 = executor.persistent_launches;
+  feature_t &fets = t->fets;
+  config_t &conf = t->conf;
+  fets.centric = VC;
+  fets.pattern = Idem;
+  fets.fromall = false;
+  fets.toall = false;
+  conf.conf_pruning = true;
+  apply_opts(o, conf);
+  // standalone levels of the caller's variants: no fusion, no persistent launch
+  conf.force.has_fusion = true;
+  conf.force.fusion = Standalone;
+  conf.conf_persistent = false;
+  set_graph_features(fets, gr);
+  fets.use_root = root;
+  fets.first_active = 1;
+  init_conf_impl(ctx->stats, fets, conf, t->g, t->f, gr->mean_weight, gr->attr[0], false, t->root_degree);
+  t->as = ctx->aset(gr->n, conf.conf_qmode);
+  if (!t->as) return delete t, eg.finish();
+  t->as->reset();
+  t->as->init(root);
+  t->tr = loop_trace{&t->st, level_cap(gr->n)};
+  if (!ok()) return delete t, eg.finish();
+  *out = t;
+  return eg.finish();
+}
+
+gsw_status gsw_level_begin(gsw_traversal *t, gsw_level_stats *out, int *done) {
+  if (!t || !out || !done) return fail(GSW_ERR_INVALID_ARG, "gsw_level_begin: bad arguments");
+  entry_guard eg(t->ctx);
+  gsw_graph *gr = t->gr;
+  memset(out, 0, sizeof(*out));
+  out->nvertexs = gr->n;
+  out->nedges = gr->m;
+  for (int i = 0; i < 6; ++i) out->attr[i] = gr->attr[i];
+  out->pattern = 0;
+  out->level = t->g.level;
+  if (t->done) {
+    *done = 1;
+    return eg.finish();
+  }
+  timer tm(t->ctx);
+  stat_t &stats = t->ctx->stats;
+  t->inspector.inspect(*t->as, t->g, t->f, stats, t->fets, t->conf);
+  t->done = finish(*t->as, t->g, t->f, t->conf) ? 1 : 0;
+  t->ms += tm.stop();
+  if (t->first) {
+    out->first_level = 1;
+    out->active = 1;
+    out->inactive = gr->n - 1;
+    out->root_degree = t->root_degree;
+    out->push_workload = t->root_degree;
+    out->pull_workload = gr->m - t->root_degree;
+  } else {
+    out->active = (int64_t)stats.active_num();
+    out->inactive = (int64_t)stats.unactive_num();
+    out->push_workload = (int64_t)stats.push_workload();
+    out->pull_workload = (int64_t)stats.pull_workload();
+    out->max_push = (int64_t)stats.max_deg_active();
+    out->max_pull = (int64_t)stats.max_deg_unactive();
+  }
+  t->inspected = 1;
+  *done = t->done;
+  return eg.finish();
+}
+
+gsw_status gsw_level_end(gsw_traversal *t, const gsw_level_choice *choice) {
+  if (!t || !choice) return fail(GSW_ERR_INVALID_ARG, "gsw_level_end: bad arguments");
+  entry_guard eg(t->ctx);
+  if (t->done) return fail(GSW_ERR_INVALID_ARG, "gsw_level_end: the traversal is over");
+  if (!t->inspected) return fail(GSW_ERR_INVALID_ARG, "gsw_level_end: call gsw_level_begin first");
+  if ((choice->direction != GSW_PUSH && choice->direction != GSW_PULL) ||
+      (choice->asfmt != GSW_QUEUE && choice->asfmt != GSW_BITMAP) ||
+      !(choice->lb == GSW_LB_TM || choice->lb == GSW_LB_WM || choice->lb == GSW_LB_CM ||
+        choice->lb == GSW_LB_STRICT || choice->lb == GSW_LB_TWC))
+    return fail(GSW_ERR_INVALID_ARG, "gsw_level_end: bad choice (push/pull, queue/bitmap, TM/WM/CM/STRICT/TWC)");
+  config_t &conf = t->conf;
+  const auto force0 = conf.force;
+  conf.conf_dir = choice->direction == GSW_PULL ? Pull : Push;
+  conf.conf_asfmt = choice->asfmt == GSW_BITMAP ? Bitmap : Queue;
+  conf.conf_lb = (LB)choice->lb;
+  conf.conf_fuse_inspect = false;
+  conf.conf_centric = VC;
+  conf.conf_fromall = false;
+  conf.conf_toall = false;
+  selector_t::set_target(conf);
+  conf.force.has_lb = true;  // the level runs the caller's load balance as given
+  conf.force.lb = conf.conf_lb;
+  executor_t &executor = t->ctx->executor;
+  executor.insp = &t->inspector;
+  stat_t &stats = t->ctx->stats;
+  timer tm(t->ctx);
+  executor.filter(*t->as, t->g, t->f, stats, t->fets, conf);
+  t->g.update_level();
+  t->tr.level(conf, hints().frontier);
+  executor.expand(*t->as, t->g, t->f, stats, t->fets, conf);
+  t->tr.done(stats, t->fets);
+  t->done = finish(*t->as, t->g, t->f, conf) ? 1 : 0;
+  t->ms += tm.stop();
+  conf.force = force0;
+  t->first = 0;
+  t->inspected = 0;
+  return eg.finish();
+}
+
+gsw_status gsw_traversal_end(gsw_traversal *t, int32_t *values, gsw_run_stats *st) {
+  if (!t) return fail(GSW_ERR_INVALID_ARG, "gsw_traversal_end: NULL traversal");
+  entry_guard eg(t->ctx);
+  gsw_graph *gr = t->gr;
+  t->tr.resolve();
+  end_checks(t->as, &t->st);
+  add_persistent_levels(&t->st, t->ctx->executor, t->plv0, t->pln0);
+  t->st.ms = t->ms;
+  t->st.edges = reached_edges(t->ctx, gr, t->f.data.dg_wa, 1, -1);
+  if (values && ok())
+    GSW_CUDA(cudaMemcpyAsync(values, t->f.data.dg_wa, sizeof(int) * gr->n, cudaMemcpyDeviceToHost, stream()));
+  GSW_CUDA(cudaStreamSynchronize(stream()));
+  if (st) *st = t->st;
+  t->ctx->executor.insp = nullptr;
+  delete t;
+  return eg.finish();
+}
+
+// ---------------------------------------------------------------------------
 // SSSP: application/sssp.cu:106-126 (loop) and :128-160 (set-up)
 // ---------------------------------------------------------------------------
 gsw_status gsw_sssp(gsw_ctx *ctx, gsw_graph *gr, int32_t root, const gsw_run_opts *o, int32_t *dist,

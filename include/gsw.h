@@ -304,6 +304,33 @@ typedef struct gsw_level_choice {
   int done;                    /* 1: the counters end the run (no active vertex) */
 } gsw_level_choice;
 gsw_status gsw_select(gsw_ctx *ctx, const gsw_level_stats *in, int selector, gsw_level_choice *out);
+
+/* ---- a level loop the caller drives --------------------------------------
+ * Replaces the per-level calls of application/bfs.cu:78-102 (inspector.
+ * inspect, selector.select, executor.filter, g.update_level, executor.expand,
+ * as.finish) for a host framework that cannot instantiate the templates:
+ *
+ *   gsw_traversal_begin(ctx, g, GSW_APP_BFS, root, &o, &t);
+ *   for (;;) {
+ *     gsw_level_begin(t, &stats, &done);        inspection: the six counters
+ *     if (done) break;
+ *     gsw_select(ctx, &stats, GSW_SELECT_MLP, &choice);   or the caller's own
+ *     gsw_level_end(t, &choice);                filter + one standalone expand
+ *   }
+ *   gsw_traversal_end(t, levels, &st);          levels back; frees t
+ *
+ * BFS only (app GSW_APP_BFS); every level is standalone and runs exactly the
+ * given variant (TM / WM / CM / STRICT / TWC).  The state lives in the
+ * context's buffers: nothing else may run on the context between begin and
+ * end.  stats.first_level = 1 on the first level (not inspected: the root
+ * and its degree).  gsw_level_end after the loop ended, or without a
+ * gsw_level_begin for the level, is GSW_ERR_INVALID_ARG. */
+typedef struct gsw_traversal gsw_traversal;
+gsw_status gsw_traversal_begin(gsw_ctx *ctx, gsw_graph *g, int app, int32_t root, const gsw_run_opts *opts,
+                               gsw_traversal **out);
+gsw_status gsw_level_begin(gsw_traversal *t, gsw_level_stats *stats, int *done);
+gsw_status gsw_level_end(gsw_traversal *t, const gsw_level_choice *choice);
+gsw_status gsw_traversal_end(gsw_traversal *t, int32_t *values, gsw_run_stats *st);
 /* The second network: whether a Mono-pattern run (SSSP) runs fused or
  * standalone levels, from graph features (avg, std and range of degree, Gini,
  * entropy, log n, log m, pattern); class 0 standalone, 1 fused.  Used with
