@@ -2,8 +2,9 @@
 load balance, and the fused push forms) times the variant's expands under
 grid caps of 1/4 .. 16x the kernel's resident grid and, where the variant has
 them, under each of its shapes (STRICT: tiles of 512 / 1,024 / 2,048 slots;
-thread-mapped pull: candidates per thread) on seeded synthetic graphs, and
-keeps the fastest
+thread-mapped push: 256 / 128 / 512 threads per CTA; thread-mapped pull:
+candidates per thread 2 / 1 / 4 at each of those CTA sizes) on seeded
+synthetic graphs, and keeps the fastest
 (CUDA-event expand times summed over levels; BFS from three roots per graph).
 The tables load with Context.tune_load() and Context.tune_load_shapes().
 
@@ -24,14 +25,15 @@ import gswitch_b200 as gs  # noqa: E402
 
 QUARTERS = (1, 2, 4, 8, 16, 32, 64)  # grid cap = resident grid x q / 4
 STRICT_SHAPES = 3   # tile 1024 (default), 512, 2048
-PULL_TM_SHAPES = 3  # candidates per thread: 2 (default), 1, 4
+PUSH_TM_SHAPES = 3  # threads per CTA: 256 (default), 128, 512
+PULL_TM_SHAPES = 9  # candidates per thread 2 (default), 1, 4 (shape % 3) at those CTA sizes (shape // 3)
 
 
 def shapes_of(direction, lb):
     if lb == "STRICT":
         return STRICT_SHAPES
-    if direction == "Pull" and lb == "TM":
-        return PULL_TM_SHAPES
+    if lb == "TM":
+        return PULL_TM_SHAPES if direction == "Pull" else PUSH_TM_SHAPES
     return 1
 VARIANTS = [(d, f, lb, False) for d in ("Push", "Pull") for f in ("Queue", "Bitmap")
             for lb in ("TM", "WM", "CM", "STRICT", "TWC")] + [("Push", "Queue", lb, True)
@@ -47,11 +49,14 @@ def expand_ms(g, roots, cfg):
     return tot
 
 
-def tune(ctx, graphs, reps=2, log=None):
+def tune(ctx, graphs, reps=2, log=None, only=None):
+    """only: load-balance names to tune (None: all); the other entries stay 0."""
     table = np.zeros(gs.TUNE_ENTRIES, dtype=np.int32)
     shapes = np.zeros(gs.TUNE_ENTRIES, dtype=np.int32)
     report = {}
     for d, f, lb, fused in VARIANTS:
+        if only and lb not in only:
+            continue
         cfg = f"{d}-{f}-{lb}-{'Fused' if fused else 'Standalone'}"
         idx = gs.Context.tune_index(d, f, lb, fused)
         times = {}
@@ -108,22 +113,33 @@ def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=DEFAULT_PATH)
     ap.add_argument("--scale", type=int, default=20)
+    ap.add_argument("--only", default=None,
+                    help="comma-separated load balances to re-tune; the other entries are kept from --out")
     args = ap.parse_args(argv)
+    only = set(args.only.split(",")) if args.only else None
     ctx = gs.Context(0)
     graphs = []
     for g in (ctx.rmat(args.scale, 16, seed=11), ctx.grid(1024, 1024, 100, seed=12),
               ctx.er(1 << args.scale, 8 << args.scale, seed=13)):
         graphs.append((g, g.roots(5, 3)))
-    table, shapes, report = tune(ctx, graphs, log=lambda m: print(m, file=sys.stderr, flush=True))
+    table, shapes, report = tune(ctx, graphs, log=lambda m: print(m, file=sys.stderr, flush=True), only=only)
+    if only and os.path.exists(args.out):
+        old = json.load(open(args.out))
+        keep = [i for d, f, lb, fused in VARIANTS if lb not in only
+                for i in [gs.Context.tune_index(d, f, lb, fused)]]
+        for i in keep:
+            table[i] = old["quarters"][i]
+            shapes[i] = old.get("shapes", [0] * gs.TUNE_ENTRIES)[i]
+        report = {**{k: v for k, v in old.get("report", {}).items() if k.split("-")[2] not in only}, **report}
     os.makedirs(os.path.dirname(args.out), exist_ok=True)
     with open(args.out, "w") as f:
         json.dump({"format": "gswitch_b200 expand grid caps, quarters of the resident grid, and shapes (STRICT "
-                             "tile, thread-mapped pull candidates per thread), "
+                             "tile, thread-mapped CTA size and pull candidates per thread), "
                              "index ((pull*2+bitmap)*8+lb)*2+fused", "quarters": [int(x) for x in table],
                    "shapes": [int(x) for x in shapes],
                    "graphs": [f"rmat{args.scale}", "grid1024x1024_lr100", f"er2^{args.scale}"], "report": report}, f,
                   indent=0)
-    print(json.dumps({k: [v["shape"], v["quarters"]] for k, v in report.items()}))
+    print(json.dumps({k: [v.get("shape", 0), v.get("quarters")] for k, v in report.items()}))
     ctx.close()
 
 

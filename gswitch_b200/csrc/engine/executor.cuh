@@ -491,13 +491,16 @@ struct selector_t {
 // ===========================================================================
 constexpr int STRICT_TILE_MIN = 512;
 constexpr int STRICT_SHAPES = 3;   // tile 1024 (default), 512, 2048
-constexpr int PULL_TM_SHAPES = 3;  // candidates per thread: 2 (default), 1, 4
+constexpr int PUSH_TM_SHAPES = 3;  // threads per CTA: 256 (default), 128, 512
+constexpr int PULL_TM_SHAPES = 9;  // candidates per thread 2 (default), 1, 4, times those CTA sizes
 inline int strict_tile_of(int shape) { return shape == 1 ? 512 : (shape == 2 ? 2048 : STRICT_TILE); }
-inline int pull_tm_k_of(int shape) { return shape == 1 ? 1 : (shape == 2 ? 4 : 2); }
+inline int pull_tm_k_of(int shape) { return shape % 3 == 1 ? 1 : (shape % 3 == 2 ? 4 : 2); }
+// thread-mapped variants: threads per CTA (push: of the shape, pull: of shape / 3)
+inline int tm_threads_of(int cta_shape) { return cta_shape == 1 ? 128 : (cta_shape == 2 ? 512 : EXPAND_THREADS); }
 // shapes a variant may take (1: none but the default)
 inline int shape_count(bool pull, int lb) {
   if (lb == STRICT) return STRICT_SHAPES;
-  if (pull && lb == TM) return PULL_TM_SHAPES;
+  if (lb == TM) return pull ? PULL_TM_SHAPES : PUSH_TM_SHAPES;
   return 1;
 }
 
@@ -693,6 +696,13 @@ struct executor_t {
       const int cap = tq > 0 ? (int)MAX((int64_t)1, (int64_t)res * tq / 4) : res;
       return want < 0 ? cap : clamp_grid(want, cap);
     };
+    // the same for a kernel launched with bt threads per CTA
+    auto grid_for_bt = [&](auto kern, int64_t want, int bt) {
+      const int res = resident_grid(kern, bt);
+      if (fg > 0) return fg;
+      const int cap = tq > 0 ? (int)MAX((int64_t)1, (int64_t)res * tq / 4) : res;
+      return want < 0 ? cap : clamp_grid(want, cap);
+    };
 #define GSW_GO(kern, want, ...)                                   \
   do {                                                            \
     auto _k = kern;                                               \
@@ -717,8 +727,19 @@ struct executor_t {
     if (conf.conf_dir == Push) {
       switch (conf.conf_lb) {
         case TM:
-          if (fused) GSW_GO((k_push_tm<true, G, F>), fr < 0 ? -1 : fr / B + 1, as, g, f, conf);
-          else GSW_GO((k_push_tm<false, G, F>), fr < 0 ? -1 : fr / B + 1, as, g, f, conf);
+        {
+          // thread-mapped: the tuned CTA size (BT threads)
+          auto go = [&](auto bt) {
+            constexpr int BT = decltype(bt)::value;
+            auto k = fused ? k_push_tm<true, BT, G, F> : k_push_tm<false, BT, G, F>;
+            k<<<grid_for_bt(k, fr < 0 ? -1 : fr / BT + 1, BT), BT, 0, stream()>>>(as, g, f, conf);
+          };
+          switch (tm_threads_of(shape)) {
+            case 128: go(std::integral_constant<int, 128>{}); break;
+            case 512: go(std::integral_constant<int, 512>{}); break;
+            default: go(std::integral_constant<int, EXPAND_THREADS>{}); break;
+          }
+        }
           break;
         case CM:
           {
@@ -800,13 +821,24 @@ struct executor_t {
         }
         case TM:
         default: {
-          const int k = pull_tm_k_of(shape);
-          if (k == 1)
-            GSW_GO((k_pull_tm<1, G, F>), fr < 0 ? -1 : fr / B + 1, as, g, f, conf);
-          else if (k == 4)
-            GSW_GO((k_pull_tm<4, G, F>), fr < 0 ? -1 : fr / B + 1, as, g, f, conf);
-          else
-            GSW_GO((k_pull_tm<2, G, F>), fr < 0 ? -1 : fr / B + 1, as, g, f, conf);
+          // K candidates per thread and BT threads per CTA, as tuned
+          auto go = [&](auto kc, auto bt) {
+            constexpr int K = decltype(kc)::value, BT = decltype(bt)::value;
+            auto kern = k_pull_tm<K, BT, G, F>;
+            kern<<<grid_for_bt(kern, fr < 0 ? -1 : fr / BT + 1, BT), BT, 0, stream()>>>(as, g, f, conf);
+          };
+          auto with_k = [&](auto bt) {
+            switch (pull_tm_k_of(shape)) {
+              case 1: go(std::integral_constant<int, 1>{}, bt); break;
+              case 4: go(std::integral_constant<int, 4>{}, bt); break;
+              default: go(std::integral_constant<int, 2>{}, bt); break;
+            }
+          };
+          switch (tm_threads_of(shape / 3)) {
+            case 128: with_k(std::integral_constant<int, 128>{}); break;
+            case 512: with_k(std::integral_constant<int, 512>{}); break;
+            default: with_k(std::integral_constant<int, EXPAND_THREADS>{}); break;
+          }
           break;
         }
       }

@@ -193,15 +193,16 @@ __device__ __forceinline__ void push_tm_fused_body(active_set_t &as, const G &g,
   account(as, conf, cnt);
 }
 
-template <bool FUSED, typename G, typename F>
-__global__ void __launch_bounds__(EXPAND_THREADS) k_push_tm(active_set_t as, G g, F f, config_t conf) {
+// BT: threads per CTA (a tuned shape: 128, 256 or 512)
+template <bool FUSED, int BT, typename G, typename F>
+__global__ void __launch_bounds__(BT) k_push_tm(active_set_t as, G g, F f, config_t conf) {
   const int64_t n = as.get_size();
   GSW_HALT_IF_EMPTY(n);
   const Status want = conf.want();
   const int64_t STRIDE = (int64_t)blockDim.x * gridDim.x;
   unsigned long long cnt = 0;
   if constexpr (FUSED) {
-    __shared__ int s_stage[EXPAND_THREADS / 32][STAGE_SLOTS];
+    __shared__ int s_stage[BT / 32][STAGE_SLOTS];
     warp_stage_t stage(s_stage[warp_id()], as);
     push_tm_fused_body(as, g, f, conf, as_src_t{&as, want}, n, stage);
     stage.flush();
@@ -231,9 +232,10 @@ __global__ void __launch_bounds__(EXPAND_THREADS) k_push_tm(active_set_t as, G g
 // warp-cooperative walk of the unresolved candidates, a first-in-neighbour
 // side array (less DRAM traffic, no faster), skipping vertices without
 // in-edges by a bitmap, and capping thread walks at 8 edges with 8-lane
-// groups finishing the rest (40 registers, 75% occupancy, slower).
-template <int K, typename G, typename F>
-__global__ void __launch_bounds__(EXPAND_THREADS) k_pull_tm(active_set_t as, G g, F f, config_t conf) {
+// groups finishing the rest (40 registers, 75% occupancy, slower).  BT:
+// threads per CTA (a tuned shape together with K: 128, 256 or 512).
+template <int K, int BT, typename G, typename F>
+__global__ void __launch_bounds__(BT) k_pull_tm(active_set_t as, G g, F f, config_t conf) {
   using WA = typename F::wa_t;
   const int64_t n = as.get_size();
   GSW_HALT_IF_EMPTY(n);

@@ -347,9 +347,11 @@ gsw_status gsw_mlp_load_fusion(gsw_ctx *ctx, const float *model, float min_conf)
 gsw_status gsw_tune_load(gsw_ctx *ctx, const int32_t *quarters); /* NULL: defaults */
 gsw_status gsw_tune_save(gsw_ctx *ctx, int32_t *quarters);
 /* Tuned shapes, same indexing (0 = default everywhere): the STRICT variants'
- * tile (0: 1,024 slots, 1: 512, 2: 2,048; from-all pulls use at most 1,024)
- * and the thread-mapped pull's candidates per thread (0: 2, 1: 1, 2: 4);
- * every other variant takes 0 only.  The reference fixes these in THDNUM / SCRATH
+ * tile (0: 1,024 slots, 1: 512, 2: 2,048; from-all pulls use at most 1,024);
+ * the thread-mapped push's threads per CTA (0: 256, 1: 128, 2: 512); the
+ * thread-mapped pull's candidates per thread (shape % 3 -- 0: 2, 1: 1, 2: 4)
+ * and threads per CTA (shape / 3, as for the push), shapes 0..8; every other
+ * variant takes 0 only.  The reference fixes these in THDNUM / SCRATH
  * (src/utils/common.cuh:12-24); NULL restores the defaults. */
 gsw_status gsw_tune_load_shapes(gsw_ctx *ctx, const int32_t *shapes);
 gsw_status gsw_tune_save_shapes(gsw_ctx *ctx, int32_t *shapes);

@@ -52,15 +52,17 @@ def test_committed_table_is_well_formed():
 
 
 def test_shape_table_round_trip_and_validation(ctx):
-    """Shapes exist only for the STRICT variants (3 tiles) and the thread-mapped
-    pull (3 candidates-per-thread counts); anything else is rejected."""
+    """Shapes exist only for the STRICT variants (3 tiles), the thread-mapped
+    push (3 CTA sizes) and the thread-mapped pull (3 candidates-per-thread
+    counts x 3 CTA sizes); anything else is rejected."""
     s = np.zeros(gs.TUNE_ENTRIES, dtype=np.int32)
     s[gs.Context.tune_index("Push", "Queue", "STRICT")] = 2
-    s[gs.Context.tune_index("Pull", "Bitmap", "TM")] = 2
+    s[gs.Context.tune_index("Pull", "Bitmap", "TM")] = 8
+    s[gs.Context.tune_index("Push", "Queue", "TM", True)] = 2
     ctx.tune_load_shapes(s)
     assert np.array_equal(ctx.tune_save_shapes(), s)
     for bad in ((gs.Context.tune_index("Push", "Queue", "WM"), 1), (gs.Context.tune_index("Pull", "Bitmap", "STRICT"), 3),
-                (gs.Context.tune_index("Pull", "Bitmap", "TM"), 3)):
+                (gs.Context.tune_index("Pull", "Bitmap", "TM"), 9), (gs.Context.tune_index("Push", "Bitmap", "TM"), 3)):
         b = s.copy()
         b[bad[0]] = bad[1]
         with pytest.raises(gs.GswError):
@@ -69,10 +71,10 @@ def test_shape_table_round_trip_and_validation(ctx):
     assert not ctx.tune_save_shapes().any()
 
 
-@pytest.mark.parametrize("shape", [1, 2])
+@pytest.mark.parametrize("shape", [1, 2, 3, 4, 5, 6, 7, 8])
 def test_results_exact_under_every_shape(ctx, shape):
-    """Every STRICT tile and every pull candidates-per-thread count gives the
-    oracle's BFS, SSSP and PageRank."""
+    """Every STRICT tile, every thread-mapped CTA size and every pull
+    candidates-per-thread count gives the oracle's BFS, SSSP and PageRank."""
     h = oracle.rmat(14, 16, seed=7)
     hw = oracle.add_weights(h, 3, 64)
     root = int(oracle.roots(h, 4, 1)[0])
@@ -82,13 +84,14 @@ def test_results_exact_under_every_shape(ctx, shape):
     for d in ("Push", "Pull"):
         for f in ("Queue", "Bitmap"):
             for fused in ((False, True) if d == "Push" else (False,)):
-                s[gs.Context.tune_index(d, f, "STRICT", fused)] = shape
+                s[gs.Context.tune_index(d, f, "STRICT", fused)] = shape % 3
+                s[gs.Context.tune_index("Push", f, "TM", fused)] = shape % 3
             s[gs.Context.tune_index("Pull", f, "TM")] = shape
     ctx.tune_load_shapes(s)
     try:
         ref, dref = oracle.bfs(h, root), oracle.sssp_dijkstra(hw, root)
         for cfg in ["Push-Queue-STRICT", "Pull-Bitmap-STRICT", "Push-Queue-STRICT-Fused", "Pull-Bitmap-TM",
-                    "Pull-Queue-TM", ""]:
+                    "Pull-Queue-TM", "Push-Queue-TM", "Push-Bitmap-TM", "Push-Queue-TM-Fused", ""]:
             lv, _ = gu.bfs(root, gs.RunOpts.from_config(cfg, persistent=False))
             assert np.array_equal(lv, ref), (shape, cfg)
             d, _ = g.sssp(root, gs.RunOpts.from_config(cfg, persistent=False))
