@@ -726,6 +726,7 @@ def run_reference(args):
 PROFILE_CASES = {
     "bfs": "three BFS runs on RMAT scale 22 (ef 16, seed 1), learned selector",
     "bfs24": "one BFS on RMAT scale 24 (ef 16, seed 1: the bench graph), learned selector",
+    "bfs24cap": "one BFS on the bench graph, learned selector, through the captured level loop",
     "sssp": "SSSP on the 4096 x 4096 grid with 1% long-range edges (weights U[1, 1000]), "
             "Push-Queue-WM-Fused levels one launch each",
     "pr": "two PageRank iterations on RMAT scale 22, Pull-Bitmap-STRICT then 2D",
@@ -754,9 +755,9 @@ def run_case(case: str) -> None:
         g = ctx.rmat(22, 16, seed=1)
         for r in g.roots(1000, 3):
             g.bfs(int(r), gs.RunOpts(selector="mlp"), out=False)
-    elif case == "bfs24":
+    elif case in ("bfs24", "bfs24cap"):
         g = ctx.rmat(24, 16, seed=1)
-        g.bfs(int(g.roots(1000, 1)[0]), gs.RunOpts(selector="mlp"), out=False)
+        g.bfs(int(g.roots(1000, 1)[0]), gs.RunOpts(selector="mlp", captured=case == "bfs24cap"), out=False)
     elif case == "sssp":
         g = ctx.grid(4096, 4096, 100, seed=1, wmax=1000, wseed=5)
         o = gs.RunOpts.from_config("Push-Queue-WM-Fused")

@@ -27,7 +27,13 @@
 // levels run one launch per level (never the cooperative multi-level kernel,
 // whose early exit needs a host decision), and the wall-clock rule that
 // returns a slow fused level to the standalone form (executor.cuh:128-131)
-// does not apply.
+// does not apply.  With persistent launches on (the default), a fused
+// push-queue body is the host loop's persistent launch: the multi-level
+// cooperative kernel, then k_dl_persist_commit, which advances the level,
+// the iteration count and the queue cursor by the levels it ran, halts the
+// loop on an empty frontier, and otherwise returns it to inspected levels --
+// that iteration's inspection always runs after such a body (it skips itself
+// once the loop has halted).
 #pragma once
 #include <vector>
 
@@ -73,6 +79,10 @@ struct dloop_t {
   int *trace_cfg;
   long long *trace_frontier;
   long long *trace_edges;
+  // globaltimer (ns) at the start of each iteration's decision ([i]: level i
+  // begins, level i-1 ends) and after it ([i]: the decision of level i took
+  // trace_sel[i] - trace_t[i]); trace_cap + 1 entries each
+  long long *trace_t, *trace_sel;
   unsigned long long *info;     // the inspector's statistics block
   unsigned long long *scanned;  // accounting counter (null: not counting)
   int *qsize;                   // the Normal queue's two size words
@@ -84,6 +94,8 @@ struct dloop_t {
   int filter_kernels[DL_FILTER_BODIES];
   int inspect_kernels;
   int n_expand_bodies;
+  int persist_fused;            // fused push-queue bodies are persistent launches
+  int pad_;
   cudaGraphConditionalHandle h_loop, h_filter, h_expand, h_inspect;
   // stepping window of Mono patterns (SSSP): the kernels read `win` through
   // vdata_t::dwin; when a level finds no input the probe body (the deferred
@@ -225,6 +237,11 @@ __device__ inline void dl_commit(dloop_t &d) {
   conf.conf_first_round = false;
   d.iter++;
   d.inspected = !conf.conf_fuse_inspect;
+  if (conf.conf_fuse_inspect && d.persist_fused && conf.conf_dir == Push && conf.conf_asfmt == Queue) {
+    // a persistent body: its inspection runs after it (see k_dl_persist_commit)
+    d.inspected = 1;
+    if (d.ntrace - 1 < d.trace_cap) d.trace_cfg[d.ntrace - 1] |= 1 << 6;
+  }
   d.launches += 1 + (fbody < DL_FILTER_BODIES ? d.filter_kernels[fbody] : 0) + d.expand_kernels[ebody] +
                 (d.inspected ? d.inspect_kernels : 0);
   cudaGraphSetConditional(d.h_filter, fbody);
@@ -233,6 +250,31 @@ __device__ inline void dl_commit(dloop_t &d) {
   // the window the next inspection and expand read (the host loop adjusts it
   // at the start of its next inspection, from the same features)
   if (d.window_on) d.win.adjust_with(fets, conf, d.stepping);
+}
+
+// After a persistent body (prep, the cooperative multi-level kernel): the
+// launch ran L levels, the first of them the one this iteration committed;
+// its last output sits in the queue slot out = cur ^ (L & 1), where the next
+// level's swap expects it.  An empty frontier halts the loop; any other exit
+// returns it to inspected (standalone) levels, as the host loop does after a
+// frontier grew past its limit; a barrier timeout or a scan overflow (in the
+// error word) halts it too.
+__global__ void k_dl_persist_commit(dloop_t *d, as_counters_t *c, int cur) {
+  const int L = c->plevels, reason = c->preason;
+  if (L > 1) {
+    d->level += L - 1;
+    d->iter += L - 1;
+  }
+  d->cursor = (cur ^ (L & 1)) ^ 1;
+  if (d->ntrace - 1 >= 0 && d->ntrace - 1 < d->trace_cap)
+    d->trace_cfg[d->ntrace - 1] = (d->trace_cfg[d->ntrace - 1] & ~(7 << 2)) | ((c->plb & 7) << 2);
+  d->conf.conf_fuse_inspect = false;
+  if (reason == 0 || reason == 3 || reason == 4 || reason < 0) {
+    d->halt = 1;
+  } else {
+    c->qsize[0] = 0;  // the next level builds its queue from the bitmaps
+    c->qsize[1] = 0;
+  }
 }
 
 // The decision thread works on a shared-memory copy of the loop state and of
@@ -253,6 +295,7 @@ __global__ void __launch_bounds__(256) k_dl_select(dloop_t *d) {
   const unsigned long long *src = reinterpret_cast<const unsigned long long *>(d);
   for (int i = threadIdx.x; i < WORDS; i += blockDim.x) s_state[i] = src[i];
   if (threadIdx.x == 0) {
+    if (d->trace_t) d->trace_t[min(d->ntrace, d->trace_cap)] = (long long)globaltimer_ns();
     const unsigned long long *info = d->info;
     s_c.active = (int64_t)info[0];
     s_c.inactive = (int64_t)info[1];
@@ -263,9 +306,28 @@ __global__ void __launch_bounds__(256) k_dl_select(dloop_t *d) {
     s_scanned = d->scanned ? *d->scanned : 0ull;
   }
   __syncthreads();
+  // the trees (about 32 KB) in 16-byte loads, all of a thread's issued
+  // before its stores: one L2 round trip instead of one per loop step
   const int tree_words = min(sd.tree_nodes, DL_MAX_TREE_NODES) * (int)(sizeof(tree_node) / 8);
   const unsigned long long *tsrc = reinterpret_cast<const unsigned long long *>(sd.tree_base);
-  for (int i = threadIdx.x; i < tree_words; i += blockDim.x) s_tree[i] = __ldg(tsrc + i);
+  {
+    constexpr int PER = (DL_MAX_TREE_NODES * (int)sizeof(tree_node) / 16 + 255) / 256;  // int4 per thread
+    const int n4 = tree_words / 2;
+    const int4 *s4 = reinterpret_cast<const int4 *>(tsrc);
+    int4 *d4 = reinterpret_cast<int4 *>(s_tree);
+    int4 r[PER];
+#pragma unroll
+    for (int k = 0; k < PER; ++k) {
+      const int i = threadIdx.x + k * 256;
+      if (i < n4) r[k] = __ldg(s4 + i);
+    }
+#pragma unroll
+    for (int k = 0; k < PER; ++k) {
+      const int i = threadIdx.x + k * 256;
+      if (i < n4) d4[i] = r[k];
+    }
+    if (threadIdx.x == 0 && (tree_words & 1)) s_tree[tree_words - 1] = __ldg(tsrc + tree_words - 1);
+  }
   // the counters start from zero for the next inspection
   for (int i = threadIdx.x; i < STAT_SLOTS; i += blockDim.x) sd.info[i] = 0;
   __syncthreads();
@@ -297,6 +359,8 @@ __global__ void __launch_bounds__(256) k_dl_select(dloop_t *d) {
   }
   __syncthreads();
   if (threadIdx.x == 0 && s_go) dl_commit(sd);
+  if (threadIdx.x == 0 && sd.trace_sel && s_go && sd.ntrace - 1 < sd.trace_cap)
+    sd.trace_sel[sd.ntrace - 1] = (long long)globaltimer_ns();
   __syncthreads();
   unsigned long long *dst = reinterpret_cast<unsigned long long *>(d);
   for (int i = threadIdx.x; i < WORDS; i += blockDim.x) dst[i] = s_state[i];
@@ -342,6 +406,57 @@ inline bool dl_capture(cudaGraph_t body, L &&launch) {
   return good && ok();
 }
 
+// The persistent body of a fused push-queue variant: the host loop's
+// persistent launch (executor_t::launch_persistent_lb) without its host
+// side -- the results go to k_dl_persist_commit instead of the host.
+template <int LB, typename G, typename F>
+void dl_persistent_lb(executor_t &ex, active_set_t &as, G &g, F &f, config_t &conf, const feature_t &fets, dloop_t *d,
+                      int cur) {
+  auto kern = k_fused_persistent<LB, G, F>;
+  const int grid = resident_grid(kern, EXPAND_THREADS);
+  if (LB == STRICT && grid > as.workset.bsum_cap)
+    return (void)set_error(GSW_ERR_OVERFLOW, "persistent strict: %s", "block sums");
+  as_counters_t *c = as.dg_cnt;
+  k_persist_prep<<<1, 1, 0, stream()>>>(c, cur);
+  persist_state ps;
+  ps.q[0] = as.queue.subqueue[cur].dg_queue;
+  ps.q[1] = as.queue.subqueue[cur ^ 1].dg_queue;
+  ps.cnt = c->pq;
+  ps.cap = as.queue.subqueue[0].max_size;
+  ps.grow_limit = fets.pattern == Idem ? (int)MAX((int64_t)4096, as.size / 64) : INT32_MAX;
+  ps.max_levels = (int)MIN(as.size + 2, (int64_t)(1 << 24));
+  ps.budget_ns = 2000000000ull;
+  ps.leave_block = -1;
+  ps.levels_done = &c->plevels;
+  ps.exit_reason = &c->preason;
+  ps.lb_out = &c->plb;
+  ps.cur = cur;
+  ps.level0 = &d->level;
+  ps.sig = nullptr;
+  ps.seq = 0;
+  ps.eoff = as.workset.dg_eoff;
+  ps.eoff_cap = as.size + 2;
+  ps.bsum = as.workset.dg_bsum;
+  ps.tile_lo = ex.dg_tile;
+  ps.tile_cap = ex.tile_cap;
+  void *args[] = {(void *)&as, (void *)&g, (void *)&f, (void *)&conf, (void *)&ps};
+  if (GSW_CUDA(cudaLaunchCooperativeKernel((const void *)kern, grid, EXPAND_THREADS, args, 0, stream()))) return;
+  k_dl_persist_commit<<<1, 1, 0, stream()>>>(d, c, cur);
+  GSW_LAUNCHED();
+}
+template <typename E, typename F>
+void dl_persistent_body(executor_t &ex, active_set_t &as, device_graph_t<CSR, E> &g, F &f, config_t &conf,
+                        const feature_t &fets, dloop_t *d, int cur) {
+  using G = device_graph_t<CSR, E>;
+  switch (conf.conf_lb) {
+    case TM: return dl_persistent_lb<TM, G, F>(ex, as, g, f, conf, fets, d, cur);
+    case CM: return dl_persistent_lb<CM, G, F>(ex, as, g, f, conf, fets, d, cur);
+    case STRICT: return dl_persistent_lb<STRICT, G, F>(ex, as, g, f, conf, fets, d, cur);
+    case TWC: return dl_persistent_lb<TWC, G, F>(ex, as, g, f, conf, fets, d, cur);
+    default: return dl_persistent_lb<WM, G, F>(ex, as, g, f, conf, fets, d, cur);
+  }
+}
+
 // A built loop: the executable graph plus what the host needs to drive it.
 struct dloop_graph {
   cudaGraph_t graph = nullptr;
@@ -371,6 +486,7 @@ bool dl_build(dloop_graph &L, executor_t &ex, dloop_t *d, active_set_t as, devic
   as.nt.dg_tag = &d->halt;
   as.nt.already = false;
   as.queue.traceback = false;
+  const bool persist = conf.conf_persistent && as.queue.mode == Normal;
   conf.conf_persistent = false;
   const bool saved_timing = opts().timing;
   opts().timing = false;
@@ -382,6 +498,7 @@ bool dl_build(dloop_graph &L, executor_t &ex, dloop_t *d, active_set_t as, devic
   ex.ensure_tiles(g.nedges + as.size + 1);
   dloop_t &im = L.image;
   im = dloop_t();
+  im.persist_fused = persist ? 1 : 0;
   for (int &b : im.variant_body) b = -1;
   bool good = ok();
   // the variants this run can reach
@@ -484,7 +601,10 @@ bool dl_build(dloop_graph &L, executor_t &ex, dloop_t *d, active_set_t as, devic
       a.queue.cursor = cur;
       G gg = g;
       const int b = (int)i * 2 + cur;
-      good = dl_capture(ebodies[b], [&] { ex.launch_vc(a, gg, f, c); });
+      if (persist && v.fused && v.d == Push && v.a == Queue)
+        good = dl_capture(ebodies[b], [&] { dl_persistent_body(ex, a, gg, f, c, fets, d, cur); });
+      else
+        good = dl_capture(ebodies[b], [&] { ex.launch_vc(a, gg, f, c); });
       im.expand_kernels[b] = dl_count_nodes(ebodies[b]);
     }
   // inspection body

@@ -670,6 +670,13 @@ struct executor_t {
     if (nb == 1 && hints().frontier >= 0) {
       // a frontier known to fit one scan block: one launch, no block sums
       k_strict_scan<PULL, T><<<1, 256, 0, stream()>>>(as, g, want, nullptr, 1, dg_tile, tile_cap);
+    } else if (hints().frontier < 0) {
+      // a frontier only the device knows (fused levels, captured loops): a
+      // fixed grid over its own number of scan blocks, not the capacity's
+      const int grid = (int)MIN(nb, (int64_t)sm_count() * 8);
+      k_strict_count<PULL><<<grid, 256, 0, stream()>>>(as, g, want, as.workset.dg_bsum);
+      k_strict_bsum_scan<<<1, 1024, 0, stream()>>>(as, as.workset.dg_bsum);
+      k_strict_scan<PULL, T><<<grid, 256, 0, stream()>>>(as, g, want, as.workset.dg_bsum, -1, dg_tile, tile_cap);
     } else {
       k_strict_count<PULL><<<(unsigned)nb, 256, 0, stream()>>>(as, g, want, as.workset.dg_bsum);
       k_scan_single_block<<<1, 1024, 0, stream()>>>(as.workset.dg_bsum, nb);
@@ -893,6 +900,7 @@ struct executor_t {
     ps.exit_reason = &c->preason;
     ps.lb_out = &c->plb;
     ps.cur = cur;
+    ps.level0 = nullptr;
     if (!h_psig) {
       // without the mapped block the launch reports through a copy-back
       if (cudaHostAlloc((void **)&h_psig, 4 * sizeof(unsigned long long), cudaHostAllocMapped) == cudaSuccess) {

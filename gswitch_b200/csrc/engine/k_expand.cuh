@@ -611,24 +611,51 @@ template <bool PULL, typename G>
 __global__ void __launch_bounds__(256) k_strict_count(active_set_t as, G g, Status want, int64_t *bsum) {
   __shared__ int64_t s_red[32];
   const int64_t n = as.get_size();
-  const int64_t b0 = (int64_t)blockIdx.x * STRICT_ITEMS;
-  int64_t s = 0;
-  for (int k = threadIdx.x; k < STRICT_ITEMS; k += blockDim.x) {
-    const int64_t idx = b0 + k;
-    if (idx < n) s += strict_slots<PULL>(as, g, idx, want);
+  // scan blocks blk = blockIdx.x, + gridDim.x, ... of the frontier's n / STRICT_ITEMS + 1
+  // (a launch of that many CTAs takes one each; a captured body, which cannot
+  // know n, launches a fixed grid)
+  // (every CTA of the launch writes its first sum, zero past the frontier, so
+  // a host-sized scan of the sums never reads a stale one)
+  const int64_t nb = MAX(n / STRICT_ITEMS + 1, (int64_t)gridDim.x);
+  for (int64_t blk = blockIdx.x; blk < nb; blk += gridDim.x) {
+    const int64_t b0 = blk * STRICT_ITEMS;
+    int64_t s = 0;
+    for (int k = threadIdx.x; k < STRICT_ITEMS; k += blockDim.x) {
+      const int64_t idx = b0 + k;
+      if (idx < n) s += strict_slots<PULL>(as, g, idx, want);
+    }
+    s = block_reduce(s, s_red);
+    if (threadIdx.x == 0) bsum[blk] = s;
   }
-  s = block_reduce(s, s_red);
-  if (threadIdx.x == 0) bsum[blockIdx.x] = s;
 }
 
 // eoff[idx] = exclusive scan of (degree+1); tile_lo[t] = frontier index that
 // owns slot t*STRICT_TILE.  Each thread scans 4 consecutive entries.
 template <bool PULL, int T, typename G>
+__device__ __forceinline__ void strict_scan_block(active_set_t &as, const G &g, Status want, const int64_t *bsum,
+                                                  int64_t nblocks, int *tile_lo, int64_t tile_cap, int64_t blk,
+                                                  int64_t n, int64_t *s);
+// the block sums of a frontier whose size only the device knows
+__global__ void __launch_bounds__(1024) k_strict_bsum_scan(active_set_t as, int64_t *bsum) {
+  scan_single_block_body(bsum, as.get_size() / STRICT_ITEMS + 1);
+}
+template <bool PULL, int T, typename G>
 __global__ void __launch_bounds__(256) k_strict_scan(active_set_t as, G g, Status want, const int64_t *bsum,
                                                      int64_t nblocks, int *tile_lo, int64_t tile_cap) {
   __shared__ int64_t s[33];
   const int64_t n = as.get_size();
-  const int64_t base = (int64_t)blockIdx.x * STRICT_ITEMS + threadIdx.x * 4;
+  // scan blocks as in k_strict_count; nblocks < 0: the frontier's own count
+  const int64_t nb = bsum ? (nblocks >= 0 ? nblocks : n / STRICT_ITEMS + 1) : 1;
+  for (int64_t blk = blockIdx.x; blk < nb; blk += gridDim.x) {
+    strict_scan_block<PULL, T>(as, g, want, bsum, nb, tile_lo, tile_cap, blk, n, s);
+    __syncthreads();  // s is reused by the next block
+  }
+}
+template <bool PULL, int T, typename G>
+__device__ __forceinline__ void strict_scan_block(active_set_t &as, const G &g, Status want, const int64_t *bsum,
+                                                  int64_t nblocks, int *tile_lo, int64_t tile_cap, int64_t blk,
+                                                  int64_t n, int64_t *s) {
+  const int64_t base = blk * STRICT_ITEMS + threadIdx.x * 4;
   int64_t d[4], loc = 0;
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
@@ -647,10 +674,10 @@ __global__ void __launch_bounds__(256) k_strict_scan(active_set_t as, G g, Statu
   }
   __syncthreads();
   // bsum == nullptr: the whole frontier is this one block (no block sums)
-  const int64_t off = (bsum ? bsum[blockIdx.x] : 0) + s[warp_id()] + incl - loc;
+  const int64_t off = (bsum ? bsum[blk] : 0) + s[warp_id()] + incl - loc;
   int64_t *eoff = as.workset.dg_eoff;
   strict_scan_epilogue<T>(as, base, n, d, off, eoff, tile_lo, tile_cap);
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
+  if (blk == 0 && threadIdx.x == 0) {
     const int64_t total = bsum ? bsum[nblocks] : s[32];
     eoff[n] = total;
     as.dg_cnt->total_edges = (unsigned long long)total;

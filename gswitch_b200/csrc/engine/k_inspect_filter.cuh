@@ -348,7 +348,7 @@ __global__ void __launch_bounds__(FILTER_WORDS) k_filter_count(active_set_t as, 
 }
 
 // In-place exclusive scan of a[0..len) by one block; a[len] receives the total.
-__global__ void __launch_bounds__(1024) k_scan_single_block(int64_t *a, int64_t len) {
+__device__ __forceinline__ void scan_single_block_body(int64_t *a, int64_t len) {
   __shared__ int64_t s[33];
   int64_t carry = 0;
   for (int64_t base = 0; base < len; base += blockDim.x) {
@@ -372,6 +372,7 @@ __global__ void __launch_bounds__(1024) k_scan_single_block(int64_t *a, int64_t 
   }
   if (threadIdx.x == 0) a[len] = carry;
 }
+__global__ void __launch_bounds__(1024) k_scan_single_block(int64_t *a, int64_t len) { scan_single_block_body(a, len); }
 
 __global__ void __launch_bounds__(FILTER_WORDS) k_filter_write(active_set_t as, Status want, const int64_t *bsum,
                                                                int64_t nblocks) {

@@ -35,6 +35,8 @@ struct persist_state {
                         // timeout, 4 STRICT scan capacity exceeded
   int *lb_out;          // out: the kernel's load balance (LB value)
   int cur;              // the Normal queue's input cursor at the launch
+  const int *level0;    // captured loops: the first level's number, read at
+                        // the start (null: the graph view's own level)
   // zero-copy report (mapped pinned, 3 words: levels, reason + 1, LB), each
   // word tagged with `seq` in its top 24 bits; null: the host copies back
   unsigned long long *sig;
@@ -168,6 +170,10 @@ __global__ void __launch_bounds__(EXPAND_THREADS) k_fused_persistent(active_set_
   unsigned gen = 0;
   int L = 0;
   int reason = 2;
+  if (ps.level0) {  // the levels advance in this launch's own copy
+    g.level = *(volatile const int *)ps.level0;
+    g.dlevel = nullptr;
+  }
   for (; L < ps.max_levels; ++L) {
     const int n = ((volatile int *)ps.cnt)[L % 3];
     if (n == 0) {

@@ -877,7 +877,7 @@ struct dl_run {
   dloop_graph *L = nullptr;
   dloop_t *d = nullptr;
   int *trace_cfg = nullptr;
-  long long *trace_frontier = nullptr, *trace_edges = nullptr;
+  long long *trace_frontier = nullptr, *trace_edges = nullptr, *trace_t = nullptr, *trace_sel = nullptr;
   dloop_t image;
   unsigned long long push_sum = 0;  // after dl_collect: the loop's push workload
 };
@@ -893,7 +893,10 @@ bool dl_prepare(dl_run &R, gsw_ctx *ctx, int app, dl_key key, active_set_t &as, 
   R.trace_cfg = (int *)ctx->buf("dl_trace_cfg", sizeof(int) * GSW_MAX_TRACE);
   R.trace_frontier = (long long *)ctx->buf("dl_trace_frontier", sizeof(long long) * GSW_MAX_TRACE);
   R.trace_edges = (long long *)ctx->buf("dl_trace_edges", sizeof(long long) * GSW_MAX_TRACE);
-  if (!trees || !R.d || !R.trace_cfg || !R.trace_frontier || !R.trace_edges) return false;
+  R.trace_t = (long long *)ctx->buf("dl_trace_t", sizeof(long long) * (GSW_MAX_TRACE + 1));
+  R.trace_sel = (long long *)ctx->buf("dl_trace_sel", sizeof(long long) * (GSW_MAX_TRACE + 1));
+  if (!trees || !R.d || !R.trace_cfg || !R.trace_frontier || !R.trace_edges || !R.trace_t || !R.trace_sel)
+    return false;
   executor_t &ex = ctx->executor;
   ex.ensure_tiles(g.nedges + as.size + 1);
   if (!ok()) return false;
@@ -904,7 +907,7 @@ bool dl_prepare(dl_run &R, gsw_ctx *ctx, int app, dl_key key, active_set_t &as, 
       << as.dg_cnt << as.workset.dg_eoff << as.workset.dg_bsum << as.workset.bsum_cap;
   key << conf.conf_pruning << conf.conf_count_edges << conf.conf_sorted_queue << fets.fromall << fets.toall
       << ex.dg_tile << ex.tile_cap << ex.twod.edge << opts().force_grid << ctx->stats.dg_runtime_info;
-  key << conf.conf_window << conf.conf_fusion << f.data.dg_ra;
+  key << conf.conf_window << conf.conf_fusion << f.data.dg_ra << conf.conf_persistent;
   for (int q : ex.tune.quarters[0][0][0]) key << q;  // first row: cheap change detector
   {
     const int *flat = &ex.tune.quarters[0][0][0][0];
@@ -943,6 +946,8 @@ bool dl_prepare(dl_run &R, gsw_ctx *ctx, int app, dl_key key, active_set_t &as, 
   im.trace_cfg = R.trace_cfg;
   im.trace_frontier = R.trace_frontier;
   im.trace_edges = R.trace_edges;
+  im.trace_t = R.trace_t;
+  im.trace_sel = R.trace_sel;
   im.info = ctx->stats.dg_runtime_info;
   im.scanned = conf.conf_count_edges ? &as.dg_cnt->scanned : nullptr;
   im.qsize = as.dg_cnt->qsize;
@@ -983,17 +988,22 @@ void dl_collect(dl_run &R, gsw_run_stats *st) {
   st->ntrace = nt;
   if (nt > 0) {
     std::vector<int> cfg(nt);
-    std::vector<long long> fr(nt), ed(nt);
+    std::vector<long long> fr(nt), ed(nt), t0(nt + 1), ts(nt);
     GSW_CUDA(cudaMemcpyAsync(cfg.data(), R.trace_cfg, sizeof(int) * nt, cudaMemcpyDeviceToHost, stream()));
     GSW_CUDA(cudaMemcpyAsync(fr.data(), R.trace_frontier, sizeof(long long) * nt, cudaMemcpyDeviceToHost, stream()));
     GSW_CUDA(cudaMemcpyAsync(ed.data(), R.trace_edges, sizeof(long long) * nt, cudaMemcpyDeviceToHost, stream()));
+    // iteration i: from its decision's start to the next one's (the final
+    // decision, which stops the loop, writes t0[nt])
+    const int nts = out.ntrace <= out.trace_cap && nt == out.ntrace ? nt + 1 : nt;
+    GSW_CUDA(cudaMemcpyAsync(t0.data(), R.trace_t, sizeof(long long) * nts, cudaMemcpyDeviceToHost, stream()));
+    GSW_CUDA(cudaMemcpyAsync(ts.data(), R.trace_sel, sizeof(long long) * nt, cudaMemcpyDeviceToHost, stream()));
     GSW_CUDA(cudaStreamSynchronize(stream()));
     for (int i = 0; i < nt; ++i) {
       st->level_cfg[i] = cfg[i];
       st->level_frontier[i] = fr[i];
       st->level_edges[i] = ed[i];
-      st->level_ms[i] = 0;
-      st->level_inspect_ms[i] = 0;
+      st->level_ms[i] = i + 1 < nts ? (float)((t0[i + 1] - t0[i]) * 1e-6) : 0.f;
+      st->level_inspect_ms[i] = (float)((ts[i] - t0[i]) * 1e-6);
     }
   }
 }

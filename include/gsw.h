@@ -172,8 +172,13 @@ typedef struct gsw_run_stats {
    * kernel reported back */
   int32_t level_cfg[GSW_MAX_TRACE];
   int64_t level_frontier[GSW_MAX_TRACE];
-  float level_ms[GSW_MAX_TRACE];         /* expand time, with opts.timing */
-  float level_inspect_ms[GSW_MAX_TRACE]; /* inspection time, with opts.timing */
+  float level_ms[GSW_MAX_TRACE];         /* expand time, with opts.timing; captured
+                                            loops: the whole iteration (decision,
+                                            queue build, expand, next inspection),
+                                            from device timestamps, always */
+  float level_inspect_ms[GSW_MAX_TRACE]; /* inspection time, with opts.timing;
+                                            captured loops: the device-side
+                                            decision (k_dl_select) of the level */
   int64_t level_edges[GSW_MAX_TRACE];    /* edges touched, with opts.account */
 } gsw_run_stats;
 

@@ -37,7 +37,14 @@ def test_captured_bfs_goldens_every_variant(ctx, name):
         lv, st = g.bfs(int(d["root"]), cap(cfg))
         assert np.array_equal(lv, d["lvl"]), (name, cfg)
         assert st.device_error == 0
-        assert st.levels == len(st.trace)
+        # one trace entry per level, except that a persistent launch of
+        # fused levels is one entry for all the levels it ran
+        if any(st.level_persistent):
+            assert st.levels >= len(st.trace)
+        else:
+            assert st.levels == len(st.trace)
+        _, host = g.bfs(int(d["root"]), gs.RunOpts.from_config(cfg))
+        assert st.levels == host.levels, (name, cfg)
 
 
 @pytest.mark.parametrize("name", ["rmat14", "grid64", "er20k"])
@@ -63,6 +70,32 @@ def test_captured_selector_takes_host_decisions(ctx, graphs, name):
         _, dev = g.bfs(root, cap(cfg))
         assert dev.trace == host.trace, (name, cfg)
         assert dev.levels == host.levels
+
+
+@pytest.mark.parametrize("name", ["rmat14", "er20k", "grid64"])
+def test_captured_persistent_fused_levels(ctx, graphs, name):
+    """Fused levels of the captured loop run as the host loop's persistent
+    launch (the cooperative multi-level kernel inside the graph): exact
+    results, the same levels and variants as the host loop, the persistent
+    entries reporting the load balance the kernel ran, and per-launch fused
+    levels when persistent launches are off."""
+    h, root = graphs[name]
+    g = ctx.upload(h.off, h.col)
+    ref = oracle.bfs(h, root)
+    for cfg in ["", "Push-Queue-WM-Fused", "Push-Queue-STRICT-Fused", "Push-Queue-TWC-Fused", "Push-Queue-CM-Fused"]:
+        _, host = g.bfs(root, gs.RunOpts.from_config(cfg))
+        for _ in range(2):
+            lv, st = g.bfs(root, cap(cfg))
+            assert np.array_equal(lv, ref), (name, cfg)
+            assert st.device_error == 0
+            assert st.levels == host.levels, (name, cfg, st.levels, host.levels)
+            assert [t[:4] for t in st.trace] == [t[:4] for t in host.trace], (name, cfg)
+            assert st.level_persistent == host.level_persistent, (name, cfg)
+        if cfg:
+            assert any(st.level_persistent), (name, cfg)
+        lv, st = g.bfs(root, cap(cfg, persistent=False))
+        assert np.array_equal(lv, ref), (name, cfg)
+        assert not any(st.level_persistent)
 
 
 def test_captured_graph_reused_across_roots_and_rebuilt_per_graph(ctx, graphs):
