@@ -72,6 +72,8 @@ struct gsw_graph {
 struct gsw_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
+  cudaStream_t upload_stream = nullptr;  // graph uploads: the column copy
+  cudaEvent_t up0 = nullptr, up1 = nullptr;
   executor_t executor;
   std::map<std::pair<int64_t, int>, active_set_t> as_cache;
   std::map<std::string, std::pair<void *, size_t>> bufs;
@@ -1195,6 +1197,12 @@ gsw_status gsw_destroy(gsw_ctx *ctx) {
   ctx->stats.destroy();
   if (ctx->e0) cudaEventDestroy(ctx->e0);
   if (ctx->e1) cudaEventDestroy(ctx->e1);
+  if (ctx->up0) cudaEventDestroy(ctx->up0);
+  if (ctx->up1) cudaEventDestroy(ctx->up1);
+  if (ctx->upload_stream) {
+    cudaStreamSynchronize(ctx->upload_stream);
+    cudaStreamDestroy(ctx->upload_stream);
+  }
   cudaStreamDestroy(ctx->stream);
   stream() = 0;
   delete ctx;
@@ -1212,13 +1220,33 @@ gsw_status gsw_graph_upload(gsw_ctx *ctx, int64_t n, int64_t m, const int64_t *r
   g->m = m;
   g->directed = directed != 0;
   g->weighted = weights != nullptr;
-  auto up = [&](void **dst, const void *src, size_t bytes) {
+  auto up = [&](void **dst, const void *src, size_t bytes, cudaStream_t s) {
     if (!(*dst = ctx->graph_alloc(bytes))) return false;
-    if (bytes && GSW_CUDA(cudaMemcpyAsync(*dst, src, bytes, cudaMemcpyHostToDevice, stream()))) return false;
+    if (bytes && GSW_CUDA(cudaMemcpyAsync(*dst, src, bytes, cudaMemcpyHostToDevice, s))) return false;
     return true;
   };
-  bool okk = up((void **)&g->off, row_off, sizeof(int64_t) * (n + 1)) && up((void **)&g->col, col, sizeof(int) * m);
-  if (okk && weights) okk = up((void **)&g->w, weights, sizeof(int) * m);
+  // The columns (and weights) copy on a second stream while the degrees and
+  // the degree statistics come from the offsets on the context's stream.  The
+  // second stream first waits for everything queued before the upload, so a
+  // pooled block reused here is not overwritten while an earlier kernel still
+  // reads it, and the context's stream waits for the copy before returning.
+  if (!ctx->upload_stream) {
+    if (GSW_CUDA(cudaStreamCreateWithFlags(&ctx->upload_stream, cudaStreamNonBlocking)) ||
+        GSW_CUDA(cudaEventCreateWithFlags(&ctx->up0, cudaEventDisableTiming)) ||
+        GSW_CUDA(cudaEventCreateWithFlags(&ctx->up1, cudaEventDisableTiming))) {
+      free_graph(g);
+      return eg.finish();
+    }
+  }
+  cudaStream_t s2 = ctx->upload_stream;
+  GSW_CUDA(cudaEventRecord(ctx->up0, stream()));
+  GSW_CUDA(cudaStreamWaitEvent(s2, ctx->up0, 0));
+  bool okk = up((void **)&g->off, row_off, sizeof(int64_t) * (n + 1), stream()) &&
+             up((void **)&g->col, col, sizeof(int) * m, s2);
+  if (okk && weights) okk = up((void **)&g->w, weights, sizeof(int) * m, s2);
+  GSW_CUDA(cudaEventRecord(ctx->up1, s2));
+  // the weights' mean and the reverse CSR need the copy first
+  if (weights || g->directed) GSW_CUDA(cudaStreamWaitEvent(stream(), ctx->up1, 0));
   if (okk && g->directed) {
     // reverse CSR on the host (counting sort by destination)
     std::vector<int64_t> roff(n + 1, 0);
@@ -1232,9 +1260,9 @@ gsw_status gsw_graph_upload(gsw_ctx *ctx, int64_t n, int64_t m, const int64_t *r
         rcol[p] = (int)v;
         if (weights) rw[p] = weights[e];
       }
-    okk = up((void **)&g->roff, roff.data(), sizeof(int64_t) * (n + 1)) &&
-          up((void **)&g->rcol, rcol.data(), sizeof(int) * m);
-    if (okk && weights) okk = up((void **)&g->rw, rw.data(), sizeof(int) * m);
+    okk = up((void **)&g->roff, roff.data(), sizeof(int64_t) * (n + 1), stream()) &&
+          up((void **)&g->rcol, rcol.data(), sizeof(int) * m, stream());
+    if (okk && weights) okk = up((void **)&g->rw, rw.data(), sizeof(int) * m, stream());
     if (okk) {
       okk = (g->rdeg = (int *)ctx->graph_alloc(sizeof(int) * (n + 1))) != nullptr;
       if (okk) k_deg_to_i32<<<grid_for(n), 256, 0, stream()>>>(g->roff, n, g->rdeg);
@@ -1242,6 +1270,7 @@ gsw_status gsw_graph_upload(gsw_ctx *ctx, int64_t n, int64_t m, const int64_t *r
     GSW_CUDA(cudaStreamSynchronize(stream()));
   }
   if (okk) finalize_graph(g);
+  GSW_CUDA(cudaStreamWaitEvent(stream(), ctx->up1, 0));
   GSW_CUDA(cudaStreamSynchronize(stream()));
   if (!ok()) {
     free_graph(g);
