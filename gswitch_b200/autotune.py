@@ -87,6 +87,20 @@ def tune(ctx, graphs, reps=2, log=None, only=None):
     return table, shapes, report
 
 
+def merge(old, table, shapes, report, only):
+    """A re-tune of the load balances in `only` on top of an earlier table
+    (the parsed json): the other variants keep their old entries."""
+    table, shapes = table.copy(), shapes.copy()
+    for d, f, lb, fused in VARIANTS:
+        if lb in only:
+            continue
+        i = gs.Context.tune_index(d, f, lb, fused)
+        table[i] = old["quarters"][i]
+        shapes[i] = old.get("shapes", [0] * gs.TUNE_ENTRIES)[i]
+    report = {**{k: v for k, v in old.get("report", {}).items() if k.split("-")[2] not in only}, **report}
+    return table, shapes, report
+
+
 def load_table(path=None):
     path = path or DEFAULT_PATH
     if not os.path.exists(path):
@@ -124,13 +138,7 @@ def main(argv=None):
         graphs.append((g, g.roots(5, 3)))
     table, shapes, report = tune(ctx, graphs, log=lambda m: print(m, file=sys.stderr, flush=True), only=only)
     if only and os.path.exists(args.out):
-        old = json.load(open(args.out))
-        keep = [i for d, f, lb, fused in VARIANTS if lb not in only
-                for i in [gs.Context.tune_index(d, f, lb, fused)]]
-        for i in keep:
-            table[i] = old["quarters"][i]
-            shapes[i] = old.get("shapes", [0] * gs.TUNE_ENTRIES)[i]
-        report = {**{k: v for k, v in old.get("report", {}).items() if k.split("-")[2] not in only}, **report}
+        table, shapes, report = merge(json.load(open(args.out)), table, shapes, report, only)
     os.makedirs(os.path.dirname(args.out), exist_ok=True)
     with open(args.out, "w") as f:
         json.dump({"format": "gswitch_b200 expand grid caps, quarters of the resident grid, and shapes (STRICT "

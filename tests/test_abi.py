@@ -58,3 +58,18 @@ def test_init_reports_status_without_device():
     with pytest.raises(gs.GswError) as e:
         gs.Context(0)
     assert e.value.code in (3, 7)
+
+
+def test_caller_driven_loop_rejects_null_handles(lib):
+    """The level-loop entry points check their handles before touching a
+    device: NULL context, graph or traversal is INVALID_ARG."""
+    L = gs.lib()
+    t = ctypes.c_void_p()
+    assert L.gsw_traversal_begin(None, None, gs.APP_BFS, 0, None, ctypes.byref(t)) == 1
+    st = gs.LevelStats()
+    done = ctypes.c_int(0)
+    assert L.gsw_level_begin(None, ctypes.byref(st), ctypes.byref(done)) == 1
+    ch = gs.LevelChoice(gs.PUSH, gs.QUEUE, 0, 0)
+    assert L.gsw_level_end(None, ctypes.byref(ch)) == 1
+    assert L.gsw_traversal_end(None, None, None) == 1
+    assert L.gsw_select(None, ctypes.byref(st), 0, ctypes.byref(ch)) == 1
