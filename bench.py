@@ -367,7 +367,7 @@ def switch_headroom(g, app, root, pr_iters=2, ctx=None, model=None):
 
 
 def app_table(ctx, g, gs, args, roots, selector):
-    """BFS, SSSP, CC and PageRank on the same RMAT
+    """The per-application table: BFS, SSSP, CC and PageRank on the same RMAT
     graph (SSSP on an int32-weighted copy, weights U[1, 64]): the switched
     form (rules, and the learned selector; host-driven and captured loop)
     against every fixed variant, GTEPS by each app's definition (BFS / SSSP:
