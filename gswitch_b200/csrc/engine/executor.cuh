@@ -552,6 +552,10 @@ struct executor_t {
   // bitmap -> queue (src/kernel_libs/filter.cuh:197-252)
   void build_queue(active_set_t &as, Status target, bool sorted) {
     const int64_t nwords = (as.size + 31) >> 5;
+    if (nwords == 0) {  // an empty set (an edge-centric run without edges): an empty queue
+      GSW_CUDA(cudaMemsetAsync(as.queue.output_size_ptr(), 0, sizeof(int), stream()));
+      return;
+    }
     if (sorted) {
       const int64_t nb = (nwords + FILTER_WORDS - 1) / FILTER_WORDS;
       if (nb + 1 > as.workset.bsum_cap) return (void)set_error(GSW_ERR_OVERFLOW, "filter: %s", "block sums");

@@ -1209,6 +1209,19 @@ gsw_status gsw_destroy(gsw_ctx *ctx) {
   return GSW_OK;
 }
 
+// Checks of a caller's CSR before any kernel indexes with it: offsets that
+// never decrease (bit 1), column indices in [0, n) (bit 2).
+__global__ void k_check_offsets(const int64_t *off, int64_t n, int *bad) {
+  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x)
+    if (off[v + 1] < off[v]) atomicOr(bad, 1);
+}
+__global__ void k_check_cols(const int *col, int64_t m, int64_t n, int *bad) {
+  bool b = false;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < m; e += (int64_t)gridDim.x * blockDim.x)
+    b |= (unsigned)col[e] >= (unsigned long long)n;
+  if (__any_sync(0xffffffffu, b) && (threadIdx.x & 31) == 0) atomicOr(bad, 2);
+}
+
 gsw_status gsw_graph_upload(gsw_ctx *ctx, int64_t n, int64_t m, const int64_t *row_off, const int32_t *col,
                             const int32_t *weights, int directed, gsw_graph **out) {
   entry_guard eg(ctx);
@@ -1239,16 +1252,39 @@ gsw_status gsw_graph_upload(gsw_ctx *ctx, int64_t n, int64_t m, const int64_t *r
     }
   }
   cudaStream_t s2 = ctx->upload_stream;
+  int *bad = (int *)ctx->buf("csr_check", sizeof(int));
+  int hbad = 0, host_bad = 0;
+  if (bad) GSW_CUDA(cudaMemsetAsync(bad, 0, sizeof(int), stream()));
   GSW_CUDA(cudaEventRecord(ctx->up0, stream()));
   GSW_CUDA(cudaStreamWaitEvent(s2, ctx->up0, 0));
   bool okk = up((void **)&g->off, row_off, sizeof(int64_t) * (n + 1), stream()) &&
-             up((void **)&g->col, col, sizeof(int) * m, s2);
+             (g->col = (int *)ctx->graph_alloc(sizeof(int) * m)) != nullptr;
+  // the columns in chunks, each checked on the copy stream while the next
+  // one crosses the link (the reverse CSR of a directed graph is built, and
+  // its columns checked, on the host)
+  constexpr int64_t COL_CHUNK = (int64_t)1 << 26;
+  for (int64_t c0 = 0; okk && c0 < m; c0 += COL_CHUNK) {
+    const int64_t cn = std::min(COL_CHUNK, m - c0);
+    okk = !GSW_CUDA(cudaMemcpyAsync(g->col + c0, col + c0, sizeof(int) * cn, cudaMemcpyHostToDevice, s2));
+    if (okk && bad && !g->directed) k_check_cols<<<grid_for(cn), 256, 0, s2>>>(g->col + c0, cn, n, bad);
+  }
   if (okk && weights) okk = up((void **)&g->w, weights, sizeof(int) * m, s2);
   GSW_CUDA(cudaEventRecord(ctx->up1, s2));
   // the weights' mean and the reverse CSR need the copy first
   if (weights || g->directed) GSW_CUDA(cudaStreamWaitEvent(stream(), ctx->up1, 0));
+  // the offsets are checked before anything derives degrees from them
+  if (okk && bad) {
+    k_check_offsets<<<grid_for(n), 256, 0, stream()>>>(g->off, n, bad);
+    GSW_CUDA(cudaMemcpyAsync(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, stream()));
+    GSW_CUDA(cudaStreamSynchronize(stream()));
+    if (hbad & 1) okk = false;
+  }
   if (okk && g->directed) {
     // reverse CSR on the host (counting sort by destination)
+    for (int64_t e = 0; e < m && okk; ++e) okk = col[e] >= 0 && col[e] < n;
+    if (!okk) host_bad = 2;
+  }
+  if (okk && g->directed) {
     std::vector<int64_t> roff(n + 1, 0);
     for (int64_t e = 0; e < m; ++e) roff[(size_t)col[e] + 1]++;
     for (int64_t v = 0; v < n; ++v) roff[v + 1] += roff[v];
@@ -1271,7 +1307,14 @@ gsw_status gsw_graph_upload(gsw_ctx *ctx, int64_t n, int64_t m, const int64_t *r
   }
   if (okk) finalize_graph(g);
   GSW_CUDA(cudaStreamWaitEvent(stream(), ctx->up1, 0));
+  if (bad) GSW_CUDA(cudaMemcpyAsync(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, stream()));
   GSW_CUDA(cudaStreamSynchronize(stream()));
+  hbad |= host_bad;
+  if (ok() && hbad) {
+    free_graph(g);
+    return fail(GSW_ERR_INVALID_ARG, (hbad & 1) ? "gsw_graph_upload: row offsets decrease at some vertex"
+                                                : "gsw_graph_upload: a column index is outside [0, n)");
+  }
   if (!ok()) {
     free_graph(g);
     return eg.finish();

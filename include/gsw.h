@@ -54,7 +54,10 @@ int gsw_version(void);
 
 /* ---- graphs -------------------------------------------------------------
  * Replaces build_graph<VC|EC> / device_graph_t<CSR,E>::build
- * (src/data_structures/graph.cuh:149-215,268-280): upload a host CSR. */
+ * (src/data_structures/graph.cuh:149-215,268-280): upload a host CSR.  The
+ * CSR is checked before any kernel indexes with it: row_off[0] = 0,
+ * row_off[n] = m, offsets that never decrease and column indices in [0, n);
+ * anything else is GSW_ERR_INVALID_ARG (the reference reads out of bounds). */
 gsw_status gsw_graph_upload(gsw_ctx *ctx, int64_t n, int64_t m, const int64_t *row_off, const int32_t *col,
                             const int32_t *weights, int directed, gsw_graph **out);
 /* Device-side generators (the reference reads .mtx files instead,

@@ -222,6 +222,56 @@ def test_errors_are_status_codes(ctx):
         ctx.upload(np.array([0, 5], dtype=np.int64), np.array([0], dtype=np.int32))
 
 
+def test_upload_rejects_a_bad_csr(ctx):
+    """A caller's CSR is checked before any kernel indexes with it: a column
+    index outside [0, n) (too large or negative, undirected or directed) and
+    offsets that decrease are INVALID_ARG, and the context keeps working."""
+    off = np.array([0, 2, 3, 4], dtype=np.int64)
+    good = np.array([1, 2, 0, 0], dtype=np.int32)
+    for col, directed in (([1, 3, 0, 0], False), ([1, -1, 0, 0], False), ([1, 2, 0, 7], True)):
+        with pytest.raises(gs.GswError) as e:
+            ctx.upload(off, np.array(col, dtype=np.int32), directed=directed)
+        assert e.value.code == 1, (col, directed)
+        assert "column" in str(e.value)
+    with pytest.raises(gs.GswError) as e:
+        ctx.upload(np.array([0, 3, 1, 4], dtype=np.int64), good)
+    assert e.value.code == 1 and "offsets" in str(e.value)
+    g = ctx.upload(off, good)
+    lv, _ = g.bfs(0)
+    assert list(lv) == [0, 1, 1]
+    g.close()
+
+
+def test_graphs_without_edges(ctx):
+    """One vertex and no arcs, and many vertices and no arcs: every
+    application answers for the root (or every vertex) alone."""
+    for n in (1, 1000):
+        off = np.zeros(n + 1, dtype=np.int64)
+        col = np.zeros(0, dtype=np.int32)
+        g = ctx.upload(off, col)
+        root = n // 2
+        ref = np.full(n, -1, dtype=np.int32)
+        ref[root] = 0
+        for o in (gs.RunOpts(), gs.RunOpts(selector="mlp"), gs.RunOpts(captured=True), "Push-Queue-STRICT-Fused",
+                  "Pull-Bitmap-TM-Standalone"):
+            lv, st = g.bfs(root, o)
+            assert np.array_equal(lv, ref), (n, o)
+            assert st.edges == 0
+        lab, _ = g.cc()
+        assert np.array_equal(lab, np.arange(n))
+        col_, _ = g.gc()
+        assert oracle.gc_check(oracle.Csr(off, col), col_) < 0
+        nsp, dep, _ = g.bc(root)
+        assert nsp[root] == 1 and not dep.any()
+        lv2, _ = g.mbfs([root, 0], batched=True)
+        assert lv2[0][root] == 0 and lv2[1][0] == 0
+        gw = ctx.upload(off, col, np.zeros(0, dtype=np.int32))
+        d, _ = gw.sssp(root)
+        assert d[root] == 0 and (n == 1 or d[(root + 1) % n] > 10**8)
+        g.close()
+        gw.close()
+
+
 @pytest.mark.parametrize("persistent", [True, False])
 def test_fused_levels_persistent_and_per_launch(ctx, big, persistent):
     """Fused levels run either in one grid-wide launch with a level barrier or
